@@ -1,0 +1,644 @@
+// SWESim / Settings: the C-linkage surface of rodrigomarher/HHG-Solids (src/cwrapper.cpp:5-28)
+// over a GPU propagation.
+//
+// Setup (SWESim::_init, src/swe.cpp:49-93) runs on the host where it is bookkeeping and its
+// rounding must follow the reference: TB parse, supercell, (int)-Cramer placement, field,
+// velocity on the current window.  Everything per k-point (Wannier sums, eigensolve, rho0, the
+// nt RK4 steps and the current) runs in the CUDA kernels of ../kernels.  There is no CPU path:
+// without a CUDA device, SWESim_init fails with a message.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <complex>
+#include <cstdio>
+#include <cstring>
+#include <filesystem>
+#include <fstream>
+#include <functional>
+#include <map>
+#include <memory>
+#include <sstream>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../kernels/sbe_device.h"
+#include "hhg_swe.h"
+#include "tb_model.hpp"
+
+namespace hhg {
+namespace refarith {
+void cramer3(double** rows, double* v, double* c);
+void supercell(int N1, int N2, int N3, double lat[3][3], double* R);
+void time_grid(int nt, double dt_fs, double* t);
+void efield(int nt, const double* t, double lambda_nm, double tmax_field_fs, double intensity, const double* s,
+            const double* phi, double* E, double* A);
+}  // namespace refarith
+}  // namespace hhg
+
+// Defaults of include/settings.h:8-22 of the reference.
+struct Settings {
+  int nr1 = 400, nr2 = 400, nr3 = 1;
+  double tmax = 90.0;
+  double dt = 10.98e-3 / 0.5;
+  int nt = (int)(90.0 / (10.98e-3 / 0.5));
+  double lambda_nm = 3000;
+  double tmax_field = 80.0;
+  double intensity_wcm2 = 5e10;
+  double sx = 0.96, sy = 0.25, sz = 0.0;
+  double phi_x = 0.0, phi_y = 0.0, phi_z = 0.0;
+};
+
+namespace {
+
+using hhg::cd;
+constexpr double kEv2Ha = 1.0 / 27.2114;       // include/constants.h:10
+constexpr double kA2Bohr = 1.0 / 0.5291772;    // include/constants.h:6
+
+thread_local std::string g_last_error;
+thread_local bool g_has_error = false;
+
+void check_cuda(cudaError_t e, const char* what) {
+  if (e != cudaSuccess) throw std::runtime_error(std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+template <typename T>
+struct DevBuf {
+  T* p = nullptr;
+  size_t n = 0;
+  void alloc(size_t count) {
+    release();
+    if (count == 0) count = 1;
+    check_cuda(cudaMalloc(&p, count * sizeof(T)), "cudaMalloc");
+    n = count;
+  }
+  void upload(const std::vector<T>& v, cudaStream_t s) {
+    alloc(v.size());
+    if (!v.empty()) check_cuda(cudaMemcpyAsync(p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, s), "H2D");
+  }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+  }
+  ~DevBuf() { release(); }
+};
+
+inline double2 d2(cd z) { return make_double2(z.real(), z.imag()); }
+
+}  // namespace
+
+struct SWESim {
+  std::string path_tb;
+  Settings* settings = nullptr;
+  int device = -1;
+  std::string err;
+  bool has_err = false;
+  bool ready = false;
+
+  hhg::TBModel model;
+  int N1 = 0, N2 = 0, Nk = 0, nw = 0, nw2 = 0, nt = -1;
+  double lat_au[3][3] = {};
+  std::vector<double> Rgrid;  // [Nk][3] Angstrom
+  std::vector<int> site_of_cell;
+  std::vector<double> t, E, A;
+  std::vector<hhg::StepParams> steps;
+  std::vector<int2> cell_n;
+  std::vector<double2> H0, Rtab, V, T1, T2;
+  int nax = 0, ax_id[3] = {0, 0, 0}, nj = 0, j_id[3] = {0, 0, 0};
+
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  DevBuf<int2> d_cell;
+  DevBuf<double2> d_H0, d_R, d_V, d_T1, d_T2, d_rho0, d_rho, d_Jpart, d_J;
+  DevBuf<hhg::StepParams> d_steps;
+  hhg::SolveTables tab{};
+  hhg::LaunchShape shape{};
+  double2* h_J = nullptr;  // pinned [3][nt]
+  std::vector<cd> Jhist[3];
+  float last_ms = 0.f;
+  int last_launches = 0;
+
+  ~SWESim() { release(); }
+
+  void release() {
+    d_cell.release();
+    for (auto* b : {&d_H0, &d_R, &d_V, &d_T1, &d_T2, &d_rho0, &d_rho, &d_Jpart, &d_J}) b->release();
+    d_steps.release();
+    if (h_J) cudaFreeHost(h_J);
+    h_J = nullptr;
+    if (ev0) cudaEventDestroy(ev0);
+    if (ev1) cudaEventDestroy(ev1);
+    ev0 = ev1 = nullptr;
+    if (stream) cudaStreamDestroy(stream);
+    stream = nullptr;
+    ready = false;
+    for (auto& j : Jhist) j.clear();
+  }
+
+  void init();
+  void run();
+  void reset_state();
+  void test_files();
+  void write_fields_files(const std::string& dir);
+};
+
+namespace {
+
+// Placement of src/hamiltonian.cpp:8-39: site index per grid cell (first matching TB cell), -1 if none.
+void place_sites(const hhg::TBModel& m, int N1, int N2, const std::vector<double>& R, std::vector<int>& site) {
+  std::map<std::tuple<int, int, int>, int> first;
+  for (int s = 0; s < m.nsites; ++s) {
+    auto key = std::make_tuple(m.R[3 * s], m.R[3 * s + 1], m.R[3 * s + 2]);
+    if (!first.count(key)) first[key] = s;
+  }
+  double rows[3][3];
+  std::memcpy(rows, m.lattice, sizeof rows);
+  double* mat[3] = {rows[0], rows[1], rows[2]};
+  const int Nk = N1 * N2;
+  site.assign(Nk, -1);
+  for (int c = 0; c < Nk; ++c) {
+    double v[3] = {R[3 * c], R[3 * c + 1], R[3 * c + 2]};
+    double coef[3];
+    hhg::refarith::cramer3(mat, v, coef);
+    auto it = first.find(std::make_tuple((int)coef[0], (int)coef[1], (int)coef[2]));
+    if (it != first.end()) site[c] = it->second;
+  }
+}
+
+inline int wrapi(long x, int n) {
+  long r = x % n;
+  return (int)(r < 0 ? r + n : r);
+}
+
+}  // namespace
+
+void SWESim::init() {
+  release();
+  if (!settings) throw std::runtime_error("SWESim_init: settings not set (call SWESim_set_settings first)");
+  if (path_tb.empty()) throw std::runtime_error("SWESim_init: TB path not set (call SWESim_set_path_tb first)");
+  model = hhg::parse_tb(path_tb);
+  Settings& s = *settings;
+  nt = (int)(s.tmax / s.dt);
+  s.nt = nt;
+  N1 = s.nr1;
+  N2 = s.nr2;
+  nw = model.nw;
+  nw2 = nw * nw;
+  if (s.nr3 != 1) throw std::runtime_error("SWESim_init: only 2D grids (nr3 = 1) are supported");
+  if (N1 < 4 || N2 < 4 || (N1 % 2) || (N2 % 2))
+    throw std::runtime_error(
+        "SWESim_init: nr1 and nr2 must be even and >= 4 (odd sizes shift the reference's fftshift/ifftshift pair "
+        "by one cell; sizes below 4 put its 4x4 current window outside the grid)");
+  if (nt < 2) throw std::runtime_error("SWESim_init: tmax/dt must give at least 2 time steps");
+  if (nw > hhg::kMaxOrb) throw std::runtime_error("SWESim_init: more than 16 orbitals is not supported");
+  if ((long)N1 * N2 > (1L << 30)) throw std::runtime_error("SWESim_init: grid too large");
+  Nk = N1 * N2;
+
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+    throw std::runtime_error("SWESim_init: no CUDA device (this library has no CPU path)");
+  if (device < 0) check_cuda(cudaGetDevice(&device), "cudaGetDevice");
+  check_cuda(cudaSetDevice(device), "cudaSetDevice");
+  check_cuda(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking), "cudaStreamCreate");
+  check_cuda(cudaEventCreate(&ev0), "cudaEventCreate");
+  check_cuda(cudaEventCreate(&ev1), "cudaEventCreate");
+
+  // Supercell and placement (src/grid.cpp:64-111, src/hamiltonian.cpp:8-39, src/berry_connection.cpp:7-50).
+  Rgrid.assign((size_t)Nk * 3, 0.0);
+  hhg::refarith::supercell(N1, N2, 1, model.lattice, Rgrid.data());
+  place_sites(model, N1, N2, Rgrid, site_of_cell);
+  for (int a = 0; a < 3; ++a)
+    for (int b = 0; b < 3; ++b) lat_au[a][b] = model.lattice[a][b] * kA2Bohr;
+
+  // Fields (src/efield.cpp:30-50) and the per-step table (src/solver.cpp:109-148, src/swe.cpp:192-196).
+  t.assign(nt, 0.0);
+  E.assign((size_t)3 * nt, 0.0);
+  A.assign((size_t)3 * nt, 0.0);
+  hhg::refarith::time_grid(nt, s.dt, t.data());
+  const double pol[3] = {s.sx, s.sy, s.sz}, phi[3] = {s.phi_x, s.phi_y, s.phi_z};
+  hhg::refarith::efield(nt, t.data(), s.lambda_nm, s.tmax_field, s.intensity_wcm2, pol, phi, E.data(), A.data());
+  nax = 0;
+  for (int a = 0; a < 3; ++a)
+    if (pol[a] != 0.0) ax_id[nax++] = a;
+  steps.assign(nt, hhg::StepParams{});
+  for (int ti = 0; ti < nt; ++ti) {
+    hhg::StepParams& p = steps[ti];
+    for (int a = 0; a < 3; ++a) {
+      const double* Ea = E.data() + (size_t)a * nt;
+      if (ti < nt - 1) {
+        p.es[0][a] = Ea[ti];
+        p.es[1][a] = 0.5 * Ea[ti] + 0.5 * Ea[ti + 1];
+        p.es[2][a] = Ea[ti + 1];
+      } else {
+        p.es[0][a] = p.es[1][a] = p.es[2][a] = Ea[nt - 1];
+      }
+    }
+    const double ax = A[ti], ay = A[nt + ti], az = A[2 * (size_t)nt + ti];
+    const double th1 = ax * lat_au[0][0] + ay * lat_au[0][1] + az * lat_au[0][2];
+    const double th2 = ax * lat_au[1][0] + ay * lat_au[1][1] + az * lat_au[1][2];
+    p.p1 = make_double2(std::cos(th1), std::sin(th1));
+    p.p2 = make_double2(std::cos(th2), std::sin(th2));
+  }
+
+  // Support cells: placed cells whose H0 or field-coupled r block is non-zero (zero blocks add exact zeros).
+  cell_n.clear();
+  H0.clear();
+  std::vector<std::vector<double2>> Rax(nax);
+  for (int c = 0; c < Nk; ++c) {
+    const int st = site_of_cell[c];
+    if (st < 0) continue;
+    bool nz = false;
+    for (int o = 0; o < nw2 && !nz; ++o) {
+      nz = model.hop[(size_t)st * nw2 + o] != cd(0, 0);
+      for (int a = 0; a < nax && !nz; ++a) nz = model.bc[ax_id[a]][(size_t)st * nw2 + o] != cd(0, 0);
+    }
+    if (!nz) continue;
+    cell_n.push_back(make_int2(c / N2 - N1 / 2, c % N2 - N2 / 2));
+    for (int o = 0; o < nw2; ++o) {
+      H0.push_back(d2(model.hop[(size_t)st * nw2 + o] * kEv2Ha));
+      for (int a = 0; a < nax; ++a) Rax[a].push_back(d2(-model.bc[ax_id[a]][(size_t)st * nw2 + o] * kA2Bohr));
+    }
+  }
+  const int ncell = (int)cell_n.size();
+  Rtab.clear();
+  for (int a = 0; a < nax; ++a) Rtab.insert(Rtab.end(), Rax[a].begin(), Rax[a].end());
+
+  // Velocity on the 4x4 window (src/velocity.cpp:41-115, evaluated in SI with the to-au factor 1.0 of
+  // include/constants.h:13): v_a(n) = i (R_a(n) H(n) - sum_n' [r(n') H(n - n') - H(n') r(n - n')]),
+  // with the cyclic convolution of the reference's FFT product taken directly.
+  auto cell_of = [&](int n1, int n2) { return wrapi((long)n1 + N1 / 2, N1) * N2 + wrapi((long)n2 + N2 / 2, N2); };
+  std::vector<int> placed;
+  for (int c = 0; c < Nk; ++c)
+    if (site_of_cell[c] >= 0) placed.push_back(c);
+  std::vector<cd> vw((size_t)3 * hhg::kWindow * nw2, cd(0, 0));
+  for (int a = 0; a < 3; ++a)
+    for (int w = 0; w < hhg::kWindow; ++w) {
+      const int n1 = w / 4 - 2, n2 = w % 4 - 2;
+      const int c = cell_of(n1, n2);
+      std::vector<cd> acc(nw2, cd(0, 0));
+      for (int q : placed) {
+        const int q1 = q / N2 - N1 / 2, q2 = q % N2 - N2 / 2;
+        const int d = cell_of(n1 - q1, n2 - q2);
+        const int sd = site_of_cell[d];
+        if (sd < 0) continue;
+        const int sq = site_of_cell[q];
+        const cd* rq = model.bc[a].data() + (size_t)sq * nw2;
+        const cd* Hq = model.hop.data() + (size_t)sq * nw2;
+        const cd* rd = model.bc[a].data() + (size_t)sd * nw2;
+        const cd* Hd = model.hop.data() + (size_t)sd * nw2;
+        for (int i = 0; i < nw; ++i)
+          for (int j = 0; j < nw; ++j) {
+            cd sum(0, 0);
+            for (int k = 0; k < nw; ++k) sum += (-rq[i * nw + k]) * Hd[k * nw + j] - Hq[i * nw + k] * (-rd[k * nw + j]);
+            acc[i * nw + j] += sum;
+          }
+      }
+      const int sc = site_of_cell[c];
+      const double Ra = Rgrid[3 * (size_t)c + a];
+      for (int o = 0; o < nw2; ++o) {
+        const cd h = sc >= 0 ? model.hop[(size_t)sc * nw2 + o] : cd(0, 0);
+        vw[((size_t)a * hhg::kWindow + w) * nw2 + o] = cd(0, 1) * (Ra * h - acc[o]);
+      }
+    }
+  nj = 0;
+  V.clear();
+  for (int a = 0; a < 3; ++a) {
+    bool nz = false;
+    for (size_t o = 0; o < (size_t)hhg::kWindow * nw2 && !nz; ++o) nz = vw[(size_t)a * hhg::kWindow * nw2 + o] != cd(0, 0);
+    if (!nz) continue;  // J_a is then exactly zero, as in the reference
+    j_id[nj++] = a;
+    for (size_t o = 0; o < (size_t)hhg::kWindow * nw2; ++o) V.push_back(d2(vw[(size_t)a * hhg::kWindow * nw2 + o]));
+  }
+
+  // Hermitian symmetry of the placed operators on the grid: block(-n) == block(n)^+ for every cell.
+  // It fails when the grid is smaller than the model's R range or a misplacement is one-sided; the
+  // kernel then forms the full HX - XH instead of HX - (HX)^+.
+  bool herm = true;
+  for (int c = 0; c < Nk && herm; ++c) {
+    const int n1 = c / N2 - N1 / 2, n2 = c % N2 - N2 / 2;
+    const int st = site_of_cell[c], sm = site_of_cell[cell_of(-n1, -n2)];
+    if (st < 0 && sm < 0) continue;
+    auto blk = [&](const std::vector<cd>& v, int s, int i, int j) { return s < 0 ? cd(0, 0) : v[(size_t)s * nw2 + i * nw + j]; };
+    for (int i = 0; i < nw && herm; ++i)
+      for (int j = 0; j < nw && herm; ++j) {
+        herm = blk(model.hop, st, i, j) == std::conj(blk(model.hop, sm, j, i));
+        for (int a = 0; a < nax && herm; ++a)
+          herm = blk(model.bc[ax_id[a]], st, i, j) == std::conj(blk(model.bc[ax_id[a]], sm, j, i));
+      }
+  }
+
+  T1.resize(N1);
+  T2.resize(N2);
+  for (int m = 0; m < N1; ++m) {
+    const double ang = 2.0 * M_PI * (double)m / (double)N1;
+    T1[m] = make_double2(std::cos(ang), -std::sin(ang));
+  }
+  for (int m = 0; m < N2; ++m) {
+    const double ang = 2.0 * M_PI * (double)m / (double)N2;
+    T2[m] = make_double2(std::cos(ang), -std::sin(ang));
+  }
+
+  // Device tables.
+  d_cell.upload(cell_n, stream);
+  d_H0.upload(H0, stream);
+  d_R.upload(Rtab, stream);
+  d_V.upload(V, stream);
+  d_T1.upload(T1, stream);
+  d_T2.upload(T2, stream);
+  d_steps.upload(steps, stream);
+  d_rho0.alloc((size_t)Nk * nw2);
+  d_rho.alloc((size_t)Nk * nw2);
+  d_J.alloc((size_t)3 * nt);
+  tab.nw = nw;
+  tab.nw2 = nw2;
+  tab.N1 = N1;
+  tab.N2 = N2;
+  tab.Nk = Nk;
+  tab.nt = nt;
+  tab.ncell = ncell;
+  tab.cell_n = d_cell.p;
+  tab.H0 = d_H0.p;
+  tab.nax = nax;
+  for (int a = 0; a < 3; ++a) tab.ax_id[a] = ax_id[a];
+  tab.R = d_R.p;
+  tab.nj = nj;
+  for (int a = 0; a < 3; ++a) tab.j_id[a] = j_id[a];
+  tab.V = d_V.p;
+  tab.T1 = d_T1.p;
+  tab.T2 = d_T2.p;
+  tab.steps = d_steps.p;
+  tab.dt = t[1] - t[0];
+  tab.hermitian = herm ? 1 : 0;
+
+  int sms = 0;
+  check_cuda(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device), "cudaDeviceGetAttribute");
+  char why[256] = {0};
+  if (!hhg::plan_propagate(tab, sms, &shape, why, sizeof why)) throw std::runtime_error(std::string("SWESim_init: ") + why);
+  d_Jpart.alloc((size_t)shape.ctas * nt * 3);
+  check_cuda(cudaMallocHost(&h_J, sizeof(double2) * 3 * (size_t)nt), "cudaMallocHost");
+
+  // Equilibrium density matrix (src/swe.cpp:82-90) on the GPU.
+  hhg::launch_rho0_fp64(tab, d_rho0.p, stream);
+  check_cuda(cudaGetLastError(), "rho0 launch");
+  check_cuda(cudaMemcpyAsync(d_rho.p, d_rho0.p, sizeof(double2) * (size_t)Nk * nw2, cudaMemcpyDeviceToDevice, stream),
+             "D2D");
+  check_cuda(cudaStreamSynchronize(stream), "init");
+  ready = true;
+}
+
+void SWESim::reset_state() {
+  if (!ready) throw std::runtime_error("SWESim_reset: SWESim_init has not succeeded");
+  check_cuda(cudaMemcpyAsync(d_rho.p, d_rho0.p, sizeof(double2) * (size_t)Nk * nw2, cudaMemcpyDeviceToDevice, stream),
+             "D2D");
+  check_cuda(cudaStreamSynchronize(stream), "reset");
+  for (auto& j : Jhist) j.clear();
+}
+
+void SWESim::run() {
+  if (!ready) throw std::runtime_error("SWESim_run_simulation: SWESim_init has not succeeded");
+  check_cuda(cudaSetDevice(device), "cudaSetDevice");
+  check_cuda(cudaMemsetAsync(d_Jpart.p, 0, sizeof(double2) * d_Jpart.n, stream), "memset");
+  check_cuda(cudaEventRecord(ev0, stream), "event");
+  last_launches = hhg::launch_propagate_fp64(tab, shape, d_rho.p, d_Jpart.p, d_J.p, stream);
+  check_cuda(cudaGetLastError(), "propagate launch");
+  check_cuda(cudaEventRecord(ev1, stream), "event");
+  check_cuda(cudaMemcpyAsync(h_J, d_J.p, sizeof(double2) * 3 * (size_t)nt, cudaMemcpyDeviceToHost, stream), "D2H");
+  check_cuda(cudaStreamSynchronize(stream), "run_simulation");
+  check_cuda(cudaEventElapsedTime(&last_ms, ev0, ev1), "event time");
+  // The reference appends one sample per step to each Observable (src/observable.cpp:29);
+  // SWESim_get_current returns the first nt of them.
+  for (int a = 0; a < 3; ++a)
+    for (int ti = 0; ti < nt; ++ti) Jhist[a].push_back(cd(h_J[(size_t)a * nt + ti].x, h_J[(size_t)a * nt + ti].y));
+}
+
+namespace {
+
+void write_matrix_field(const std::string& path, const char* unit, int npts, int nw2,
+                        const std::function<cd(int, int)>& get) {
+  std::ofstream f(path);
+  if (!f) return;
+  f << unit << "\n";
+  for (int i = 0; i < npts; ++i)
+    for (int o = 0; o < nw2; ++o) {
+      const cd z = get(i, o);
+      f << i << " " << std::abs(z) << " " << std::atan2(z.imag(), z.real()) << "\n";
+    }
+}
+
+}  // namespace
+
+// src/efield.cpp:91-113: fields/efield.dat and fields/afield.dat, "t E_x E_y E_z" per line.
+void SWESim::write_fields_files(const std::string& dir) {
+  std::filesystem::create_directories(dir);
+  std::ofstream fe(dir + "/efield.dat"), fa(dir + "/afield.dat");
+  fe << 1 << "\n";
+  fa << 1 << "\n";
+  for (int i = 0; i < nt; ++i) {
+    fe << t[i] << " " << E[i] << " " << E[nt + i] << " " << E[2 * (size_t)nt + i] << "\n";
+    fa << t[i] << " " << A[i] << " " << A[nt + i] << " " << A[2 * (size_t)nt + i] << "\n";
+  }
+}
+
+// Debug dumps in the text format of src/matrix_field.cpp:28-53 ("index |z| arg z"), following
+// src/swe.cpp:131-181: supercell and k vectors (SI and AU), the placed Hamiltonian (SI and AU),
+// the equilibrium rho(k) (W gauge, AU), the Berry connections and the fields.
+void SWESim::test_files() {
+  if (!ready) throw std::runtime_error("SWESim_test_files: SWESim_init has not succeeded");
+  std::filesystem::create_directories("test");
+  double b[3][3];
+  {
+    const double(*a)[3] = model.lattice;
+    double cr[3][3];
+    for (int r = 0; r < 3; ++r) {
+      const int p = (r + 1) % 3, q = (r + 2) % 3;
+      cr[r][0] = a[p][1] * a[q][2] - a[p][2] * a[q][1];
+      cr[r][1] = a[p][2] * a[q][0] - a[p][0] * a[q][2];
+      cr[r][2] = a[p][0] * a[q][1] - a[p][1] * a[q][0];
+    }
+    const double vol = a[0][0] * cr[0][0] + a[0][1] * cr[0][1] + a[0][2] * cr[0][2];
+    for (int r = 0; r < 3; ++r)
+      for (int c = 0; c < 3; ++c) b[r][c] = 2.0 * M_PI / vol * cr[r][c];
+  }
+  for (int au = 0; au < 2; ++au) {
+    const double lf = au ? kA2Bohr : 1.0;
+    const char* tag = au ? "AU" : "SI";
+    std::ofstream fr(std::string("test/Rvecs_") + tag + ".dat"), fk(std::string("test/Kvecs_") + tag + ".dat");
+    fr << "_" << tag << "_\n";
+    fk << "_" << tag << "_\n";
+    for (int c = 0; c < Nk; ++c) {
+      const int m1 = c / N2, m2 = c % N2;
+      fr << Rgrid[3 * c] * lf << " " << Rgrid[3 * c + 1] * lf << " " << Rgrid[3 * c + 2] * lf << "\n";
+      double k[3];
+      for (int x = 0; x < 3; ++x) k[x] = ((double)m1 / N1 * b[0][x] + (double)m2 / N2 * b[1][x]) / lf;
+      fk << k[0] << " " << k[1] << " " << k[2] << "\n";
+    }
+    const double ef = au ? kEv2Ha : 1.0;
+    write_matrix_field(std::string("test/hamiltonian_") + tag + ".dat", au ? "_AU_" : "_SI_", Nk, nw2,
+                       [&](int c, int o) {
+                         const int st = site_of_cell[c];
+                         return st >= 0 ? model.hop[(size_t)st * nw2 + o] * ef : cd(0, 0);
+                       });
+  }
+  std::vector<double2> rho((size_t)Nk * nw2);
+  check_cuda(cudaMemcpy(rho.data(), d_rho0.p, sizeof(double2) * rho.size(), cudaMemcpyDeviceToHost), "D2H");
+  write_matrix_field("test/rho_k_W_AU.dat", "_AU_", Nk, nw2,
+                     [&](int c, int o) { return cd(rho[(size_t)c * nw2 + o].x, rho[(size_t)c * nw2 + o].y); });
+  const char* names[3] = {"test/x_bc.dat", "test/y_bc.dat", "test/z_bc.dat"};
+  for (int a = 0; a < 3; ++a)
+    write_matrix_field(names[a], "_AU_", Nk, nw2, [&](int c, int o) {
+      const int st = site_of_cell[c];
+      return st >= 0 ? -model.bc[a][(size_t)st * nw2 + o] * kA2Bohr : cd(0, 0);
+    });
+  write_fields_files("fields");
+}
+
+// ------------------------------------------------------------------------------------- C ABI
+
+namespace {
+
+void set_error(SWESim* swe, const std::string& msg) {
+  g_last_error = msg;
+  g_has_error = true;
+  if (swe) {
+    swe->err = msg;
+    swe->has_err = true;
+  }
+}
+
+void clear_error(SWESim* swe) {
+  g_has_error = false;
+  if (swe) swe->has_err = false;
+}
+
+template <typename F>
+void guarded(SWESim* swe, const char* name, F&& f) {
+  if (!swe) {
+    set_error(nullptr, std::string(name) + ": null SWESim");
+    return;
+  }
+  try {
+    clear_error(swe);
+    f();
+  } catch (const std::exception& e) {
+    set_error(swe, e.what());
+  } catch (...) {
+    set_error(swe, std::string(name) + ": unknown error");
+  }
+}
+
+}  // namespace
+
+extern "C" {
+
+SWESim* SWESim_new(void) {
+  try {
+    clear_error(nullptr);
+    return new SWESim();
+  } catch (...) {
+    set_error(nullptr, "SWESim_new: out of memory");
+    return nullptr;
+  }
+}
+
+void SWESim_run_simulation(SWESim* swe) { guarded(swe, "SWESim_run_simulation", [&] { swe->run(); }); }
+
+void SWESim_test_files(SWESim* swe) { guarded(swe, "SWESim_test_files", [&] { swe->test_files(); }); }
+
+void SWESim_set_path_tb(SWESim* swe, char* path_tb) {
+  guarded(swe, "SWESim_set_path_tb", [&] { swe->path_tb = path_tb ? std::string(path_tb) : std::string(); });
+}
+
+void SWESim_set_settings(SWESim* swe, Settings* settings) {
+  guarded(swe, "SWESim_set_settings", [&] { swe->settings = settings; });
+}
+
+void SWESim_init(SWESim* swe) { guarded(swe, "SWESim_init", [&] { swe->init(); }); }
+
+void SWESim_restart(SWESim* swe) { guarded(swe, "SWESim_restart", [&] { swe->init(); }); }
+
+void SWESim_get_current(SWESim* swe, double* t, hhg_cdouble* jx, hhg_cdouble* jy, hhg_cdouble* jz) {
+  guarded(swe, "SWESim_get_current", [&] {
+    if (!swe->ready) throw std::runtime_error("SWESim_get_current: SWESim_init has not succeeded");
+    if ((int)swe->Jhist[0].size() < swe->nt)
+      throw std::runtime_error("SWESim_get_current: run_simulation has not been called");
+    hhg_cdouble* out[3] = {jx, jy, jz};
+    for (int ti = 0; ti < swe->nt; ++ti) {
+      if (t) t[ti] = swe->t[ti];
+      for (int a = 0; a < 3; ++a)
+        if (out[a]) out[a][ti] = hhg_cdouble{swe->Jhist[a][ti].real(), swe->Jhist[a][ti].imag()};
+    }
+  });
+}
+
+void SWESim_delete(SWESim* swe) {
+  try {
+    delete swe;
+  } catch (...) {
+  }
+}
+
+Settings* Settings_new(void) { return new Settings(); }
+void Settings_delete(Settings* s) { delete s; }
+void Settings_set_nr1(Settings* s, int v) { if (s) s->nr1 = v; }
+void Settings_set_nr2(Settings* s, int v) { if (s) s->nr2 = v; }
+void Settings_set_nr3(Settings* s, int v) { if (s) s->nr3 = v; }
+void Settings_set_tmax(Settings* s, double v) { if (s) s->tmax = v; }
+void Settings_set_dt(Settings* s, double v) { if (s) s->dt = v; }
+void Settings_set_intensity(Settings* s, double v) { if (s) s->intensity_wcm2 = v; }
+void Settings_set_lambda(Settings* s, double v) { if (s) s->lambda_nm = v; }
+void Settings_set_tmax_field(Settings* s, double v) { if (s) s->tmax_field = v; }
+void Settings_set_pol_vec(Settings* s, double* v) {
+  if (s && v) {
+    s->sx = v[0];
+    s->sy = v[1];
+    s->sz = v[2];
+  }
+}
+void Settings_set_phi_vec(Settings* s, double* v) {
+  if (s && v) {
+    s->phi_x = v[0];
+    s->phi_y = v[1];
+    s->phi_z = v[2];
+  }
+}
+
+const char* SWESim_last_error(SWESim* swe) { return (swe && swe->has_err) ? swe->err.c_str() : nullptr; }
+const char* HHG_last_error(void) { return g_has_error ? g_last_error.c_str() : nullptr; }
+int SWESim_get_nt(SWESim* swe) { return (swe && swe->ready) ? swe->nt : -1; }
+int SWESim_get_num_orb(SWESim* swe) { return (swe && swe->ready) ? swe->nw : -1; }
+void SWESim_set_device(SWESim* swe, int device) {
+  guarded(swe, "SWESim_set_device", [&] { swe->device = device; });
+}
+double SWESim_last_kernel_ms(SWESim* swe) { return swe ? (double)swe->last_ms : -1.0; }
+int SWESim_last_launches(SWESim* swe) { return swe ? swe->last_launches : -1; }
+
+void SWESim_get_rho_k(SWESim* swe, hhg_cdouble* out) {
+  guarded(swe, "SWESim_get_rho_k", [&] {
+    if (!swe->ready) throw std::runtime_error("SWESim_get_rho_k: SWESim_init has not succeeded");
+    check_cuda(cudaMemcpy(out, swe->d_rho.p, sizeof(double2) * (size_t)swe->Nk * swe->nw2, cudaMemcpyDeviceToHost),
+               "D2H");
+  });
+}
+
+void SWESim_get_fields(SWESim* swe, double* t, double* E, double* A) {
+  guarded(swe, "SWESim_get_fields", [&] {
+    if (!swe->ready) throw std::runtime_error("SWESim_get_fields: SWESim_init has not succeeded");
+    if (t) std::copy(swe->t.begin(), swe->t.end(), t);
+    if (E) std::copy(swe->E.begin(), swe->E.end(), E);
+    if (A) std::copy(swe->A.begin(), swe->A.end(), A);
+  });
+}
+
+void SWESim_reset(SWESim* swe) { guarded(swe, "SWESim_reset", [&] { swe->reset_state(); }); }
+
+int HHG_measure_peaks(double* fp64_tflops, double* fp32_tflops) {
+  try {
+    return hhg::measure_fma_peaks(fp64_tflops, fp32_tflops);
+  } catch (...) {
+    return -1;
+  }
+}
+
+}  // extern "C"

@@ -1,0 +1,100 @@
+// Reader for the *_tb.dat layout of src/wannier_tb.cpp:15-113.
+//
+// Line structure: comment; three lattice rows; num_wann; nrpts; (nrpts-1)/15+1 degeneracy lines;
+// one separator line; per R cell an "n1 n2 n3" line, nw^2 lines "m n Re Im", one separator line;
+// then per R cell (same order) a header line and nw^2 lines "m n xRe xIm yRe yIm zRe zIm", one
+// separator line.  The element of line "m n" is stored at [n-1][m-1] (src/wannier_tb.cpp:73-74,
+// 101-102).  Unlike the reference, malformed files raise an error instead of reading garbage.
+#include "tb_model.hpp"
+
+#include <fstream>
+#include <sstream>
+#include <stdexcept>
+
+namespace hhg {
+namespace {
+
+struct LineReader {
+  std::ifstream in;
+  std::string path;
+  int lineno = 0;
+  std::string next(const char* what) {
+    std::string line;
+    if (!std::getline(in, line)) {
+      std::ostringstream os;
+      os << "TB file " << path << ": unexpected end of file while reading " << what << " (line " << lineno + 1
+         << ")";
+      throw std::runtime_error(os.str());
+    }
+    ++lineno;
+    return line;
+  }
+  [[noreturn]] void fail(const std::string& msg) {
+    std::ostringstream os;
+    os << "TB file " << path << " line " << lineno << ": " << msg;
+    throw std::runtime_error(os.str());
+  }
+};
+
+}  // namespace
+
+TBModel parse_tb(const std::string& path) {
+  LineReader rd;
+  rd.path = path;
+  rd.in.open(path);
+  if (!rd.in) throw std::runtime_error("Error opening wannier tb file: " + path);
+  TBModel m;
+  m.comment = rd.next("comment");
+  for (int i = 0; i < 3; ++i) {
+    std::istringstream is(rd.next("lattice vectors"));
+    if (!(is >> m.lattice[i][0] >> m.lattice[i][1] >> m.lattice[i][2])) rd.fail("bad lattice vector");
+  }
+  {
+    std::istringstream is(rd.next("num_wann"));
+    if (!(is >> m.nw) || m.nw <= 0) rd.fail("bad number of orbitals");
+  }
+  {
+    std::istringstream is(rd.next("nrpts"));
+    if (!(is >> m.nsites) || m.nsites <= 0) rd.fail("bad number of R cells");
+  }
+  const int ndeg = (m.nsites - 1) / 15 + 1;
+  for (int i = 0; i < ndeg; ++i) {
+    std::istringstream is(rd.next("degeneracies"));
+    int d;
+    while (is >> d) m.degeneracy.push_back(d);
+  }
+  rd.next("separator");
+  const int nw = m.nw, nw2 = nw * nw;
+  m.R.assign((size_t)m.nsites * 3, 0);
+  m.hop.assign((size_t)m.nsites * nw2, cd(0, 0));
+  for (int a = 0; a < 3; ++a) m.bc[a].assign((size_t)m.nsites * nw2, cd(0, 0));
+  for (int s = 0; s < m.nsites; ++s) {
+    std::istringstream is(rd.next("R cell"));
+    if (!(is >> m.R[3 * s] >> m.R[3 * s + 1] >> m.R[3 * s + 2])) rd.fail("bad R cell line");
+    for (int q = 0; q < nw2; ++q) {
+      std::istringstream ls(rd.next("hopping"));
+      int o1, o2;
+      double re, im;
+      if (!(ls >> o1 >> o2 >> re >> im) || o1 < 1 || o1 > nw || o2 < 1 || o2 > nw) rd.fail("bad hopping line");
+      m.hop[(size_t)s * nw2 + (o2 - 1) * nw + (o1 - 1)] = cd(re, im);
+    }
+    rd.next("separator");
+  }
+  for (int s = 0; s < m.nsites; ++s) {
+    rd.next("position block header");
+    for (int q = 0; q < nw2; ++q) {
+      std::istringstream ls(rd.next("position element"));
+      int o1, o2;
+      double v[6];
+      if (!(ls >> o1 >> o2 >> v[0] >> v[1] >> v[2] >> v[3] >> v[4] >> v[5]) || o1 < 1 || o1 > nw || o2 < 1 ||
+          o2 > nw)
+        rd.fail("bad position line");
+      for (int a = 0; a < 3; ++a) m.bc[a][(size_t)s * nw2 + (o2 - 1) * nw + (o1 - 1)] = cd(v[2 * a], v[2 * a + 1]);
+    }
+    std::string sep;
+    if (std::getline(rd.in, sep)) ++rd.lineno;  // the last separator may be missing
+  }
+  return m;
+}
+
+}  // namespace hhg

@@ -1,0 +1,203 @@
+"""Python API over ``libhhg_b200.so`` with the classes and parameter dict of the reference's
+``pySWE/pyswe.py`` (rodrigomarher/HHG-Solids): ``Settings(param)`` and ``SWE(settings)`` with
+``run_simulation``, ``get_current``, ``test_files``, ``restart``, ``delete``.
+
+``param`` keys, as in the reference: ``path_lib``, ``path_tb``, ``nr1``, ``nr2``, ``nr3``, ``tmax``
+(fs), ``dt`` (fs), ``intensity`` (W/cm^2), ``lambda`` (nm), ``tmax_field`` (fs), ``pol_vec`` and
+``phi_vec`` (3 floats each).  ``path_lib`` may be omitted to use this package's library; any
+library with the reference's C ABI works, including the reference's own build.
+
+Error behaviour: the reference aborts the process on a bad TB path or settings (an exception
+thrown through extern "C").  Here every call checks the library's last-error message and raises
+:class:`SWEError` instead.  Against a library without ``SWESim_last_error`` (the reference's own
+build) no check is possible and calls behave as in the reference.
+"""
+from __future__ import annotations
+
+import ctypes as ct
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_PKG = os.path.dirname(_HERE)
+
+ND_POINTER_1_double = np.ctypeslib.ndpointer(dtype=np.float64, ndim=1, flags="C")
+ND_POINTER_1_complex = np.ctypeslib.ndpointer(dtype=np.complex128, ndim=1, flags="C")
+_libs: dict = {}
+
+
+class SWEError(RuntimeError):
+    """A call into the propagator library failed; the message is the library's."""
+
+
+def default_library() -> str:
+    return os.path.join(_PKG, "lib", "libhhg_b200.so")
+
+
+def _load(path: str):
+    path = os.path.abspath(path)
+    if path in _libs:
+        return _libs[path]
+    if not os.path.exists(path):
+        raise SWEError(f"propagator library not found: {path} (build it with `make -C hhg-solids_b200`)")
+    L = ct.CDLL(path)
+    vp = ct.c_void_p
+    L.SWESim_new.argtypes = []
+    L.SWESim_new.restype = vp
+    for name in ("SWESim_run_simulation", "SWESim_test_files", "SWESim_init", "SWESim_restart", "SWESim_delete"):
+        getattr(L, name).argtypes = [vp]
+        getattr(L, name).restype = None
+    L.SWESim_set_path_tb.argtypes = [vp, ct.c_char_p]
+    L.SWESim_set_settings.argtypes = [vp, vp]
+    L.SWESim_get_current.argtypes = [vp, ND_POINTER_1_double, ND_POINTER_1_complex, ND_POINTER_1_complex,
+                                     ND_POINTER_1_complex]
+    L.Settings_new.argtypes = []
+    L.Settings_new.restype = vp
+    for name in ("nr1", "nr2", "nr3"):
+        getattr(L, f"Settings_set_{name}").argtypes = [vp, ct.c_int]
+    for name in ("tmax", "dt", "intensity", "lambda", "tmax_field"):
+        getattr(L, f"Settings_set_{name}").argtypes = [vp, ct.c_double]
+    L.Settings_set_pol_vec.argtypes = [vp, ND_POINTER_1_double]
+    L.Settings_set_phi_vec.argtypes = [vp, ND_POINTER_1_double]
+    ext = hasattr(L, "SWESim_last_error")
+    if ext:
+        L.SWESim_last_error.argtypes = [vp]
+        L.SWESim_last_error.restype = ct.c_char_p
+        L.Settings_delete.argtypes = [vp]
+        L.SWESim_get_nt.argtypes = [vp]
+        L.SWESim_get_num_orb.argtypes = [vp]
+        L.SWESim_set_device.argtypes = [vp, ct.c_int]
+        L.SWESim_last_kernel_ms.argtypes = [vp]
+        L.SWESim_last_kernel_ms.restype = ct.c_double
+        L.SWESim_last_launches.argtypes = [vp]
+        L.SWESim_reset.argtypes = [vp]
+        L.SWESim_get_rho_k.argtypes = [vp, ND_POINTER_1_complex]
+        L.SWESim_get_fields.argtypes = [vp, ND_POINTER_1_double, ND_POINTER_1_double, ND_POINTER_1_double]
+    _libs[path] = (L, ext)
+    return _libs[path]
+
+
+class Settings:
+    """Simulation parameters (include/settings.h of the reference); owns a C ``Settings``."""
+
+    def __init__(self, param):
+        self.path_lib = param.get("path_lib") or default_library()
+        self.path_tb = param["path_tb"]
+        self.nt = int(param["tmax"] / param["dt"])
+        self.param = dict(param)
+        self.settings_swe, self._ext = _load(self.path_lib)
+        L = self.settings_swe
+        self.ptr = L.Settings_new()
+        L.Settings_set_nr1(self.ptr, int(param["nr1"]))
+        L.Settings_set_nr2(self.ptr, int(param["nr2"]))
+        L.Settings_set_nr3(self.ptr, int(param.get("nr3", 1)))
+        L.Settings_set_tmax(self.ptr, float(param["tmax"]))
+        L.Settings_set_dt(self.ptr, float(param["dt"]))
+        L.Settings_set_intensity(self.ptr, float(param["intensity"]))
+        L.Settings_set_lambda(self.ptr, float(param["lambda"]))
+        L.Settings_set_tmax_field(self.ptr, float(param["tmax_field"]))
+        L.Settings_set_pol_vec(self.ptr, np.ascontiguousarray(param["pol_vec"], dtype=np.float64))
+        L.Settings_set_phi_vec(self.ptr, np.ascontiguousarray(param["phi_vec"], dtype=np.float64))
+
+    def __del__(self):
+        try:
+            if self._ext and self.ptr:
+                self.settings_swe.Settings_delete(self.ptr)
+                self.ptr = None
+        except Exception:
+            pass
+
+
+class SWE:
+    """One propagation: setup on construction (SWESim_init), then run_simulation / get_current."""
+
+    def __init__(self, settings: Settings, device: int | None = None):
+        self.settings = settings
+        self.swe_cpp, self._ext = _load(settings.path_lib)
+        self.ptr = self.swe_cpp.SWESim_new()
+        if not self.ptr:
+            raise SWEError("SWESim_new failed")
+        if device is not None:
+            self._call("SWESim_set_device", int(device))
+        self.set_path_tb(settings.path_tb.encode("UTF-8"))
+        self.set_settings(settings.ptr)
+        self.init()
+
+    def _call(self, name, *args):
+        if self.ptr is None:
+            raise SWEError(f"{name}: SWE object already deleted")
+        out = getattr(self.swe_cpp, name)(self.ptr, *args)
+        if self._ext:
+            msg = self.swe_cpp.SWESim_last_error(self.ptr)
+            if msg:
+                raise SWEError(msg.decode())
+        return out
+
+    # --- the reference's methods (pySWE/pyswe.py:37-57) ---
+    def run_simulation(self):
+        self._call("SWESim_run_simulation")
+
+    def test_files(self):
+        self._call("SWESim_test_files")
+
+    def set_path_tb(self, val):
+        self._call("SWESim_set_path_tb", val)
+
+    def set_settings(self, val):
+        self._call("SWESim_set_settings", val)
+
+    def init(self):
+        self._call("SWESim_init")
+
+    def restart(self):
+        self._call("SWESim_restart")
+
+    def delete(self):
+        if self.ptr is not None:
+            self.swe_cpp.SWESim_delete(self.ptr)
+            self.ptr = None
+
+    def get_current(self):
+        n = self.settings.nt
+        t = np.zeros(n, dtype=np.float64)
+        jx = np.zeros(n, dtype=np.complex128)
+        jy = np.zeros(n, dtype=np.complex128)
+        jz = np.zeros(n, dtype=np.complex128)
+        self._call("SWESim_get_current", t, jx, jy, jz)
+        return np.array([t, jx, jy, jz])
+
+    # --- additions ---
+    def reset(self):
+        """Back to rho0 with an empty current record, keeping the setup."""
+        self._call("SWESim_reset")
+
+    def last_kernel_ms(self) -> float:
+        return float(self.swe_cpp.SWESim_last_kernel_ms(self.ptr))
+
+    def last_launches(self) -> int:
+        return int(self.swe_cpp.SWESim_last_launches(self.ptr))
+
+    def num_orb(self) -> int:
+        return int(self.swe_cpp.SWESim_get_num_orb(self.ptr))
+
+    def get_rho_k(self):
+        nk = int(self.settings.param["nr1"]) * int(self.settings.param["nr2"])
+        nw = self.num_orb()
+        out = np.zeros(nk * nw * nw, dtype=np.complex128)
+        self._call("SWESim_get_rho_k", out)
+        return out.reshape(nk, nw * nw)
+
+    def get_fields(self):
+        n = self.settings.nt
+        t = np.zeros(n)
+        E = np.zeros(3 * n)
+        A = np.zeros(3 * n)
+        self._call("SWESim_get_fields", t, E, A)
+        return t, E.reshape(3, n), A.reshape(3, n)
+
+    def __del__(self):
+        try:
+            self.delete()
+        except Exception:
+            pass

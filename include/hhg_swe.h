@@ -1,0 +1,102 @@
+/* hhg-b200: B200-native drop-in for the SBE time propagation of rodrigomarher/HHG-Solids.
+ *
+ * The first block re-exports, with the same names, signatures and argument meaning, the C-linkage
+ * surface that the reference's ctypes wrapper (pySWE/pyswe.py:13-35,65-98) binds, declared in the
+ * reference's src/cwrapper.cpp:5-28.  Each entry cites the line it replaces.  A `SWESim` here owns
+ * GPU state; `Settings` is opaque to callers exactly as in the reference.
+ *
+ * Differences in error behaviour: the reference throws through extern "C" or calls exit() on bad
+ * input (src/wannier_tb.cpp:18, src/operator.cpp:167-168).  Here no entry point throws or exits:
+ * a failure records a message, leaves the object in a defined state, and SWESim_last_error() /
+ * HHG_last_error() return it (NULL when the last call on that object succeeded).
+ *
+ * The second block holds additions with no counterpart in the reference (precision and solver
+ * selection, device-resident timing, the batched API); the reference-facing block does not
+ * depend on them. */
+#ifndef HHG_SWE_H
+#define HHG_SWE_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct SWESim SWESim;
+typedef struct Settings Settings;
+/* std::complex<double> / numpy complex128 layout: {re, im}. */
+typedef struct hhg_cdouble {
+  double re, im;
+} hhg_cdouble;
+
+/* ---- reference C ABI (src/cwrapper.cpp) -------------------------------------------------- */
+
+/* src/cwrapper.cpp:7   SWESim* SWESim_new()                       caller owns; free with SWESim_delete */
+SWESim* SWESim_new(void);
+/* src/cwrapper.cpp:8   void SWESim_run_simulation(SWESim*)        propagates nt RK4 steps, records J(t) */
+void SWESim_run_simulation(SWESim* swe);
+/* src/cwrapper.cpp:9   void SWESim_test_files(SWESim*)            text dumps into test/ and fields/ */
+void SWESim_test_files(SWESim* swe);
+/* src/cwrapper.cpp:10  void SWESim_set_path_tb(SWESim*, char*)   path is copied */
+void SWESim_set_path_tb(SWESim* swe, char* path_tb);
+/* src/cwrapper.cpp:11  void SWESim_set_settings(SWESim*, Settings*)   borrowed: must outlive the SWESim */
+void SWESim_set_settings(SWESim* swe, Settings* settings);
+/* src/cwrapper.cpp:12  void SWESim_init(SWESim*)                 full setup (src/swe.cpp:49-93) */
+void SWESim_init(SWESim* swe);
+/* src/cwrapper.cpp:13  void SWESim_restart(SWESim*)              setup again from scratch */
+void SWESim_restart(SWESim* swe);
+/* src/cwrapper.cpp:14  void SWESim_get_current(SWESim*, double* t, cdouble* jx, cdouble* jy, cdouble* jz)
+ * caller-allocated arrays of nt entries; t in atomic units. */
+void SWESim_get_current(SWESim* swe, double* t, hhg_cdouble* jx, hhg_cdouble* jy, hhg_cdouble* jz);
+/* src/cwrapper.cpp:15  void SWESim_delete(SWESim*) */
+void SWESim_delete(SWESim* swe);
+
+/* src/cwrapper.cpp:17  Settings* Settings_new()   defaults of include/settings.h:8-22 */
+Settings* Settings_new(void);
+/* src/cwrapper.cpp:18-20  grid sizes */
+void Settings_set_nr1(Settings* s, int val);
+void Settings_set_nr2(Settings* s, int val);
+void Settings_set_nr3(Settings* s, int val);
+/* src/cwrapper.cpp:21-25  tmax (fs), dt (fs), intensity (W/cm^2), lambda (nm), tmax_field (fs) */
+void Settings_set_tmax(Settings* s, double val);
+void Settings_set_dt(Settings* s, double val);
+void Settings_set_intensity(Settings* s, double val);
+void Settings_set_lambda(Settings* s, double val);
+void Settings_set_tmax_field(Settings* s, double val);
+/* src/cwrapper.cpp:26-27  polarisation vector and CEP phases, 3 doubles each */
+void Settings_set_pol_vec(Settings* s, double* val);
+void Settings_set_phi_vec(Settings* s, double* val);
+
+/* ---- additions (no counterpart in the reference) ----------------------------------------- */
+
+/* Message of the last failed call on `swe` (NULL if it succeeded); valid until the next call. */
+const char* SWESim_last_error(SWESim* swe);
+/* Message of the last failed call in this thread on any object (NULL if none). */
+const char* HHG_last_error(void);
+/* Frees a Settings made by Settings_new (the reference never frees them). */
+void Settings_delete(Settings* s);
+/* Number of time steps nt = (int)(tmax/dt) (src/swe.cpp:52), -1 before SWESim_init. */
+int SWESim_get_nt(SWESim* swe);
+/* Orbitals per k-point, -1 before SWESim_init. */
+int SWESim_get_num_orb(SWESim* swe);
+/* CUDA device ordinal used by the next SWESim_init (default: the current device). */
+void SWESim_set_device(SWESim* swe, int device);
+/* Device time in milliseconds of the last SWESim_run_simulation's propagation kernels. */
+double SWESim_last_kernel_ms(SWESim* swe);
+/* Number of kernel launches issued by the last SWESim_run_simulation. */
+int SWESim_last_launches(SWESim* swe);
+/* Put rho back to the equilibrium rho0 and clear the recorded current, keeping the setup
+ * (a fresh propagation without re-running SWESim_init). */
+void SWESim_reset(SWESim* swe);
+/* Copy the k-space density matrix, [nr1*nr2][nw*nw] complex (W gauge), to host memory. */
+void SWESim_get_rho_k(SWESim* swe, hhg_cdouble* out);
+/* Fields the propagation uses: t (au, nt), E and A (au, [3][nt]). */
+void SWESim_get_fields(SWESim* swe, double* t, double* E, double* A);
+
+/* FP64 FMA / FP32 FMA chain throughput of the current device (TFLOP/s), for roofline denominators. */
+int HHG_measure_peaks(double* fp64_tflops, double* fp32_tflops);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

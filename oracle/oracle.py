@@ -62,6 +62,7 @@ def lib():
         L.oracle_velocity_window.argtypes = [ct.c_char_p, P, dp]
         L.oracle_rho0.argtypes = [ct.c_char_p, P, dp]
         L.oracle_run.argtypes = [ct.c_char_p, P, ct.c_int, ct.c_int, dp, dp]
+        L.oracle_run_steps.argtypes = [ct.c_char_p, P, ct.c_int, ct.c_int, ct.c_int, dp, dp]
         _lib = L
     return _lib
 
@@ -122,15 +123,17 @@ def rho0(tb: str, param: dict):
     return rho
 
 
-def run(tb: str, param: dict, k_begin: int = 0, k_end: int | None = None):
-    """Propagate; returns (t, J[3, nt]) with J the (partial, if a k-range is given) current."""
+def run(tb: str, param: dict, k_begin: int = 0, k_end: int | None = None, nsteps: int = -1):
+    """Propagate; returns (t, J[3, nt]) with J the (partial, if a k-range is given) current.
+
+    ``nsteps`` >= 0 stops after that many steps (the later samples stay zero)."""
     s = settings(param)
     n = lib().oracle_nt(ct.byref(s))
     if k_end is None:
         k_end = s.nr1 * s.nr2
     t = np.zeros(n)
     J = np.zeros((3, n), dtype=np.complex128)
-    got = lib().oracle_run(tb.encode(), ct.byref(s), int(k_begin), int(k_end), _dp(t), _dp(J))
+    got = lib().oracle_run_steps(tb.encode(), ct.byref(s), int(k_begin), int(k_end), int(nsteps), _dp(t), _dp(J))
     if got != n:
         raise ValueError(f"oracle_run failed ({got})")
     return t, J

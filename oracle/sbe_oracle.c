@@ -333,23 +333,33 @@ static cplx* twiddles(int N) {
   return T;
 }
 
-/* rho0(k) = U f U^+ with f_n = [E_n < 0] for H(k) = sum_R e^{-ik.R} H_R in au
- * (src/swe.cpp:82-87, src/hamiltonian.cpp:70-101, src/rdm.cpp:23-38). */
+/* rho0(k) = U f U^+ for H(k) = sum_R e^{-ik.R} H_R in au (src/swe.cpp:82-87,
+ * src/hamiltonian.cpp:70-101, src/rdm.cpp:23-38).  U holds the eigenvectors of the Hermitian matrix
+ * built from the lower triangle (zheevd 'L'); the occupation is f_n = [Re (U^+ H U)_nn < 0] with the
+ * full H, as the reference takes it from the rotated H.  The two differ only when the placed H(R)
+ * is not Hermitian-symmetric on the grid (a grid smaller than the model's R range). */
 static void rho0_at(const tb_model* m, const cell_ref* sup, int ns, const cplx* T1, const cplx* T2, int N1,
                     int N2, int m1, int m2, cplx* Hk, cplx* U, double* w, cplx* rho) {
   const int nw = m->nw, nw2 = nw * nw;
+  cplx* Hf = malloc(sizeof(cplx) * nw2);
   for (int o = 0; o < nw2; ++o) Hk[o] = 0;
   for (int q = 0; q < ns; ++q) {
     cplx ph = T1[wrap((long)m1 * sup[q].n1, N1)] * T2[wrap((long)m2 * sup[q].n2, N2)];
     const cplx* h = m->hop + (size_t)sup[q].site * nw2;
     for (int o = 0; o < nw2; ++o) Hk[o] += ph * (h[o] * (1.0 / 27.2114));
   }
-  /* zheevd(..., 'L') reads the lower triangle: symmetrise from it. */
+  memcpy(Hf, Hk, sizeof(cplx) * nw2);
   for (int i = 0; i < nw; ++i) {
     Hk[i * nw + i] = creal(Hk[i * nw + i]);
     for (int j = i + 1; j < nw; ++j) Hk[i * nw + j] = conj(Hk[j * nw + i]);
   }
   jacobi_herm(nw, Hk, w, U);
+  for (int n = 0; n < nw; ++n) {
+    cplx d = 0;
+    for (int i = 0; i < nw; ++i)
+      for (int j = 0; j < nw; ++j) d += conj(U[i * nw + n]) * Hf[i * nw + j] * U[j * nw + n];
+    w[n] = creal(d);
+  }
   for (int i = 0; i < nw; ++i)
     for (int j = 0; j < nw; ++j) {
       cplx sum = 0;
@@ -357,6 +367,7 @@ static void rho0_at(const tb_model* m, const cell_ref* sup, int ns, const cplx* 
         if (w[n] < 0.0) sum += U[i * nw + n] * conj(U[j * nw + n]);
       rho[i * nw + j] = sum;
     }
+  free(Hf);
 }
 
 int oracle_rho0(const char* tb, const oracle_settings* s, double* rho_out) {
@@ -399,6 +410,11 @@ static void rk_stage(int nw, const cplx* H, const cplx* X, cplx* out) {
 }
 
 int oracle_run(const char* tb, const oracle_settings* s, int k_begin, int k_end, double* t, double* Jout) {
+  return oracle_run_steps(tb, s, k_begin, k_end, -1, t, Jout);
+}
+
+int oracle_run_steps(const char* tb, const oracle_settings* s, int k_begin, int k_end, int nsteps, double* t,
+                     double* Jout) {
   tb_model m;
   if (tb_parse(tb, &m)) return -1;
   placed_grid g;
@@ -475,7 +491,8 @@ int oracle_run(const char* tb, const oracle_settings* s, int k_begin, int k_end,
   cplx* Wk = malloc(sizeof(cplx) * 3 * nw2);
   cplx pw[16];
 
-  for (int ti = 0; ti < nt; ++ti) {
+  const int nrun = (nsteps < 0 || nsteps > nt) ? nt : nsteps;
+  for (int ti = 0; ti < nrun; ++ti) {
     /* src/solver.cpp:109-148: field samples at t, t + dt/2 (mean of the end points), t + dt. */
     double Es[3][3];
     for (int a = 0; a < 3; ++a) {

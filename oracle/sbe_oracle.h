@@ -48,6 +48,10 @@ int oracle_rho0(const char* tb, const oracle_settings* s, double* rho_k);
  * t (au, nt) and the partial current J (complex, [3][nt]) normalised by the FULL nr1*nr2, so that
  * partial currents over a partition of the k-grid add up to the full current. Returns nt. */
 int oracle_run(const char* tb, const oracle_settings* s, int k_begin, int k_end, double* t, double* J);
+/* As oracle_run, but only the first nsteps steps (fields still built for the full nt, so the
+ * samples equal the first nsteps samples of the full run); J entries after nsteps stay zero. */
+int oracle_run_steps(const char* tb, const oracle_settings* s, int k_begin, int k_end, int nsteps, double* t,
+                     double* J);
 
 #ifdef __cplusplus
 }

@@ -1,0 +1,187 @@
+"""GPU propagation through the reference-facing C ABI (libhhg_b200.so via the pySWE classes) against
+the golden J(t) made by the reference's own build, and against the CPU oracle."""
+import os
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN, golden_names, load_golden, rel_l2
+
+pytestmark = pytest.mark.gpu
+
+TOL = 1e-10  # relative L2 on J(t), per axis: the plain FP64 parity bar
+
+
+@pytest.fixture(scope="module")
+def pyswe():
+    from pySWE import pyswe as mod
+
+    return mod
+
+
+def run_swe(pyswe, param, device=None):
+    s = pyswe.Settings(dict(param))
+    swe = pyswe.SWE(s, device=device)
+    swe.run_simulation()
+    t, jx, jy, jz = swe.get_current()
+    out = (np.real(t), np.stack([jx, jy, jz]), swe)
+    return out
+
+
+def check_current(J, J_ref, name):
+    for a in range(3):
+        if np.abs(J_ref[a]).max() == 0:
+            assert np.abs(J[a]).max() == 0, (name, a)
+        else:
+            err = rel_l2(J[a], J_ref[a])
+            assert err < TOL, (name, a, err)
+
+
+@pytest.mark.parametrize("name", golden_names())
+def test_current_matches_reference_golden(pyswe, name):
+    meta, param, t_ref, J_ref = load_golden(name)
+    t, J, swe = run_swe(pyswe, param)
+    assert np.array_equal(t, t_ref)
+    check_current(J, J_ref, name)
+    swe.delete()
+
+
+def harmonic_spectrum(J, dt):
+    """|fftshift(fft(ifftshift(gradient(J, dt))))|^2 as in the reference's scripts/pol_scan.py:34-40."""
+    acc = np.gradient(J, dt)
+    return np.abs(np.fft.fftshift(np.fft.fft(np.fft.ifftshift(acc)))) ** 2
+
+
+@pytest.mark.parametrize("name", [n for n in ("c0", "c1") if os.path.exists(os.path.join(GOLDEN, f"{n}.npz"))])
+def test_harmonic_spectrum_matches_up_to_cutoff(pyswe, name):
+    meta, param, t_ref, J_ref = load_golden(name)
+    _, J, swe = run_swe(pyswe, param)
+    dt = param["dt"]
+    nt = J.shape[1]
+    S = harmonic_spectrum(J[1], dt)
+    S_ref = harmonic_spectrum(J_ref[1], dt)
+    # harmonic-order axis of scripts/pol_scan.py:48-57
+    dw = 2.0 * np.pi / param["tmax"]
+    wmax = nt * dw / 2.0
+    order = np.linspace(-wmax, wmax, nt) / (2.0 * np.pi * 300 / param["lambda"])
+    fund = S_ref[(order > 0.5) & (order < 1.5)].sum()
+    checked = 0
+    for h in range(1, 200, 2):
+        win = (order > h - 0.5) & (order < h + 0.5)
+        I_ref = S_ref[win].sum()
+        if not win.any() or I_ref < 1e-12 * fund:
+            break
+        assert abs(S[win].sum() - I_ref) / I_ref < 1e-10, (name, h)
+        checked += 1
+    assert checked >= 3
+    swe.delete()
+
+
+def test_fields_match_reference_arithmetic(pyswe, oracle_mod):
+    meta, param, _, _ = load_golden("c0")
+    s = pyswe.Settings(dict(param))
+    swe = pyswe.SWE(s)
+    t, E, A = swe.get_fields()
+    if oracle_mod.have_ref():
+        tr, Er, Ar = oracle_mod.ref_fields(param["path_tb"], param)
+    else:
+        tr, Er, Ar = oracle_mod.fields(param["path_tb"], param)
+    assert np.array_equal(t, tr)
+    assert np.abs(E - Er).max() <= 1e-14 * np.abs(Er).max()
+    assert np.abs(A - Ar).max() <= 1e-14 * np.abs(Ar).max()
+    swe.delete()
+
+
+@pytest.mark.parametrize("model,n", [("haldane", 12), ("tmd6_s1", 8), ("tmd11_s7", 10), ("tmd12_s3", 6)])
+def test_rho0_matches_oracle(pyswe, oracle_mod, model, n):
+    import tbgen
+
+    tb = tbgen.model_path(model)
+    param = dict(path_tb=tb, nr1=n, nr2=n, nr3=1, tmax=1.0, dt=0.02197, intensity=1e12, tmax_field=80.0,
+                 pol_vec=np.array([0.0, 1.0, 0.0]), phi_vec=np.zeros(3), **{"lambda": 3000.0})
+    swe = pyswe.SWE(pyswe.Settings(param))
+    rho = swe.get_rho_k()
+    ref = oracle_mod.rho0(tb, param)
+    assert np.abs(rho - ref).max() < 1e-12
+    swe.delete()
+
+
+def test_reruns_are_bitwise_deterministic(pyswe):
+    meta, param, _, J_ref = load_golden("haldane_12_pol")
+    s = pyswe.Settings(dict(param))
+    swe = pyswe.SWE(s)
+    swe.run_simulation()
+    J1 = swe.get_current()[1:]
+    swe.reset()
+    swe.run_simulation()
+    J2 = swe.get_current()[1:]
+    assert np.array_equal(J1, J2)
+    swe.delete()
+
+
+def test_second_run_continues_and_keeps_first_record(pyswe):
+    """As in the reference, a second run_simulation continues from the propagated state and
+    get_current keeps returning the first nt samples (src/observable.cpp:29, src/swe.cpp:235-242)."""
+    meta, param, _, J_ref = load_golden("haldane_8_y")
+    s = pyswe.Settings(dict(param))
+    swe = pyswe.SWE(s)
+    swe.run_simulation()
+    rho1 = swe.get_rho_k()
+    swe.run_simulation()
+    rho2 = swe.get_rho_k()
+    J = swe.get_current()[1:]
+    assert not np.array_equal(rho1, rho2)
+    check_current(J, J_ref, "haldane_8_y")
+    swe.delete()
+
+
+def test_restart_gives_a_fresh_run(pyswe):
+    meta, param, _, J_ref = load_golden("tmd6_8")
+    swe = pyswe.SWE(pyswe.Settings(dict(param)))
+    swe.run_simulation()
+    swe.restart()
+    swe.run_simulation()
+    check_current(swe.get_current()[1:], J_ref, "tmd6_8")
+    swe.delete()
+
+
+def test_get_current_before_run_raises(pyswe):
+    meta, param, _, _ = load_golden("haldane_8_y")
+    swe = pyswe.SWE(pyswe.Settings(dict(param)))
+    with pytest.raises(pyswe.SWEError, match="run_simulation"):
+        swe.get_current()
+    swe.delete()
+
+
+def test_non_hermitian_placement_matches_oracle(pyswe, oracle_mod):
+    """A 6x6 grid under a 7x7-cell model drops the +3 cells: H(k) is not Hermitian and the
+    full-commutator path must follow the reference (pinned through the oracle)."""
+    import tbgen
+
+    tb = tbgen.model_path("tmd6_s1")
+    param = dict(path_tb=tb, nr1=6, nr2=6, nr3=1, tmax=0.6, dt=0.02197, intensity=1.5e12, tmax_field=80.0,
+                 pol_vec=np.array([1.0, 0.0, 0.0]), phi_vec=np.array([0.2, 0.0, 0.0]), **{"lambda": 2500.0})
+    t, J, swe = run_swe(pyswe, param)
+    _, Jo = oracle_mod.run(tb, param)
+    for a in range(2):
+        assert rel_l2(J[a], Jo[a]) < TOL
+    swe.delete()
+
+
+@pytest.mark.parametrize("model,n,pol", [("haldane", 20, [0.8, 0.6, 0.0]), ("tmd12_s3", 8, [0.0, 1.0, 0.0]),
+                                         ("haldane", 4, [0.0, 1.0, 0.3])])
+def test_matches_oracle_on_other_shapes(pyswe, oracle_mod, model, n, pol):
+    import tbgen
+
+    tb = tbgen.model_path(model)
+    param = dict(path_tb=tb, nr1=n, nr2=n + 2, nr3=1, tmax=1.5, dt=0.02197, intensity=2e12, tmax_field=80.0,
+                 pol_vec=np.array(pol), phi_vec=np.array([0.0, 0.5, 0.0]), **{"lambda": 2000.0})
+    t, J, swe = run_swe(pyswe, param)
+    to, Jo = oracle_mod.run(tb, param)
+    assert np.array_equal(t, to)
+    for a in range(3):
+        if np.abs(Jo[a]).max() == 0:
+            assert np.abs(J[a]).max() == 0
+        else:
+            assert rel_l2(J[a], Jo[a]) < TOL
+    swe.delete()
