@@ -1,0 +1,457 @@
+#!/usr/bin/env python
+"""Benchmark of the SBE propagation: k-point x RK4-step throughput of one B200 (or N, one process each).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload c1|c0|c2] [--impl ours|reference]
+
+A *step* is one full solve of the workload: nt RK4 steps of every k-point plus the current J(t).
+The default workload is "c1": the 2-orbital Haldane-like model on a 200 x 200 k-grid under the
+full pulse (nt = 4096), plain FP64 -- the drop-in configuration for the reference's propagation.
+
+Printed JSON line (rank 0):
+  value         k-pt*RK4-steps/s of the whole job, from CUDA events around the propagation kernels
+                (library stream), inputs already on the device; L2 flushed between solves.
+  e2e           the same metric through the reference-facing C ABI: SWESim_restart (TB parse,
+                placement, host->device tables, rho0 on the GPU) + SWESim_run_simulation +
+                SWESim_get_current into host arrays, wall-clocked.
+  roofline      the propagation kernel's algorithmic FP64 rate against the FP64 FMA peak measured
+                live on the same GPU (the driver's peaks file has HBM and bf16 only).
+  cpu_baseline  the reference's own CPU build (oracle/_ref/libwannier.so) on the host cores, one
+                single-threaded process per core (the reference's pol_scan model), bounded sample.
+
+With --impl reference the line instead times that reference CPU build alone on all host cores.
+For N > 1 (torchrun), every rank runs its own solve at its own polarisation angle (replicas, no
+data-path collective); the time is the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(REPO, "hhg-solids_b200")
+sys.path.insert(0, PKG)
+
+PULSE = dict(tmax=90.0, dt=21.97e-3, intensity=1e12, tmax_field=80.0, phi_vec=[0.0, 0.0, 0.0], **{"lambda": 3000.0})
+WORKLOADS = {
+    "c0": dict(model="haldane", n=60, window=5,
+               desc="2-orbital Haldane-like TB (a=2.5 A, 25 R cells), 60x60 k-grid, full pulse, plain FP64"),
+    "c1": dict(model="haldane", n=200, window=5,
+               desc="2-orbital Haldane-like TB (a=2.5 A, 25 R cells), 200x200 k-grid, full pulse, plain FP64"),
+    "c2": dict(model="tmd11_s7", n=150, window=7,
+               desc="11-orbital TMD-like TB (seed 7, 49 R cells), 150x150 k-grid, full pulse, plain FP64"),
+}
+
+
+def workload_param(name: str, rank: int = 0, world: int = 1) -> dict:
+    import numpy as np
+    import tbgen
+
+    w = WORKLOADS[name]
+    ang = math.pi * rank / max(world, 1)  # replicas: one polarisation angle per rank
+    pol = [math.sin(ang), math.cos(ang), 0.0]
+    p = dict(PULSE, nr1=w["n"], nr2=w["n"], nr3=1, path_tb=tbgen.model_path(w["model"]))
+    p["pol_vec"] = np.array(pol)
+    p["phi_vec"] = np.array(p["phi_vec"])
+    return p
+
+
+def flops_per_kstep(nw: int, window: int, n: int, n_op: int, n_j: int) -> float:
+    """Algorithmic FP64 flops of one k-point x RK4 step (minimal form):
+    4 stages x one complex nw^3 product (Hermitian commutator), the Wannier sum of H0 and the
+    field-coupled r as a separable pruned DFT over the window x window cells, the windowed velocity
+    (4x4 pruned DFT) and Tr(W rho), and the RK axpys."""
+    f_comm = 32.0 * nw ** 3
+    f_w = 8.0 * nw * nw * n_op * window * (1.0 + window / n)
+    f_j = n_j * 8.0 * nw * nw * (4.0 * (1.0 + 4.0 / n) + 1.0)
+    f_rk = 12.0 * nw * nw
+    return f_comm + f_w + f_j + f_rk
+
+
+class ClockSampler:
+    """nvidia-smi samples of SM clock and throttle reasons during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "100",
+                 "-i", str(self.device)], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except (FileNotFoundError, OSError):
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"], "samples": 0}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.thread.join(timeout=2)
+        sm, smax, power, reasons = [], [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+                power.append(float(parts[3]))
+            except ValueError:
+                continue
+            for nm, flag in zip(names, parts[5:9]):
+                if flag.lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(smax), "reasons": sorted(reasons),
+                "samples": len(sm), "power_w_max": max(power)}
+
+
+# ---------------------------------------------------------------- the reference's CPU build
+
+
+def _ref_worker(conn, lib_path, tb, param, nt_sample):
+    """One single-threaded reference process (its own SWESim), driven through the reference C ABI."""
+    import ctypes as ct
+
+    import numpy as np
+
+    devnull = os.open(os.devnull, os.O_WRONLY)
+    os.dup2(devnull, 1)  # the reference prints progress to stdout
+    L = ct.CDLL(lib_path)
+    vp = ct.c_void_p
+    L.SWESim_new.restype = vp
+    L.Settings_new.restype = vp
+    for name in ("SWESim_run_simulation", "SWESim_init", "SWESim_delete"):
+        getattr(L, name).argtypes = [vp]
+    L.SWESim_set_path_tb.argtypes = [vp, ct.c_char_p]
+    L.SWESim_set_settings.argtypes = [vp, vp]
+    for name in ("nr1", "nr2", "nr3"):
+        getattr(L, f"Settings_set_{name}").argtypes = [vp, ct.c_int]
+    for name in ("tmax", "dt", "intensity", "lambda", "tmax_field"):
+        getattr(L, f"Settings_set_{name}").argtypes = [vp, ct.c_double]
+    dp = ct.POINTER(ct.c_double)
+    L.Settings_set_pol_vec.argtypes = [vp, dp]
+    L.Settings_set_phi_vec.argtypes = [vp, dp]
+    s = L.Settings_new()
+    L.Settings_set_nr1(s, int(param["nr1"]))
+    L.Settings_set_nr2(s, int(param["nr2"]))
+    L.Settings_set_nr3(s, 1)
+    L.Settings_set_tmax(s, (nt_sample + 0.5) * param["dt"])
+    L.Settings_set_dt(s, param["dt"])
+    L.Settings_set_intensity(s, param["intensity"])
+    L.Settings_set_lambda(s, param["lambda"])
+    L.Settings_set_tmax_field(s, param["tmax_field"])
+    pol = np.ascontiguousarray(param["pol_vec"], dtype=np.float64)
+    phi = np.ascontiguousarray(param["phi_vec"], dtype=np.float64)
+    L.Settings_set_pol_vec(s, pol.ctypes.data_as(dp))
+    L.Settings_set_phi_vec(s, phi.ctypes.data_as(dp))
+    sim = L.SWESim_new()
+    L.SWESim_set_path_tb(sim, tb.encode())
+    L.SWESim_set_settings(sim, s)
+    L.SWESim_init(sim)
+    conn.send("ready")
+    while True:
+        msg = conn.recv()
+        if msg != "run":
+            break
+        t0 = time.perf_counter()
+        L.SWESim_run_simulation(sim)  # nt_sample RK4 steps (the state keeps evolving; the cost per step does not change)
+        conn.send(time.perf_counter() - t0)
+    L.SWESim_delete(sim)
+
+
+class ReferencePool:
+    """`cores` concurrent single-threaded reference solves of the workload's grid and model."""
+
+    def __init__(self, param: dict, nt_sample: int, cores: int):
+        import multiprocessing as mp
+
+        sys.path.insert(0, os.path.join(REPO, "oracle"))
+        import oracle
+
+        lib = oracle.ref_paths()[0]
+        if not os.path.exists(lib):
+            raise FileNotFoundError("oracle/_ref/libwannier.so (build: make -C oracle with the reference checkout)")
+        os.environ["OPENBLAS_NUM_THREADS"] = "1"
+        os.environ["OMP_NUM_THREADS"] = "1"
+        ctx = mp.get_context("spawn")
+        self.nt_sample, self.cores, self.param = nt_sample, cores, param
+        self.conns, self.procs = [], []
+        for _ in range(cores):
+            a, b = ctx.Pipe()
+            p = ctx.Process(target=_ref_worker, args=(b, lib, param["path_tb"], param, nt_sample), daemon=True)
+            p.start()
+            self.conns.append(a)
+            self.procs.append(p)
+        for c in self.conns:
+            if c.recv() != "ready":
+                raise RuntimeError("reference worker failed")
+
+    def step(self) -> float:
+        t0 = time.perf_counter()
+        for c in self.conns:
+            c.send("run")
+        for c in self.conns:
+            c.recv()
+        return time.perf_counter() - t0
+
+    def kpoint_steps(self) -> int:
+        return self.cores * self.param["nr1"] * self.param["nr2"] * self.nt_sample
+
+    def close(self):
+        for c in self.conns:
+            try:
+                c.send("stop")
+            except Exception:
+                pass
+        for p in self.procs:
+            p.join(timeout=10)
+            if p.is_alive():
+                p.terminate()
+
+
+def reference_sample_steps(workload: str) -> int:
+    # about 2-4 s of wall time per sample on one core of a current Xeon (measured here: 0.11 s per
+    # RK4 step for c1, 6 ms for c0, 2.2 s for c2)
+    return {"c0": 400, "c1": 24, "c2": 2}[workload]
+
+
+def run_reference_arm(args, rank: int, world: int):
+    if rank != 0:
+        return
+    param = workload_param(args.workload)
+    cores = os.cpu_count() or 1
+    nt_sample = reference_sample_steps(args.workload)
+    line = {"metric": "k-pt*RK4-steps/s", "impl": "reference", "unit": "k-pt*RK4-steps/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded TB model)",
+            "config": {"workload": f"{args.workload}: {WORKLOADS[args.workload]['desc']}",
+                       "sample": f"{cores} concurrent single-threaded processes x {nt_sample} RK4 steps",
+                       "l2": "n/a (CPU)"}}
+    try:
+        pool = ReferencePool(param, nt_sample, cores)
+    except Exception as e:  # noqa: BLE001
+        print(json.dumps({"impl": "reference", "unavailable": f"reference CPU build not runnable: {e}"}))
+        return
+    try:
+        for _ in range(args.warmup):
+            pool.step()
+        times = [pool.step() for _ in range(args.steps)]
+    finally:
+        pool.close()
+    total = sum(times)
+    value = pool.kpoint_steps() * len(times) / total
+    line.update(value=value, ms_per_step=1e3 * total / len(times),
+                cpu_baseline={"value": value, "unit": "k-pt*RK4-steps/s", "cores": cores, "kind": "reference",
+                              "sample": line["config"]["sample"]},
+                e2e={"value": value, "unit": "k-pt*RK4-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0})
+    print(json.dumps(line), flush=True)
+
+
+def cpu_baseline(workload: str) -> dict:
+    """Reference CPU build on the host cores, bounded sample (one warm and one timed round)."""
+    param = workload_param(workload)
+    cores = os.cpu_count() or 1
+    nt_sample = reference_sample_steps(workload)
+    try:
+        pool = ReferencePool(param, nt_sample, cores)
+    except Exception as e:  # noqa: BLE001
+        return {"value": None, "unit": "k-pt*RK4-steps/s", "cores": cores, "kind": "reference",
+                "sample": f"unavailable: {e}"}
+    try:
+        pool.step()
+        t = pool.step()
+    finally:
+        pool.close()
+    return {"value": pool.kpoint_steps() / t, "unit": "k-pt*RK4-steps/s", "cores": cores, "kind": "reference",
+            "sample": f"{cores} concurrent single-threaded processes x {nt_sample} RK4 steps of the same grid and model "
+                      f"({t:.1f} s wall)"}
+
+
+# ---------------------------------------------------------------- our arm
+
+
+def load_traffic(workload: str):
+    path = os.path.join(REPO, "profiles", f"propagate_fp64_{workload}_traffic.json")
+    if not os.path.exists(path):
+        return None, None
+    with open(path) as f:
+        d = json.load(f)
+    return d.get("dram_bytes_per_launch"), d.get("source")
+
+
+def main():
+    ap = argparse.ArgumentParser(description=__doc__.split("\n\n")[0])
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--workload", default="c1", choices=sorted(WORKLOADS))
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        ap.error("--warmup must be >= 3")
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference_arm(args, rank, world)
+        return
+
+    import torch
+
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=torch.device("cuda", local))
+
+    def barrier():
+        if dist is not None:
+            dist.barrier(device_ids=[local])
+        torch.cuda.synchronize()
+
+    def max_over_ranks(x: float) -> float:
+        if dist is None:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    from pySWE import pyswe
+
+    import ctypes as ct
+
+    lib = ct.CDLL(pyswe.default_library())
+    lib.HHG_measure_peaks.argtypes = [ct.POINTER(ct.c_double), ct.POINTER(ct.c_double)]
+    fp64_peak, fp32_peak = ct.c_double(), ct.c_double()
+
+    param = workload_param(args.workload, rank, world)
+    w = WORKLOADS[args.workload]
+    settings = pyswe.Settings(dict(param))
+    swe = pyswe.SWE(settings, device=local)
+    nk = param["nr1"] * param["nr2"]
+    nt = settings.nt
+    nw = swe.num_orb()
+    n_op = 1 + sum(1 for v in param["pol_vec"] if v != 0.0)
+    n_j = 2  # v_z = 0 for these 2D models; jz is returned as exact zeros
+
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")  # 256 MiB > 126 MB L2
+
+    for _ in range(args.warmup):
+        swe.reset()
+        swe.run_simulation()
+    lib.HHG_measure_peaks(ct.byref(fp64_peak), ct.byref(fp32_peak))
+
+    clocks = ClockSampler(local)
+    barrier()
+    if rank == 0:
+        clocks.start()
+    dev_ms, prop_ms, launches = [], [], 0
+    t_wall0 = time.perf_counter()
+    for i in range(args.steps):
+        flush.fill_(float(i))
+        torch.cuda.synchronize()
+        swe.reset()
+        swe.run_simulation()
+        dev_ms.append(swe.last_kernel_ms())
+        prop_ms.append(swe.last_propagate_ms())
+        launches += swe.last_launches()
+    barrier()
+    t_wall = time.perf_counter() - t_wall0
+    clk = clocks.stop() if rank == 0 else None
+    total_ms = max_over_ranks(sum(dev_ms))
+    value = world * nk * nt * args.steps / (total_ms * 1e-3)
+
+    # End to end through the reference-facing API with host buffers.
+    e2e = None
+    if not args.no_e2e:
+        barrier()
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            swe.restart()
+            swe.run_simulation()
+            t_, jx, jy, jz = swe.get_current()
+        barrier()
+        e2e_s = max_over_ranks(time.perf_counter() - t0)
+        e2e = {"value": world * nk * nt * args.steps / e2e_s, "unit": "k-pt*RK4-steps/s",
+               "h2d_bytes_per_step": swe.h2d_bytes(), "d2h_bytes_per_step": 3 * nt * 16,
+               "calls": "SWESim_restart + SWESim_run_simulation + SWESim_get_current", "ms_per_step": 1e3 * e2e_s / args.steps}
+
+    shape = swe.launch_shape()
+    swe.delete()
+    if dist is not None:
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+
+    fpk = flops_per_kstep(nw, w["window"], param["nr1"], n_op, n_j)
+    prop_mean = statistics.mean(prop_ms)
+    achieved = fpk * nk * nt / (prop_mean * 1e-3) / 1e12
+    traffic, traffic_src = load_traffic(args.workload)
+    line = {
+        "metric": "k-pt*RK4-steps/s",
+        "value": value,
+        "unit": "k-pt*RK4-steps/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": total_ms / args.steps,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64",
+        "data": "synthetic (seeded TB model, generated by hhg-solids_b200/tbgen.py)",
+        "impl": "hhg-b200",
+        "config": {"workload": f"{args.workload}: {WORKLOADS[args.workload]['desc']}", "k_grid": [param["nr1"], param["nr2"]],
+                   "nt": nt, "num_orb": nw, "precision": "fp64", "parallelism": f"replicas x{world}" if world > 1 else "single",
+                   "l2": "flushed between timed solves (256 MiB write)", "launch": shape},
+        "solves_per_hour": 3600.0 * world * args.steps / (total_ms * 1e-3),
+        "roofline": {"bound": "fp64", "achieved": achieved, "peak": fp64_peak.value, "unit": "TFLOP/s",
+                     "frac": achieved / fp64_peak.value if fp64_peak.value > 0 else None, "traffic": traffic,
+                     "kernel": "propagate_fp64_kernel", "flops_per_kstep": fpk,
+                     "peak_source": "live FP64 FMA-chain probe on this GPU (HHG_measure_peaks); "
+                                    "MEASURED_PEAKS.json has no FP64 figure",
+                     "fp32_peak": fp32_peak.value, "kernel_ms": prop_mean, "traffic_source": traffic_src},
+        "gpu_launches": launches,
+        "clocks": clk,
+        "wall_s_timed_region": t_wall,
+    }
+    if e2e:
+        line["e2e"] = e2e
+    if world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(args.workload)
+    print(json.dumps(line), flush=True)
+
+
+if __name__ == "__main__":
+    main()

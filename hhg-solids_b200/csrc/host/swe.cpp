@@ -109,7 +109,7 @@ struct SWESim {
   int nax = 0, ax_id[3] = {0, 0, 0}, nj = 0, j_id[3] = {0, 0, 0};
 
   cudaStream_t stream = nullptr;
-  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr, evm = nullptr;
   DevBuf<int2> d_cell;
   DevBuf<double2> d_H0, d_R, d_V, d_T1, d_T2, d_rho0, d_rho, d_Jpart, d_J;
   DevBuf<hhg::StepParams> d_steps;
@@ -117,7 +117,8 @@ struct SWESim {
   hhg::LaunchShape shape{};
   double2* h_J = nullptr;  // pinned [3][nt]
   std::vector<cd> Jhist[3];
-  float last_ms = 0.f;
+  float last_ms = 0.f, last_prop_ms = 0.f;
+  size_t h2d_bytes = 0;
   int last_launches = 0;
 
   ~SWESim() { release(); }
@@ -130,7 +131,8 @@ struct SWESim {
     h_J = nullptr;
     if (ev0) cudaEventDestroy(ev0);
     if (ev1) cudaEventDestroy(ev1);
-    ev0 = ev1 = nullptr;
+    if (evm) cudaEventDestroy(evm);
+    ev0 = ev1 = evm = nullptr;
     if (stream) cudaStreamDestroy(stream);
     stream = nullptr;
     ready = false;
@@ -204,6 +206,7 @@ void SWESim::init() {
   check_cuda(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking), "cudaStreamCreate");
   check_cuda(cudaEventCreate(&ev0), "cudaEventCreate");
   check_cuda(cudaEventCreate(&ev1), "cudaEventCreate");
+  check_cuda(cudaEventCreate(&evm), "cudaEventCreate");
 
   // Supercell and placement (src/grid.cpp:64-111, src/hamiltonian.cpp:8-39, src/berry_connection.cpp:7-50).
   Rgrid.assign((size_t)Nk * 3, 0.0);
@@ -341,6 +344,8 @@ void SWESim::init() {
   }
 
   // Device tables.
+  h2d_bytes = sizeof(int2) * cell_n.size() + sizeof(double2) * (H0.size() + Rtab.size() + V.size() + T1.size() + T2.size()) +
+              sizeof(hhg::StepParams) * steps.size();
   d_cell.upload(cell_n, stream);
   d_H0.upload(H0, stream);
   d_R.upload(Rtab, stream);
@@ -401,12 +406,13 @@ void SWESim::run() {
   check_cuda(cudaSetDevice(device), "cudaSetDevice");
   check_cuda(cudaMemsetAsync(d_Jpart.p, 0, sizeof(double2) * d_Jpart.n, stream), "memset");
   check_cuda(cudaEventRecord(ev0, stream), "event");
-  last_launches = hhg::launch_propagate_fp64(tab, shape, d_rho.p, d_Jpart.p, d_J.p, stream);
+  last_launches = hhg::launch_propagate_fp64(tab, shape, d_rho.p, d_Jpart.p, d_J.p, stream, evm);
   check_cuda(cudaGetLastError(), "propagate launch");
   check_cuda(cudaEventRecord(ev1, stream), "event");
   check_cuda(cudaMemcpyAsync(h_J, d_J.p, sizeof(double2) * 3 * (size_t)nt, cudaMemcpyDeviceToHost, stream), "D2H");
   check_cuda(cudaStreamSynchronize(stream), "run_simulation");
   check_cuda(cudaEventElapsedTime(&last_ms, ev0, ev1), "event time");
+  check_cuda(cudaEventElapsedTime(&last_prop_ms, ev0, evm), "event time");
   // The reference appends one sample per step to each Observable (src/observable.cpp:29);
   // SWESim_get_current returns the first nt of them.
   for (int a = 0; a < 3; ++a)
@@ -612,6 +618,16 @@ void SWESim_set_device(SWESim* swe, int device) {
   guarded(swe, "SWESim_set_device", [&] { swe->device = device; });
 }
 double SWESim_last_kernel_ms(SWESim* swe) { return swe ? (double)swe->last_ms : -1.0; }
+double SWESim_last_propagate_ms(SWESim* swe) { return swe ? (double)swe->last_prop_ms : -1.0; }
+long long SWESim_h2d_bytes(SWESim* swe) { return swe ? (long long)swe->h2d_bytes : -1; }
+int SWESim_launch_shape(SWESim* swe, int* ctas, int* threads, int* k_per_cta, long long* smem) {
+  if (!swe || !swe->ready) return -1;
+  if (ctas) *ctas = swe->shape.ctas;
+  if (threads) *threads = swe->shape.k_per_cta * swe->shape.group;
+  if (k_per_cta) *k_per_cta = swe->shape.k_per_cta;
+  if (smem) *smem = (long long)swe->shape.smem;
+  return 0;
+}
 int SWESim_last_launches(SWESim* swe) { return swe ? swe->last_launches : -1; }
 
 void SWESim_get_rho_k(SWESim* swe, hhg_cdouble* out) {

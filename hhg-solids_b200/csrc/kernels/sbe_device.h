@@ -44,8 +44,9 @@ bool plan_propagate(const SolveTables& t, int sm_count, LaunchShape* out, char* 
 
 // rho[Nk][nw2] in/out (k-space, W gauge). Jpart[ctas][nt][3] is accumulated (zero it first);
 // J[3][nt] receives the reduced, 1/Nk-normalised current. Returns the number of launches.
+// If `after_propagate` is non-null it is recorded between the propagation and the reduction.
 int launch_propagate_fp64(const SolveTables& t, const LaunchShape& s, double2* rho, double2* Jpart, double2* J,
-                          cudaStream_t stream);
+                          cudaStream_t stream, cudaEvent_t after_propagate = nullptr);
 
 // rho0(k) = U f U^+ of H(k) = sum_cells e^{-ik.R} H0 (no field), one k-point per thread.
 int launch_rho0_fp64(const SolveTables& t, double2* rho, cudaStream_t stream);

@@ -415,9 +415,10 @@ bool plan_propagate(const SolveTables& t, int sm_count, LaunchShape* out, char* 
 }
 
 int launch_propagate_fp64(const SolveTables& t, const LaunchShape& s, double2* rho, double2* Jpart, double2* J,
-                          cudaStream_t stream) {
+                          cudaStream_t stream, cudaEvent_t after_propagate) {
   cudaFuncSetAttribute(propagate_fp64_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s.smem);
   propagate_fp64_kernel<<<s.ctas, s.k_per_cta * s.group, s.smem, stream>>>(t, s.k_per_cta, s.group, rho, Jpart);
+  if (after_propagate) cudaEventRecord(after_propagate, stream);
   const int n = 3 * t.nt;
   reduce_current_kernel<<<(n + 255) / 256, 256, 0, stream>>>(Jpart, s.ctas, t.nt, 1.0 / (double)t.Nk, J);
   return 2;

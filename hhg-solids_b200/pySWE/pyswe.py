@@ -71,6 +71,11 @@ def _load(path: str):
         L.SWESim_last_kernel_ms.argtypes = [vp]
         L.SWESim_last_kernel_ms.restype = ct.c_double
         L.SWESim_last_launches.argtypes = [vp]
+        L.SWESim_last_propagate_ms.argtypes = [vp]
+        L.SWESim_last_propagate_ms.restype = ct.c_double
+        L.SWESim_h2d_bytes.argtypes = [vp]
+        L.SWESim_h2d_bytes.restype = ct.c_longlong
+        L.SWESim_launch_shape.argtypes = [vp] + [ct.POINTER(ct.c_int)] * 3 + [ct.POINTER(ct.c_longlong)]
         L.SWESim_reset.argtypes = [vp]
         L.SWESim_get_rho_k.argtypes = [vp, ND_POINTER_1_complex]
         L.SWESim_get_fields.argtypes = [vp, ND_POINTER_1_double, ND_POINTER_1_double, ND_POINTER_1_double]
@@ -174,6 +179,18 @@ class SWE:
 
     def last_kernel_ms(self) -> float:
         return float(self.swe_cpp.SWESim_last_kernel_ms(self.ptr))
+
+    def last_propagate_ms(self) -> float:
+        return float(self.swe_cpp.SWESim_last_propagate_ms(self.ptr))
+
+    def h2d_bytes(self) -> int:
+        return int(self.swe_cpp.SWESim_h2d_bytes(self.ptr))
+
+    def launch_shape(self) -> dict:
+        c, t, k = ct.c_int(), ct.c_int(), ct.c_int()
+        s = ct.c_longlong()
+        self.swe_cpp.SWESim_launch_shape(self.ptr, ct.byref(c), ct.byref(t), ct.byref(k), ct.byref(s))
+        return {"ctas": c.value, "threads": t.value, "k_per_cta": k.value, "smem_bytes": s.value}
 
     def last_launches(self) -> int:
         return int(self.swe_cpp.SWESim_last_launches(self.ptr))

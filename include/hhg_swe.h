@@ -83,6 +83,12 @@ int SWESim_get_num_orb(SWESim* swe);
 void SWESim_set_device(SWESim* swe, int device);
 /* Device time in milliseconds of the last SWESim_run_simulation's propagation kernels. */
 double SWESim_last_kernel_ms(SWESim* swe);
+/* Device time in milliseconds of the last run's propagation kernel alone (without the J reduction). */
+double SWESim_last_propagate_ms(SWESim* swe);
+/* Bytes copied host->device by the last SWESim_init (model tables, twiddles, field table). */
+long long SWESim_h2d_bytes(SWESim* swe);
+/* Launch shape chosen for the propagation kernel; returns -1 before SWESim_init. */
+int SWESim_launch_shape(SWESim* swe, int* ctas, int* threads, int* k_per_cta, long long* smem);
 /* Number of kernel launches issued by the last SWESim_run_simulation. */
 int SWESim_last_launches(SWESim* swe);
 /* Put rho back to the equilibrium rho0 and clear the recorded current, keeping the setup
