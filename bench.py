@@ -49,14 +49,15 @@ WORKLOADS = {
 }
 
 
-def workload_param(name: str, rank: int = 0, world: int = 1) -> dict:
+def workload_param(name: str, rank: int = 0, world: int = 1, grid: int | None = None) -> dict:
     import numpy as np
     import tbgen
 
     w = WORKLOADS[name]
     ang = math.pi * rank / max(world, 1)  # replicas: one polarisation angle per rank
     pol = [math.sin(ang), math.cos(ang), 0.0]
-    p = dict(PULSE, nr1=w["n"], nr2=w["n"], nr3=1, path_tb=tbgen.model_path(w["model"]))
+    n = grid or w["n"]
+    p = dict(PULSE, nr1=n, nr2=n, nr3=1, path_tb=tbgen.model_path(w["model"]))
     p["pol_vec"] = np.array(pol)
     p["phi_vec"] = np.array(p["phi_vec"])
     return p
@@ -313,6 +314,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--grid", type=int, default=None,
+                    help="override the k-grid side (profiling a smaller case of the same kernel)")
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")
@@ -355,7 +358,7 @@ def main():
     lib.HHG_measure_peaks.argtypes = [ct.POINTER(ct.c_double), ct.POINTER(ct.c_double)]
     fp64_peak, fp32_peak = ct.c_double(), ct.c_double()
 
-    param = workload_param(args.workload, rank, world)
+    param = workload_param(args.workload, rank, world, args.grid)
     w = WORKLOADS[args.workload]
     settings = pyswe.Settings(dict(param))
     swe = pyswe.SWE(settings, device=local)
@@ -432,7 +435,9 @@ def main():
         "dtype": "f64",
         "data": "synthetic (seeded TB model, generated by hhg-solids_b200/tbgen.py)",
         "impl": "hhg-b200",
-        "config": {"workload": f"{args.workload}: {WORKLOADS[args.workload]['desc']}", "k_grid": [param["nr1"], param["nr2"]],
+        "config": {"workload": f"{args.workload}: {WORKLOADS[args.workload]['desc']}"
+                   + (f" (grid overridden to {args.grid}x{args.grid})" if args.grid else ""),
+                   "k_grid": [param["nr1"], param["nr2"]],
                    "nt": nt, "num_orb": nw, "precision": "fp64", "parallelism": f"replicas x{world}" if world > 1 else "single",
                    "l2": "flushed between timed solves (256 MiB write)", "launch": shape},
         "solves_per_hour": 3600.0 * world * args.steps / (total_ms * 1e-3),
@@ -448,7 +453,7 @@ def main():
     }
     if e2e:
         line["e2e"] = e2e
-    if world == 1 and not args.no_cpu_baseline:
+    if world == 1 and not args.no_cpu_baseline and not args.grid:
         line["cpu_baseline"] = cpu_baseline(args.workload)
     print(json.dumps(line), flush=True)
 

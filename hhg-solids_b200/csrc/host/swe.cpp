@@ -103,16 +103,16 @@ struct SWESim {
   std::vector<double> Rgrid;  // [Nk][3] Angstrom
   std::vector<int> site_of_cell;
   std::vector<double> t, E, A;
-  std::vector<hhg::StepParams> steps;
-  std::vector<int2> cell_n;
-  std::vector<double2> H0, Rtab, V, T1, T2;
+  std::vector<double> es;          // [nt][3][3]
+  std::vector<int2> cell_n, win_n;
+  std::vector<double2> H0, Rtab, V, Q, Hd, Rd, Vd, P, T1, T2;
   int nax = 0, ax_id[3] = {0, 0, 0}, nj = 0, j_id[3] = {0, 0, 0};
 
   cudaStream_t stream = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr, evm = nullptr;
-  DevBuf<int2> d_cell;
-  DevBuf<double2> d_H0, d_R, d_V, d_T1, d_T2, d_rho0, d_rho, d_Jpart, d_J;
-  DevBuf<hhg::StepParams> d_steps;
+  DevBuf<int2> d_cell, d_win;
+  DevBuf<double2> d_H0, d_R, d_V, d_Q, d_Hd, d_Rd, d_Vd, d_P, d_T1, d_T2, d_rho0, d_rho, d_Jpart, d_J;
+  DevBuf<double> d_es;
   hhg::SolveTables tab{};
   hhg::LaunchShape shape{};
   double2* h_J = nullptr;  // pinned [3][nt]
@@ -125,8 +125,10 @@ struct SWESim {
 
   void release() {
     d_cell.release();
-    for (auto* b : {&d_H0, &d_R, &d_V, &d_T1, &d_T2, &d_rho0, &d_rho, &d_Jpart, &d_J}) b->release();
-    d_steps.release();
+    d_win.release();
+    for (auto* b : {&d_H0, &d_R, &d_V, &d_Q, &d_Hd, &d_Rd, &d_Vd, &d_P, &d_T1, &d_T2, &d_rho0, &d_rho, &d_Jpart, &d_J})
+      b->release();
+    d_es.release();
     if (h_J) cudaFreeHost(h_J);
     h_J = nullptr;
     if (ev0) cudaEventDestroy(ev0);
@@ -225,24 +227,19 @@ void SWESim::init() {
   nax = 0;
   for (int a = 0; a < 3; ++a)
     if (pol[a] != 0.0) ax_id[nax++] = a;
-  steps.assign(nt, hhg::StepParams{});
+  es.assign((size_t)nt * 9, 0.0);
   for (int ti = 0; ti < nt; ++ti) {
-    hhg::StepParams& p = steps[ti];
+    double* p = es.data() + (size_t)ti * 9;
     for (int a = 0; a < 3; ++a) {
       const double* Ea = E.data() + (size_t)a * nt;
       if (ti < nt - 1) {
-        p.es[0][a] = Ea[ti];
-        p.es[1][a] = 0.5 * Ea[ti] + 0.5 * Ea[ti + 1];
-        p.es[2][a] = Ea[ti + 1];
+        p[0 * 3 + a] = Ea[ti];
+        p[1 * 3 + a] = 0.5 * Ea[ti] + 0.5 * Ea[ti + 1];
+        p[2 * 3 + a] = Ea[ti + 1];
       } else {
-        p.es[0][a] = p.es[1][a] = p.es[2][a] = Ea[nt - 1];
+        p[0 * 3 + a] = p[1 * 3 + a] = p[2 * 3 + a] = Ea[nt - 1];
       }
     }
-    const double ax = A[ti], ay = A[nt + ti], az = A[2 * (size_t)nt + ti];
-    const double th1 = ax * lat_au[0][0] + ay * lat_au[0][1] + az * lat_au[0][2];
-    const double th2 = ax * lat_au[1][0] + ay * lat_au[1][1] + az * lat_au[1][2];
-    p.p1 = make_double2(std::cos(th1), std::sin(th1));
-    p.p2 = make_double2(std::cos(th2), std::sin(th2));
   }
 
   // Support cells: placed cells whose H0 or field-coupled r block is non-zero (zero blocks add exact zeros).
@@ -306,14 +303,92 @@ void SWESim::init() {
       }
     }
   nj = 0;
-  V.clear();
   for (int a = 0; a < 3; ++a) {
     bool nz = false;
     for (size_t o = 0; o < (size_t)hhg::kWindow * nw2 && !nz; ++o) nz = vw[(size_t)a * hhg::kWindow * nw2 + o] != cd(0, 0);
-    if (!nz) continue;  // J_a is then exactly zero, as in the reference
-    j_id[nj++] = a;
-    for (size_t o = 0; o < (size_t)hhg::kWindow * nw2; ++o) V.push_back(d2(vw[(size_t)a * hhg::kWindow * nw2 + o]));
+    if (nz) j_id[nj++] = a;  // otherwise J_a is exactly zero, as in the reference
   }
+  // Window cells with a non-zero velocity on some current axis (sparse form) ...
+  win_n.clear();
+  V.clear();
+  std::vector<int> win_w;
+  for (int w = 0; w < hhg::kWindow; ++w) {
+    bool nz = false;
+    for (int a = 0; a < nj && !nz; ++a)
+      for (int o = 0; o < nw2 && !nz; ++o) nz = vw[((size_t)j_id[a] * hhg::kWindow + w) * nw2 + o] != cd(0, 0);
+    if (nz) {
+      win_w.push_back(w);
+      win_n.push_back(make_int2(w / 4 - 2, w % 4 - 2));
+    }
+  }
+  for (int a = 0; a < nj; ++a)
+    for (int w : win_w)
+      for (int o = 0; o < nw2; ++o) V.push_back(d2(vw[((size_t)j_id[a] * hhg::kWindow + w) * nw2 + o]));
+  // ... and dense over the 4x4 window (separable form).
+  Vd.assign((size_t)nj * hhg::kWindow * nw2, make_double2(0.0, 0.0));
+  for (int a = 0; a < nj; ++a)
+    for (int w = 0; w < hhg::kWindow; ++w)
+      for (int o = 0; o < nw2; ++o) Vd[((size_t)a * hhg::kWindow + w) * nw2 + o] = d2(vw[((size_t)j_id[a] * hhg::kWindow + w) * nw2 + o]);
+  const int nwin = (int)win_n.size();
+
+  // Peierls phase e^{i A(t_i).R_c} of every listed cell at every step (src/swe.cpp:225-233), R_c the
+  // cell's supercell position in bohr.
+  const int ncw = ncell + nwin;
+  Q.assign((size_t)nt * ncw, make_double2(1.0, 0.0));
+  {
+    std::vector<double> Rc((size_t)ncw * 3);
+    for (int c = 0; c < ncw; ++c) {
+      const int2 n = c < ncell ? cell_n[c] : win_n[c - ncell];
+      const int cc = cell_of(n.x, n.y);
+      for (int a = 0; a < 3; ++a) Rc[3 * c + a] = Rgrid[3 * (size_t)cc + a] * kA2Bohr;
+    }
+    for (int ti = 0; ti < nt; ++ti) {
+      const double ax = A[ti], ay = A[nt + ti], az = A[2 * (size_t)nt + ti];
+      for (int c = 0; c < ncw; ++c) {
+        const double th = ax * Rc[3 * c] + ay * Rc[3 * c + 1] + az * Rc[3 * c + 2];
+        Q[(size_t)ti * ncw + c] = make_double2(std::cos(th), std::sin(th));
+      }
+    }
+  }
+
+  // Dense bounding box of the support cells for the separable Wannier sum.
+  int b1lo = 0, b1hi = 0, b2lo = 0, b2hi = 0;
+  for (int c = 0; c < ncell; ++c) {
+    if (c == 0 || cell_n[c].x < b1lo) b1lo = cell_n[c].x;
+    if (c == 0 || cell_n[c].x > b1hi) b1hi = cell_n[c].x;
+    if (c == 0 || cell_n[c].y < b2lo) b2lo = cell_n[c].y;
+    if (c == 0 || cell_n[c].y > b2hi) b2hi = cell_n[c].y;
+  }
+  const int b1n = ncell ? b1hi - b1lo + 1 : 1, b2n = ncell ? b2hi - b2lo + 1 : 1;
+  Hd.assign((size_t)b1n * b2n * nw2, make_double2(0.0, 0.0));
+  Rd.assign((size_t)nax * b1n * b2n * nw2, make_double2(0.0, 0.0));
+  for (int c = 0; c < ncell; ++c) {
+    const size_t box = (size_t)(cell_n[c].x - b1lo) * b2n + (cell_n[c].y - b2lo);
+    for (int o = 0; o < nw2; ++o) {
+      Hd[box * nw2 + o] = H0[(size_t)c * nw2 + o];
+      for (int a = 0; a < nax; ++a)
+        Rd[((size_t)a * b1n * b2n + box) * nw2 + o] = Rtab[((size_t)a * ncell + c) * nw2 + o];
+    }
+  }
+  // e^{i n A(t_i).a_1}, e^{i n A(t_i).a_2} for |n| <= np.
+  int np_ = 2;
+  for (int c = 0; c < ncell; ++c) np_ = std::max(np_, std::max(std::abs(cell_n[c].x), std::abs(cell_n[c].y)));
+  const int npw = 2 * np_ + 1;
+  P.assign((size_t)nt * 2 * npw, make_double2(1.0, 0.0));
+  for (int ti = 0; ti < nt; ++ti) {
+    const double ax = A[ti], ay = A[nt + ti], az = A[2 * (size_t)nt + ti];
+    for (int d = 0; d < 2; ++d) {
+      const double th = ax * lat_au[d][0] + ay * lat_au[d][1] + az * lat_au[d][2];
+      for (int n = -np_; n <= np_; ++n)
+        P[((size_t)ti * 2 + d) * npw + (n + np_)] = make_double2(std::cos(n * th), std::sin(n * th));
+    }
+  }
+  tab.nwin = nwin;
+  tab.b1lo = b1lo;
+  tab.b1n = b1n;
+  tab.b2lo = b2lo;
+  tab.b2n = b2n;
+  tab.np = np_;
 
   // Hermitian symmetry of the placed operators on the grid: block(-n) == block(n)^+ for every cell.
   // It fails when the grid is smaller than the model's R range or a misplacement is one-sided; the
@@ -344,15 +419,23 @@ void SWESim::init() {
   }
 
   // Device tables.
-  h2d_bytes = sizeof(int2) * cell_n.size() + sizeof(double2) * (H0.size() + Rtab.size() + V.size() + T1.size() + T2.size()) +
-              sizeof(hhg::StepParams) * steps.size();
+  h2d_bytes = sizeof(int2) * (cell_n.size() + win_n.size()) +
+              sizeof(double2) * (H0.size() + Rtab.size() + V.size() + Q.size() + Hd.size() + Rd.size() + Vd.size() +
+                                 P.size() + T1.size() + T2.size()) +
+              sizeof(double) * es.size();
   d_cell.upload(cell_n, stream);
+  d_win.upload(win_n, stream);
   d_H0.upload(H0, stream);
   d_R.upload(Rtab, stream);
   d_V.upload(V, stream);
+  d_Q.upload(Q, stream);
+  d_Hd.upload(Hd, stream);
+  d_Rd.upload(Rd, stream);
+  d_Vd.upload(Vd, stream);
+  d_P.upload(P, stream);
   d_T1.upload(T1, stream);
   d_T2.upload(T2, stream);
-  d_steps.upload(steps, stream);
+  d_es.upload(es, stream);
   d_rho0.alloc((size_t)Nk * nw2);
   d_rho.alloc((size_t)Nk * nw2);
   d_J.alloc((size_t)3 * nt);
@@ -362,20 +445,28 @@ void SWESim::init() {
   tab.N2 = N2;
   tab.Nk = Nk;
   tab.nt = nt;
+  tab.hermitian = herm ? 1 : 0;
+  tab.dt = t[1] - t[0];
+  tab.nax = nax;
+  tab.nj = nj;
+  for (int a = 0; a < 3; ++a) {
+    tab.ax_id[a] = ax_id[a];
+    tab.j_id[a] = j_id[a];
+  }
+  tab.es = d_es.p;
   tab.ncell = ncell;
   tab.cell_n = d_cell.p;
   tab.H0 = d_H0.p;
-  tab.nax = nax;
-  for (int a = 0; a < 3; ++a) tab.ax_id[a] = ax_id[a];
   tab.R = d_R.p;
-  tab.nj = nj;
-  for (int a = 0; a < 3; ++a) tab.j_id[a] = j_id[a];
+  tab.win_n = d_win.p;
   tab.V = d_V.p;
+  tab.Q = d_Q.p;
+  tab.Hd = d_Hd.p;
+  tab.Rd = d_Rd.p;
+  tab.Vd = d_Vd.p;
+  tab.P = d_P.p;
   tab.T1 = d_T1.p;
   tab.T2 = d_T2.p;
-  tab.steps = d_steps.p;
-  tab.dt = t[1] - t[0];
-  tab.hermitian = herm ? 1 : 0;
 
   int sms = 0;
   check_cuda(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device), "cudaDeviceGetAttribute");
@@ -626,7 +717,7 @@ int SWESim_launch_shape(SWESim* swe, int* ctas, int* threads, int* k_per_cta, lo
   if (threads) *threads = swe->shape.k_per_cta * swe->shape.group;
   if (k_per_cta) *k_per_cta = swe->shape.k_per_cta;
   if (smem) *smem = (long long)swe->shape.smem;
-  return 0;
+  return swe->shape.kernel;
 }
 int SWESim_last_launches(SWESim* swe) { return swe ? swe->last_launches : -1; }
 

@@ -4,46 +4,57 @@
 
 namespace hhg {
 
-constexpr int kMaxOrb = 16;       // largest nw the kernels take
-constexpr int kWindow = 16;       // 4x4 current window of the reference observable
+constexpr int kMaxOrb = 16;   // largest nw the kernels take
+constexpr int kWindow = 16;   // 4x4 current window of the reference observable (n in {-2,-1,0,1}^2)
+constexpr int kRing = 32;     // time steps per staged chunk (field table in, current partials out)
 
-// Per time step, precomputed on the host in FP64.
-struct StepParams {
-  double es[3][3];   // field samples [t, t+dt/2, t+dt][axis] (src/solver.cpp:109-148), au
-  double2 p1, p2;    // e^{i A(t_i).a1}, e^{i A(t_i).a2}: Peierls phase per unit cell step
-};
-
-// One solve's device-resident tables.
+// One solve's device-resident tables (all pointers are device memory).
 struct SolveTables {
   int nw, nw2, N1, N2, Nk, nt;
-  int ncell;                 // support cells of H0 / r
-  const int2* cell_n;        // [ncell] (n1, n2)
-  const double2* H0;         // [ncell][nw2] Hartree
-  int nax;                   // field axes with a non-zero polarisation component
-  int ax_id[3];
-  const double2* R;          // [nax][ncell][nw2] bohr (r = -x_bc)
-  int nj;                    // current axes with a non-zero velocity window
-  int j_id[3];
-  const double2* V;          // [nj][16][nw2] velocity on the window cells
-  const double2* T1;         // [N1] e^{-2 pi i m/N1}
-  const double2* T2;         // [N2] e^{-2 pi i m/N2}
-  const StepParams* steps;   // [nt]
-  double dt;                 // au
-  int hermitian;             // placed H0 and r are Hermitian-symmetric on the grid: [H,X] = HX - (HX)^+
+  int hermitian;     // placed H0 and r are Hermitian-symmetric on the grid: [H,X] = HX - (HX)^+
+  double dt;         // au
+  int nax, ax_id[3]; // field axes with a non-zero polarisation component
+  int nj, j_id[3];   // current axes with a non-zero velocity window
+  const double* es;  // [nt][3 stages (t, t+dt/2, t+dt)][3 axes] field samples (src/solver.cpp:109-148)
+
+  // Sparse form (thread-per-k kernel): occupied cells and non-zero window cells.
+  int ncell;
+  const int2* cell_n;   // [ncell] (n1, n2)
+  const double2* H0;    // [ncell][nw2] Hartree
+  const double2* R;     // [nax][ncell][nw2] bohr (r = -x_bc)
+  int nwin;
+  const int2* win_n;    // [nwin]
+  const double2* V;     // [nj][nwin][nw2] velocity on the window cells
+  const double2* Q;     // [nt][ncell + nwin] Peierls phase e^{i A(t_i).R_c} of each listed cell
+
+  // Dense separable form (element-group kernel): bounding box of the occupied cells.
+  int b1lo, b1n, b2lo, b2n;
+  const double2* Hd;    // [b1n][b2n][nw2]
+  const double2* Rd;    // [nax][b1n][b2n][nw2]
+  const double2* Vd;    // [nj][4][4][nw2]  (window n1, n2 in -2..1)
+  int np;               // |n| range of the P table
+  const double2* P;     // [nt][2][2np+1]: e^{i n A(t_i).a_1}, e^{i n A(t_i).a_2}, n in [-np, np]
+
+  const double2* T1;    // [N1] e^{-2 pi i m/N1}
+  const double2* T2;    // [N2] e^{-2 pi i m/N2}
 };
 
 struct LaunchShape {
-  int k_per_cta;   // k-points (element groups) per CTA
-  int group;       // threads per k-point (power of two <= 32, or a multiple of 32)
+  int kernel;      // 0: thread per k-point (nw <= 2, Hermitian); 1: element groups
+  int k_per_cta;   // k-points per CTA
+  int group;       // threads per k-point
+  int threads;     // threads per CTA
   int ctas;        // grid size (persistent CTAs)
+  int ntiles;      // work tiles
   size_t smem;     // dynamic shared memory bytes
 };
 
-// Picks the launch shape for a solve on the current device; returns false if nw/ncell don't fit.
+// Picks kernel and launch shape for a solve on the current device; false (with a reason) if it
+// cannot run it.
 bool plan_propagate(const SolveTables& t, int sm_count, LaunchShape* out, char* why, int why_len);
 
 // rho[Nk][nw2] in/out (k-space, W gauge). Jpart[ctas][nt][3] is accumulated (zero it first);
-// J[3][nt] receives the reduced, 1/Nk-normalised current. Returns the number of launches.
+// J[3][nt] receives the reduced, 1/Nk-normalised current.  Returns the number of launches.
 // If `after_propagate` is non-null it is recorded between the propagation and the reduction.
 int launch_propagate_fp64(const SolveTables& t, const LaunchShape& s, double2* rho, double2* Jpart, double2* J,
                           cudaStream_t stream, cudaEvent_t after_propagate = nullptr);

@@ -5,18 +5,22 @@
 // of rho(R) + c k_{n-1}(R), a per-k commutator, an inverse FFT.  Because the four stages are
 // linear in rho and the Peierls phase is fixed for the step (src/swe.cpp:192-196), the same
 // propagation runs with rho resident in k space:
-//   H_s(k)  = sum_cells u1^{n1} u2^{n2} (H0_cell + E_s . r_cell),  u_a = e^{-2 pi i m_a/N_a} e^{i A(t_i).a_a}
+//   H_s(k)  = sum_cells e^{-ik.R} e^{iA(t_i).R} (H0_cell + E_s . r_cell)
 //   k_n     = -i [H_s(k), rho(k) + c_n k_{n-1}],  c = 0, dt/2, dt/2, dt
 //   rho    += 0.1666666666666 dt (k1 + 2 k2 + 2 k3 + k4)                       (src/solver.cpp:170-180)
-//   J_a(t_i) = (1/Nk) sum_k sum_ij W_a,ij(k) conj(rho_ij(k)),  W_a = sum_{n in 4x4} u1^{n1} u2^{n2} v_a(n)
+//   J_a(t_i) = (1/Nk) sum_k sum_ij W_a,ij(k) conj(rho_ij(k)),  W_a = sum_{n in 4x4} e^{-ik.R_n} e^{iA.R_n} v_a(n)
 // (the 4x4 real-space window of src/observable.cpp:16-30 in Parseval form).  Every k-point is
-// independent for the whole pulse, so one persistent kernel keeps each k-point's matrices on chip
-// for all nt steps: no per-step FFT, no HBM round trip of rho, one launch per solve.
+// independent for the whole pulse, so each kernel keeps its k-points' matrices on chip for all nt
+// steps: no per-step FFT, no HBM round trip of rho, one launch per solve.  The field table comes in
+// and the current partials go out through a kRing-step shared-memory ring.
 //
-// Thread layout: a k-point is a group of G threads, thread e of the group owns matrix element
-// e = i*nw + j.  G is the next power of two >= nw^2 when nw^2 <= 32 (several k-points per warp,
-// __syncwarp between phases) or nw^2 rounded up to whole warps (one named barrier per group).
-// The commutator uses [H, X] = HX - (HX)^+ for Hermitian H, X: one nw^3 product per stage.
+// propagate_kpt_kernel<NW>  (nw <= 2, Hermitian placement): one thread per k-point, the whole
+//   state in registers; per-cell phases e^{-ik.R_c} (per thread, fixed) x e^{iA.R_c} (per step).
+// propagate_group_kernel    (any nw <= 16): a k-point is a group of G threads, thread e owning
+//   element e = i*nw + j.  A CTA holds k-points of one k-grid column m2, which share
+//   G(n1) = sum_n2 e^{-i(k2 - A).a2 n2} X(n1, n2): the Wannier sum is computed separably, the
+//   inner half once per CTA and step.  [H, X] = HX - (HX)^+ for Hermitian placements (one nw^3
+//   product per stage), HX - XH otherwise.
 #include <cstdio>
 #include <cstring>
 
@@ -26,7 +30,7 @@ namespace hhg {
 namespace {
 
 __device__ __forceinline__ double2 cmul(double2 a, double2 b) {
-  return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+  return make_double2(fma(a.x, b.x, -a.y * b.y), fma(a.x, b.y, a.y * b.x));
 }
 // c + a * b
 __device__ __forceinline__ double2 cfma(double2 a, double2 b, double2 c) {
@@ -37,14 +41,223 @@ __device__ __forceinline__ double2 cfma(double2 a, double2 b, double2 c) {
   return c;
 }
 __device__ __forceinline__ double2 cconj(double2 a) { return make_double2(a.x, -a.y); }
-// u^n for |u| = 1 (u^{-1} = conj(u)).
-__device__ __forceinline__ double2 cpow_unit(double2 u, int n) {
-  const double2 b = n >= 0 ? u : cconj(u);
-  const int m = n >= 0 ? n : -n;
-  double2 r = make_double2(1.0, 0.0);
-  for (int q = 0; q < m; ++q) r = cmul(r, b);
-  return r;
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
 }
+
+__device__ __forceinline__ int wrap_mod(long long x, int n) {
+  int r = (int)(x % n);
+  return r < 0 ? r + n : r;
+}
+
+// Adds the ring of per-warp current partials of `nsteps` steps into this CTA's Jpart rows.
+__device__ __forceinline__ void flush_current(const SolveTables& t, const double* sJ, int nwarps, int ti0, int nsteps,
+                                              double2* Jpart) {
+  const int nj = t.nj;
+  for (int idx = threadIdx.x; idx < nsteps * nj; idx += blockDim.x) {
+    const int s = idx / nj, a = idx % nj;
+    double re = 0.0, im = 0.0;
+    for (int w = 0; w < nwarps; ++w) {
+      re += sJ[(s * nwarps + w) * 2 * nj + 2 * a];
+      im += sJ[(s * nwarps + w) * 2 * nj + 2 * a + 1];
+    }
+    double2* dst = Jpart + ((size_t)blockIdx.x * t.nt + ti0 + s) * 3 + t.j_id[a];
+    const double2 old = *dst;
+    *dst = make_double2(old.x + re, old.y + im);
+  }
+}
+
+// ------------------------------------------------------------------ thread per k-point (nw <= 2)
+
+constexpr int kKptMaxThreads = 512;
+
+template <int NW>
+__global__ void __launch_bounds__(kKptMaxThreads) propagate_kpt_kernel(SolveTables t, double2* rho, double2* Jpart) {
+  constexpr int NW2 = NW * NW;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  const int nc = t.ncell, nwn = t.nwin, ncw = nc + nwn, nax = t.nax, nj = t.nj;
+  const int nthr = blockDim.x, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarps = nthr >> 5;
+  double2* sH = reinterpret_cast<double2*>(smraw);  // [nc][NW2]
+  double2* sR = sH + nc * NW2;                      // [nax][nc][NW2]
+  double2* sV = sR + nax * nc * NW2;                // [nj][nwn][NW2]
+  double2* sTk = sV + nj * nwn * NW2;               // [ncw][nthr]
+  double2* sQ = sTk + ncw * nthr;                   // [kRing][ncw]
+  double* sE = reinterpret_cast<double*>(sQ + kRing * ncw);  // [kRing][9]
+  double* sJ = sE + kRing * 9;                      // [kRing][nwarps][2 nj]
+
+  for (int idx = tid; idx < nc * NW2; idx += nthr) sH[idx] = t.H0[idx];
+  for (int idx = tid; idx < nax * nc * NW2; idx += nthr) sR[idx] = t.R[idx];
+  for (int idx = tid; idx < nj * nwn * NW2; idx += nthr) sV[idx] = t.V[idx];
+
+  const double dt = t.dt;
+  const double prefac = 0.1666666666666 * dt;
+  const int ntiles = (t.Nk + nthr - 1) / nthr;
+  for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    const int k = tile * nthr + tid;
+    const bool kval = k < t.Nk;
+    double2 r[NW2];
+#pragma unroll
+    for (int e = 0; e < NW2; ++e) r[e] = kval ? rho[(size_t)k * NW2 + e] : make_double2(0.0, 0.0);
+    const int m1 = kval ? k / t.N2 : 0, m2 = kval ? k % t.N2 : 0;
+    for (int c = 0; c < ncw; ++c) {
+      const int2 n = c < nc ? t.cell_n[c] : t.win_n[c - nc];
+      sTk[c * nthr + tid] = cmul(t.T1[wrap_mod((long long)m1 * n.x, t.N1)], t.T2[wrap_mod((long long)m2 * n.y, t.N2)]);
+    }
+
+    for (int ti0 = 0; ti0 < t.nt; ti0 += kRing) {
+      const int nsteps = min(kRing, t.nt - ti0);
+      __syncthreads();
+      for (int idx = tid; idx < nsteps * ncw; idx += nthr) sQ[idx] = t.Q[(size_t)ti0 * ncw + idx];
+      for (int idx = tid; idx < nsteps * 9; idx += nthr) sE[idx] = t.es[(size_t)ti0 * 9 + idx];
+      __syncthreads();
+      for (int s = 0; s < nsteps; ++s) {
+        // Wannier sums, Hermitian parts: diagonal real, upper triangle complex.
+        double hd[NW], rd[3][NW];
+        double2 hu[NW2], ru[3][NW2], w[3][NW2];
+#pragma unroll
+        for (int i = 0; i < NW; ++i) {
+          hd[i] = 0.0;
+#pragma unroll
+          for (int a = 0; a < 3; ++a) rd[a][i] = 0.0;
+        }
+#pragma unroll
+        for (int e = 0; e < NW2; ++e) {
+          hu[e] = make_double2(0.0, 0.0);
+#pragma unroll
+          for (int a = 0; a < 3; ++a) {
+            ru[a][e] = make_double2(0.0, 0.0);
+            w[a][e] = make_double2(0.0, 0.0);
+          }
+        }
+        const double2* q = sQ + s * ncw;
+#pragma unroll 2
+        for (int c = 0; c < nc; ++c) {
+          const double2 ph = cmul(sTk[c * nthr + tid], q[c]);
+          const double2* hc = sH + c * NW2;
+#pragma unroll
+          for (int i = 0; i < NW; ++i) {
+            hd[i] = fma(ph.x, hc[i * NW + i].x, fma(-ph.y, hc[i * NW + i].y, hd[i]));
+#pragma unroll
+            for (int j = i + 1; j < NW; ++j) hu[i * NW + j] = cfma(ph, hc[i * NW + j], hu[i * NW + j]);
+          }
+#pragma unroll
+          for (int a = 0; a < 3; ++a)
+            if (a < nax) {
+              const double2* rc = sR + (a * nc + c) * NW2;
+#pragma unroll
+              for (int i = 0; i < NW; ++i) {
+                rd[a][i] = fma(ph.x, rc[i * NW + i].x, fma(-ph.y, rc[i * NW + i].y, rd[a][i]));
+#pragma unroll
+                for (int j = i + 1; j < NW; ++j) ru[a][i * NW + j] = cfma(ph, rc[i * NW + j], ru[a][i * NW + j]);
+              }
+            }
+        }
+#pragma unroll 2
+        for (int c = 0; c < nwn; ++c) {
+          const double2 ph = cmul(sTk[(nc + c) * nthr + tid], q[nc + c]);
+#pragma unroll
+          for (int a = 0; a < 3; ++a)
+            if (a < nj) {
+              const double2* vc = sV + (a * nwn + c) * NW2;
+#pragma unroll
+              for (int e = 0; e < NW2; ++e) w[a][e] = cfma(ph, vc[e], w[a][e]);
+            }
+        }
+
+        // Four RK4 stages (src/solver.cpp:157-163), fields at t, t+dt/2, t+dt/2, t+dt.
+        double2 K[NW2], S[NW2];
+#pragma unroll
+        for (int st = 0; st < 4; ++st) {
+          const int f = st == 0 ? 0 : (st == 3 ? 2 : 1);
+          const double* es = sE + s * 9 + f * 3;
+          double2 H[NW2], X[NW2];
+#pragma unroll
+          for (int i = 0; i < NW; ++i) {
+            double d = hd[i];
+#pragma unroll
+            for (int a = 0; a < 3; ++a)
+              if (a < nax) d = fma(es[t.ax_id[a]], rd[a][i], d);
+            H[i * NW + i] = make_double2(d, 0.0);
+#pragma unroll
+            for (int j = i + 1; j < NW; ++j) {
+              double2 u = hu[i * NW + j];
+#pragma unroll
+              for (int a = 0; a < 3; ++a)
+                if (a < nax) {
+                  const double ea = es[t.ax_id[a]];
+                  u.x = fma(ea, ru[a][i * NW + j].x, u.x);
+                  u.y = fma(ea, ru[a][i * NW + j].y, u.y);
+                }
+              H[i * NW + j] = u;
+              H[j * NW + i] = cconj(u);
+            }
+          }
+          const double cs = (st == 3 ? 1.0 : 0.5) * dt;
+#pragma unroll
+          for (int e = 0; e < NW2; ++e)
+            X[e] = st == 0 ? r[e] : make_double2(r[e].x + cs * K[e].x, r[e].y + cs * K[e].y);
+          double2 HX[NW2];
+#pragma unroll
+          for (int i = 0; i < NW; ++i)
+#pragma unroll
+            for (int j = 0; j < NW; ++j) {
+              double2 acc = make_double2(0.0, 0.0);
+#pragma unroll
+              for (int l = 0; l < NW; ++l) acc = cfma(H[i * NW + l], X[l * NW + j], acc);
+              HX[i * NW + j] = acc;
+            }
+#pragma unroll
+          for (int i = 0; i < NW; ++i)
+#pragma unroll
+            for (int j = 0; j < NW; ++j) {
+              // k = -i (HX - (HX)^+)
+              const double cx = HX[i * NW + j].x - HX[j * NW + i].x, cy = HX[i * NW + j].y + HX[j * NW + i].y;
+              K[i * NW + j] = make_double2(cy, -cx);
+            }
+          const double wgt = st == 3 ? 1.0 : 2.0;
+#pragma unroll
+          for (int e = 0; e < NW2; ++e)
+            S[e] = st == 0 ? K[e] : make_double2(S[e].x + wgt * K[e].x, S[e].y + wgt * K[e].y);
+        }
+#pragma unroll
+        for (int e = 0; e < NW2; ++e) r[e] = make_double2(r[e].x + prefac * S[e].x, r[e].y + prefac * S[e].y);
+
+        // Current partials.
+#pragma unroll
+        for (int a = 0; a < 3; ++a)
+          if (a < nj) {
+            double re = 0.0, im = 0.0;
+            if (kval) {
+#pragma unroll
+              for (int e = 0; e < NW2; ++e) {
+                re = fma(w[a][e].x, r[e].x, fma(w[a][e].y, r[e].y, re));
+                im = fma(w[a][e].y, r[e].x, fma(-w[a][e].x, r[e].y, im));
+              }
+            }
+            re = warp_sum(re);
+            im = warp_sum(im);
+            if (lane == 0) {
+              sJ[(s * nwarps + warp) * 2 * nj + 2 * a] = re;
+              sJ[(s * nwarps + warp) * 2 * nj + 2 * a + 1] = im;
+            }
+          }
+      }
+      __syncthreads();
+      flush_current(t, sJ, nwarps, ti0, nsteps, Jpart);
+    }
+    if (kval) {
+#pragma unroll
+      for (int e = 0; e < NW2; ++e) rho[(size_t)k * NW2 + e] = r[e];
+    }
+  }
+}
+
+// ------------------------------------------------------------------ element groups (any nw)
+
+constexpr int kGroupMaxThreads = 640;
 
 __device__ __forceinline__ void group_sync(int g, int G) {
   if (G <= 32) {
@@ -54,160 +267,224 @@ __device__ __forceinline__ void group_sync(int g, int G) {
   }
 }
 
-__device__ __forceinline__ double warp_sum(double v) {
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-  return v;
+struct GroupSmem {
+  double2 *Hs, *Xs, *HXs;  // per group [nw2] (group-local)
+  double2 *tw1, *tw2;      // per tile twiddles: [B][W1+4], [W2+4]
+  double2 *pw1, *pw2;      // per step (x2 buffers): [2][B][W1+4], [2][W2+4]
+  double2 *Gb, *GW;        // per step (x2): [2][1+nax][W1][nw2], [2][nj][4][nw2]
+  double* sJ;              // [kRing][nwarps][2 nj]
+};
+
+__device__ __forceinline__ GroupSmem group_smem_layout(const SolveTables& t, int B, int g, unsigned char* base) {
+  GroupSmem m;
+  const int nw2 = t.nw2, W1 = t.b1n + 4, W2 = t.b2n + 4;
+  double2* p = reinterpret_cast<double2*>(base);
+  m.Hs = p + g * 3 * nw2;
+  m.Xs = m.Hs + nw2;
+  m.HXs = m.Xs + nw2;
+  p += B * 3 * nw2;
+  m.tw1 = p;
+  p += B * W1;
+  m.tw2 = p;
+  p += W2;
+  m.pw1 = p;
+  p += 2 * B * W1;
+  m.pw2 = p;
+  p += 2 * W2;
+  m.Gb = p;
+  p += 2 * (1 + t.nax) * t.b1n * nw2;
+  m.GW = p;
+  p += 2 * t.nj * 4 * nw2;
+  m.sJ = reinterpret_cast<double*>(p);
+  return m;
 }
 
-constexpr int kMaxThreads = 512;
-
-__global__ void __launch_bounds__(kMaxThreads) propagate_fp64_kernel(SolveTables t, int kpc, int G, double2* rho,
-                                                                     double2* Jpart) {
-  extern __shared__ double2 sm[];
-  const int nw = t.nw, nw2 = t.nw2, nt = t.nt;
-  const int tid = threadIdx.x;
+__global__ void __launch_bounds__(kGroupMaxThreads, 1) propagate_group_kernel(SolveTables t, int B, int G,
+                                                                               double2* rho, double2* Jpart) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  const int nw = t.nw, nw2 = t.nw2, nax = t.nax, nj = t.nj;
+  const int nthr = blockDim.x, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarps = (nthr + 31) >> 5;
   const int g = tid / G, e = tid % G;
   const bool act = e < nw2;
   const int i = act ? e / nw : 0, j = act ? e % nw : 0;
-  const int per = 3 * nw2 + t.ncell + kWindow;
-  double2* Hs = sm + g * per;
-  double2* Xs = Hs + nw2;
-  double2* HXs = Xs + nw2;
-  double2* ph = HXs + nw2;
-  double2* phw = ph + t.ncell;
-  const int nwarps = blockDim.x >> 5, warp = tid >> 5, lane = tid & 31;
-  double2* Jw = sm + kpc * per;  // [2][nwarps][3]
-  const double2 zero = make_double2(0.0, 0.0);
+  const int W1n = t.b1n, W2n = t.b2n, W1 = W1n + 4, W2 = W2n + 4, nmat = 1 + nax;
+  const GroupSmem sm = group_smem_layout(t, B, g, smraw);
   const double dt = t.dt;
   const double prefac = 0.1666666666666 * dt;
-  const int ntiles = (t.Nk + kpc - 1) / kpc;
+  const int bpc = (t.N1 + B - 1) / B;  // m1 blocks per column
+  const int ntiles = t.N2 * bpc;
+  const int npw = 2 * t.np + 1;
+  const int gpairs = nmat * W1n * nw2, wpairs = nj * 4 * nw2;
+  const double2 zero = make_double2(0.0, 0.0);
 
   for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-    const int k = tile * kpc + g;
-    const bool kval = k < t.Nk;
+    const int m2 = tile / bpc, m10 = (tile % bpc) * B;
+    const int m1 = m10 + g;
+    const bool kval = m1 < t.N1;
     const bool own = act && kval;
-    double2 r = own ? rho[(size_t)k * nw2 + e] : zero;
-    const int m1 = kval ? k / t.N2 : 0, m2 = kval ? k % t.N2 : 0;
-    const double2 T1 = t.T1[m1], T2 = t.T2[m2];
+    const size_t k = (size_t)m1 * t.N2 + m2;
+    double2 r = own ? rho[k * nw2 + e] : zero;
+    // Per-tile twiddles e^{-2 pi i m n / N} of the box (then window) offsets.
+    for (int idx = tid; idx < W2; idx += nthr) {
+      const int n2 = idx < W2n ? t.b2lo + idx : idx - W2n - 2;
+      sm.tw2[idx] = t.T2[wrap_mod((long long)m2 * n2, t.N2)];
+    }
+    for (int idx = tid; idx < B * W1; idx += nthr) {
+      const int gg = idx / W1, q = idx % W1;
+      const int n1 = q < W1n ? t.b1lo + q : q - W1n - 2;
+      const int mm1 = min(m10 + gg, t.N1 - 1);
+      sm.tw1[idx] = t.T1[wrap_mod((long long)mm1 * n1, t.N1)];
+    }
+    __syncthreads();
 
-    for (int ti = 0; ti < nt; ++ti) {
-      const StepParams* sp = t.steps + ti;
-      const double2 u1 = cmul(T1, sp->p1), u2 = cmul(T2, sp->p2);
-      for (int c = e; c < t.ncell; c += G) {
-        const int2 n = t.cell_n[c];
-        ph[c] = cmul(cpow_unit(u1, n.x), cpow_unit(u2, n.y));
-      }
-      for (int w = e; w < kWindow; w += G) phw[w] = cmul(cpow_unit(u1, (w >> 2) - 2), cpow_unit(u2, (w & 3) - 2));
-      group_sync(g, G);
-
-      // Wannier sums: H0(k - A), r_a(k - A) and the windowed velocity W_a(k).
-      double2 h0 = zero;
-      double2 rk[3] = {zero, zero, zero};
-      double2 wk[3] = {zero, zero, zero};
-      if (act) {
-        for (int c = 0; c < t.ncell; ++c) {
-          const double2 p = ph[c];
-          h0 = cfma(p, t.H0[(size_t)c * nw2 + e], h0);
-#pragma unroll
-          for (int a = 0; a < 3; ++a)
-            if (a < t.nax) rk[a] = cfma(p, t.R[((size_t)a * t.ncell + c) * nw2 + e], rk[a]);
+    for (int ti0 = 0; ti0 < t.nt; ti0 += kRing) {
+      const int nsteps = min(kRing, t.nt - ti0);
+      for (int s = 0; s < nsteps; ++s) {
+        const int ti = ti0 + s, buf = ti & 1;
+        const double2* P1 = t.P + (size_t)ti * 2 * npw + t.np;  // index by n
+        const double2* P2 = P1 + npw;
+        double2* pw1 = sm.pw1 + buf * B * W1;
+        double2* pw2 = sm.pw2 + buf * W2;
+        double2* Gb = sm.Gb + buf * nmat * W1n * nw2;
+        double2* GW = sm.GW + buf * nj * 4 * nw2;
+        // (1) phase factors e^{-i n (k - A).a} = twiddle x e^{i n A.a}
+        for (int idx = tid; idx < W2; idx += nthr) {
+          const int n2 = idx < W2n ? t.b2lo + idx : idx - W2n - 2;
+          pw2[idx] = cmul(sm.tw2[idx], P2[n2]);
         }
-        for (int w = 0; w < kWindow; ++w) {
-          const double2 p = phw[w];
-#pragma unroll
-          for (int a = 0; a < 3; ++a)
-            if (a < t.nj) wk[a] = cfma(p, t.V[((size_t)a * kWindow + w) * nw2 + e], wk[a]);
+        for (int idx = tid; idx < B * W1; idx += nthr) {
+          const int q = idx % W1;
+          const int n1 = q < W1n ? t.b1lo + q : q - W1n - 2;
+          pw1[idx] = cmul(sm.tw1[idx], P1[n1]);
         }
-      }
-
-      // Four RK4 stages (src/solver.cpp:157-163): fields at t, t+dt/2, t+dt/2, t+dt.
-      double2 K = zero, S = zero;
+        __syncthreads();
+        // (2) inner sums over n2, shared by the CTA's k-points (same column m2)
+        for (int p = tid; p < gpairs + wpairs; p += nthr) {
+          double2 acc = zero;
+          if (p < gpairs) {
+            const int mat = p / (W1n * nw2), rem = p % (W1n * nw2), q1 = rem / nw2, ee = rem % nw2;
+            const double2* X = (mat == 0 ? t.Hd : t.Rd + (size_t)(mat - 1) * W1n * W2n * nw2) + (size_t)q1 * W2n * nw2 + ee;
+            // Batches of four loads in flight together.
+            for (int q0 = 0; q0 < W2n; q0 += 4) {
+              double2 xv[4];
+#pragma unroll
+              for (int q = 0; q < 4; ++q)
+                if (q0 + q < W2n) xv[q] = __ldg(X + (size_t)(q0 + q) * nw2);
+#pragma unroll
+              for (int q = 0; q < 4; ++q)
+                if (q0 + q < W2n) acc = cfma(pw2[q0 + q], xv[q], acc);
+            }
+            Gb[p] = acc;
+          } else {
+            const int pp = p - gpairs, a = pp / (4 * nw2), rem = pp % (4 * nw2), q1 = rem / nw2, ee = rem % nw2;
+            const double2* X = t.Vd + ((size_t)(a * 4 + q1) * 4) * nw2 + ee;
+            double2 xv[4];
+#pragma unroll
+            for (int q2 = 0; q2 < 4; ++q2) xv[q2] = __ldg(X + (size_t)q2 * nw2);
+#pragma unroll
+            for (int q2 = 0; q2 < 4; ++q2) acc = cfma(pw2[W2n + q2], xv[q2], acc);
+            GW[pp] = acc;
+          }
+        }
+        __syncthreads();
+        // (3) outer sums over n1 for this k-point
+        double2 h0 = zero, rk[3] = {zero, zero, zero}, wk[3] = {zero, zero, zero};
+        if (act) {
+          const double2* p1 = pw1 + g * W1;
+          for (int q1 = 0; q1 < W1n; ++q1) {
+            const double2 ph = p1[q1];
+            h0 = cfma(ph, Gb[q1 * nw2 + e], h0);
+#pragma unroll
+            for (int a = 0; a < 3; ++a)
+              if (a < nax) rk[a] = cfma(ph, Gb[((1 + a) * W1n + q1) * nw2 + e], rk[a]);
+          }
+#pragma unroll
+          for (int q1 = 0; q1 < 4; ++q1) {
+            const double2 ph = p1[W1n + q1];
+#pragma unroll
+            for (int a = 0; a < 3; ++a)
+              if (a < nj) wk[a] = cfma(ph, GW[(a * 4 + q1) * nw2 + e], wk[a]);
+          }
+        }
+        // (4) RK4 stages
+        const double* esb = t.es + (size_t)ti * 9;
+        double2 K = zero, S = zero;
 #pragma unroll 1
-      for (int s = 0; s < 4; ++s) {
-        const int f = s == 0 ? 0 : (s == 3 ? 2 : 1);
-        double2 hs = h0;
+        for (int st = 0; st < 4; ++st) {
+          const int f = st == 0 ? 0 : (st == 3 ? 2 : 1);
+          double2 hs = h0;
+#pragma unroll
+          for (int a = 0; a < 3; ++a)
+            if (a < nax) {
+              const double ea = esb[f * 3 + t.ax_id[a]];
+              hs.x = fma(ea, rk[a].x, hs.x);
+              hs.y = fma(ea, rk[a].y, hs.y);
+            }
+          double2 x = r;
+          if (st > 0) {
+            const double cs = (st == 3 ? 1.0 : 0.5) * dt;
+            x.x = r.x + cs * K.x;
+            x.y = r.y + cs * K.y;
+          }
+          if (act) {
+            sm.Hs[e] = hs;
+            sm.Xs[e] = x;
+          }
+          group_sync(g, G);
+          double2 hx = zero;
+          if (t.hermitian) {
+            if (act) {
+              for (int l = 0; l < nw; ++l) hx = cfma(sm.Hs[i * nw + l], sm.Xs[l * nw + j], hx);
+              sm.HXs[e] = hx;
+            }
+            group_sync(g, G);
+            if (act) {
+              const double2 ht = sm.HXs[j * nw + i];
+              K = make_double2(hx.y + ht.y, -(hx.x - ht.x));  // -i (HX - (HX)^+)
+            }
+          } else {
+            double2 xh = zero;
+            if (act) {
+              for (int l = 0; l < nw; ++l) {
+                hx = cfma(sm.Hs[i * nw + l], sm.Xs[l * nw + j], hx);
+                xh = cfma(sm.Xs[i * nw + l], sm.Hs[l * nw + j], xh);
+              }
+              K = make_double2(hx.y - xh.y, -(hx.x - xh.x));  // -i (HX - XH)
+            }
+            group_sync(g, G);
+          }
+          if (st == 0) {
+            S = K;
+          } else {
+            const double wgt = st == 3 ? 1.0 : 2.0;
+            S.x += wgt * K.x;
+            S.y += wgt * K.y;
+          }
+        }
+        r.x = r.x + prefac * S.x;
+        r.y = r.y + prefac * S.y;
+        // (5) current partials
 #pragma unroll
         for (int a = 0; a < 3; ++a)
-          if (a < t.nax) {
-            const double ea = sp->es[f][t.ax_id[a]];
-            hs.x = fma(ea, rk[a].x, hs.x);
-            hs.y = fma(ea, rk[a].y, hs.y);
-          }
-        double2 x = r;
-        if (s > 0) {
-          const double cs = (s == 3 ? 1.0 : 0.5) * dt;
-          x.x = r.x + cs * K.x;
-          x.y = r.y + cs * K.y;
-        }
-        if (act) {
-          Hs[e] = hs;
-          Xs[e] = x;
-        }
-        group_sync(g, G);
-        double2 hx = zero;
-        if (t.hermitian) {
-          if (act) {
-            for (int l = 0; l < nw; ++l) hx = cfma(Hs[i * nw + l], Xs[l * nw + j], hx);
-            HXs[e] = hx;
-          }
-          group_sync(g, G);
-          if (act) {
-            const double2 ht = HXs[j * nw + i];
-            // k = -i (HX - (HX)^+)
-            const double cx = hx.x - ht.x, cy = hx.y + ht.y;
-            K = make_double2(cy, -cx);
-          }
-        } else {
-          // Placed operators not Hermitian-symmetric on the grid: full HX - XH.
-          double2 xh = zero;
-          if (act) {
-            for (int l = 0; l < nw; ++l) {
-              hx = cfma(Hs[i * nw + l], Xs[l * nw + j], hx);
-              xh = cfma(Xs[i * nw + l], Hs[l * nw + j], xh);
+          if (a < nj) {
+            double re = 0.0, im = 0.0;
+            if (own) {
+              re = fma(wk[a].x, r.x, wk[a].y * r.y);
+              im = fma(wk[a].y, r.x, -wk[a].x * r.y);
             }
-            K = make_double2(hx.y - xh.y, -(hx.x - xh.x));
+            re = warp_sum(re);
+            im = warp_sum(im);
+            if (lane == 0) {
+              sm.sJ[(s * nwarps + warp) * 2 * nj + 2 * a] = re;
+              sm.sJ[(s * nwarps + warp) * 2 * nj + 2 * a + 1] = im;
+            }
           }
-          group_sync(g, G);
-        }
-        if (s == 0) {
-          S = K;
-        } else {
-          const double wgt = s == 3 ? 1.0 : 2.0;
-          S.x += wgt * K.x;
-          S.y += wgt * K.y;
-        }
-      }
-      r.x = r.x + prefac * S.x;
-      r.y = r.y + prefac * S.y;
-
-      // Current partials: sum_ij W_ij conj(rho_ij), reduced over the CTA in a fixed order.
-      double jr[3], jim[3];
-#pragma unroll
-      for (int a = 0; a < 3; ++a) {
-        double2 c = zero;
-        if (own && a < t.nj) c = cmul(wk[a], cconj(r));
-        jr[a] = warp_sum(c.x);
-        jim[a] = warp_sum(c.y);
-      }
-      double2* slot = Jw + (ti & 1) * nwarps * 3;
-      if (lane == 0) {
-#pragma unroll
-        for (int a = 0; a < 3; ++a) slot[warp * 3 + a] = make_double2(jr[a], jim[a]);
       }
       __syncthreads();
-      if (tid < t.nj) {
-        double2 acc = zero;
-        for (int w = 0; w < nwarps; ++w) {
-          acc.x += slot[w * 3 + tid].x;
-          acc.y += slot[w * 3 + tid].y;
-        }
-        double2* dst = Jpart + ((size_t)blockIdx.x * nt + ti) * 3 + t.j_id[tid];
-        double2 old = *dst;
-        *dst = make_double2(old.x + acc.x, old.y + acc.y);
-      }
+      flush_current(t, sm.sJ, nwarps, ti0, nsteps, Jpart);
     }
-    if (own) rho[(size_t)k * nw2 + e] = r;
+    if (own) rho[k * nw2 + e] = r;
+    __syncthreads();
   }
 }
 
@@ -273,8 +550,10 @@ __device__ void jacobi_hermitian(int n, double2* A, double2* V, double* w) {
   for (int p = 0; p < n; ++p) w[p] = A[p * n + p].x;
 }
 
-// rho0(k) = U f U^+, f_n = [E_n(k) < 0]: the equilibrium of src/rdm.cpp:23-38 taken back to the
-// W gauge (src/swe.cpp:80-90), with H(k) from the field-free Wannier sum.
+// rho0(k) = U f U^+ for H(k) = sum_cells e^{-ik.R} H0 (no field): the equilibrium of
+// src/rdm.cpp:23-38 taken back to the W gauge (src/swe.cpp:80-90).  U diagonalises the Hermitian
+// matrix read from the lower triangle (zheevd 'L', src/hamiltonian.cpp:83-91); f_n = [Re (U^+ H U)_nn < 0]
+// with the full H as the reference rotates H (src/operator.cpp:165-221) before reading its diagonal.
 __global__ void rho0_fp64_kernel(SolveTables t, double2* rho) {
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= t.Nk) return;
@@ -285,14 +564,9 @@ __global__ void rho0_fp64_kernel(SolveTables t, double2* rho) {
   for (int o = 0; o < nw2; ++o) A[o] = make_double2(0.0, 0.0);
   for (int c = 0; c < t.ncell; ++c) {
     const int2 n = t.cell_n[c];
-    int i1 = (int)(((long long)m1 * n.x) % t.N1);
-    if (i1 < 0) i1 += t.N1;
-    int i2 = (int)(((long long)m2 * n.y) % t.N2);
-    if (i2 < 0) i2 += t.N2;
-    const double2 p = cmul(t.T1[i1], t.T2[i2]);
+    const double2 p = cmul(t.T1[wrap_mod((long long)m1 * n.x, t.N1)], t.T2[wrap_mod((long long)m2 * n.y, t.N2)]);
     for (int o = 0; o < nw2; ++o) A[o] = cfma(p, t.H0[(size_t)c * nw2 + o], A[o]);
   }
-  // zheevd(..., 'L') reads the lower triangle (src/hamiltonian.cpp:83-91).
   for (int p = 0; p < nw; ++p) {
     B[p * nw + p] = make_double2(A[p * nw + p].x, 0.0);
     for (int q = 0; q < p; ++q) {
@@ -301,8 +575,6 @@ __global__ void rho0_fp64_kernel(SolveTables t, double2* rho) {
     }
   }
   jacobi_hermitian(nw, B, V, w);
-  // Occupation from Re (U^+ H U)_nn with the full H, as the reference rotates H (src/operator.cpp:165-221)
-  // before src/rdm.cpp:23-38 reads its diagonal; equal to the eigenvalue when H is Hermitian.
   for (int n = 0; n < nw; ++n) {
     double d = 0.0;
     for (int p = 0; p < nw; ++p) {
@@ -359,13 +631,59 @@ double time_fma(int sms) {
   return flops / (ms * 1e-3) / 1e12;
 }
 
+size_t kpt_smem(const SolveTables& t, int threads) {
+  const int ncw = t.ncell + t.nwin;
+  const size_t n2 = (size_t)(t.ncell * t.nw2 * (1 + t.nax) + t.nj * t.nwin * t.nw2 + ncw * threads + kRing * ncw);
+  return n2 * sizeof(double2) + sizeof(double) * (kRing * 9 + kRing * (threads / 32) * 2 * t.nj);
+}
+
+size_t group_smem(const SolveTables& t, int B, int G) {
+  const int W1 = t.b1n + 4, W2 = t.b2n + 4, nwarps = (B * G + 31) / 32;
+  const size_t n2 = (size_t)B * 3 * t.nw2 + (size_t)B * W1 + W2 + 2 * (size_t)B * W1 + 2 * W2 +
+                    2 * (size_t)(1 + t.nax) * t.b1n * t.nw2 + 2 * (size_t)t.nj * 4 * t.nw2;
+  return n2 * sizeof(double2) + sizeof(double) * (size_t)kRing * nwarps * 2 * t.nj;
+}
+
+using KptKernel = void (*)(SolveTables, double2*, double2*);
+KptKernel kpt_kernel_for(int nw) { return nw == 1 ? propagate_kpt_kernel<1> : propagate_kpt_kernel<2>; }
+
+bool plan_kpt(const SolveTables& t, int sm_count, LaunchShape* out, size_t smem_max) {
+  KptKernel kern = kpt_kernel_for(t.nw);
+  int threads = (int)((t.Nk + sm_count - 1) / sm_count);
+  threads = (threads + 31) / 32 * 32;
+  threads = threads < 64 ? 64 : (threads > kKptMaxThreads ? kKptMaxThreads : threads);
+  while (threads > 64 && kpt_smem(t, threads) > smem_max) threads -= 32;
+  if (kpt_smem(t, threads) > smem_max) return false;
+  cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kpt_smem(t, threads));
+  int occ = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, threads, kpt_smem(t, threads));
+  if (occ < 1) return false;
+  const long slots = (long)occ * sm_count;
+  long ntiles = (t.Nk + threads - 1) / threads;
+  const long rounds = (ntiles + slots - 1) / slots;
+  int balanced = (int)((t.Nk + rounds * slots - 1) / (rounds * slots));
+  balanced = (balanced + 31) / 32 * 32;
+  if (balanced >= 64 && balanced < threads) threads = balanced;
+  ntiles = (t.Nk + threads - 1) / threads;
+  out->kernel = 0;
+  out->k_per_cta = threads;
+  out->group = 1;
+  out->threads = threads;
+  out->ntiles = (int)ntiles;
+  out->ctas = (int)(ntiles < slots ? ntiles : slots);
+  out->smem = kpt_smem(t, threads);
+  return true;
+}
+
 }  // namespace
 
 bool plan_propagate(const SolveTables& t, int sm_count, LaunchShape* out, char* why, int why_len) {
+  const size_t kSmemMax = 220 * 1024;
   if (t.nw < 1 || t.nw > kMaxOrb) {
     snprintf(why, why_len, "num_orb=%d outside the supported range 1..%d", t.nw, kMaxOrb);
     return false;
   }
+  if (t.hermitian && t.nw <= 2 && plan_kpt(t, sm_count, out, kSmemMax)) return true;
   int G;
   if (t.nw2 <= 32) {
     G = 1;
@@ -373,51 +691,56 @@ bool plan_propagate(const SolveTables& t, int sm_count, LaunchShape* out, char* 
   } else {
     G = (t.nw2 + 31) / 32 * 32;
   }
-  const int per = 3 * t.nw2 + t.ncell + kWindow;
-  int kpc_max = kMaxThreads / G;
-  if (G > 32 && kpc_max > 15) kpc_max = 15;  // one named barrier per group, ids 1..15
-  if (kpc_max < 1) {
-    snprintf(why, why_len, "num_orb=%d needs %d threads per k-point (> %d)", t.nw, G, kMaxThreads);
+  const int step = G < 32 ? 32 / G : 1;  // whole warps per CTA
+  int Bmax = kGroupMaxThreads / G;
+  if (G > 32 && Bmax > 15) Bmax = 15;  // one named barrier per group, ids 1..15
+  Bmax = Bmax / step * step;
+  while (Bmax > step && group_smem(t, Bmax, G) > kSmemMax) Bmax -= step;
+  if (Bmax < 1 || group_smem(t, Bmax, G) > kSmemMax) {
+    snprintf(why, why_len, "model (%d orbitals, %dx%d cell box) does not fit in shared memory", t.nw, t.b1n, t.b2n);
     return false;
   }
-  auto smem_of = [&](int kpc) {
-    const int threads = kpc * G;
-    const int nwarps = (threads + 31) / 32;
-    return (size_t)(kpc * per + 2 * nwarps * 3) * sizeof(double2);
-  };
-  while (kpc_max > 1 && smem_of(kpc_max) > 200 * 1024) --kpc_max;
-  if (smem_of(kpc_max) > 200 * 1024) {
-    snprintf(why, why_len, "model with %d support cells does not fit in shared memory", t.ncell);
-    return false;
-  }
-  // Whole warps per CTA when several k-points share a warp.
-  const int gran = G < 32 ? 32 / G : 1;
-  kpc_max = kpc_max / gran * gran;
-  if (kpc_max < gran) kpc_max = gran;
+  cudaFuncSetAttribute(propagate_group_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)group_smem(t, Bmax, G));
   int occ = 0;
-  cudaFuncSetAttribute(propagate_fp64_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_of(kpc_max));
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, propagate_fp64_kernel, kpc_max * G, smem_of(kpc_max));
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, propagate_group_kernel, Bmax * G, group_smem(t, Bmax, G));
   if (occ < 1) occ = 1;
   const long slots = (long)occ * sm_count;
-  const long ntiles_max = (t.Nk + kpc_max - 1) / kpc_max;
-  const long rounds = (ntiles_max + slots - 1) / slots;
-  // Spread the k-points evenly over rounds x slots.
-  long kpc = (t.Nk + rounds * slots - 1) / (rounds * slots);
-  kpc = (kpc + gran - 1) / gran * gran;
-  if (kpc > kpc_max) kpc = kpc_max;
-  if (kpc < gran) kpc = gran;
-  const long ntiles = (t.Nk + kpc - 1) / kpc;
-  out->k_per_cta = (int)kpc;
+  // B (k-points per CTA) minimising rounds x (B + shared), where `shared` is the per-step work a CTA
+  // does once for its column (the inner Wannier sums) in units of one k-point's work; ties go to the
+  // larger B.
+  const double per_k = (double)t.nw2 * ((1 + t.nax) * t.b1n + 4 * t.nj + 4 * t.nw);
+  const double shared = ((double)(1 + t.nax) * t.b1n * t.b2n * t.nw2 + 16.0 * t.nj * t.nw2) / per_k;
+  int best = Bmax;
+  double best_cost = -1;
+  for (int B = Bmax; B >= step; B -= step) {
+    const long ntiles = (long)t.N2 * ((t.N1 + B - 1) / B);
+    const double cost = (double)((ntiles + slots - 1) / slots) * (B + shared);
+    if (best_cost < 0 || cost < best_cost) {
+      best_cost = cost;
+      best = B;
+    }
+  }
+  const long ntiles = (long)t.N2 * ((t.N1 + best - 1) / best);
+  out->kernel = 1;
+  out->k_per_cta = best;
   out->group = G;
+  out->threads = best * G;
+  out->ntiles = (int)ntiles;
   out->ctas = (int)(ntiles < slots ? ntiles : slots);
-  out->smem = smem_of((int)kpc);
+  out->smem = group_smem(t, best, G);
   return true;
 }
 
 int launch_propagate_fp64(const SolveTables& t, const LaunchShape& s, double2* rho, double2* Jpart, double2* J,
                           cudaStream_t stream, cudaEvent_t after_propagate) {
-  cudaFuncSetAttribute(propagate_fp64_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s.smem);
-  propagate_fp64_kernel<<<s.ctas, s.k_per_cta * s.group, s.smem, stream>>>(t, s.k_per_cta, s.group, rho, Jpart);
+  if (s.kernel == 0) {
+    KptKernel kern = kpt_kernel_for(t.nw);
+    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s.smem);
+    kern<<<s.ctas, s.threads, s.smem, stream>>>(t, rho, Jpart);
+  } else {
+    cudaFuncSetAttribute(propagate_group_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s.smem);
+    propagate_group_kernel<<<s.ctas, s.threads, s.smem, stream>>>(t, s.k_per_cta, s.group, rho, Jpart);
+  }
   if (after_propagate) cudaEventRecord(after_propagate, stream);
   const int n = 3 * t.nt;
   reduce_current_kernel<<<(n + 255) / 256, 256, 0, stream>>>(Jpart, s.ctas, t.nt, 1.0 / (double)t.Nk, J);
