@@ -740,6 +740,23 @@ void SWESim_get_fields(SWESim* swe, double* t, double* E, double* A) {
 
 void SWESim_reset(SWESim* swe) { guarded(swe, "SWESim_reset", [&] { swe->reset_state(); }); }
 
+// Allocation-free variant of SWESim_run_simulation; see include/hhg_swe.h.
+int SWESim_run_simulation_noalloc(SWESim* swe, hhg_cdouble* rho_k, hhg_cdouble* current, void* stream) {
+  int rc = -1;
+  guarded(swe, "SWESim_run_simulation_noalloc", [&] {
+    if (!swe->ready) throw std::runtime_error("SWESim_run_simulation_noalloc: SWESim_init has not succeeded");
+    if (!rho_k || !current) throw std::runtime_error("SWESim_run_simulation_noalloc: null rho_k or current pointer");
+    check_cuda(cudaSetDevice(swe->device), "cudaSetDevice");
+    char why[512] = {0};
+    if (hhg::propagate_fp64_static_scratch(swe->tab, swe->shape, reinterpret_cast<double2*>(rho_k),
+                                           reinterpret_cast<double2*>(current), static_cast<cudaStream_t>(stream), why,
+                                           sizeof why) != 0)
+      throw std::runtime_error(std::string("SWESim_run_simulation_noalloc: ") + why);
+    rc = 0;
+  });
+  return rc;
+}
+
 int HHG_measure_peaks(double* fp64_tflops, double* fp32_tflops) {
   try {
     return hhg::measure_fma_peaks(fp64_tflops, fp32_tflops);

@@ -1,0 +1,80 @@
+// Propagation with library-owned scratch, for callers that must not allocate GPU memory.
+//
+// The propagation kernels accumulate the current in per-CTA partial sums ([ctas][nt][3] complex)
+// before one reduction writes J.  SWESim_run_simulation keeps that scratch in a buffer it
+// cudaMallocs at SWESim_init.  This file instead holds it in one fixed array of device global
+// memory, g_current_scratch, which the CUDA driver reserves on every device where this library is
+// used and keeps until the process exits.  A call therefore allocates nothing.
+//
+// Host code cannot use the array's name as a device address (on the host it names a stand-in
+// object), so the first call on each device looks the address up with cudaGetSymbolAddress while
+// that device is current and caches it per device.  All calls on a device share the one array:
+// it is cleared at the start of every call, and two calls whose work overlaps on the GPU (for
+// example on two streams) corrupt each other's current.
+#include <cuda_runtime.h>
+
+#include <cstdio>
+#include <mutex>
+
+#include "sbe_device.h"
+
+namespace hhg {
+namespace {
+
+constexpr size_t kStaticScratchBytes = size_t(32) << 20;  // 32 MiB: [ctas][nt][3] complex128 partials
+static __device__ __align__(256) unsigned char g_current_scratch[kStaticScratchBytes];
+
+constexpr int kMaxDevices = 64;
+std::mutex g_scratch_mutex;
+void* g_scratch_address[kMaxDevices] = {};
+
+}  // namespace
+
+size_t static_scratch_capacity() { return kStaticScratchBytes; }
+
+int propagate_fp64_static_scratch(const SolveTables& t, const LaunchShape& s, double2* rho, double2* J,
+                                  cudaStream_t stream, char* why, int why_len) {
+  int dev = -1;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess || dev < 0 || dev >= kMaxDevices) {
+    snprintf(why, why_len, "no usable current CUDA device (%s)", cudaGetErrorString(e));
+    return -1;
+  }
+  const size_t need = (size_t)s.ctas * (size_t)t.nt * 3 * sizeof(double2);
+  if (need > kStaticScratchBytes) {
+    snprintf(why, why_len,
+             "this solve needs %zu bytes of scratch for its current partials (%d CTAs x %d steps x 3 axes); "
+             "the allocation-free entry point has %zu bytes: use SWESim_run_simulation instead",
+             need, s.ctas, t.nt, kStaticScratchBytes);
+    return -1;
+  }
+  void* scratch = nullptr;
+  {
+    std::lock_guard<std::mutex> lock(g_scratch_mutex);
+    if (!g_scratch_address[dev]) {
+      void* addr = nullptr;
+      e = cudaGetSymbolAddress(&addr, g_current_scratch);
+      if (e != cudaSuccess || addr == nullptr) {
+        snprintf(why, why_len, "cudaGetSymbolAddress of the static scratch failed on device %d: %s", dev,
+                 cudaGetErrorString(e));
+        return -1;
+      }
+      g_scratch_address[dev] = addr;
+    }
+    scratch = g_scratch_address[dev];
+  }
+  e = cudaMemsetAsync(scratch, 0, need, stream);
+  if (e != cudaSuccess) {
+    snprintf(why, why_len, "clearing the static scratch failed: %s", cudaGetErrorString(e));
+    return -1;
+  }
+  launch_propagate_fp64(t, s, rho, static_cast<double2*>(scratch), J, stream);
+  e = cudaGetLastError();
+  if (e != cudaSuccess) {
+    snprintf(why, why_len, "propagation launch failed: %s", cudaGetErrorString(e));
+    return -1;
+  }
+  return 0;
+}
+
+}  // namespace hhg

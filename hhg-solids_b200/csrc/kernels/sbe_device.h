@@ -59,6 +59,12 @@ bool plan_propagate(const SolveTables& t, int sm_count, LaunchShape* out, char* 
 int launch_propagate_fp64(const SolveTables& t, const LaunchShape& s, double2* rho, double2* Jpart, double2* J,
                           cudaStream_t stream, cudaEvent_t after_propagate = nullptr);
 
+// Same as launch_propagate_fp64, with the current partials in a fixed device array owned by the
+// library instead of a caller buffer (see noalloc.cu).  Returns 0, or -1 with a reason in `why`.
+int propagate_fp64_static_scratch(const SolveTables& t, const LaunchShape& s, double2* rho, double2* J,
+                                  cudaStream_t stream, char* why, int why_len);
+size_t static_scratch_capacity();
+
 // rho0(k) = U f U^+ of H(k) = sum_cells e^{-ik.R} H0 (no field), one k-point per thread.
 int launch_rho0_fp64(const SolveTables& t, double2* rho, cudaStream_t stream);
 

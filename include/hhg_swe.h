@@ -99,6 +99,30 @@ void SWESim_get_rho_k(SWESim* swe, hhg_cdouble* out);
 /* Fields the propagation uses: t (au, nt), E and A (au, [3][nt]). */
 void SWESim_get_fields(SWESim* swe, double* t, double* E, double* A);
 
+/* Allocation-free propagation.  No counterpart in the reference.
+ *
+ * For callers that cannot allocate GPU memory while they run: code whose device memory is owned
+ * by another framework's pool (a PyTorch or JAX process, a simulation code with its own arena),
+ * where a foreign cudaMalloc fragments that pool and a cudaFree stalls every stream on the device
+ * because it synchronises the whole GPU; and latency-critical loops that cannot take those stalls.
+ *
+ * Does what SWESim_run_simulation does with the tables SWESim_init put on the device, but the
+ * caller supplies the state and the result, both in device memory on the SWESim's device:
+ *   rho_k    [nr1*nr2][nw*nw] complex, in: the starting density matrix (e.g. the equilibrium that
+ *            SWESim_get_rho_k returns before any run), out: the state after nt steps;
+ *   current  [3][nt] complex, out: J(t) (no record is added to SWESim_get_current's history).
+ * Work is queued on `stream` (a cudaStream_t, NULL for the default stream) and the call returns
+ * without waiting; it makes the SWESim's device current.
+ *
+ * It calls no cudaMalloc / cudaFree: the current partials go to a fixed 32 MiB array of device
+ * memory that the library holds on each device it is used on until the process exits.  Solves
+ * that need more (CTAs x nt x 48 bytes > 32 MiB, e.g. nt above about 4700 when a solve fills all 148 SMs) are
+ * rejected with -1 and a message.  The first call on a device looks up that array's address, so
+ * make it before capturing the stream into a graph.  All calls on a device share the array and
+ * clear it at their start: calls whose work overlaps on the GPU (different streams, or different
+ * host threads) corrupt each other's result.  Returns 0, or -1 (message in SWESim_last_error). */
+int SWESim_run_simulation_noalloc(SWESim* swe, hhg_cdouble* rho_k, hhg_cdouble* current, void* stream);
+
 /* FP64 FMA / FP32 FMA chain throughput of the current device (TFLOP/s), for roofline denominators. */
 int HHG_measure_peaks(double* fp64_tflops, double* fp32_tflops);
 
