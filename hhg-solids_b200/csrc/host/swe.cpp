@@ -9,6 +9,8 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <chrono>
+#include <cstdlib>
 #include <cmath>
 #include <complex>
 #include <cstdio>
@@ -53,6 +55,31 @@ struct Settings {
 namespace {
 
 using hhg::cd;
+
+// Setup phase timer, printed to stderr when the environment sets HHG_TRACE=1.
+struct PhaseTrace {
+  bool on = false;
+  std::chrono::steady_clock::time_point t0, last;
+  std::string line;
+  PhaseTrace() {
+    const char* e = std::getenv("HHG_TRACE");
+    on = e && e[0] && e[0] != '0';
+    t0 = last = std::chrono::steady_clock::now();
+  }
+  void mark(const char* name) {
+    if (!on) return;
+    const auto now = std::chrono::steady_clock::now();
+    char buf[96];
+    snprintf(buf, sizeof buf, " %s=%.2fms", name, std::chrono::duration<double, std::milli>(now - last).count());
+    line += buf;
+    last = now;
+  }
+  ~PhaseTrace() {
+    if (on)
+      fprintf(stderr, "[hhg] init%s total=%.2fms\n", line.c_str(),
+              std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count());
+  }
+};
 constexpr double kEv2Ha = 1.0 / 27.2114;       // include/constants.h:10
 constexpr double kA2Bohr = 1.0 / 0.5291772;    // include/constants.h:6
 
@@ -67,11 +94,17 @@ template <typename T>
 struct DevBuf {
   T* p = nullptr;
   size_t n = 0;
+  size_t cap = 0;
+  // Keeps the current allocation when it is large enough (re-initialisation reuses buffers).
   void alloc(size_t count) {
-    release();
     if (count == 0) count = 1;
+    if (p && count <= cap) {
+      n = count;
+      return;
+    }
+    release();
     check_cuda(cudaMalloc(&p, count * sizeof(T)), "cudaMalloc");
-    n = count;
+    n = cap = count;
   }
   void upload(const std::vector<T>& v, cudaStream_t s) {
     alloc(v.size());
@@ -80,7 +113,7 @@ struct DevBuf {
   void release() {
     if (p) cudaFree(p);
     p = nullptr;
-    n = 0;
+    n = cap = 0;
   }
   ~DevBuf() { release(); }
 };
@@ -93,6 +126,7 @@ struct SWESim {
   std::string path_tb;
   Settings* settings = nullptr;
   int device = -1;
+  int req_row0 = 0, req_row1 = -1;  // k-grid row slab requested with SWESim_set_k_rows (-1: all)
   std::string err;
   bool has_err = false;
   bool ready = false;
@@ -109,6 +143,7 @@ struct SWESim {
   int nax = 0, ax_id[3] = {0, 0, 0}, nj = 0, j_id[3] = {0, 0, 0};
 
   cudaStream_t stream = nullptr;
+  int stream_device = -1;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr, evm = nullptr;
   DevBuf<int2> d_cell, d_win;
   DevBuf<double2> d_H0, d_R, d_V, d_Q, d_Hd, d_Rd, d_Vd, d_P, d_T1, d_T2, d_rho0, d_rho, d_Jpart, d_J;
@@ -116,12 +151,20 @@ struct SWESim {
   hhg::SolveTables tab{};
   hhg::LaunchShape shape{};
   double2* h_J = nullptr;  // pinned [3][nt]
+  size_t h_J_cap = 0;
   std::vector<cd> Jhist[3];
   float last_ms = 0.f, last_prop_ms = 0.f;
   size_t h2d_bytes = 0;
   int last_launches = 0;
 
   ~SWESim() { release(); }
+
+  // Forget the previous setup but keep device buffers, stream, events and the pinned host
+  // buffer for reuse: a restart then costs no cudaFree / cudaFreeHost (both synchronise).
+  void invalidate() {
+    ready = false;
+    for (auto& j : Jhist) j.clear();
+  }
 
   void release() {
     d_cell.release();
@@ -131,6 +174,7 @@ struct SWESim {
     d_es.release();
     if (h_J) cudaFreeHost(h_J);
     h_J = nullptr;
+    h_J_cap = 0;
     if (ev0) cudaEventDestroy(ev0);
     if (ev1) cudaEventDestroy(ev1);
     if (evm) cudaEventDestroy(evm);
@@ -179,10 +223,12 @@ inline int wrapi(long x, int n) {
 }  // namespace
 
 void SWESim::init() {
-  release();
+  PhaseTrace trace;
+  invalidate();
   if (!settings) throw std::runtime_error("SWESim_init: settings not set (call SWESim_set_settings first)");
   if (path_tb.empty()) throw std::runtime_error("SWESim_init: TB path not set (call SWESim_set_path_tb first)");
   model = hhg::parse_tb(path_tb);
+  trace.mark("parse");
   Settings& s = *settings;
   nt = (int)(s.tmax / s.dt);
   s.nt = nt;
@@ -204,16 +250,22 @@ void SWESim::init() {
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
     throw std::runtime_error("SWESim_init: no CUDA device (this library has no CPU path)");
   if (device < 0) check_cuda(cudaGetDevice(&device), "cudaGetDevice");
+  if (stream && device != stream_device) release();  // device changed: start over
   check_cuda(cudaSetDevice(device), "cudaSetDevice");
-  check_cuda(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking), "cudaStreamCreate");
-  check_cuda(cudaEventCreate(&ev0), "cudaEventCreate");
-  check_cuda(cudaEventCreate(&ev1), "cudaEventCreate");
-  check_cuda(cudaEventCreate(&evm), "cudaEventCreate");
+  if (!stream) {
+    check_cuda(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking), "cudaStreamCreate");
+    check_cuda(cudaEventCreate(&ev0), "cudaEventCreate");
+    check_cuda(cudaEventCreate(&ev1), "cudaEventCreate");
+    check_cuda(cudaEventCreate(&evm), "cudaEventCreate");
+    stream_device = device;
+  }
+  trace.mark("cuda_objects");
 
   // Supercell and placement (src/grid.cpp:64-111, src/hamiltonian.cpp:8-39, src/berry_connection.cpp:7-50).
   Rgrid.assign((size_t)Nk * 3, 0.0);
   hhg::refarith::supercell(N1, N2, 1, model.lattice, Rgrid.data());
   place_sites(model, N1, N2, Rgrid, site_of_cell);
+  trace.mark("placement");
   for (int a = 0; a < 3; ++a)
     for (int b = 0; b < 3; ++b) lat_au[a][b] = model.lattice[a][b] * kA2Bohr;
 
@@ -242,6 +294,7 @@ void SWESim::init() {
     }
   }
 
+  trace.mark("fields");
   // Support cells: placed cells whose H0 or field-coupled r block is non-zero (zero blocks add exact zeros).
   cell_n.clear();
   H0.clear();
@@ -418,6 +471,7 @@ void SWESim::init() {
     T2[m] = make_double2(std::cos(ang), -std::sin(ang));
   }
 
+  trace.mark("tables");
   // Device tables.
   h2d_bytes = sizeof(int2) * (cell_n.size() + win_n.size()) +
               sizeof(double2) * (H0.size() + Rtab.size() + V.size() + Q.size() + Hd.size() + Rd.size() + Vd.size() +
@@ -439,6 +493,12 @@ void SWESim::init() {
   d_rho0.alloc((size_t)Nk * nw2);
   d_rho.alloc((size_t)Nk * nw2);
   d_J.alloc((size_t)3 * nt);
+  const int row0 = req_row0, row1 = req_row1 < 0 ? N1 : req_row1;
+  if (row0 < 0 || row1 > N1 || row0 >= row1)
+    throw std::runtime_error("SWESim_init: k-row slab [" + std::to_string(row0) + ", " + std::to_string(row1) +
+                             ") is not inside the grid's " + std::to_string(N1) + " rows");
+  tab.row0 = row0;
+  tab.row1 = row1;
   tab.nw = nw;
   tab.nw2 = nw2;
   tab.N1 = N1;
@@ -471,9 +531,16 @@ void SWESim::init() {
   int sms = 0;
   check_cuda(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device), "cudaDeviceGetAttribute");
   char why[256] = {0};
+  trace.mark("upload");
   if (!hhg::plan_propagate(tab, sms, &shape, why, sizeof why)) throw std::runtime_error(std::string("SWESim_init: ") + why);
+  trace.mark("plan");
   d_Jpart.alloc((size_t)shape.ctas * nt * 3);
-  check_cuda(cudaMallocHost(&h_J, sizeof(double2) * 3 * (size_t)nt), "cudaMallocHost");
+  if (!h_J || h_J_cap < (size_t)3 * nt) {
+    if (h_J) cudaFreeHost(h_J);
+    h_J = nullptr;
+    check_cuda(cudaMallocHost(&h_J, sizeof(double2) * 3 * (size_t)nt), "cudaMallocHost");
+    h_J_cap = (size_t)3 * nt;
+  }
 
   // Equilibrium density matrix (src/swe.cpp:82-90) on the GPU.
   hhg::launch_rho0_fp64(tab, d_rho0.p, stream);
@@ -481,6 +548,7 @@ void SWESim::init() {
   check_cuda(cudaMemcpyAsync(d_rho.p, d_rho0.p, sizeof(double2) * (size_t)Nk * nw2, cudaMemcpyDeviceToDevice, stream),
              "D2D");
   check_cuda(cudaStreamSynchronize(stream), "init");
+  trace.mark("rho0");
   ready = true;
 }
 
@@ -735,6 +803,13 @@ void SWESim_get_fields(SWESim* swe, double* t, double* E, double* A) {
     if (t) std::copy(swe->t.begin(), swe->t.end(), t);
     if (E) std::copy(swe->E.begin(), swe->E.end(), E);
     if (A) std::copy(swe->A.begin(), swe->A.end(), A);
+  });
+}
+
+void SWESim_set_k_rows(SWESim* swe, int row0, int row1) {
+  guarded(swe, "SWESim_set_k_rows", [&] {
+    swe->req_row0 = row0;
+    swe->req_row1 = row1;
   });
 }
 

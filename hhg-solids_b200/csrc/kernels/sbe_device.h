@@ -11,6 +11,9 @@ constexpr int kRing = 32;     // time steps per staged chunk (field table in, cu
 // One solve's device-resident tables (all pointers are device memory).
 struct SolveTables {
   int nw, nw2, N1, N2, Nk, nt;
+  int row0, row1;    // k-grid rows m1 in [row0, row1) are propagated (a slab of a sharded solve);
+                     // J is still normalised by the full Nk, so slab currents add up
+
   int hermitian;     // placed H0 and r are Hermitian-symmetric on the grid: [H,X] = HX - (HX)^+
   double dt;         // au
   int nax, ax_id[3]; // field axes with a non-zero polarisation component
@@ -65,7 +68,7 @@ int propagate_fp64_static_scratch(const SolveTables& t, const LaunchShape& s, do
                                   cudaStream_t stream, char* why, int why_len);
 size_t static_scratch_capacity();
 
-// rho0(k) = U f U^+ of H(k) = sum_cells e^{-ik.R} H0 (no field), one k-point per thread.
+// rho0(k) = U f U^+ of H(k) = sum_cells e^{-ik.R} H0 (no field), one warp per k-point.
 int launch_rho0_fp64(const SolveTables& t, double2* rho, cudaStream_t stream);
 
 // FMA-chain throughput probe (TFLOP/s) on the current device.

@@ -94,10 +94,11 @@ __global__ void __launch_bounds__(kKptMaxThreads) propagate_kpt_kernel(SolveTabl
 
   const double dt = t.dt;
   const double prefac = 0.1666666666666 * dt;
-  const int ntiles = (t.Nk + nthr - 1) / nthr;
+  const int kbeg = t.row0 * t.N2, kend = t.row1 * t.N2;
+  const int ntiles = (kend - kbeg + nthr - 1) / nthr;
   for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-    const int k = tile * nthr + tid;
-    const bool kval = k < t.Nk;
+    const int k = kbeg + tile * nthr + tid;
+    const bool kval = k < kend;
     double2 r[NW2];
 #pragma unroll
     for (int e = 0; e < NW2; ++e) r[e] = kval ? rho[(size_t)k * NW2 + e] : make_double2(0.0, 0.0);
@@ -311,16 +312,16 @@ __global__ void __launch_bounds__(kGroupMaxThreads, 1) propagate_group_kernel(So
   const GroupSmem sm = group_smem_layout(t, B, g, smraw);
   const double dt = t.dt;
   const double prefac = 0.1666666666666 * dt;
-  const int bpc = (t.N1 + B - 1) / B;  // m1 blocks per column
+  const int bpc = (t.row1 - t.row0 + B - 1) / B;  // m1 blocks per column
   const int ntiles = t.N2 * bpc;
   const int npw = 2 * t.np + 1;
   const int gpairs = nmat * W1n * nw2, wpairs = nj * 4 * nw2;
   const double2 zero = make_double2(0.0, 0.0);
 
   for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-    const int m2 = tile / bpc, m10 = (tile % bpc) * B;
+    const int m2 = tile / bpc, m10 = t.row0 + (tile % bpc) * B;
     const int m1 = m10 + g;
-    const bool kval = m1 < t.N1;
+    const bool kval = m1 < t.row1;
     const bool own = act && kval;
     const size_t k = (size_t)m1 * t.N2 + m2;
     double2 r = own ? rho[k * nw2 + e] : zero;
@@ -332,7 +333,7 @@ __global__ void __launch_bounds__(kGroupMaxThreads, 1) propagate_group_kernel(So
     for (int idx = tid; idx < B * W1; idx += nthr) {
       const int gg = idx / W1, q = idx % W1;
       const int n1 = q < W1n ? t.b1lo + q : q - W1n - 2;
-      const int mm1 = min(m10 + gg, t.N1 - 1);
+      const int mm1 = min(m10 + gg, t.row1 - 1);
       sm.tw1[idx] = t.T1[wrap_mod((long long)mm1 * n1, t.N1)];
     }
     __syncthreads();
@@ -502,80 +503,91 @@ __global__ void reduce_current_kernel(const double2* Jpart, int ctas, int nt, do
   J[(size_t)a * nt + ti] = make_double2(acc.x * inv_nk, acc.y * inv_nk);
 }
 
-// Cyclic complex Jacobi on a Hermitian nw x nw matrix (row-major in A), eigenvectors as columns of V.
-__device__ void jacobi_hermitian(int n, double2* A, double2* V, double* w) {
-  for (int p = 0; p < n * n; ++p) V[p] = make_double2(0.0, 0.0);
-  for (int p = 0; p < n; ++p) V[p * n + p] = make_double2(1.0, 0.0);
+// rho0(k) = U f U^+ for H(k) = sum_cells e^{-ik.R} H0 (no field): the equilibrium of
+// src/rdm.cpp:23-38 taken back to the W gauge (src/swe.cpp:80-90).  U diagonalises the Hermitian
+// matrix read from the lower triangle (zheevd 'L', src/hamiltonian.cpp:83-91) by cyclic complex
+// Jacobi rotations; f_n = [Re (U^+ H U)_nn < 0] with the full H, as the reference rotates H
+// (src/operator.cpp:165-221) before reading its diagonal.  One warp per k-point, matrices in shared
+// memory, lanes over rows / columns; the rotation order is fixed, so results are deterministic.
+constexpr int kRho0Warps = 8;
+
+__global__ void __launch_bounds__(kRho0Warps * 32) rho0_fp64_kernel(SolveTables t, double2* rho) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  const int nw = t.nw, nw2 = t.nw2;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int k = blockIdx.x * kRho0Warps + warp;
+  if (k >= t.Nk) return;  // whole warps exit together
+  double2* A = reinterpret_cast<double2*>(smraw) + (size_t)warp * 3 * nw2;
+  double2* B = A + nw2;
+  double2* V = B + nw2;
+  __shared__ double w[kRho0Warps][kMaxOrb];
+  const int m1 = k / t.N2, m2 = k % t.N2;
+  for (int o = lane; o < nw2; o += 32) {
+    double2 acc = make_double2(0.0, 0.0);
+    for (int c = 0; c < t.ncell; ++c) {
+      const int2 n = t.cell_n[c];
+      const double2 p = cmul(t.T1[wrap_mod((long long)m1 * n.x, t.N1)], t.T2[wrap_mod((long long)m2 * n.y, t.N2)]);
+      acc = cfma(p, t.H0[(size_t)c * nw2 + o], acc);
+    }
+    A[o] = acc;
+  }
+  __syncwarp();
+  for (int o = lane; o < nw2; o += 32) {
+    const int i = o / nw, j = o % nw;
+    B[o] = i == j ? make_double2(A[o].x, 0.0) : (i > j ? A[o] : cconj(A[j * nw + i]));
+    V[o] = make_double2(i == j ? 1.0 : 0.0, 0.0);
+  }
+  __syncwarp();
   for (int sweep = 0; sweep < 60; ++sweep) {
     double off = 0.0, tot = 0.0;
-    for (int p = 0; p < n; ++p)
-      for (int q = 0; q < n; ++q) {
-        const double a2 = A[p * n + q].x * A[p * n + q].x + A[p * n + q].y * A[p * n + q].y;
-        tot += a2;
-        if (p != q) off += a2;
-      }
+    for (int o = lane; o < nw2; o += 32) {
+      const double a2 = B[o].x * B[o].x + B[o].y * B[o].y;
+      tot += a2;
+      if (o / nw != o % nw) off += a2;
+    }
+    off = warp_sum(off);
+    tot = warp_sum(tot);
     if (off == 0.0 || off <= 1e-32 * tot) break;
-    for (int p = 0; p < n - 1; ++p)
-      for (int q = p + 1; q < n; ++q) {
-        const double2 apq = A[p * n + q];
+    for (int p = 0; p < nw - 1; ++p)
+      for (int q = p + 1; q < nw; ++q) {
+        const double2 apq = B[p * nw + q];
         const double mag = hypot(apq.x, apq.y);
-        if (mag == 0.0) continue;
+        if (mag == 0.0) continue;  // uniform over the warp
         const double2 ph = make_double2(apq.x / mag, apq.y / mag);
-        const double tau = (A[q * n + q].x - A[p * n + p].x) / (2.0 * mag);
+        const double tau = (B[q * nw + q].x - B[p * nw + p].x) / (2.0 * mag);
         const double tt = (tau >= 0.0 ? 1.0 : -1.0) / (fabs(tau) + sqrt(1.0 + tau * tau));
         const double c = 1.0 / sqrt(1.0 + tt * tt), s = tt * c;
         const double2 se = make_double2(s * ph.x, s * ph.y), sec = make_double2(s * ph.x, -s * ph.y);
-        for (int k = 0; k < n; ++k) {
-          const double2 akp = A[k * n + p], akq = A[k * n + q];
+        __syncwarp();
+        // B <- J^+ B J with J = [[c, s e], [-s conj(e), c]] on (p, q): columns, then rows.
+        if (lane < nw) {
+          const double2 akp = B[lane * nw + p], akq = B[lane * nw + q];
           const double2 t1 = cmul(sec, akq), t2 = cmul(se, akp);
-          A[k * n + p] = make_double2(c * akp.x - t1.x, c * akp.y - t1.y);
-          A[k * n + q] = make_double2(t2.x + c * akq.x, t2.y + c * akq.y);
+          B[lane * nw + p] = make_double2(c * akp.x - t1.x, c * akp.y - t1.y);
+          B[lane * nw + q] = make_double2(t2.x + c * akq.x, t2.y + c * akq.y);
         }
-        for (int k = 0; k < n; ++k) {
-          const double2 apk = A[p * n + k], aqk = A[q * n + k];
+        __syncwarp();
+        if (lane < nw) {
+          const double2 apk = B[p * nw + lane], aqk = B[q * nw + lane];
           const double2 t1 = cmul(se, aqk), t2 = cmul(sec, apk);
-          A[p * n + k] = make_double2(c * apk.x - t1.x, c * apk.y - t1.y);
-          A[q * n + k] = make_double2(t2.x + c * aqk.x, t2.y + c * aqk.y);
+          B[p * nw + lane] = make_double2(c * apk.x - t1.x, c * apk.y - t1.y);
+          B[q * nw + lane] = make_double2(t2.x + c * aqk.x, t2.y + c * aqk.y);
+          const double2 vkp = V[lane * nw + p], vkq = V[lane * nw + q];
+          const double2 t3 = cmul(sec, vkq), t4 = cmul(se, vkp);
+          V[lane * nw + p] = make_double2(c * vkp.x - t3.x, c * vkp.y - t3.y);
+          V[lane * nw + q] = make_double2(t4.x + c * vkq.x, t4.y + c * vkq.y);
         }
-        A[p * n + q] = make_double2(0.0, 0.0);
-        A[q * n + p] = make_double2(0.0, 0.0);
-        for (int k = 0; k < n; ++k) {
-          const double2 vkp = V[k * n + p], vkq = V[k * n + q];
-          const double2 t1 = cmul(sec, vkq), t2 = cmul(se, vkp);
-          V[k * n + p] = make_double2(c * vkp.x - t1.x, c * vkp.y - t1.y);
-          V[k * n + q] = make_double2(t2.x + c * vkq.x, t2.y + c * vkq.y);
+        __syncwarp();
+        if (lane == 0) {
+          B[p * nw + q] = make_double2(0.0, 0.0);
+          B[q * nw + p] = make_double2(0.0, 0.0);
         }
+        __syncwarp();
       }
   }
-  for (int p = 0; p < n; ++p) w[p] = A[p * n + p].x;
-}
-
-// rho0(k) = U f U^+ for H(k) = sum_cells e^{-ik.R} H0 (no field): the equilibrium of
-// src/rdm.cpp:23-38 taken back to the W gauge (src/swe.cpp:80-90).  U diagonalises the Hermitian
-// matrix read from the lower triangle (zheevd 'L', src/hamiltonian.cpp:83-91); f_n = [Re (U^+ H U)_nn < 0]
-// with the full H as the reference rotates H (src/operator.cpp:165-221) before reading its diagonal.
-__global__ void rho0_fp64_kernel(SolveTables t, double2* rho) {
-  const int k = blockIdx.x * blockDim.x + threadIdx.x;
-  if (k >= t.Nk) return;
-  const int nw = t.nw, nw2 = t.nw2;
-  const int m1 = k / t.N2, m2 = k % t.N2;
-  double2 A[kMaxOrb * kMaxOrb], B[kMaxOrb * kMaxOrb], V[kMaxOrb * kMaxOrb];
-  double w[kMaxOrb];
-  for (int o = 0; o < nw2; ++o) A[o] = make_double2(0.0, 0.0);
-  for (int c = 0; c < t.ncell; ++c) {
-    const int2 n = t.cell_n[c];
-    const double2 p = cmul(t.T1[wrap_mod((long long)m1 * n.x, t.N1)], t.T2[wrap_mod((long long)m2 * n.y, t.N2)]);
-    for (int o = 0; o < nw2; ++o) A[o] = cfma(p, t.H0[(size_t)c * nw2 + o], A[o]);
-  }
-  for (int p = 0; p < nw; ++p) {
-    B[p * nw + p] = make_double2(A[p * nw + p].x, 0.0);
-    for (int q = 0; q < p; ++q) {
-      B[p * nw + q] = A[p * nw + q];
-      B[q * nw + p] = cconj(A[p * nw + q]);
-    }
-  }
-  jacobi_hermitian(nw, B, V, w);
-  for (int n = 0; n < nw; ++n) {
+  // Occupations from the full H.
+  if (lane < nw) {
+    const int n = lane;
     double d = 0.0;
     for (int p = 0; p < nw; ++p) {
       double2 hv = make_double2(0.0, 0.0);
@@ -583,15 +595,16 @@ __global__ void rho0_fp64_kernel(SolveTables t, double2* rho) {
       const double2 u = V[p * nw + n];
       d += u.x * hv.x + u.y * hv.y;
     }
-    w[n] = d;
+    w[warp][n] = d;
   }
-  for (int p = 0; p < nw; ++p)
-    for (int q = 0; q < nw; ++q) {
-      double2 acc = make_double2(0.0, 0.0);
-      for (int n = 0; n < nw; ++n)
-        if (w[n] < 0.0) acc = cfma(V[p * nw + n], cconj(V[q * nw + n]), acc);
-      rho[(size_t)k * nw2 + p * nw + q] = acc;
-    }
+  __syncwarp();
+  for (int o = lane; o < nw2; o += 32) {
+    const int p = o / nw, q = o % nw;
+    double2 acc = make_double2(0.0, 0.0);
+    for (int n = 0; n < nw; ++n)
+      if (w[warp][n] < 0.0) acc = cfma(V[p * nw + n], cconj(V[q * nw + n]), acc);
+    rho[(size_t)k * nw2 + o] = acc;
+  }
 }
 
 template <typename T>
@@ -649,7 +662,8 @@ KptKernel kpt_kernel_for(int nw) { return nw == 1 ? propagate_kpt_kernel<1> : pr
 
 bool plan_kpt(const SolveTables& t, int sm_count, LaunchShape* out, size_t smem_max) {
   KptKernel kern = kpt_kernel_for(t.nw);
-  int threads = (int)((t.Nk + sm_count - 1) / sm_count);
+  const long nk_local = (long)(t.row1 - t.row0) * t.N2;
+  int threads = (int)((nk_local + sm_count - 1) / sm_count);
   threads = (threads + 31) / 32 * 32;
   threads = threads < 64 ? 64 : (threads > kKptMaxThreads ? kKptMaxThreads : threads);
   while (threads > 64 && kpt_smem(t, threads) > smem_max) threads -= 32;
@@ -659,12 +673,12 @@ bool plan_kpt(const SolveTables& t, int sm_count, LaunchShape* out, size_t smem_
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, threads, kpt_smem(t, threads));
   if (occ < 1) return false;
   const long slots = (long)occ * sm_count;
-  long ntiles = (t.Nk + threads - 1) / threads;
+  long ntiles = (nk_local + threads - 1) / threads;
   const long rounds = (ntiles + slots - 1) / slots;
-  int balanced = (int)((t.Nk + rounds * slots - 1) / (rounds * slots));
+  int balanced = (int)((nk_local + rounds * slots - 1) / (rounds * slots));
   balanced = (balanced + 31) / 32 * 32;
   if (balanced >= 64 && balanced < threads) threads = balanced;
-  ntiles = (t.Nk + threads - 1) / threads;
+  ntiles = (nk_local + threads - 1) / threads;
   out->kernel = 0;
   out->k_per_cta = threads;
   out->group = 1;
@@ -712,15 +726,16 @@ bool plan_propagate(const SolveTables& t, int sm_count, LaunchShape* out, char* 
   const double shared = ((double)(1 + t.nax) * t.b1n * t.b2n * t.nw2 + 16.0 * t.nj * t.nw2) / per_k;
   int best = Bmax;
   double best_cost = -1;
+  const int rows = t.row1 - t.row0;
   for (int B = Bmax; B >= step; B -= step) {
-    const long ntiles = (long)t.N2 * ((t.N1 + B - 1) / B);
+    const long ntiles = (long)t.N2 * ((rows + B - 1) / B);
     const double cost = (double)((ntiles + slots - 1) / slots) * (B + shared);
     if (best_cost < 0 || cost < best_cost) {
       best_cost = cost;
       best = B;
     }
   }
-  const long ntiles = (long)t.N2 * ((t.N1 + best - 1) / best);
+  const long ntiles = (long)t.N2 * ((rows + best - 1) / best);
   out->kernel = 1;
   out->k_per_cta = best;
   out->group = G;
@@ -748,7 +763,9 @@ int launch_propagate_fp64(const SolveTables& t, const LaunchShape& s, double2* r
 }
 
 int launch_rho0_fp64(const SolveTables& t, double2* rho, cudaStream_t stream) {
-  rho0_fp64_kernel<<<(t.Nk + 63) / 64, 64, 0, stream>>>(t, rho);
+  const size_t smem = (size_t)kRho0Warps * 3 * t.nw2 * sizeof(double2);
+  cudaFuncSetAttribute(rho0_fp64_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  rho0_fp64_kernel<<<(t.Nk + kRho0Warps - 1) / kRho0Warps, kRho0Warps * 32, smem, stream>>>(t, rho);
   return 1;
 }
 

@@ -91,6 +91,10 @@ long long SWESim_h2d_bytes(SWESim* swe);
 int SWESim_launch_shape(SWESim* swe, int* ctas, int* threads, int* k_per_cta, long long* smem);
 /* Number of kernel launches issued by the last SWESim_run_simulation. */
 int SWESim_last_launches(SWESim* swe);
+/* Restrict the next SWESim_init to k-grid rows m1 in [row0, row1) (row1 = -1: to the end): one
+ * slab of a solve split over several GPUs.  The current stays normalised by the full grid, so the
+ * currents of a partition of the rows add up to the full current. */
+void SWESim_set_k_rows(SWESim* swe, int row0, int row1);
 /* Put rho back to the equilibrium rho0 and clear the recorded current, keeping the setup
  * (a fresh propagation without re-running SWESim_init). */
 void SWESim_reset(SWESim* swe);

@@ -185,3 +185,18 @@ def test_matches_oracle_on_other_shapes(pyswe, oracle_mod, model, n, pol):
         else:
             assert rel_l2(J[a], Jo[a]) < TOL
     swe.delete()
+
+
+@pytest.mark.parametrize("name,cuts", [("haldane_16_rect", [0, 5, 11, 16]), ("tmd11_10", [0, 3, 10])])
+def test_row_slabs_add_up_to_the_full_current(pyswe, name, cuts):
+    """The slabs of a multi-GPU split (SWESim_set_k_rows), run one after another on one GPU."""
+    import shard  # noqa: F401  (the helper the multi-GPU path uses)
+
+    meta, param, _, J_ref = load_golden(name)
+    total = 0
+    for r0, r1 in zip(cuts, cuts[1:]):
+        s = pyswe.SWE(pyswe.Settings(dict(param)), k_rows=(r0, r1))
+        s.run_simulation()
+        total = total + s.get_current()[1:]
+        s.delete()
+    check_current(total, J_ref, name)
