@@ -296,6 +296,44 @@ def cpu_baseline(workload: str) -> dict:
 # ---------------------------------------------------------------- our arm
 
 
+def harmonic_errors(J, J_ref, param):
+    """Per odd harmonic (up to the cutoff, 1e-12 of the fundamental): relative error of the intensity
+    of |FFT(dJ/dt)|^2, with the spectrum and order axis of the reference's scripts/pol_scan.py."""
+    import numpy as np
+
+    def spec(x):
+        return np.abs(np.fft.fftshift(np.fft.fft(np.fft.ifftshift(np.gradient(x, param["dt"]))))) ** 2
+
+    nt = len(J)
+    S, S_ref = spec(J), spec(J_ref)
+    dw = 2.0 * np.pi / param["tmax"]
+    order = np.linspace(-nt * dw / 2.0, nt * dw / 2.0, nt) / (2.0 * np.pi * 300 / param["lambda"])
+    fund = S_ref[(order > 0.5) & (order < 1.5)].sum()
+    out = []
+    for h in range(1, 400, 2):
+        win = (order > h - 0.5) & (order < h + 0.5)
+        I_ref = S_ref[win].sum()
+        if not win.any() or I_ref < 1e-12 * fund:
+            break
+        out.append(abs(S[win].sum() - I_ref) / I_ref)
+    return out
+
+
+def mixed_report(J_mixed, J_fp64, param, fp64_ms, mixed_ms):
+    import numpy as np
+
+    rel = {"vector": float(np.linalg.norm(J_mixed - J_fp64) / np.linalg.norm(J_fp64))}
+    for a, ax in enumerate("xyz"):
+        n = np.linalg.norm(J_fp64[a])
+        if n > 0:
+            rel[ax] = float(np.linalg.norm(J_mixed[a] - J_fp64[a]) / n)
+    axis = int(np.argmax([np.linalg.norm(J_fp64[a]) for a in range(3)]))
+    errs = harmonic_errors(J_mixed[axis], J_fp64[axis], param)
+    return {"J_rel_l2_vs_fp64": rel, "harmonics_checked": len(errs),
+            "harmonic_intensity_max_rel_err": max(errs) if errs else None,
+            "fp64_ms_per_solve": fp64_ms, "mixed_ms_per_solve": mixed_ms, "speedup_vs_fp64": fp64_ms / mixed_ms}
+
+
 def load_traffic(workload: str):
     path = os.path.join(REPO, "profiles", f"propagate_fp64_{workload}_traffic.json")
     if not os.path.exists(path):
@@ -314,6 +352,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"],
+                    help="mixed: FP32 Wannier sums and commutators, FP64 state / RK accumulation / k-sum")
     ap.add_argument("--grid", type=int, default=None,
                     help="override the k-grid side (profiling a smaller case of the same kernel)")
     args = ap.parse_args()
@@ -361,7 +401,7 @@ def main():
     param = workload_param(args.workload, rank, world, args.grid)
     w = WORKLOADS[args.workload]
     settings = pyswe.Settings(dict(param))
-    swe = pyswe.SWE(settings, device=local)
+    swe = pyswe.SWE(settings, device=local, precision=args.precision)
     nk = param["nr1"] * param["nr2"]
     nt = settings.nt
     nw = swe.num_orb()
@@ -411,6 +451,18 @@ def main():
                "calls": "SWESim_restart + SWESim_run_simulation + SWESim_get_current", "ms_per_step": 1e3 * e2e_s / args.steps}
 
     shape = swe.launch_shape()
+    mixed = None
+    if args.precision == "mixed" and rank == 0:
+        # Error and speed against the plain FP64 form of the same solve.
+        swe.reset()
+        swe.run_simulation()
+        J_mixed = swe.get_current()[1:]
+        ref = pyswe.SWE(pyswe.Settings(dict(param)), device=local)
+        ref.run_simulation()
+        J_fp64 = ref.get_current()[1:]
+        fp64_ms = ref.last_kernel_ms()
+        ref.delete()
+        mixed = mixed_report(J_mixed, J_fp64, param, fp64_ms, total_ms / args.steps)
     swe.delete()
     if dist is not None:
         dist.destroy_process_group()
@@ -432,13 +484,13 @@ def main():
         "higher_is_better": True,
         "scaling": "weak",
         "vs_baseline": None,
-        "dtype": "f64",
+        "dtype": "f64" if args.precision == "fp64" else "c64 commutators/Wannier sums, f64 state/RK/k-sum",
         "data": "synthetic (seeded TB model, generated by hhg-solids_b200/tbgen.py)",
         "impl": "hhg-b200",
         "config": {"workload": f"{args.workload}: {WORKLOADS[args.workload]['desc']}"
                    + (f" (grid overridden to {args.grid}x{args.grid})" if args.grid else ""),
                    "k_grid": [param["nr1"], param["nr2"]],
-                   "nt": nt, "num_orb": nw, "precision": "fp64", "parallelism": f"replicas x{world}" if world > 1 else "single",
+                   "nt": nt, "num_orb": nw, "precision": args.precision, "parallelism": f"replicas x{world}" if world > 1 else "single",
                    "l2": "flushed between timed solves (256 MiB write)", "launch": shape},
         "solves_per_hour": 3600.0 * world * args.steps / (total_ms * 1e-3),
         "roofline": {"bound": "fp64", "achieved": achieved, "peak": fp64_peak.value, "unit": "TFLOP/s",
@@ -453,6 +505,8 @@ def main():
     }
     if e2e:
         line["e2e"] = e2e
+    if mixed:
+        line["mixed_vs_fp64"] = mixed
     if world == 1 and not args.no_cpu_baseline and not args.grid:
         line["cpu_baseline"] = cpu_baseline(args.workload)
     print(json.dumps(line), flush=True)

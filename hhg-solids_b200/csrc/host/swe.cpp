@@ -139,14 +139,17 @@ struct SWESim {
   std::vector<double> t, E, A;
   std::vector<double> es;          // [nt][3][3]
   std::vector<int2> cell_n, win_n;
-  std::vector<double2> H0, Rtab, V, Q, Hd, Rd, Vd, P, T1, T2;
+  std::vector<double2> H0, Rtab, V, Q, Xbox, Vd, P, T1, T2;
+  int precision = 0;  // 0 plain FP64, 1 mixed
   int nax = 0, ax_id[3] = {0, 0, 0}, nj = 0, j_id[3] = {0, 0, 0};
 
   cudaStream_t stream = nullptr;
   int stream_device = -1;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr, evm = nullptr;
   DevBuf<int2> d_cell, d_win;
-  DevBuf<double2> d_H0, d_R, d_V, d_Q, d_Hd, d_Rd, d_Vd, d_P, d_T1, d_T2, d_rho0, d_rho, d_Jpart, d_J;
+  DevBuf<double2> d_H0, d_R, d_V, d_Q, d_Xbox, d_Vd, d_P, d_T1, d_T2, d_rho0, d_rho, d_Jpart, d_J;
+  DevBuf<float2> d_Xbox32, d_Vd32, d_P32, d_T1_32, d_T2_32;
+  hhg::GroupTables gtab{};
   DevBuf<double> d_es;
   hhg::SolveTables tab{};
   hhg::LaunchShape shape{};
@@ -169,8 +172,9 @@ struct SWESim {
   void release() {
     d_cell.release();
     d_win.release();
-    for (auto* b : {&d_H0, &d_R, &d_V, &d_Q, &d_Hd, &d_Rd, &d_Vd, &d_P, &d_T1, &d_T2, &d_rho0, &d_rho, &d_Jpart, &d_J})
+    for (auto* b : {&d_H0, &d_R, &d_V, &d_Q, &d_Xbox, &d_Vd, &d_P, &d_T1, &d_T2, &d_rho0, &d_rho, &d_Jpart, &d_J})
       b->release();
+    for (auto* b : {&d_Xbox32, &d_Vd32, &d_P32, &d_T1_32, &d_T2_32}) b->release();
     d_es.release();
     if (h_J) cudaFreeHost(h_J);
     h_J = nullptr;
@@ -413,14 +417,14 @@ void SWESim::init() {
     if (c == 0 || cell_n[c].y > b2hi) b2hi = cell_n[c].y;
   }
   const int b1n = ncell ? b1hi - b1lo + 1 : 1, b2n = ncell ? b2hi - b2lo + 1 : 1;
-  Hd.assign((size_t)b1n * b2n * nw2, make_double2(0.0, 0.0));
-  Rd.assign((size_t)nax * b1n * b2n * nw2, make_double2(0.0, 0.0));
+  // Box table [1 + nax][b1n][b2n][nw2]: H0, then the field-coupled r of each active axis.
+  Xbox.assign((size_t)(1 + nax) * b1n * b2n * nw2, make_double2(0.0, 0.0));
   for (int c = 0; c < ncell; ++c) {
     const size_t box = (size_t)(cell_n[c].x - b1lo) * b2n + (cell_n[c].y - b2lo);
     for (int o = 0; o < nw2; ++o) {
-      Hd[box * nw2 + o] = H0[(size_t)c * nw2 + o];
+      Xbox[box * nw2 + o] = H0[(size_t)c * nw2 + o];
       for (int a = 0; a < nax; ++a)
-        Rd[((size_t)a * b1n * b2n + box) * nw2 + o] = Rtab[((size_t)a * ncell + c) * nw2 + o];
+        Xbox[((size_t)(1 + a) * b1n * b2n + box) * nw2 + o] = Rtab[((size_t)a * ncell + c) * nw2 + o];
     }
   }
   // e^{i n A(t_i).a_1}, e^{i n A(t_i).a_2} for |n| <= np.
@@ -474,8 +478,8 @@ void SWESim::init() {
   trace.mark("tables");
   // Device tables.
   h2d_bytes = sizeof(int2) * (cell_n.size() + win_n.size()) +
-              sizeof(double2) * (H0.size() + Rtab.size() + V.size() + Q.size() + Hd.size() + Rd.size() + Vd.size() +
-                                 P.size() + T1.size() + T2.size()) +
+              sizeof(double2) * (H0.size() + Rtab.size() + V.size() + Q.size() + Xbox.size() + Vd.size() + P.size() +
+                                 T1.size() + T2.size()) +
               sizeof(double) * es.size();
   d_cell.upload(cell_n, stream);
   d_win.upload(win_n, stream);
@@ -483,13 +487,29 @@ void SWESim::init() {
   d_R.upload(Rtab, stream);
   d_V.upload(V, stream);
   d_Q.upload(Q, stream);
-  d_Hd.upload(Hd, stream);
-  d_Rd.upload(Rd, stream);
+  d_Xbox.upload(Xbox, stream);
   d_Vd.upload(Vd, stream);
   d_P.upload(P, stream);
   d_T1.upload(T1, stream);
   d_T2.upload(T2, stream);
   d_es.upload(es, stream);
+  if (precision == 1) {
+    // FP32 copies for the mixed form (Wannier sums and commutators in complex FP32).
+    auto to32 = [](const std::vector<double2>& v) {
+      std::vector<float2> o(v.size());
+      for (size_t q = 0; q < v.size(); ++q) o[q] = make_float2((float)v[q].x, (float)v[q].y);
+      return o;
+    };
+    d_Xbox32.upload(to32(Xbox), stream);
+    d_Vd32.upload(to32(Vd), stream);
+    d_P32.upload(to32(P), stream);
+    d_T1_32.upload(to32(T1), stream);
+    d_T2_32.upload(to32(T2), stream);
+    h2d_bytes += sizeof(float2) * (Xbox.size() + Vd.size() + P.size() + T1.size() + T2.size());
+    check_cuda(cudaStreamSynchronize(stream), "H2D");  // the host vectors above are temporaries
+  }
+  gtab = hhg::GroupTables{d_Xbox.p, d_Vd.p, d_P.p, d_T1.p, d_T2.p,
+                          d_Xbox32.p, d_Vd32.p, d_P32.p, d_T1_32.p, d_T2_32.p};
   d_rho0.alloc((size_t)Nk * nw2);
   d_rho.alloc((size_t)Nk * nw2);
   d_J.alloc((size_t)3 * nt);
@@ -521,10 +541,6 @@ void SWESim::init() {
   tab.win_n = d_win.p;
   tab.V = d_V.p;
   tab.Q = d_Q.p;
-  tab.Hd = d_Hd.p;
-  tab.Rd = d_Rd.p;
-  tab.Vd = d_Vd.p;
-  tab.P = d_P.p;
   tab.T1 = d_T1.p;
   tab.T2 = d_T2.p;
 
@@ -532,7 +548,7 @@ void SWESim::init() {
   check_cuda(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device), "cudaDeviceGetAttribute");
   char why[256] = {0};
   trace.mark("upload");
-  if (!hhg::plan_propagate(tab, sms, &shape, why, sizeof why)) throw std::runtime_error(std::string("SWESim_init: ") + why);
+  if (!hhg::plan_propagate(tab, precision, sms, &shape, why, sizeof why)) throw std::runtime_error(std::string("SWESim_init: ") + why);
   trace.mark("plan");
   d_Jpart.alloc((size_t)shape.ctas * nt * 3);
   if (!h_J || h_J_cap < (size_t)3 * nt) {
@@ -565,7 +581,7 @@ void SWESim::run() {
   check_cuda(cudaSetDevice(device), "cudaSetDevice");
   check_cuda(cudaMemsetAsync(d_Jpart.p, 0, sizeof(double2) * d_Jpart.n, stream), "memset");
   check_cuda(cudaEventRecord(ev0, stream), "event");
-  last_launches = hhg::launch_propagate_fp64(tab, shape, d_rho.p, d_Jpart.p, d_J.p, stream, evm);
+  last_launches = hhg::launch_propagate(tab, gtab, shape, d_rho.p, d_Jpart.p, d_J.p, stream, evm);
   check_cuda(cudaGetLastError(), "propagate launch");
   check_cuda(cudaEventRecord(ev1, stream), "event");
   check_cuda(cudaMemcpyAsync(h_J, d_J.p, sizeof(double2) * 3 * (size_t)nt, cudaMemcpyDeviceToHost, stream), "D2H");
@@ -806,6 +822,13 @@ void SWESim_get_fields(SWESim* swe, double* t, double* E, double* A) {
   });
 }
 
+void SWESim_set_precision(SWESim* swe, int mode) {
+  guarded(swe, "SWESim_set_precision", [&] {
+    if (mode != 0 && mode != 1) throw std::runtime_error("SWESim_set_precision: mode must be 0 (plain FP64) or 1 (mixed)");
+    swe->precision = mode;
+  });
+}
+
 void SWESim_set_k_rows(SWESim* swe, int row0, int row1) {
   guarded(swe, "SWESim_set_k_rows", [&] {
     swe->req_row0 = row0;
@@ -823,7 +846,7 @@ int SWESim_run_simulation_noalloc(SWESim* swe, hhg_cdouble* rho_k, hhg_cdouble* 
     if (!rho_k || !current) throw std::runtime_error("SWESim_run_simulation_noalloc: null rho_k or current pointer");
     check_cuda(cudaSetDevice(swe->device), "cudaSetDevice");
     char why[512] = {0};
-    if (hhg::propagate_fp64_static_scratch(swe->tab, swe->shape, reinterpret_cast<double2*>(rho_k),
+    if (hhg::propagate_static_scratch(swe->tab, swe->gtab, swe->shape, reinterpret_cast<double2*>(rho_k),
                                            reinterpret_cast<double2*>(current), static_cast<cudaStream_t>(stream), why,
                                            sizeof why) != 0)
       throw std::runtime_error(std::string("SWESim_run_simulation_noalloc: ") + why);

@@ -32,8 +32,8 @@ void* g_scratch_address[kMaxDevices] = {};
 
 size_t static_scratch_capacity() { return kStaticScratchBytes; }
 
-int propagate_fp64_static_scratch(const SolveTables& t, const LaunchShape& s, double2* rho, double2* J,
-                                  cudaStream_t stream, char* why, int why_len) {
+int propagate_static_scratch(const SolveTables& t, const GroupTables& gt, const LaunchShape& s, double2* rho,
+                             double2* J, cudaStream_t stream, char* why, int why_len) {
   int dev = -1;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess || dev < 0 || dev >= kMaxDevices) {
@@ -68,7 +68,7 @@ int propagate_fp64_static_scratch(const SolveTables& t, const LaunchShape& s, do
     snprintf(why, why_len, "clearing the static scratch failed: %s", cudaGetErrorString(e));
     return -1;
   }
-  launch_propagate_fp64(t, s, rho, static_cast<double2*>(scratch), J, stream);
+  launch_propagate(t, gt, s, rho, static_cast<double2*>(scratch), J, stream);
   e = cudaGetLastError();
   if (e != cudaSuccess) {
     snprintf(why, why_len, "propagation launch failed: %s", cudaGetErrorString(e));

@@ -30,42 +30,52 @@ struct SolveTables {
   const double2* V;     // [nj][nwin][nw2] velocity on the window cells
   const double2* Q;     // [nt][ncell + nwin] Peierls phase e^{i A(t_i).R_c} of each listed cell
 
-  // Dense separable form (element-group kernel): bounding box of the occupied cells.
+  // Bounding box of the occupied cells (element-group kernel, tables in GroupTables).
   int b1lo, b1n, b2lo, b2n;
-  const double2* Hd;    // [b1n][b2n][nw2]
-  const double2* Rd;    // [nax][b1n][b2n][nw2]
-  const double2* Vd;    // [nj][4][4][nw2]  (window n1, n2 in -2..1)
-  int np;               // |n| range of the P table
-  const double2* P;     // [nt][2][2np+1]: e^{i n A(t_i).a_1}, e^{i n A(t_i).a_2}, n in [-np, np]
+  int np;               // |n| range of the P tables
 
   const double2* T1;    // [N1] e^{-2 pi i m/N1}
   const double2* T2;    // [N2] e^{-2 pi i m/N2}
 };
 
+// Tables of the element-group kernel in both precisions: box [1+nax][b1n][b2n][nw2] (H0 then the
+// field-coupled r), window velocity [nj][4][4][nw2], P [nt][2][2np+1] = e^{i n A(t_i).a_1|2}, twiddles.
+struct GroupTables {
+  const double2 *Xbox64, *Xwin64, *P64, *T1_64, *T2_64;
+  const float2 *Xbox32, *Xwin32, *P32, *T1_32, *T2_32;
+};
+
 struct LaunchShape {
-  int kernel;      // 0: thread per k-point (nw <= 2, Hermitian); 1: element groups
+  int kernel;      // 0: thread per k-point (FP64, nw <= 2, Hermitian); 1: element groups FP64; 2: element groups mixed
   int k_per_cta;   // k-points per CTA
   int group;       // threads per k-point
   int threads;     // threads per CTA
   int ctas;        // grid size (persistent CTAs)
   int ntiles;      // work tiles
+  int box_sm, win_sm;  // element groups: cell tables staged in shared memory
+  int ept;             // element groups: matrix elements per thread
+  int variant;         // element groups: compiled shape (-1: runtime-shaped instance)
   size_t smem;     // dynamic shared memory bytes
 };
 
 // Picks kernel and launch shape for a solve on the current device; false (with a reason) if it
-// cannot run it.
-bool plan_propagate(const SolveTables& t, int sm_count, LaunchShape* out, char* why, int why_len);
+// cannot run it.  precision 0: plain FP64; 1: mixed (FP32 commutators and Wannier sums, FP64 state,
+// RK accumulation and current sum).
+bool plan_propagate(const SolveTables& t, int precision, int sm_count, LaunchShape* out, char* why, int why_len);
+bool plan_group(const SolveTables& t, int precision, int sm_count, LaunchShape* out, char* why, int why_len);
+void launch_group(const SolveTables& t, const GroupTables& gt, const LaunchShape& s, double2* rho, double2* Jpart,
+                  cudaStream_t stream);
 
 // rho[Nk][nw2] in/out (k-space, W gauge). Jpart[ctas][nt][3] is accumulated (zero it first);
 // J[3][nt] receives the reduced, 1/Nk-normalised current.  Returns the number of launches.
 // If `after_propagate` is non-null it is recorded between the propagation and the reduction.
-int launch_propagate_fp64(const SolveTables& t, const LaunchShape& s, double2* rho, double2* Jpart, double2* J,
-                          cudaStream_t stream, cudaEvent_t after_propagate = nullptr);
+int launch_propagate(const SolveTables& t, const GroupTables& gt, const LaunchShape& s, double2* rho, double2* Jpart,
+                     double2* J, cudaStream_t stream, cudaEvent_t after_propagate = nullptr);
 
-// Same as launch_propagate_fp64, with the current partials in a fixed device array owned by the
+// Same as launch_propagate, with the current partials in a fixed device array owned by the
 // library instead of a caller buffer (see noalloc.cu).  Returns 0, or -1 with a reason in `why`.
-int propagate_fp64_static_scratch(const SolveTables& t, const LaunchShape& s, double2* rho, double2* J,
-                                  cudaStream_t stream, char* why, int why_len);
+int propagate_static_scratch(const SolveTables& t, const GroupTables& gt, const LaunchShape& s, double2* rho,
+                             double2* J, cudaStream_t stream, char* why, int why_len);
 size_t static_scratch_capacity();
 
 // rho0(k) = U f U^+ of H(k) = sum_cells e^{-ik.R} H0 (no field), one warp per k-point.

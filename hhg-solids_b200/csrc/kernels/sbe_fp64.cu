@@ -16,11 +16,7 @@
 //
 // propagate_kpt_kernel<NW>  (nw <= 2, Hermitian placement): one thread per k-point, the whole
 //   state in registers; per-cell phases e^{-ik.R_c} (per thread, fixed) x e^{iA.R_c} (per step).
-// propagate_group_kernel    (any nw <= 16): a k-point is a group of G threads, thread e owning
-//   element e = i*nw + j.  A CTA holds k-points of one k-grid column m2, which share
-//   G(n1) = sum_n2 e^{-i(k2 - A).a2 n2} X(n1, n2): the Wannier sum is computed separably, the
-//   inner half once per CTA and step.  [H, X] = HX - (HX)^+ for Hermitian placements (one nw^3
-//   product per stage), HX - XH otherwise.
+// propagate_group_kernel    (any nw <= 16, FP64 or mixed precision): in sbe_group.cu.
 #include <cstdio>
 #include <cstring>
 
@@ -74,11 +70,12 @@ __device__ __forceinline__ void flush_current(const SolveTables& t, const double
 
 constexpr int kKptMaxThreads = 512;
 
-template <int NW>
+// NAXc, NJc: field axes and current axes fixed at compile time (0: read from t).
+template <int NW, int NAXc, int NJc>
 __global__ void __launch_bounds__(kKptMaxThreads) propagate_kpt_kernel(SolveTables t, double2* rho, double2* Jpart) {
   constexpr int NW2 = NW * NW;
   extern __shared__ __align__(16) unsigned char smraw[];
-  const int nc = t.ncell, nwn = t.nwin, ncw = nc + nwn, nax = t.nax, nj = t.nj;
+  const int nc = t.ncell, nwn = t.nwin, ncw = nc + nwn, nax = NAXc ? NAXc : t.nax, nj = NJc ? NJc : t.nj;
   const int nthr = blockDim.x, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarps = nthr >> 5;
   double2* sH = reinterpret_cast<double2*>(smraw);  // [nc][NW2]
   double2* sR = sH + nc * NW2;                      // [nax][nc][NW2]
@@ -256,239 +253,6 @@ __global__ void __launch_bounds__(kKptMaxThreads) propagate_kpt_kernel(SolveTabl
   }
 }
 
-// ------------------------------------------------------------------ element groups (any nw)
-
-constexpr int kGroupMaxThreads = 640;
-
-__device__ __forceinline__ void group_sync(int g, int G) {
-  if (G <= 32) {
-    __syncwarp();
-  } else {
-    asm volatile("bar.sync %0, %1;" ::"r"(1 + g), "r"(G) : "memory");
-  }
-}
-
-struct GroupSmem {
-  double2 *Hs, *Xs, *HXs;  // per group [nw2] (group-local)
-  double2 *tw1, *tw2;      // per tile twiddles: [B][W1+4], [W2+4]
-  double2 *pw1, *pw2;      // per step (x2 buffers): [2][B][W1+4], [2][W2+4]
-  double2 *Gb, *GW;        // per step (x2): [2][1+nax][W1][nw2], [2][nj][4][nw2]
-  double* sJ;              // [kRing][nwarps][2 nj]
-};
-
-__device__ __forceinline__ GroupSmem group_smem_layout(const SolveTables& t, int B, int g, unsigned char* base) {
-  GroupSmem m;
-  const int nw2 = t.nw2, W1 = t.b1n + 4, W2 = t.b2n + 4;
-  double2* p = reinterpret_cast<double2*>(base);
-  m.Hs = p + g * 3 * nw2;
-  m.Xs = m.Hs + nw2;
-  m.HXs = m.Xs + nw2;
-  p += B * 3 * nw2;
-  m.tw1 = p;
-  p += B * W1;
-  m.tw2 = p;
-  p += W2;
-  m.pw1 = p;
-  p += 2 * B * W1;
-  m.pw2 = p;
-  p += 2 * W2;
-  m.Gb = p;
-  p += 2 * (1 + t.nax) * t.b1n * nw2;
-  m.GW = p;
-  p += 2 * t.nj * 4 * nw2;
-  m.sJ = reinterpret_cast<double*>(p);
-  return m;
-}
-
-__global__ void __launch_bounds__(kGroupMaxThreads, 1) propagate_group_kernel(SolveTables t, int B, int G,
-                                                                               double2* rho, double2* Jpart) {
-  extern __shared__ __align__(16) unsigned char smraw[];
-  const int nw = t.nw, nw2 = t.nw2, nax = t.nax, nj = t.nj;
-  const int nthr = blockDim.x, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarps = (nthr + 31) >> 5;
-  const int g = tid / G, e = tid % G;
-  const bool act = e < nw2;
-  const int i = act ? e / nw : 0, j = act ? e % nw : 0;
-  const int W1n = t.b1n, W2n = t.b2n, W1 = W1n + 4, W2 = W2n + 4, nmat = 1 + nax;
-  const GroupSmem sm = group_smem_layout(t, B, g, smraw);
-  const double dt = t.dt;
-  const double prefac = 0.1666666666666 * dt;
-  const int bpc = (t.row1 - t.row0 + B - 1) / B;  // m1 blocks per column
-  const int ntiles = t.N2 * bpc;
-  const int npw = 2 * t.np + 1;
-  const int gpairs = nmat * W1n * nw2, wpairs = nj * 4 * nw2;
-  const double2 zero = make_double2(0.0, 0.0);
-
-  for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-    const int m2 = tile / bpc, m10 = t.row0 + (tile % bpc) * B;
-    const int m1 = m10 + g;
-    const bool kval = m1 < t.row1;
-    const bool own = act && kval;
-    const size_t k = (size_t)m1 * t.N2 + m2;
-    double2 r = own ? rho[k * nw2 + e] : zero;
-    // Per-tile twiddles e^{-2 pi i m n / N} of the box (then window) offsets.
-    for (int idx = tid; idx < W2; idx += nthr) {
-      const int n2 = idx < W2n ? t.b2lo + idx : idx - W2n - 2;
-      sm.tw2[idx] = t.T2[wrap_mod((long long)m2 * n2, t.N2)];
-    }
-    for (int idx = tid; idx < B * W1; idx += nthr) {
-      const int gg = idx / W1, q = idx % W1;
-      const int n1 = q < W1n ? t.b1lo + q : q - W1n - 2;
-      const int mm1 = min(m10 + gg, t.row1 - 1);
-      sm.tw1[idx] = t.T1[wrap_mod((long long)mm1 * n1, t.N1)];
-    }
-    __syncthreads();
-
-    for (int ti0 = 0; ti0 < t.nt; ti0 += kRing) {
-      const int nsteps = min(kRing, t.nt - ti0);
-      for (int s = 0; s < nsteps; ++s) {
-        const int ti = ti0 + s, buf = ti & 1;
-        const double2* P1 = t.P + (size_t)ti * 2 * npw + t.np;  // index by n
-        const double2* P2 = P1 + npw;
-        double2* pw1 = sm.pw1 + buf * B * W1;
-        double2* pw2 = sm.pw2 + buf * W2;
-        double2* Gb = sm.Gb + buf * nmat * W1n * nw2;
-        double2* GW = sm.GW + buf * nj * 4 * nw2;
-        // (1) phase factors e^{-i n (k - A).a} = twiddle x e^{i n A.a}
-        for (int idx = tid; idx < W2; idx += nthr) {
-          const int n2 = idx < W2n ? t.b2lo + idx : idx - W2n - 2;
-          pw2[idx] = cmul(sm.tw2[idx], P2[n2]);
-        }
-        for (int idx = tid; idx < B * W1; idx += nthr) {
-          const int q = idx % W1;
-          const int n1 = q < W1n ? t.b1lo + q : q - W1n - 2;
-          pw1[idx] = cmul(sm.tw1[idx], P1[n1]);
-        }
-        __syncthreads();
-        // (2) inner sums over n2, shared by the CTA's k-points (same column m2)
-        for (int p = tid; p < gpairs + wpairs; p += nthr) {
-          double2 acc = zero;
-          if (p < gpairs) {
-            const int mat = p / (W1n * nw2), rem = p % (W1n * nw2), q1 = rem / nw2, ee = rem % nw2;
-            const double2* X = (mat == 0 ? t.Hd : t.Rd + (size_t)(mat - 1) * W1n * W2n * nw2) + (size_t)q1 * W2n * nw2 + ee;
-            // Batches of four loads in flight together.
-            for (int q0 = 0; q0 < W2n; q0 += 4) {
-              double2 xv[4];
-#pragma unroll
-              for (int q = 0; q < 4; ++q)
-                if (q0 + q < W2n) xv[q] = __ldg(X + (size_t)(q0 + q) * nw2);
-#pragma unroll
-              for (int q = 0; q < 4; ++q)
-                if (q0 + q < W2n) acc = cfma(pw2[q0 + q], xv[q], acc);
-            }
-            Gb[p] = acc;
-          } else {
-            const int pp = p - gpairs, a = pp / (4 * nw2), rem = pp % (4 * nw2), q1 = rem / nw2, ee = rem % nw2;
-            const double2* X = t.Vd + ((size_t)(a * 4 + q1) * 4) * nw2 + ee;
-            double2 xv[4];
-#pragma unroll
-            for (int q2 = 0; q2 < 4; ++q2) xv[q2] = __ldg(X + (size_t)q2 * nw2);
-#pragma unroll
-            for (int q2 = 0; q2 < 4; ++q2) acc = cfma(pw2[W2n + q2], xv[q2], acc);
-            GW[pp] = acc;
-          }
-        }
-        __syncthreads();
-        // (3) outer sums over n1 for this k-point
-        double2 h0 = zero, rk[3] = {zero, zero, zero}, wk[3] = {zero, zero, zero};
-        if (act) {
-          const double2* p1 = pw1 + g * W1;
-          for (int q1 = 0; q1 < W1n; ++q1) {
-            const double2 ph = p1[q1];
-            h0 = cfma(ph, Gb[q1 * nw2 + e], h0);
-#pragma unroll
-            for (int a = 0; a < 3; ++a)
-              if (a < nax) rk[a] = cfma(ph, Gb[((1 + a) * W1n + q1) * nw2 + e], rk[a]);
-          }
-#pragma unroll
-          for (int q1 = 0; q1 < 4; ++q1) {
-            const double2 ph = p1[W1n + q1];
-#pragma unroll
-            for (int a = 0; a < 3; ++a)
-              if (a < nj) wk[a] = cfma(ph, GW[(a * 4 + q1) * nw2 + e], wk[a]);
-          }
-        }
-        // (4) RK4 stages
-        const double* esb = t.es + (size_t)ti * 9;
-        double2 K = zero, S = zero;
-#pragma unroll 1
-        for (int st = 0; st < 4; ++st) {
-          const int f = st == 0 ? 0 : (st == 3 ? 2 : 1);
-          double2 hs = h0;
-#pragma unroll
-          for (int a = 0; a < 3; ++a)
-            if (a < nax) {
-              const double ea = esb[f * 3 + t.ax_id[a]];
-              hs.x = fma(ea, rk[a].x, hs.x);
-              hs.y = fma(ea, rk[a].y, hs.y);
-            }
-          double2 x = r;
-          if (st > 0) {
-            const double cs = (st == 3 ? 1.0 : 0.5) * dt;
-            x.x = r.x + cs * K.x;
-            x.y = r.y + cs * K.y;
-          }
-          if (act) {
-            sm.Hs[e] = hs;
-            sm.Xs[e] = x;
-          }
-          group_sync(g, G);
-          double2 hx = zero;
-          if (t.hermitian) {
-            if (act) {
-              for (int l = 0; l < nw; ++l) hx = cfma(sm.Hs[i * nw + l], sm.Xs[l * nw + j], hx);
-              sm.HXs[e] = hx;
-            }
-            group_sync(g, G);
-            if (act) {
-              const double2 ht = sm.HXs[j * nw + i];
-              K = make_double2(hx.y + ht.y, -(hx.x - ht.x));  // -i (HX - (HX)^+)
-            }
-          } else {
-            double2 xh = zero;
-            if (act) {
-              for (int l = 0; l < nw; ++l) {
-                hx = cfma(sm.Hs[i * nw + l], sm.Xs[l * nw + j], hx);
-                xh = cfma(sm.Xs[i * nw + l], sm.Hs[l * nw + j], xh);
-              }
-              K = make_double2(hx.y - xh.y, -(hx.x - xh.x));  // -i (HX - XH)
-            }
-            group_sync(g, G);
-          }
-          if (st == 0) {
-            S = K;
-          } else {
-            const double wgt = st == 3 ? 1.0 : 2.0;
-            S.x += wgt * K.x;
-            S.y += wgt * K.y;
-          }
-        }
-        r.x = r.x + prefac * S.x;
-        r.y = r.y + prefac * S.y;
-        // (5) current partials
-#pragma unroll
-        for (int a = 0; a < 3; ++a)
-          if (a < nj) {
-            double re = 0.0, im = 0.0;
-            if (own) {
-              re = fma(wk[a].x, r.x, wk[a].y * r.y);
-              im = fma(wk[a].y, r.x, -wk[a].x * r.y);
-            }
-            re = warp_sum(re);
-            im = warp_sum(im);
-            if (lane == 0) {
-              sm.sJ[(s * nwarps + warp) * 2 * nj + 2 * a] = re;
-              sm.sJ[(s * nwarps + warp) * 2 * nj + 2 * a + 1] = im;
-            }
-          }
-      }
-      __syncthreads();
-      flush_current(t, sm.sJ, nwarps, ti0, nsteps, Jpart);
-    }
-    if (own) rho[k * nw2 + e] = r;
-    __syncthreads();
-  }
-}
-
 // J[a][ti] = (1/Nk) sum_cta Jpart[cta][ti][a], summed in CTA order.
 __global__ void reduce_current_kernel(const double2* Jpart, int ctas, int nt, double inv_nk, double2* J) {
   const int idx = blockIdx.x * blockDim.x + threadIdx.x;
@@ -650,18 +414,17 @@ size_t kpt_smem(const SolveTables& t, int threads) {
   return n2 * sizeof(double2) + sizeof(double) * (kRing * 9 + kRing * (threads / 32) * 2 * t.nj);
 }
 
-size_t group_smem(const SolveTables& t, int B, int G) {
-  const int W1 = t.b1n + 4, W2 = t.b2n + 4, nwarps = (B * G + 31) / 32;
-  const size_t n2 = (size_t)B * 3 * t.nw2 + (size_t)B * W1 + W2 + 2 * (size_t)B * W1 + 2 * W2 +
-                    2 * (size_t)(1 + t.nax) * t.b1n * t.nw2 + 2 * (size_t)t.nj * 4 * t.nw2;
-  return n2 * sizeof(double2) + sizeof(double) * (size_t)kRing * nwarps * 2 * t.nj;
+using KptKernel = void (*)(SolveTables, double2*, double2*);
+KptKernel kpt_kernel_for(const SolveTables& t) {
+  if (t.nw == 2 && t.nj == 2) {
+    if (t.nax == 1) return propagate_kpt_kernel<2, 1, 2>;
+    if (t.nax == 2) return propagate_kpt_kernel<2, 2, 2>;
+  }
+  return t.nw == 1 ? propagate_kpt_kernel<1, 0, 0> : propagate_kpt_kernel<2, 0, 0>;
 }
 
-using KptKernel = void (*)(SolveTables, double2*, double2*);
-KptKernel kpt_kernel_for(int nw) { return nw == 1 ? propagate_kpt_kernel<1> : propagate_kpt_kernel<2>; }
-
 bool plan_kpt(const SolveTables& t, int sm_count, LaunchShape* out, size_t smem_max) {
-  KptKernel kern = kpt_kernel_for(t.nw);
+  KptKernel kern = kpt_kernel_for(t);
   const long nk_local = (long)(t.row1 - t.row0) * t.N2;
   int threads = (int)((nk_local + sm_count - 1) / sm_count);
   threads = (threads + 31) / 32 * 32;
@@ -685,76 +448,33 @@ bool plan_kpt(const SolveTables& t, int sm_count, LaunchShape* out, size_t smem_
   out->threads = threads;
   out->ntiles = (int)ntiles;
   out->ctas = (int)(ntiles < slots ? ntiles : slots);
+  out->box_sm = out->win_sm = 0;
+  out->ept = 1;
+  out->variant = -1;
   out->smem = kpt_smem(t, threads);
   return true;
 }
 
 }  // namespace
 
-bool plan_propagate(const SolveTables& t, int sm_count, LaunchShape* out, char* why, int why_len) {
+bool plan_propagate(const SolveTables& t, int precision, int sm_count, LaunchShape* out, char* why, int why_len) {
   const size_t kSmemMax = 220 * 1024;
   if (t.nw < 1 || t.nw > kMaxOrb) {
     snprintf(why, why_len, "num_orb=%d outside the supported range 1..%d", t.nw, kMaxOrb);
     return false;
   }
-  if (t.hermitian && t.nw <= 2 && plan_kpt(t, sm_count, out, kSmemMax)) return true;
-  int G;
-  if (t.nw2 <= 32) {
-    G = 1;
-    while (G < t.nw2) G <<= 1;
-  } else {
-    G = (t.nw2 + 31) / 32 * 32;
-  }
-  const int step = G < 32 ? 32 / G : 1;  // whole warps per CTA
-  int Bmax = kGroupMaxThreads / G;
-  if (G > 32 && Bmax > 15) Bmax = 15;  // one named barrier per group, ids 1..15
-  Bmax = Bmax / step * step;
-  while (Bmax > step && group_smem(t, Bmax, G) > kSmemMax) Bmax -= step;
-  if (Bmax < 1 || group_smem(t, Bmax, G) > kSmemMax) {
-    snprintf(why, why_len, "model (%d orbitals, %dx%d cell box) does not fit in shared memory", t.nw, t.b1n, t.b2n);
-    return false;
-  }
-  cudaFuncSetAttribute(propagate_group_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)group_smem(t, Bmax, G));
-  int occ = 0;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, propagate_group_kernel, Bmax * G, group_smem(t, Bmax, G));
-  if (occ < 1) occ = 1;
-  const long slots = (long)occ * sm_count;
-  // B (k-points per CTA) minimising rounds x (B + shared), where `shared` is the per-step work a CTA
-  // does once for its column (the inner Wannier sums) in units of one k-point's work; ties go to the
-  // larger B.
-  const double per_k = (double)t.nw2 * ((1 + t.nax) * t.b1n + 4 * t.nj + 4 * t.nw);
-  const double shared = ((double)(1 + t.nax) * t.b1n * t.b2n * t.nw2 + 16.0 * t.nj * t.nw2) / per_k;
-  int best = Bmax;
-  double best_cost = -1;
-  const int rows = t.row1 - t.row0;
-  for (int B = Bmax; B >= step; B -= step) {
-    const long ntiles = (long)t.N2 * ((rows + B - 1) / B);
-    const double cost = (double)((ntiles + slots - 1) / slots) * (B + shared);
-    if (best_cost < 0 || cost < best_cost) {
-      best_cost = cost;
-      best = B;
-    }
-  }
-  const long ntiles = (long)t.N2 * ((rows + best - 1) / best);
-  out->kernel = 1;
-  out->k_per_cta = best;
-  out->group = G;
-  out->threads = best * G;
-  out->ntiles = (int)ntiles;
-  out->ctas = (int)(ntiles < slots ? ntiles : slots);
-  out->smem = group_smem(t, best, G);
-  return true;
+  if (precision == 0 && t.hermitian && t.nw <= 2 && plan_kpt(t, sm_count, out, kSmemMax)) return true;
+  return plan_group(t, precision, sm_count, out, why, why_len);
 }
 
-int launch_propagate_fp64(const SolveTables& t, const LaunchShape& s, double2* rho, double2* Jpart, double2* J,
-                          cudaStream_t stream, cudaEvent_t after_propagate) {
+int launch_propagate(const SolveTables& t, const GroupTables& gt, const LaunchShape& s, double2* rho, double2* Jpart,
+                     double2* J, cudaStream_t stream, cudaEvent_t after_propagate) {
   if (s.kernel == 0) {
-    KptKernel kern = kpt_kernel_for(t.nw);
+    KptKernel kern = kpt_kernel_for(t);
     cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s.smem);
     kern<<<s.ctas, s.threads, s.smem, stream>>>(t, rho, Jpart);
   } else {
-    cudaFuncSetAttribute(propagate_group_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s.smem);
-    propagate_group_kernel<<<s.ctas, s.threads, s.smem, stream>>>(t, s.k_per_cta, s.group, rho, Jpart);
+    launch_group(t, gt, s, rho, Jpart, stream);
   }
   if (after_propagate) cudaEventRecord(after_propagate, stream);
   const int n = 3 * t.nt;

@@ -1,0 +1,691 @@
+// Element-group SBE propagation kernel for any nw <= 16, in two precisions.
+//
+// Same propagation as the kernels of sbe_fp64.cu (k-space-resident RK4 of the reference's
+// src/solver.cpp:86-181 and the windowed current of src/observable.cpp:16-30); this file holds the
+// layout used for larger orbital counts:
+//
+//  * a k-point is a group of G threads, thread e owning matrix element e = i*nw + j; a CTA holds
+//    B k-points of one k-grid column m2 (rows m1 = m10 .. m10+B-1);
+//  * the Wannier sum is separable: H_s(k) = sum_n1 p1(k, n1) G(n1), G(n1) = sum_n2 p2(n2) X(n1, n2)
+//    with p_a = e^{-i n (2 pi m_a / N_a - A(t).a_a)}; the inner sums G depend only on the column and
+//    the step, so the CTA computes them once for its B k-points.  For Hermitian placements with a
+//    symmetric cell box only the rows n1 >= 0 are summed: G(-n1) = G(n1)^+.
+//  * G for step t+1 is computed during step t into the other half of a double buffer, so each step
+//    needs one CTA barrier; the phase factors of step t+2 are prepared two steps ahead in a
+//    three-slot ring.
+//  * the constant cell tables are copied to shared memory once per launch when they fit.
+//
+// Precision.  Real = double: everything FP64 (the plain form).  Real = float (the mixed form): the
+// Wannier sums of H0 and r, the field coupling and the RK4 commutators in complex FP32; the state rho,
+// the RK4 accumulation rho + dt/6 (k1 + 2 k2 + 2 k3 + k4), the windowed velocity sum and the
+// current's k-sum stay in FP64.
+#include <cstdio>
+#include <cstdlib>
+
+#include "sbe_device.h"
+
+namespace hhg {
+namespace {
+
+template <typename Real>
+struct Cx;
+template <>
+struct Cx<double> {
+  using T = double2;
+  static __device__ __forceinline__ T make(double a, double b) { return make_double2(a, b); }
+};
+template <>
+struct Cx<float> {
+  using T = float2;
+  static __device__ __forceinline__ T make(float a, float b) { return make_float2(a, b); }
+};
+
+__device__ __forceinline__ double2 mul(double2 a, double2 b) {
+  return make_double2(fma(a.x, b.x, -a.y * b.y), fma(a.x, b.y, a.y * b.x));
+}
+__device__ __forceinline__ float2 mul(float2 a, float2 b) {
+  return make_float2(fmaf(a.x, b.x, -a.y * b.y), fmaf(a.x, b.y, a.y * b.x));
+}
+__device__ __forceinline__ double2 fmac(double2 a, double2 b, double2 c) {
+  c.x = fma(a.x, b.x, c.x);
+  c.x = fma(-a.y, b.y, c.x);
+  c.y = fma(a.x, b.y, c.y);
+  c.y = fma(a.y, b.x, c.y);
+  return c;
+}
+__device__ __forceinline__ float2 fmac(float2 a, float2 b, float2 c) {
+  c.x = fmaf(a.x, b.x, c.x);
+  c.x = fmaf(-a.y, b.y, c.x);
+  c.y = fmaf(a.x, b.y, c.y);
+  c.y = fmaf(a.y, b.x, c.y);
+  return c;
+}
+template <typename V>
+__device__ __forceinline__ V conjugate(V a) {
+  a.y = -a.y;
+  return a;
+}
+template <typename V>
+__device__ __forceinline__ V add(V a, V b) {
+  a.x += b.x;
+  a.y += b.y;
+  return a;
+}
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+__device__ __forceinline__ int wrap_mod(long long x, int n) {
+  int r = (int)(x % n);
+  return r < 0 ? r + n : r;
+}
+
+__device__ __forceinline__ void group_sync(int g, int G) {
+  if (G <= 32) {
+    __syncwarp();
+  } else {
+    asm volatile("bar.sync %0, %1;" ::"r"(1 + g), "r"(G) : "memory");
+  }
+}
+
+// Upper bound on threads per CTA: 640 (96 registers per thread) with one element per thread, 512
+// (128 registers) with two.
+template <int EPT>
+constexpr int group_threads() {
+  return EPT == 1 ? 640 : 512;
+}
+constexpr int kJRing = 16;          // steps per current-partial flush
+
+// Geometry shared by host planning and the kernel.
+struct GroupGeom {
+  int W1n, W2n;   // cell box
+  int q1s;        // first box row summed (n1 = 0 row when halving, else 0)
+  int nq1;        // box rows summed
+  int nmat;       // 1 + nax (H0 and field-coupled r)
+  int nbrows;     // nmat * nq1
+  int nwrows;     // nj * 4 window rows
+  int half;       // Hermitian halving of the box rows
+};
+
+__host__ __device__ inline GroupGeom group_geom(const SolveTables& t) {
+  GroupGeom g;
+  g.W1n = t.b1n;
+  g.W2n = t.b2n;
+  g.nmat = 1 + t.nax;
+  g.half = t.hermitian && (t.b1lo == -(t.b1n - 1) / 2) && (t.b1n % 2 == 1) && (t.b2lo == -(t.b2n - 1) / 2) &&
+           (t.b2n % 2 == 1);
+  g.q1s = g.half ? (t.b1n - 1) / 2 : 0;
+  g.nq1 = t.b1n - g.q1s;
+  g.nbrows = g.nmat * g.nq1;
+  g.nwrows = t.nj * 4;
+  return g;
+}
+
+// Shared-memory layout (element counts in units of complex Real unless noted).
+template <typename Real>
+struct GroupLayout {
+  // Offsets: first block in complex Real (box part), then a block in complex double (window part:
+  // the velocity sum feeds the current and stays FP64 in both precisions), then the current ring.
+  using V = typename Cx<Real>::T;
+  size_t groups, tw1, tw2, pw1, pw2, G, Xbox, total_cx;
+  size_t wtw1, wtw2, wpw1, wpw2, GW, Xwin, total_dcx, sJ_doubles;
+  __host__ __device__ GroupLayout(const SolveTables& t, const GroupGeom& gg, int B, int nwarps, bool box_sm,
+                                  bool win_sm) {
+    const size_t nw2 = t.nw2, W1 = gg.W1n, W2 = gg.W2n;
+    size_t p = 0;
+    groups = p;
+    p += (size_t)B * 3 * nw2;
+    tw1 = p;
+    p += (size_t)B * W1;
+    tw2 = p;
+    p += W2;
+    pw1 = p;
+    p += 3 * (size_t)B * W1;
+    pw2 = p;
+    p += 3 * W2;
+    G = p;
+    p += 2 * (size_t)gg.nbrows * nw2;
+    Xbox = p;
+    if (box_sm) p += (size_t)gg.nmat * gg.nq1 * gg.W2n * nw2;
+    total_cx = (p * sizeof(V) + 15) / 16 * 16 / sizeof(V);
+    size_t q = 0;
+    wtw1 = q;
+    q += (size_t)B * 4;
+    wtw2 = q;
+    q += 4;
+    wpw1 = q;
+    q += 3 * (size_t)B * 4;
+    wpw2 = q;
+    q += 3 * 4;
+    GW = q;
+    q += 2 * (size_t)gg.nwrows * nw2;
+    Xwin = q;
+    if (win_sm) q += (size_t)t.nj * 16 * nw2;
+    total_dcx = q;
+    sJ_doubles = 2 * (size_t)kJRing * nwarps * 2 * t.nj;
+  }
+  __host__ __device__ size_t bytes() const {
+    return total_cx * sizeof(V) + total_dcx * sizeof(double2) + sJ_doubles * sizeof(double);
+  }
+};
+
+// Per-precision device tables: box [nmat][W1n][W2n][nw2], window [nj][4][4][nw2], P [nt][2][2np+1],
+// twiddles [N1], [N2].
+template <typename Real>
+struct GroupData {
+  using V = typename Cx<Real>::T;
+  const V* Xbox;
+  const V* P;
+  const V* T1;
+  const V* T2;
+  const double2* Xwin;  // window velocity and its phases: FP64 in both precisions
+  const double2* Pd;
+  const double2* T1d;
+  const double2* T2d;
+};
+
+// NWc, NAXc, NJc: orbital count, field axes and current axes fixed at compile time (0: read from t).
+template <typename Real, int EPT, int NWc, int NAXc, int NJc>
+__global__ void __launch_bounds__(group_threads<EPT>(), 1)
+    propagate_group_kernel(SolveTables t, GroupData<Real> d, int B, int G, int box_sm, int win_sm, double2* rho,
+                           double2* Jpart) {
+  using V = typename Cx<Real>::T;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  const GroupGeom gg = group_geom(t);
+  const int nw = NWc ? NWc : t.nw, nw2 = nw * nw, nax = NAXc ? NAXc : t.nax, nj = NJc ? NJc : t.nj;
+  const int nthr = blockDim.x, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarps = (nthr + 31) >> 5;
+  const int g = tid / G, e0 = tid % G;
+  // This thread owns elements e0 + u*G, u < EPT.
+  int eu[EPT], iu[EPT], ju[EPT], eTu[EPT];
+  bool actu[EPT];
+#pragma unroll
+  for (int u = 0; u < EPT; ++u) {
+    eu[u] = e0 + u * G;
+    actu[u] = eu[u] < nw2;
+    iu[u] = actu[u] ? eu[u] / nw : 0;
+    ju[u] = actu[u] ? eu[u] % nw : 0;
+    eTu[u] = ju[u] * nw + iu[u];
+  }
+  const int W1n = gg.W1n, W2n = gg.W2n, W1 = W1n, W2 = W2n;
+  const GroupLayout<Real> L(t, gg, B, nwarps, box_sm, win_sm);
+  V* sm = reinterpret_cast<V*>(smraw);
+  double2* dsm = reinterpret_cast<double2*>(sm + L.total_cx);
+  V* Hs = sm + L.groups + (size_t)g * 3 * nw2;
+  V* Xs = Hs + nw2;
+  V* HXs = Xs + nw2;
+  V* tw1 = sm + L.tw1;
+  V* tw2 = sm + L.tw2;
+  V* pw1 = sm + L.pw1;
+  V* pw2 = sm + L.pw2;
+  V* Gb = sm + L.G;
+  double2* wtw1 = dsm + L.wtw1;
+  double2* wtw2 = dsm + L.wtw2;
+  double2* wpw1 = dsm + L.wpw1;
+  double2* wpw2 = dsm + L.wpw2;
+  double2* GWb = dsm + L.GW;
+  const V* Xbox = box_sm ? sm + L.Xbox : d.Xbox;
+  const double2* Xwin = win_sm ? dsm + L.Xwin : d.Xwin;
+  double* sJ = reinterpret_cast<double*>(dsm + L.total_dcx);
+  const int npw = 2 * t.np + 1;
+  const double dt = t.dt;
+  const double prefac = 0.1666666666666 * dt;
+  const int rows = t.row1 - t.row0;
+  const int bpc = (rows + B - 1) / B;
+  const int ntiles = t.N2 * bpc;
+  const V vzero = Cx<Real>::make(0, 0);
+  const size_t gbuf = (size_t)gg.nbrows * nw2, wbuf = (size_t)gg.nwrows * nw2;
+
+  // Constant tables into shared memory (once per launch).
+  if (box_sm) {
+    const size_t n = (size_t)gg.nq1 * W2n * nw2;
+    for (int mat = 0; mat < gg.nmat; ++mat)
+      for (size_t idx = tid; idx < n; idx += nthr)
+        sm[L.Xbox + mat * n + idx] = d.Xbox[((size_t)mat * W1n + gg.q1s) * W2n * nw2 + idx];
+  }
+  if (win_sm)
+    for (size_t idx = tid; idx < (size_t)nj * 16 * nw2; idx += nthr) dsm[L.Xwin + idx] = d.Xwin[idx];
+
+  for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    const int m2 = tile / bpc, m10 = t.row0 + (tile % bpc) * B;
+    const int m1 = m10 + g;
+    const bool kval = m1 < t.row1;
+    const size_t k = (size_t)m1 * t.N2 + m2;
+    bool own[EPT];
+    double2 r[EPT];
+#pragma unroll
+    for (int u = 0; u < EPT; ++u) {
+      own[u] = actu[u] && kval;
+      r[u] = own[u] ? rho[k * nw2 + eu[u]] : make_double2(0.0, 0.0);
+    }
+
+    // Twiddles e^{-2 pi i m n / N} of the box offsets, and (FP64) of the window offsets -2..1.
+    for (int idx = tid; idx < W2; idx += nthr) tw2[idx] = d.T2[wrap_mod((long long)m2 * (t.b2lo + idx), t.N2)];
+    for (int idx = tid; idx < B * W1; idx += nthr) {
+      const int gq = idx / W1, q = idx % W1;
+      tw1[idx] = d.T1[wrap_mod((long long)min(m10 + gq, t.row1 - 1) * (t.b1lo + q), t.N1)];
+    }
+    for (int idx = tid; idx < 4; idx += nthr) wtw2[idx] = d.T2d[wrap_mod((long long)m2 * (idx - 2), t.N2)];
+    for (int idx = tid; idx < B * 4; idx += nthr) {
+      const int gq = idx / 4, q = idx % 4;
+      wtw1[idx] = d.T1d[wrap_mod((long long)min(m10 + gq, t.row1 - 1) * (q - 2), t.N1)];
+    }
+    __syncthreads();
+
+    // Phase factors of step s into ring slot s % 3: p = twiddle x e^{i n A(t_s).a}.
+    auto make_phases = [&](int s) {
+      const V* P1 = d.P + (size_t)s * 2 * npw + t.np;
+      const V* P2 = P1 + npw;
+      const double2* P1d = d.Pd + (size_t)s * 2 * npw + t.np;
+      const double2* P2d = P1d + npw;
+      V* q2 = pw2 + (s % 3) * W2;
+      V* q1 = pw1 + (s % 3) * B * W1;
+      double2* w2 = wpw2 + (s % 3) * 4;
+      double2* w1 = wpw1 + (s % 3) * B * 4;
+      const int nA = W2, nB = nA + B * W1, nC = nB + 4, nD = nC + B * 4;
+      for (int idx = tid; idx < nD; idx += nthr) {
+        if (idx < nA) {
+          q2[idx] = mul(tw2[idx], P2[t.b2lo + idx]);
+        } else if (idx < nB) {
+          const int id1 = idx - nA;
+          q1[id1] = mul(tw1[id1], P1[t.b1lo + id1 % W1]);
+        } else if (idx < nC) {
+          const int q = idx - nB;
+          w2[q] = mul(wtw2[q], P2d[q - 2]);
+        } else {
+          const int id1 = idx - nC;
+          w1[id1] = mul(wtw1[id1], P1d[id1 % 4 - 2]);
+        }
+      }
+    };
+    // Inner sums of step s into buffer s & 1 (rows assigned to groups, elements to threads).
+    auto inner_sums = [&](int s) {
+      const V* q2 = pw2 + (s % 3) * W2;
+      const double2* w2 = wpw2 + (s % 3) * 4;
+      V* Gd = Gb + (s & 1) * gbuf;
+      double2* GWd = GWb + (s & 1) * wbuf;
+      for (int row = g; row < gg.nbrows + gg.nwrows; row += B) {
+        if (row < gg.nbrows) {
+          const int mat = row / gg.nq1, qq = row % gg.nq1;
+          const V* X = box_sm ? Xbox + (((size_t)mat * gg.nq1 + qq) * W2n) * nw2
+                              : Xbox + (((size_t)mat * W1n + gg.q1s + qq) * W2n) * nw2;
+          V acc[EPT];
+#pragma unroll
+          for (int u = 0; u < EPT; ++u) acc[u] = vzero;
+          for (int q0 = 0; q0 < W2n; q0 += 4) {
+            V xv[4][EPT];
+#pragma unroll
+            for (int q = 0; q < 4; ++q)
+#pragma unroll
+              for (int u = 0; u < EPT; ++u)
+                if (q0 + q < W2n && actu[u]) xv[q][u] = X[(size_t)(q0 + q) * nw2 + eu[u]];
+#pragma unroll
+            for (int q = 0; q < 4; ++q)
+#pragma unroll
+              for (int u = 0; u < EPT; ++u)
+                if (q0 + q < W2n && actu[u]) acc[u] = fmac(q2[q0 + q], xv[q][u], acc[u]);
+          }
+#pragma unroll
+          for (int u = 0; u < EPT; ++u)
+            if (actu[u]) Gd[(size_t)row * nw2 + eu[u]] = acc[u];
+        } else {
+          const int wr = row - gg.nbrows;  // a * 4 + q1
+          const double2* X = Xwin + (size_t)wr * 4 * nw2;
+#pragma unroll
+          for (int u = 0; u < EPT; ++u)
+            if (actu[u]) {
+              double2 xv[4], wacc = make_double2(0.0, 0.0);
+#pragma unroll
+              for (int q = 0; q < 4; ++q) xv[q] = X[(size_t)q * nw2 + eu[u]];
+#pragma unroll
+              for (int q = 0; q < 4; ++q) wacc = fmac(w2[q], xv[q], wacc);
+              GWd[(size_t)wr * nw2 + eu[u]] = wacc;
+            }
+        }
+      }
+    };
+
+    make_phases(0);
+    if (t.nt > 1) make_phases(1);
+    __syncthreads();
+    inner_sums(0);
+    __syncthreads();
+
+    for (int ti = 0; ti < t.nt; ++ti) {
+      const int buf = ti & 1;
+      // (1) outer sums over n1 for this k-point: H0(k - A), r_a(k - A), W_a(k)
+      V h0[EPT], rk[3][EPT];
+      double2 wk[3][EPT];
+#pragma unroll
+      for (int u = 0; u < EPT; ++u) {
+        h0[u] = vzero;
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+          rk[a][u] = vzero;
+          wk[a][u] = make_double2(0.0, 0.0);
+        }
+      }
+      {
+        const V* p1 = pw1 + (ti % 3) * B * W1 + g * W1;
+        const V* Gd = Gb + buf * gbuf;
+        for (int q1 = 0; q1 < W1n; ++q1) {
+          const V ph = p1[q1];
+          const bool neg = q1 < gg.q1s;  // G(-n1) = G(n1)^+
+          const int row = neg ? (W1n - 1 - q1) - gg.q1s : q1 - gg.q1s;
+#pragma unroll
+          for (int u = 0; u < EPT; ++u)
+            if (actu[u]) {
+              const int el = neg ? eTu[u] : eu[u];
+              V gv = Gd[(size_t)row * nw2 + el];
+              if (neg) gv = conjugate(gv);
+              h0[u] = fmac(ph, gv, h0[u]);
+#pragma unroll
+              for (int a = 0; a < 3; ++a)
+                if (a < nax) {
+                  V rv = Gd[(size_t)((1 + a) * gg.nq1 + row) * nw2 + el];
+                  if (neg) rv = conjugate(rv);
+                  rk[a][u] = fmac(ph, rv, rk[a][u]);
+                }
+            }
+        }
+        const double2* GWd = GWb + buf * wbuf;
+        const double2* w1 = wpw1 + (ti % 3) * B * 4 + g * 4;
+#pragma unroll
+        for (int q1 = 0; q1 < 4; ++q1) {
+          const double2 ph = w1[q1];
+#pragma unroll
+          for (int u = 0; u < EPT; ++u)
+            if (actu[u])
+#pragma unroll
+              for (int a = 0; a < 3; ++a)
+                if (a < nj) wk[a][u] = fmac(ph, GWd[(size_t)(a * 4 + q1) * nw2 + eu[u]], wk[a][u]);
+        }
+      }
+      // (2) next step's phase factors and inner sums, off this step's critical path
+      if (ti + 2 < t.nt) make_phases(ti + 2);
+      if (ti + 1 < t.nt) inner_sums(ti + 1);
+
+      // (3) RK4 stages (src/solver.cpp:157-163): fields at t, t+dt/2, t+dt/2, t+dt
+      const double* esb = t.es + (size_t)ti * 9;
+      V K[EPT];
+      double2 S[EPT];
+#pragma unroll
+      for (int u = 0; u < EPT; ++u) {
+        K[u] = vzero;
+        S[u] = make_double2(0.0, 0.0);
+      }
+#pragma unroll 1
+      for (int st = 0; st < 4; ++st) {
+        const int f = st == 0 ? 0 : (st == 3 ? 2 : 1);
+        Real ea[3];
+#pragma unroll
+        for (int a = 0; a < 3; ++a) ea[a] = a < nax ? (Real)esb[f * 3 + t.ax_id[a]] : (Real)0;
+        const double cs = (st == 3 ? 1.0 : 0.5) * dt;
+#pragma unroll
+        for (int u = 0; u < EPT; ++u)
+          if (actu[u]) {
+            V hs = h0[u];
+#pragma unroll
+            for (int a = 0; a < 3; ++a)
+              if (a < nax) {
+                hs.x += ea[a] * rk[a][u].x;
+                hs.y += ea[a] * rk[a][u].y;
+              }
+            double2 x = r[u];
+            if (st > 0) {
+              x.x = r[u].x + cs * (double)K[u].x;
+              x.y = r[u].y + cs * (double)K[u].y;
+            }
+            Hs[eu[u]] = hs;
+            Xs[eu[u]] = Cx<Real>::make((Real)x.x, (Real)x.y);
+          }
+        group_sync(g, G);
+        V hx[EPT];
+        if (t.hermitian) {
+#pragma unroll
+          for (int u = 0; u < EPT; ++u) {
+            hx[u] = vzero;
+            if (actu[u]) {
+              const V* hrow = Hs + iu[u] * nw;
+              const V* xcol = Xs + ju[u];
+              V h2 = vzero;
+              int l = 0;
+#pragma unroll
+              for (; l + 1 < nw; l += 2) {
+                hx[u] = fmac(hrow[l], xcol[l * nw], hx[u]);
+                h2 = fmac(hrow[l + 1], xcol[(l + 1) * nw], h2);
+              }
+              if (l < nw) hx[u] = fmac(hrow[l], xcol[l * nw], hx[u]);
+              hx[u] = add(hx[u], h2);
+              HXs[eu[u]] = hx[u];
+            }
+          }
+          group_sync(g, G);
+#pragma unroll
+          for (int u = 0; u < EPT; ++u)
+            if (actu[u]) {
+              const V ht = HXs[eTu[u]];
+              K[u] = Cx<Real>::make(hx[u].y + ht.y, -(hx[u].x - ht.x));  // -i (HX - (HX)^+)
+            }
+        } else {
+#pragma unroll
+          for (int u = 0; u < EPT; ++u)
+            if (actu[u]) {
+              V a1 = vzero, xh = vzero;
+#pragma unroll
+              for (int l = 0; l < nw; ++l) {
+                a1 = fmac(Hs[iu[u] * nw + l], Xs[l * nw + ju[u]], a1);
+                xh = fmac(Xs[iu[u] * nw + l], Hs[l * nw + ju[u]], xh);
+              }
+              K[u] = Cx<Real>::make(a1.y - xh.y, -(a1.x - xh.x));  // -i (HX - XH)
+            }
+          group_sync(g, G);
+        }
+        const double wgt = st == 0 ? 1.0 : (st == 3 ? 1.0 : 2.0);
+#pragma unroll
+        for (int u = 0; u < EPT; ++u) {
+          if (st == 0) {
+            S[u] = make_double2((double)K[u].x, (double)K[u].y);
+          } else {
+            S[u].x += wgt * (double)K[u].x;
+            S[u].y += wgt * (double)K[u].y;
+          }
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < EPT; ++u) {
+        r[u].x = r[u].x + prefac * S[u].x;
+        r[u].y = r[u].y + prefac * S[u].y;
+      }
+
+      // (4) current partials, summed over k in FP64
+      const int slot = (ti / kJRing) & 1, s = ti % kJRing;
+#pragma unroll
+      for (int a = 0; a < 3; ++a)
+        if (a < nj) {
+          double re = 0.0, im = 0.0;
+#pragma unroll
+          for (int u = 0; u < EPT; ++u)
+            if (own[u]) {
+              const double wx = wk[a][u].x, wy = wk[a][u].y;
+              re = fma(wx, r[u].x, fma(wy, r[u].y, re));
+              im = fma(wy, r[u].x, fma(-wx, r[u].y, im));
+            }
+          re = warp_sum(re);
+          im = warp_sum(im);
+          if (lane == 0) {
+            double* dst = sJ + (((size_t)slot * kJRing + s) * nwarps + warp) * 2 * nj + 2 * a;
+            dst[0] = re;
+            dst[1] = im;
+          }
+        }
+      __syncthreads();
+      // Flush a completed ring half: the other half is being written meanwhile.
+      if (s == kJRing - 1 || ti == t.nt - 1) {
+        const int ti0 = ti - s, nsteps = s + 1;
+        const double* half = sJ + (size_t)slot * kJRing * nwarps * 2 * nj;
+        for (int idx = tid; idx < nsteps * nj; idx += nthr) {
+          const int ss = idx / nj, a = idx % nj;
+          double re = 0.0, im = 0.0;
+          for (int w = 0; w < nwarps; ++w) {
+            re += half[(ss * nwarps + w) * 2 * nj + 2 * a];
+            im += half[(ss * nwarps + w) * 2 * nj + 2 * a + 1];
+          }
+          double2* dst = Jpart + ((size_t)blockIdx.x * t.nt + ti0 + ss) * 3 + t.j_id[a];
+          const double2 old = *dst;
+          *dst = make_double2(old.x + re, old.y + im);
+        }
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < EPT; ++u)
+      if (own[u]) rho[k * nw2 + eu[u]] = r[u];
+    __syncthreads();
+  }
+}
+
+constexpr size_t kSmemMax = 220 * 1024;
+
+template <typename Real, int EPT, int NWc, int NAXc, int NJc>
+bool plan_group_t(const SolveTables& t, int sm_count, LaunchShape* out, char* why, int why_len) {
+  const GroupGeom gg = group_geom(t);
+  const int per = (t.nw2 + EPT - 1) / EPT;  // threads needed per k-point
+  int G;
+  if (per <= 32) {
+    G = 1;
+    while (G < per) G <<= 1;
+  } else {
+    G = (per + 31) / 32 * 32;
+  }
+  const int step = G < 32 ? 32 / G : 1;  // whole warps per CTA
+  int Bmax = group_threads<EPT>() / G;
+  if (G > 32 && Bmax > 15) Bmax = 15;  // one named barrier per group, ids 1..15
+  Bmax = Bmax / step * step;
+  if (Bmax < 1) {
+    snprintf(why, why_len, "num_orb=%d needs %d threads per k-point", t.nw, G);
+    return false;
+  }
+  // Shared-memory placement of the tables: both, box only, none.
+  auto bytes = [&](int B, bool bs, bool ws) {
+    return GroupLayout<Real>(t, gg, B, (B * G + 31) / 32, bs, ws).bytes();
+  };
+  int box_sm = 1, win_sm = 1;
+  while (Bmax > step && bytes(Bmax, false, false) > kSmemMax) Bmax -= step;
+  if (bytes(Bmax, false, false) > kSmemMax) {
+    snprintf(why, why_len, "model (%d orbitals, %dx%d cell box) does not fit in shared memory", t.nw, t.b1n, t.b2n);
+    return false;
+  }
+  if (bytes(Bmax, true, true) > kSmemMax) win_sm = 0;
+  if (bytes(Bmax, true, win_sm) > kSmemMax) box_sm = 0;
+  if (!box_sm && bytes(Bmax, false, true) <= kSmemMax) win_sm = 1;
+  auto kern = propagate_group_kernel<Real, EPT, NWc, NAXc, NJc>;
+  const size_t smem_max = bytes(Bmax, box_sm, win_sm);
+  cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_max);
+  int occ = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, Bmax * G, smem_max);
+  if (occ < 1) occ = 1;
+  const long slots = (long)occ * sm_count;
+  // B minimising rounds x (B + shared work in k-point units); ties to the larger B.
+  const double per_k = (double)t.nw2 * (gg.nmat * gg.W1n + 4 * t.nj + 4 * t.nw);
+  const double shared = ((double)gg.nbrows * gg.W2n * t.nw2 + 4.0 * gg.nwrows * t.nw2) / per_k;
+  const int rows = t.row1 - t.row0;
+  int best = Bmax;
+  double best_cost = -1;
+  for (int B = Bmax; B >= step; B -= step) {
+    const long ntiles = (long)t.N2 * ((rows + B - 1) / B);
+    const double cost = (double)((ntiles + slots - 1) / slots) * (B + shared);
+    if (best_cost < 0 || cost < best_cost) {
+      best_cost = cost;
+      best = B;
+    }
+  }
+  const long ntiles = (long)t.N2 * ((rows + best - 1) / best);
+  out->kernel = sizeof(Real) == 8 ? 1 : 2;
+  out->ept = EPT;
+  out->k_per_cta = best;
+  out->group = G;
+  out->threads = best * G;
+  out->ntiles = (int)ntiles;
+  out->ctas = (int)(ntiles < slots ? ntiles : slots);
+  out->box_sm = box_sm;
+  out->win_sm = win_sm;
+  out->smem = bytes(best, box_sm, win_sm);
+  return true;
+}
+
+template <typename Real, int EPT, int NWc, int NAXc, int NJc>
+void launch_group_t(const SolveTables& t, const GroupTables& gt, const LaunchShape& s, double2* rho, double2* Jpart,
+                    cudaStream_t stream) {
+  GroupData<Real> d;
+  if constexpr (sizeof(Real) == 8) {
+    d = {gt.Xbox64, gt.P64, gt.T1_64, gt.T2_64, gt.Xwin64, gt.P64, gt.T1_64, gt.T2_64};
+  } else {
+    d = {gt.Xbox32, gt.P32, gt.T1_32, gt.T2_32, gt.Xwin64, gt.P64, gt.T1_64, gt.T2_64};
+  }
+  auto kern = propagate_group_kernel<Real, EPT, NWc, NAXc, NJc>;
+  cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s.smem);
+  kern<<<s.ctas, s.threads, s.smem, stream>>>(t, d, s.k_per_cta, s.group, s.box_sm, s.win_sm, rho, Jpart);
+}
+
+// Compiled shapes: (orbitals, field axes, current axes) of the configurations this library is built
+// for, each in plain FP64 (one element per thread) and mixed precision (two elements per thread);
+// any other shape runs the runtime-shaped instance.
+using PlanFn = bool (*)(const SolveTables&, int, LaunchShape*, char*, int);
+using LaunchFn = void (*)(const SolveTables&, const GroupTables&, const LaunchShape&, double2*, double2*, cudaStream_t);
+struct GroupVariant {
+  int precision, nw, nax, nj;
+  PlanFn plan;
+  LaunchFn launch;
+};
+#define HHG_GROUP_VARIANT(P, R, E, NW, NAX, NJ) \
+  {P, NW, NAX, NJ, plan_group_t<R, E, NW, NAX, NJ>, launch_group_t<R, E, NW, NAX, NJ>}
+const GroupVariant kGroupVariants[] = {
+    HHG_GROUP_VARIANT(0, double, 1, 11, 1, 2), HHG_GROUP_VARIANT(0, double, 1, 11, 2, 2),
+    HHG_GROUP_VARIANT(0, double, 1, 12, 1, 2), HHG_GROUP_VARIANT(0, double, 1, 12, 2, 2),
+    HHG_GROUP_VARIANT(0, double, 1, 6, 1, 2),  HHG_GROUP_VARIANT(0, double, 1, 6, 2, 2),
+    HHG_GROUP_VARIANT(1, float, 2, 11, 1, 2),  HHG_GROUP_VARIANT(1, float, 2, 11, 2, 2),
+    HHG_GROUP_VARIANT(1, float, 2, 12, 1, 2),  HHG_GROUP_VARIANT(1, float, 2, 12, 2, 2),
+    HHG_GROUP_VARIANT(1, float, 1, 6, 1, 2),   HHG_GROUP_VARIANT(1, float, 1, 6, 2, 2),
+    HHG_GROUP_VARIANT(1, float, 1, 2, 1, 2),   HHG_GROUP_VARIANT(1, float, 1, 2, 2, 2),
+};
+#undef HHG_GROUP_VARIANT
+
+const GroupVariant* find_variant(const SolveTables& t, int precision) {
+  if (const char* env = std::getenv("HHG_GROUP_GENERIC"))
+    if (env[0] == '1') return nullptr;  // tuning override: runtime-shaped instance
+  for (const GroupVariant& v : kGroupVariants)
+    if (v.precision == precision && v.nw == t.nw && v.nax == t.nax && v.nj == t.nj) return &v;
+  return nullptr;
+}
+
+}  // namespace
+
+bool plan_group(const SolveTables& t, int precision, int sm_count, LaunchShape* out, char* why, int why_len) {
+  if (const GroupVariant* v = find_variant(t, precision)) {
+    out->variant = (int)(v - kGroupVariants);
+    return v->plan(t, sm_count, out, why, why_len);
+  }
+  out->variant = -1;
+  // Runtime-shaped: two elements per thread in the mixed form once a k-point needs more than a warp.
+  const bool two = precision == 1 && t.nw2 > 32;
+  if (precision == 1)
+    return two ? plan_group_t<float, 2, 0, 0, 0>(t, sm_count, out, why, why_len)
+               : plan_group_t<float, 1, 0, 0, 0>(t, sm_count, out, why, why_len);
+  return plan_group_t<double, 1, 0, 0, 0>(t, sm_count, out, why, why_len);
+}
+
+void launch_group(const SolveTables& t, const GroupTables& gt, const LaunchShape& s, double2* rho, double2* Jpart,
+                  cudaStream_t stream) {
+  if (s.variant >= 0) {
+    kGroupVariants[s.variant].launch(t, gt, s, rho, Jpart, stream);
+  } else if (s.kernel == 2) {
+    s.ept == 2 ? launch_group_t<float, 2, 0, 0, 0>(t, gt, s, rho, Jpart, stream)
+               : launch_group_t<float, 1, 0, 0, 0>(t, gt, s, rho, Jpart, stream);
+  } else {
+    launch_group_t<double, 1, 0, 0, 0>(t, gt, s, rho, Jpart, stream);
+  }
+}
+
+}  // namespace hhg

@@ -78,6 +78,7 @@ def _load(path: str):
         L.SWESim_launch_shape.argtypes = [vp] + [ct.POINTER(ct.c_int)] * 3 + [ct.POINTER(ct.c_longlong)]
         L.SWESim_reset.argtypes = [vp]
         L.SWESim_set_k_rows.argtypes = [vp, ct.c_int, ct.c_int]
+        L.SWESim_set_precision.argtypes = [vp, ct.c_int]
         L.SWESim_get_rho_k.argtypes = [vp, ND_POINTER_1_complex]
         L.SWESim_get_fields.argtypes = [vp, ND_POINTER_1_double, ND_POINTER_1_double, ND_POINTER_1_double]
     _libs[path] = (L, ext)
@@ -118,7 +119,8 @@ class Settings:
 class SWE:
     """One propagation: setup on construction (SWESim_init), then run_simulation / get_current."""
 
-    def __init__(self, settings: Settings, device: int | None = None, k_rows: tuple | None = None):
+    def __init__(self, settings: Settings, device: int | None = None, k_rows: tuple | None = None,
+                 precision: str = "fp64"):
         self.settings = settings
         self.swe_cpp, self._ext = _load(settings.path_lib)
         self.ptr = self.swe_cpp.SWESim_new()
@@ -128,6 +130,10 @@ class SWE:
             self._call("SWESim_set_device", int(device))
         if k_rows is not None:
             self._call("SWESim_set_k_rows", int(k_rows[0]), int(k_rows[1]))
+        if precision not in ("fp64", "mixed"):
+            raise SWEError(f"precision must be 'fp64' or 'mixed', not {precision!r}")
+        if precision == "mixed":
+            self._call("SWESim_set_precision", 1)
         self.set_path_tb(settings.path_tb.encode("UTF-8"))
         self.set_settings(settings.ptr)
         self.init()

@@ -91,6 +91,11 @@ long long SWESim_h2d_bytes(SWESim* swe);
 int SWESim_launch_shape(SWESim* swe, int* ctas, int* threads, int* k_per_cta, long long* smem);
 /* Number of kernel launches issued by the last SWESim_run_simulation. */
 int SWESim_last_launches(SWESim* swe);
+/* Arithmetic of the next SWESim_init: 0 = plain FP64 (default, the reference's arithmetic to
+ * 1e-10); 1 = mixed: Wannier sums, field coupling and RK4 commutators in complex FP32, the state,
+ * the RK4 accumulation and the current's k-sum in FP64 (error against plain FP64 reported by the
+ * tests and bench). */
+void SWESim_set_precision(SWESim* swe, int mode);
 /* Restrict the next SWESim_init to k-grid rows m1 in [row0, row1) (row1 = -1: to the end): one
  * slab of a solve split over several GPUs.  The current stays normalised by the full grid, so the
  * currents of a partition of the rows add up to the full current. */
