@@ -46,7 +46,86 @@ WORKLOADS = {
                desc="2-orbital Haldane-like TB (a=2.5 A, 25 R cells), 200x200 k-grid, full pulse, plain FP64"),
     "c2": dict(model="tmd11_s7", n=150, window=7,
                desc="11-orbital TMD-like TB (seed 7, 49 R cells), 150x150 k-grid, full pulse, plain FP64"),
+    "c3": dict(model=None, n=None, window=None,
+               desc="batched scan: 64 solves, nw in {2,6,11} (seeds 1-3), grids {60,100,150,200}^2, 16 angles "
+                    "0-180 deg, I in {0.5,1,1.5,2}e12, lambda in {2000,3000} nm (draws: seed 0)"),
 }
+
+
+def scan_params(n_solves: int = 64, seed: int = 0):
+    """The batched-scan draws (the BASELINE batched-scan configuration)."""
+    import numpy as np
+    import tbgen
+
+    rng = np.random.default_rng(seed)
+    models = {2: ["haldane"], 6: ["tmd6_s1", "tmd6_s2", "tmd6_s3"], 11: ["tmd11_s1", "tmd11_s2", "tmd11_s3"]}
+    out = []
+    for _ in range(n_solves):
+        nw = int(rng.choice([2, 6, 11]))
+        model = models[nw][int(rng.integers(len(models[nw])))]
+        n = int(rng.choice([60, 100, 150, 200]))
+        ang = math.radians(12.0 * int(rng.integers(16)))
+        p = dict(PULSE, nr1=n, nr2=n, nr3=1, path_tb=tbgen.model_path(model))
+        p["intensity"] = float(rng.choice([0.5e12, 1e12, 1.5e12, 2e12]))
+        p["lambda"] = float(rng.choice([2000.0, 3000.0]))
+        p["pol_vec"] = np.array([math.sin(ang), math.cos(ang), 0.0])
+        p["phi_vec"] = np.zeros(3)
+        out.append((model, nw, p))
+    return out
+
+
+def run_scan(args, local: int):
+    """Batched scan: the mixed form as one SWEBatch against the plain form as sequential solves."""
+    import numpy as np
+    from pySWE import pyswe
+
+    draws = scan_params()
+    kpts = sum(p["nr1"] * p["nr2"] for _, _, p in draws)
+    t0 = time.perf_counter()
+    mixed = [pyswe.SWE(pyswe.Settings(dict(p)), device=local, precision="mixed") for _, _, p in draws]
+    setup_s = time.perf_counter() - t0
+    nt = mixed[0].settings.nt
+    batch = pyswe.SWEBatch(mixed)
+    for _ in range(args.warmup):
+        batch.run()
+    clocks = ClockSampler(local)
+    clocks.start()
+    ms = []
+    for _ in range(args.steps):
+        batch.run()
+        ms.append(batch.last_ms())
+    clk = clocks.stop()
+    J_mixed = [s.get_current()[1:] for s in mixed]
+    batch.delete()
+    for s in mixed:
+        s.delete()
+    # Plain FP64, 64 sequential solves.
+    seq_ms, errs = 0.0, []
+    for (model, nw, p), Jm in zip(draws, J_mixed):
+        s = pyswe.SWE(pyswe.Settings(dict(p)), device=local)
+        s.run_simulation()
+        seq_ms += s.last_kernel_ms()
+        J = s.get_current()[1:]
+        errs.append(float(np.linalg.norm(Jm - J) / np.linalg.norm(J)))
+        s.delete()
+    batch_ms = statistics.mean(ms)
+    value = kpts * nt / (batch_ms * 1e-3)
+    return {
+        "metric": "k-pt*RK4-steps/s", "value": value, "unit": "k-pt*RK4-steps/s", "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": batch_ms, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "c64 commutators/Wannier sums, f64 state/RK/k-sum",
+        "data": "synthetic (seeded TB models, generated by hhg-solids_b200/tbgen.py)", "impl": "hhg-b200",
+        "config": {"workload": f"c3: {WORKLOADS['c3']['desc']}", "solves": len(draws), "k_points_total": kpts,
+                   "nt": nt, "precision": "mixed", "batch": "SWEBatch: one persistent work-stealing launch per kernel "
+                   "shape over packed (solve, virtual CTA) items, longest first, captured CUDA graph"},
+        "solves_per_hour": 3600.0 * len(draws) / (batch_ms * 1e-3),
+        "fp64_sequential": {"ms": seq_ms, "value": kpts * nt / (seq_ms * 1e-3),
+                            "solves_per_hour": 3600.0 * len(draws) / (seq_ms * 1e-3)},
+        "speedup_vs_fp64_sequential": seq_ms / batch_ms,
+        "J_rel_l2_vs_fp64": {"max": max(errs), "median": statistics.median(errs)},
+        "setup_s_64_solves": setup_s, "clocks": clk,
+    }
+
 
 
 def workload_param(name: str, rank: int = 0, world: int = 1, grid: int | None = None) -> dict:
@@ -397,6 +476,13 @@ def main():
     lib = ct.CDLL(pyswe.default_library())
     lib.HHG_measure_peaks.argtypes = [ct.POINTER(ct.c_double), ct.POINTER(ct.c_double)]
     fp64_peak, fp32_peak = ct.c_double(), ct.c_double()
+
+    if args.workload == "c3":
+        if rank == 0:
+            print(json.dumps(run_scan(args, local)), flush=True)
+        if dist is not None:
+            dist.destroy_process_group()
+        return
 
     param = workload_param(args.workload, rank, world, args.grid)
     w = WORKLOADS[args.workload]

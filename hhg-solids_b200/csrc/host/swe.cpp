@@ -141,6 +141,7 @@ struct SWESim {
   std::vector<int2> cell_n, win_n;
   std::vector<double2> H0, Rtab, V, Q, Xbox, Vd, P, T1, T2;
   int precision = 0;  // 0 plain FP64, 1 mixed
+  unsigned generation = 0;  // bumped by every successful SWESim_init (batches re-capture on change)
   int nax = 0, ax_id[3] = {0, 0, 0}, nj = 0, j_id[3] = {0, 0, 0};
 
   cudaStream_t stream = nullptr;
@@ -550,7 +551,7 @@ void SWESim::init() {
   trace.mark("upload");
   if (!hhg::plan_propagate(tab, precision, sms, &shape, why, sizeof why)) throw std::runtime_error(std::string("SWESim_init: ") + why);
   trace.mark("plan");
-  d_Jpart.alloc((size_t)shape.ctas * nt * 3);
+  d_Jpart.alloc((size_t)shape.vctas * nt * 3);
   if (!h_J || h_J_cap < (size_t)3 * nt) {
     if (h_J) cudaFreeHost(h_J);
     h_J = nullptr;
@@ -566,6 +567,7 @@ void SWESim::init() {
   check_cuda(cudaStreamSynchronize(stream), "init");
   trace.mark("rho0");
   ready = true;
+  ++generation;
 }
 
 void SWESim::reset_state() {
@@ -674,6 +676,198 @@ void SWESim::test_files() {
     });
   write_fields_files("fields");
 }
+
+// ------------------------------------------------------------------------------------- batches
+
+// Several initialised solves propagated together.  Solves that run the element-group kernel are
+// grouped by kernel shape; each group is one persistent launch whose CTAs take (solve, virtual CTA)
+// items from a packed work list (longest items first), so uneven solves share the SMs without a
+// static split.  Solves on the thread-per-k-point kernel keep their own launch on their own stream.
+// A solve keeps the tile shape and virtual-CTA split it has alone, so its current is bit for bit
+// the one it gives alone.  The launch sequence (reset to rho0, clear, propagate, reduce, copy the
+// current out) is captured once into a CUDA graph and replayed.
+struct SWEBatch {
+  int device = -1;
+  std::vector<SWESim*> sims;
+  std::vector<cudaStream_t> streams;
+  std::vector<cudaEvent_t> done;
+  cudaStream_t master = nullptr;
+  cudaEvent_t fork = nullptr, ev0 = nullptr, ev1 = nullptr;
+  cudaGraphExec_t graph = nullptr;
+  DevBuf<hhg::BatchDesc> d_desc;
+  DevBuf<int2> d_items;
+  DevBuf<int> d_counters;
+  std::vector<unsigned> generations;
+  bool dirty = true;
+  float last_ms = 0.f;
+  int groups = 0, separate = 0;
+  std::string err;
+  bool has_err = false;
+
+  ~SWEBatch() { release(); }
+  void release() {
+    if (graph) cudaGraphExecDestroy(graph);
+    graph = nullptr;
+    for (auto st : streams) cudaStreamDestroy(st);
+    streams.clear();
+    for (auto e : done) cudaEventDestroy(e);
+    done.clear();
+    for (auto* e : {&fork, &ev0, &ev1})
+      if (*e) cudaEventDestroy(*e);
+    fork = ev0 = ev1 = nullptr;
+    if (master) cudaStreamDestroy(master);
+    master = nullptr;
+  }
+
+  void prepare() {
+    if (sims.empty()) throw std::runtime_error("SWEBatch_run: empty batch");
+    for (SWESim* sim : sims)
+      if (!sim->ready) throw std::runtime_error("SWEBatch_run: a solve of the batch is not initialised");
+    device = sims[0]->device;
+    for (SWESim* sim : sims)
+      if (sim->device != device) throw std::runtime_error("SWEBatch_run: all solves of a batch must be on one device");
+    check_cuda(cudaSetDevice(device), "cudaSetDevice");
+    release();
+    int sms = 0;
+    check_cuda(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device), "cudaDeviceGetAttribute");
+
+    // Kernel-shape classes of the element-group solves; the others run alone.
+    std::map<std::tuple<int, int, int, int, int, int, int, int>, std::vector<int>> classes;
+    std::vector<int> alone;
+    for (int i = 0; i < (int)sims.size(); ++i) {
+      const hhg::LaunchShape& sh = sims[i]->shape;
+      if (sh.kernel == 0) {
+        alone.push_back(i);
+      } else {
+        const hhg::SolveTables& t = sims[i]->tab;
+        classes[std::make_tuple(sh.kernel, sh.variant, sh.ept, sh.threads, sh.group, t.nw, t.nax, t.nj)].push_back(i);
+      }
+    }
+    groups = (int)classes.size();
+    separate = (int)alone.size();
+    // Descriptors and items (per class: solves by decreasing item cost, all items of a solve).
+    std::vector<hhg::BatchDesc> descs(sims.size());
+    std::vector<int2> items;
+    std::vector<std::pair<size_t, size_t>> ranges;  // per class: [first item, end)
+    for (int i = 0; i < (int)sims.size(); ++i) {
+      SWESim* sim = sims[i];
+      hhg::BatchDesc& d = descs[i];
+      std::memset(&d, 0, sizeof d);
+      d.t = sim->tab;
+      d.gt = sim->gtab;
+      d.B = sim->shape.k_per_cta;
+      d.G = sim->shape.group;
+      d.box_sm = sim->shape.box_sm;
+      d.win_sm = sim->shape.win_sm;
+      d.vctas = sim->shape.vctas;
+      d.rho = sim->d_rho.p;
+      d.Jpart = sim->d_Jpart.p;
+    }
+    for (auto& kv : classes) {
+      std::vector<int> members = kv.second;
+      auto cost = [&](int i) {
+        const hhg::LaunchShape& sh = sims[i]->shape;
+        return (double)sh.ntiles / std::max(1, sh.vctas);  // tiles per item
+      };
+      std::stable_sort(members.begin(), members.end(), [&](int a, int b) { return cost(a) > cost(b); });
+      const size_t first = items.size();
+      for (int i : members)
+        for (int v = 0; v < sims[i]->shape.vctas; ++v) items.push_back(make_int2(i, v));
+      ranges.emplace_back(first, items.size());
+    }
+    d_desc.alloc(descs.size());
+    check_cuda(cudaMemcpy(d_desc.p, descs.data(), sizeof(hhg::BatchDesc) * descs.size(), cudaMemcpyHostToDevice), "H2D");
+    d_items.alloc(std::max<size_t>(1, items.size()));
+    if (!items.empty())
+      check_cuda(cudaMemcpy(d_items.p, items.data(), sizeof(int2) * items.size(), cudaMemcpyHostToDevice), "H2D");
+    d_counters.alloc(std::max<size_t>(1, classes.size()));
+
+    check_cuda(cudaStreamCreateWithFlags(&master, cudaStreamNonBlocking), "cudaStreamCreate");
+    for (auto* e : {&fork, &ev0, &ev1}) check_cuda(cudaEventCreate(e), "cudaEventCreate");
+    const size_t nstreams = classes.size() + alone.size();
+    streams.resize(nstreams);
+    done.resize(nstreams);
+    for (size_t q = 0; q < nstreams; ++q) {
+      check_cuda(cudaStreamCreateWithFlags(&streams[q], cudaStreamNonBlocking), "cudaStreamCreate");
+      check_cuda(cudaEventCreateWithFlags(&done[q], cudaEventDisableTiming), "cudaEventCreate");
+    }
+
+    auto reset_and_clear = [&](SWESim* sim, cudaStream_t st) {
+      check_cuda(cudaMemcpyAsync(sim->d_rho.p, sim->d_rho0.p, sizeof(double2) * (size_t)sim->Nk * sim->nw2,
+                                 cudaMemcpyDeviceToDevice, st), "D2D");
+      check_cuda(cudaMemsetAsync(sim->d_Jpart.p, 0, sizeof(double2) * (size_t)sim->shape.vctas * sim->nt * 3, st),
+                 "memset");
+    };
+    auto reduce_and_copy = [&](SWESim* sim, cudaStream_t st) {
+      hhg::launch_reduce_current(sim->d_Jpart.p, sim->shape.vctas, sim->nt, sim->Nk, sim->d_J.p, st);
+      check_cuda(cudaMemcpyAsync(sim->h_J, sim->d_J.p, sizeof(double2) * 3 * (size_t)sim->nt, cudaMemcpyDeviceToHost, st),
+                 "D2H");
+    };
+
+    cudaGraph_t g = nullptr;
+    check_cuda(cudaStreamBeginCapture(master, cudaStreamCaptureModeRelaxed), "cudaStreamBeginCapture");
+    check_cuda(cudaEventRecord(fork, master), "event");
+    size_t q = 0;
+    int ci = 0;
+    for (auto& kv : classes) {
+      cudaStream_t st = streams[q];
+      check_cuda(cudaStreamWaitEvent(st, fork, 0), "cudaStreamWaitEvent");
+      size_t smem = 0;
+      for (int i : kv.second) {
+        reset_and_clear(sims[i], st);
+        smem = std::max(smem, sims[i]->shape.smem);
+      }
+      check_cuda(cudaMemsetAsync(d_counters.p + ci, 0, sizeof(int), st), "memset");
+      const auto& rg = ranges[ci];
+      hhg::launch_group_batch(sims[kv.second[0]]->shape, d_desc.p, d_items.p + rg.first, (int)(rg.second - rg.first),
+                              d_counters.p + ci, smem, sms, st);
+      for (int i : kv.second) reduce_and_copy(sims[i], st);
+      check_cuda(cudaEventRecord(done[q], st), "event");
+      check_cuda(cudaStreamWaitEvent(master, done[q], 0), "cudaStreamWaitEvent");
+      ++q;
+      ++ci;
+    }
+    for (int i : alone) {
+      cudaStream_t st = streams[q];
+      SWESim* sim = sims[i];
+      check_cuda(cudaStreamWaitEvent(st, fork, 0), "cudaStreamWaitEvent");
+      reset_and_clear(sim, st);
+      hhg::launch_propagate(sim->tab, sim->gtab, sim->shape, sim->d_rho.p, sim->d_Jpart.p, sim->d_J.p, st);
+      check_cuda(cudaMemcpyAsync(sim->h_J, sim->d_J.p, sizeof(double2) * 3 * (size_t)sim->nt, cudaMemcpyDeviceToHost, st),
+                 "D2H");
+      check_cuda(cudaEventRecord(done[q], st), "event");
+      check_cuda(cudaStreamWaitEvent(master, done[q], 0), "cudaStreamWaitEvent");
+      ++q;
+    }
+    check_cuda(cudaStreamEndCapture(master, &g), "cudaStreamEndCapture");
+    const cudaError_t ie = cudaGraphInstantiate(&graph, g, 0);
+    cudaGraphDestroy(g);
+    check_cuda(ie, "cudaGraphInstantiate");
+    generations.clear();
+    for (SWESim* sim : sims) generations.push_back(sim->generation);
+    dirty = false;
+  }
+
+  // Every solve from its equilibrium rho0; each SWESim then holds its current as after
+  // SWESim_reset + SWESim_run_simulation.
+  void run() {
+    for (size_t i = 0; i < sims.size() && !dirty; ++i) dirty = !sims[i]->ready || generations[i] != sims[i]->generation;
+    if (dirty) prepare();
+    check_cuda(cudaSetDevice(device), "cudaSetDevice");
+    check_cuda(cudaEventRecord(ev0, master), "event");
+    check_cuda(cudaGraphLaunch(graph, master), "cudaGraphLaunch");
+    check_cuda(cudaEventRecord(ev1, master), "event");
+    check_cuda(cudaStreamSynchronize(master), "SWEBatch_run");
+    check_cuda(cudaEventElapsedTime(&last_ms, ev0, ev1), "event time");
+    for (SWESim* sim : sims) {
+      for (auto& j : sim->Jhist) j.clear();
+      for (int a = 0; a < 3; ++a)
+        for (int ti = 0; ti < sim->nt; ++ti)
+          sim->Jhist[a].push_back(cd(sim->h_J[(size_t)a * sim->nt + ti].x, sim->h_J[(size_t)a * sim->nt + ti].y));
+      sim->last_launches = 2;
+    }
+  }
+};
 
 // ------------------------------------------------------------------------------------- C ABI
 
@@ -854,6 +1048,47 @@ int SWESim_run_simulation_noalloc(SWESim* swe, hhg_cdouble* rho_k, hhg_cdouble* 
   });
   return rc;
 }
+
+SWEBatch* SWEBatch_new(void) {
+  try {
+    return new SWEBatch();
+  } catch (...) {
+    return nullptr;
+  }
+}
+
+void SWEBatch_delete(SWEBatch* b) {
+  try {
+    delete b;
+  } catch (...) {
+  }
+}
+
+int SWEBatch_add(SWEBatch* b, SWESim* swe) {
+  if (!b || !swe) return -1;
+  b->sims.push_back(swe);
+  b->dirty = true;
+  return (int)b->sims.size() - 1;
+}
+
+int SWEBatch_run(SWEBatch* b) {
+  if (!b) return -1;
+  try {
+    b->has_err = false;
+    b->run();
+    return 0;
+  } catch (const std::exception& e) {
+    b->err = e.what();
+    b->has_err = true;
+    g_last_error = b->err;
+    g_has_error = true;
+    b->dirty = true;
+    return -1;
+  }
+}
+
+double SWEBatch_last_ms(SWEBatch* b) { return b ? (double)b->last_ms : -1.0; }
+const char* SWEBatch_last_error(SWEBatch* b) { return (b && b->has_err) ? b->err.c_str() : nullptr; }
 
 int HHG_measure_peaks(double* fp64_tflops, double* fp32_tflops) {
   try {

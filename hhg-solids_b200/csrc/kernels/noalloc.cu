@@ -40,12 +40,12 @@ int propagate_static_scratch(const SolveTables& t, const GroupTables& gt, const 
     snprintf(why, why_len, "no usable current CUDA device (%s)", cudaGetErrorString(e));
     return -1;
   }
-  const size_t need = (size_t)s.ctas * (size_t)t.nt * 3 * sizeof(double2);
+  const size_t need = (size_t)s.vctas * (size_t)t.nt * 3 * sizeof(double2);
   if (need > kStaticScratchBytes) {
     snprintf(why, why_len,
              "this solve needs %zu bytes of scratch for its current partials (%d CTAs x %d steps x 3 axes); "
              "the allocation-free entry point has %zu bytes: use SWESim_run_simulation instead",
-             need, s.ctas, t.nt, kStaticScratchBytes);
+             need, s.vctas, t.nt, kStaticScratchBytes);
     return -1;
   }
   void* scratch = nullptr;

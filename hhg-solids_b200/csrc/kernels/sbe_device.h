@@ -50,12 +50,22 @@ struct LaunchShape {
   int k_per_cta;   // k-points per CTA
   int group;       // threads per k-point
   int threads;     // threads per CTA
-  int ctas;        // grid size (persistent CTAs)
+  int ctas;        // grid size (persistent physical CTAs, <= vctas)
+  int vctas;       // virtual CTAs: fixed work split and current-partial rows (result independent of ctas)
   int ntiles;      // work tiles
   int box_sm, win_sm;  // element groups: cell tables staged in shared memory
   int ept;             // element groups: matrix elements per thread
   int variant;         // element groups: compiled shape (-1: runtime-shaped instance)
   size_t smem;     // dynamic shared memory bytes
+};
+
+// One solve of a batched element-group launch (device memory).
+struct BatchDesc {
+  SolveTables t;
+  GroupTables gt;
+  int B, G, box_sm, win_sm, vctas, pad;
+  double2* rho;
+  double2* Jpart;
 };
 
 // Picks kernel and launch shape for a solve on the current device; false (with a reason) if it
@@ -65,8 +75,12 @@ bool plan_propagate(const SolveTables& t, int precision, int sm_count, LaunchSha
 bool plan_group(const SolveTables& t, int precision, int sm_count, LaunchShape* out, char* why, int why_len);
 void launch_group(const SolveTables& t, const GroupTables& gt, const LaunchShape& s, double2* rho, double2* Jpart,
                   cudaStream_t stream);
+// Persistent work-stealing launch over (solve, virtual CTA) items of solves sharing the kernel shape of
+// `s` (same variant, threads); smem = the largest member's.  Returns the grid size.
+int launch_group_batch(const LaunchShape& s, const BatchDesc* descs, const int2* items, int nitems, int* counter,
+                       size_t smem, int sm_count, cudaStream_t stream);
 
-// rho[Nk][nw2] in/out (k-space, W gauge). Jpart[ctas][nt][3] is accumulated (zero it first);
+// rho[Nk][nw2] in/out (k-space, W gauge). Jpart[vctas][nt][3] is accumulated (zero it first);
 // J[3][nt] receives the reduced, 1/Nk-normalised current.  Returns the number of launches.
 // If `after_propagate` is non-null it is recorded between the propagation and the reduction.
 int launch_propagate(const SolveTables& t, const GroupTables& gt, const LaunchShape& s, double2* rho, double2* Jpart,
@@ -77,6 +91,9 @@ int launch_propagate(const SolveTables& t, const GroupTables& gt, const LaunchSh
 int propagate_static_scratch(const SolveTables& t, const GroupTables& gt, const LaunchShape& s, double2* rho,
                              double2* J, cudaStream_t stream, char* why, int why_len);
 size_t static_scratch_capacity();
+
+// J[3][nt] = (1/Nk) sum over the vctas rows of Jpart, in row order.
+void launch_reduce_current(const double2* Jpart, int vctas, int nt, int Nk, double2* J, cudaStream_t stream);
 
 // rho0(k) = U f U^+ of H(k) = sum_cells e^{-ik.R} H0 (no field), one warp per k-point.
 int launch_rho0_fp64(const SolveTables& t, double2* rho, cudaStream_t stream);

@@ -49,7 +49,7 @@ __device__ __forceinline__ int wrap_mod(long long x, int n) {
   return r < 0 ? r + n : r;
 }
 
-// Adds the ring of per-warp current partials of `nsteps` steps into this CTA's Jpart rows.
+// Adds the ring of per-warp current partials of `nsteps` steps into a virtual CTA's Jpart row.
 __device__ __forceinline__ void flush_current(const SolveTables& t, const double* sJ, int nwarps, int ti0, int nsteps,
                                               double2* Jpart) {
   const int nj = t.nj;
@@ -60,7 +60,7 @@ __device__ __forceinline__ void flush_current(const SolveTables& t, const double
       re += sJ[(s * nwarps + w) * 2 * nj + 2 * a];
       im += sJ[(s * nwarps + w) * 2 * nj + 2 * a + 1];
     }
-    double2* dst = Jpart + ((size_t)blockIdx.x * t.nt + ti0 + s) * 3 + t.j_id[a];
+    double2* dst = Jpart + ((size_t)ti0 + s) * 3 + t.j_id[a];
     const double2 old = *dst;
     *dst = make_double2(old.x + re, old.y + im);
   }
@@ -72,7 +72,8 @@ constexpr int kKptMaxThreads = 512;
 
 // NAXc, NJc: field axes and current axes fixed at compile time (0: read from t).
 template <int NW, int NAXc, int NJc>
-__global__ void __launch_bounds__(kKptMaxThreads) propagate_kpt_kernel(SolveTables t, double2* rho, double2* Jpart) {
+__global__ void __launch_bounds__(kKptMaxThreads) propagate_kpt_kernel(SolveTables t, int vctas, double2* rho,
+                                                                       double2* Jpart) {
   constexpr int NW2 = NW * NW;
   extern __shared__ __align__(16) unsigned char smraw[];
   const int nc = t.ncell, nwn = t.nwin, ncw = nc + nwn, nax = NAXc ? NAXc : t.nax, nj = NJc ? NJc : t.nj;
@@ -93,7 +94,10 @@ __global__ void __launch_bounds__(kKptMaxThreads) propagate_kpt_kernel(SolveTabl
   const double prefac = 0.1666666666666 * dt;
   const int kbeg = t.row0 * t.N2, kend = t.row1 * t.N2;
   const int ntiles = (kend - kbeg + nthr - 1) / nthr;
-  for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+  // Virtual CTA v owns tiles v, v + vctas, ... and its own row of current partials, so the result
+  // does not depend on how many physical CTAs share the work.
+  for (int v = blockIdx.x; v < vctas; v += gridDim.x)
+  for (int tile = v; tile < ntiles; tile += vctas) {
     const int k = kbeg + tile * nthr + tid;
     const bool kval = k < kend;
     double2 r[NW2];
@@ -244,7 +248,7 @@ __global__ void __launch_bounds__(kKptMaxThreads) propagate_kpt_kernel(SolveTabl
           }
       }
       __syncthreads();
-      flush_current(t, sJ, nwarps, ti0, nsteps, Jpart);
+      flush_current(t, sJ, nwarps, ti0, nsteps, Jpart + (size_t)v * t.nt * 3);
     }
     if (kval) {
 #pragma unroll
@@ -253,7 +257,7 @@ __global__ void __launch_bounds__(kKptMaxThreads) propagate_kpt_kernel(SolveTabl
   }
 }
 
-// J[a][ti] = (1/Nk) sum_cta Jpart[cta][ti][a], summed in CTA order.
+// J[a][ti] = (1/Nk) sum_v Jpart[v][ti][a], summed in virtual-CTA order.
 __global__ void reduce_current_kernel(const double2* Jpart, int ctas, int nt, double inv_nk, double2* J) {
   const int idx = blockIdx.x * blockDim.x + threadIdx.x;
   if (idx >= 3 * nt) return;
@@ -414,7 +418,7 @@ size_t kpt_smem(const SolveTables& t, int threads) {
   return n2 * sizeof(double2) + sizeof(double) * (kRing * 9 + kRing * (threads / 32) * 2 * t.nj);
 }
 
-using KptKernel = void (*)(SolveTables, double2*, double2*);
+using KptKernel = void (*)(SolveTables, int, double2*, double2*);
 KptKernel kpt_kernel_for(const SolveTables& t) {
   if (t.nw == 2 && t.nj == 2) {
     if (t.nax == 1) return propagate_kpt_kernel<2, 1, 2>;
@@ -448,6 +452,7 @@ bool plan_kpt(const SolveTables& t, int sm_count, LaunchShape* out, size_t smem_
   out->threads = threads;
   out->ntiles = (int)ntiles;
   out->ctas = (int)(ntiles < slots ? ntiles : slots);
+  out->vctas = out->ctas;
   out->box_sm = out->win_sm = 0;
   out->ept = 1;
   out->variant = -1;
@@ -472,14 +477,19 @@ int launch_propagate(const SolveTables& t, const GroupTables& gt, const LaunchSh
   if (s.kernel == 0) {
     KptKernel kern = kpt_kernel_for(t);
     cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s.smem);
-    kern<<<s.ctas, s.threads, s.smem, stream>>>(t, rho, Jpart);
+    kern<<<s.ctas, s.threads, s.smem, stream>>>(t, s.vctas, rho, Jpart);
   } else {
     launch_group(t, gt, s, rho, Jpart, stream);
   }
   if (after_propagate) cudaEventRecord(after_propagate, stream);
   const int n = 3 * t.nt;
-  reduce_current_kernel<<<(n + 255) / 256, 256, 0, stream>>>(Jpart, s.ctas, t.nt, 1.0 / (double)t.Nk, J);
+  reduce_current_kernel<<<(n + 255) / 256, 256, 0, stream>>>(Jpart, s.vctas, t.nt, 1.0 / (double)t.Nk, J);
   return 2;
+}
+
+void launch_reduce_current(const double2* Jpart, int vctas, int nt, int Nk, double2* J, cudaStream_t stream) {
+  const int n = 3 * nt;
+  reduce_current_kernel<<<(n + 255) / 256, 256, 0, stream>>>(Jpart, vctas, nt, 1.0 / (double)Nk, J);
 }
 
 int launch_rho0_fp64(const SolveTables& t, double2* rho, cudaStream_t stream) {

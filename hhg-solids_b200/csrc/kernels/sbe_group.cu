@@ -20,6 +20,7 @@
 // the RK4 accumulation rho + dt/6 (k1 + 2 k2 + 2 k3 + k4), the windowed velocity sum and the
 // current's k-sum stay in FP64.
 #include <cstdio>
+#include <algorithm>
 #include <cstdlib>
 
 #include "sbe_device.h"
@@ -187,11 +188,12 @@ struct GroupData {
   const double2* T2d;
 };
 
+// Runs virtual CTAs v_first, v_first + v_step, ... (< vctas) of one solve on this CTA.
 // NWc, NAXc, NJc: orbital count, field axes and current axes fixed at compile time (0: read from t).
 template <typename Real, int EPT, int NWc, int NAXc, int NJc>
-__global__ void __launch_bounds__(group_threads<EPT>(), 1)
-    propagate_group_kernel(SolveTables t, GroupData<Real> d, int B, int G, int box_sm, int win_sm, double2* rho,
-                           double2* Jpart) {
+__device__ __forceinline__ void group_vctas(const SolveTables& t, const GroupData<Real>& d, int B, int G, int box_sm,
+                                            int win_sm, int v_first, int v_step, int vctas, double2* rho,
+                                            double2* Jpart) {
   using V = typename Cx<Real>::T;
   extern __shared__ __align__(16) unsigned char smraw[];
   const GroupGeom gg = group_geom(t);
@@ -248,7 +250,10 @@ __global__ void __launch_bounds__(group_threads<EPT>(), 1)
   if (win_sm)
     for (size_t idx = tid; idx < (size_t)nj * 16 * nw2; idx += nthr) dsm[L.Xwin + idx] = d.Xwin[idx];
 
-  for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+  // Virtual CTA v owns tiles v, v + vctas, ... and its own row of current partials, so the result
+  // does not depend on how many physical CTAs share the work.
+  for (int v = v_first; v < vctas; v += v_step)
+  for (int tile = v; tile < ntiles; tile += vctas) {
     const int m2 = tile / bpc, m10 = t.row0 + (tile % bpc) * B;
     const int m1 = m10 + g;
     const bool kval = m1 < t.row1;
@@ -533,7 +538,7 @@ __global__ void __launch_bounds__(group_threads<EPT>(), 1)
             re += half[(ss * nwarps + w) * 2 * nj + 2 * a];
             im += half[(ss * nwarps + w) * 2 * nj + 2 * a + 1];
           }
-          double2* dst = Jpart + ((size_t)blockIdx.x * t.nt + ti0 + ss) * 3 + t.j_id[a];
+          double2* dst = Jpart + ((size_t)v * t.nt + ti0 + ss) * 3 + t.j_id[a];
           const double2 old = *dst;
           *dst = make_double2(old.x + re, old.y + im);
         }
@@ -542,6 +547,48 @@ __global__ void __launch_bounds__(group_threads<EPT>(), 1)
 #pragma unroll
     for (int u = 0; u < EPT; ++u)
       if (own[u]) rho[k * nw2 + eu[u]] = r[u];
+    __syncthreads();
+  }
+}
+
+template <typename Real>
+__device__ __forceinline__ GroupData<Real> group_data(const GroupTables& gt) {
+  GroupData<Real> d;
+  if constexpr (sizeof(Real) == 8) {
+    d = {gt.Xbox64, gt.P64, gt.T1_64, gt.T2_64, gt.Xwin64, gt.P64, gt.T1_64, gt.T2_64};
+  } else {
+    d = {gt.Xbox32, gt.P32, gt.T1_32, gt.T2_32, gt.Xwin64, gt.P64, gt.T1_64, gt.T2_64};
+  }
+  return d;
+}
+
+// One solve: physical CTA b runs virtual CTAs b, b + gridDim.x, ...
+template <typename Real, int EPT, int NWc, int NAXc, int NJc>
+__global__ void __launch_bounds__(group_threads<EPT>(), 1)
+    propagate_group_kernel(SolveTables t, GroupData<Real> d, int B, int G, int box_sm, int win_sm, int vctas,
+                           double2* rho, double2* Jpart) {
+  group_vctas<Real, EPT, NWc, NAXc, NJc>(t, d, B, G, box_sm, win_sm, blockIdx.x, gridDim.x, vctas, rho, Jpart);
+}
+
+// Many solves of one kernel shape: persistent CTAs take (solve, virtual CTA) items from a packed
+// work list through an atomic counter.  Which CTA runs an item does not change its result.
+template <typename Real, int EPT, int NWc, int NAXc, int NJc>
+__global__ void __launch_bounds__(group_threads<EPT>(), 1)
+    propagate_group_batch_kernel(const BatchDesc* descs, const int2* items, int nitems, int* counter) {
+  __shared__ BatchDesc sd;
+  __shared__ int s_item;
+  for (;;) {
+    if (threadIdx.x == 0) s_item = atomicAdd(counter, 1);
+    __syncthreads();
+    const int it = s_item;
+    if (it >= nitems) break;
+    const int2 w = items[it];  // (solve, virtual CTA)
+    const int* src = reinterpret_cast<const int*>(descs + w.x);
+    for (int q = threadIdx.x; q < (int)(sizeof(BatchDesc) / sizeof(int)); q += blockDim.x)
+      reinterpret_cast<int*>(&sd)[q] = src[q];
+    __syncthreads();
+    group_vctas<Real, EPT, NWc, NAXc, NJc>(sd.t, group_data<Real>(sd.gt), sd.B, sd.G, sd.box_sm, sd.win_sm, w.y,
+                                           sd.vctas, sd.vctas, sd.rho, sd.Jpart);
     __syncthreads();
   }
 }
@@ -587,20 +634,10 @@ bool plan_group_t(const SolveTables& t, int sm_count, LaunchShape* out, char* wh
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, Bmax * G, smem_max);
   if (occ < 1) occ = 1;
   const long slots = (long)occ * sm_count;
-  // B minimising rounds x (B + shared work in k-point units); ties to the larger B.
-  const double per_k = (double)t.nw2 * (gg.nmat * gg.W1n + 4 * t.nj + 4 * t.nw);
-  const double shared = ((double)gg.nbrows * gg.W2n * t.nw2 + 4.0 * gg.nwrows * t.nw2) / per_k;
+  // B = the largest count that fits: the tile shape is then a property of the kernel shape and the
+  // model, the same alone and in a batch.
   const int rows = t.row1 - t.row0;
-  int best = Bmax;
-  double best_cost = -1;
-  for (int B = Bmax; B >= step; B -= step) {
-    const long ntiles = (long)t.N2 * ((rows + B - 1) / B);
-    const double cost = (double)((ntiles + slots - 1) / slots) * (B + shared);
-    if (best_cost < 0 || cost < best_cost) {
-      best_cost = cost;
-      best = B;
-    }
-  }
+  const int best = Bmax;
   const long ntiles = (long)t.N2 * ((rows + best - 1) / best);
   out->kernel = sizeof(Real) == 8 ? 1 : 2;
   out->ept = EPT;
@@ -609,6 +646,7 @@ bool plan_group_t(const SolveTables& t, int sm_count, LaunchShape* out, char* wh
   out->threads = best * G;
   out->ntiles = (int)ntiles;
   out->ctas = (int)(ntiles < slots ? ntiles : slots);
+  out->vctas = out->ctas;
   out->box_sm = box_sm;
   out->win_sm = win_sm;
   out->smem = bytes(best, box_sm, win_sm);
@@ -626,7 +664,20 @@ void launch_group_t(const SolveTables& t, const GroupTables& gt, const LaunchSha
   }
   auto kern = propagate_group_kernel<Real, EPT, NWc, NAXc, NJc>;
   cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s.smem);
-  kern<<<s.ctas, s.threads, s.smem, stream>>>(t, d, s.k_per_cta, s.group, s.box_sm, s.win_sm, rho, Jpart);
+  kern<<<s.ctas, s.threads, s.smem, stream>>>(t, d, s.k_per_cta, s.group, s.box_sm, s.win_sm, s.vctas, rho, Jpart);
+}
+
+template <typename Real, int EPT, int NWc, int NAXc, int NJc>
+int launch_group_batch_t(const BatchDesc* descs, const int2* items, int nitems, int* counter, int threads, size_t smem,
+                         int sm_count, cudaStream_t stream) {
+  auto kern = propagate_group_batch_kernel<Real, EPT, NWc, NAXc, NJc>;
+  cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  int occ = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, threads, smem);
+  if (occ < 1) occ = 1;
+  const int grid = std::min(nitems, occ * sm_count);
+  kern<<<grid, threads, smem, stream>>>(descs, items, nitems, counter);
+  return grid;
 }
 
 // Compiled shapes: (orbitals, field axes, current axes) of the configurations this library is built
@@ -634,13 +685,16 @@ void launch_group_t(const SolveTables& t, const GroupTables& gt, const LaunchSha
 // any other shape runs the runtime-shaped instance.
 using PlanFn = bool (*)(const SolveTables&, int, LaunchShape*, char*, int);
 using LaunchFn = void (*)(const SolveTables&, const GroupTables&, const LaunchShape&, double2*, double2*, cudaStream_t);
+using BatchFn = int (*)(const BatchDesc*, const int2*, int, int*, int, size_t, int, cudaStream_t);
 struct GroupVariant {
   int precision, nw, nax, nj;
   PlanFn plan;
   LaunchFn launch;
+  BatchFn batch;
 };
 #define HHG_GROUP_VARIANT(P, R, E, NW, NAX, NJ) \
-  {P, NW, NAX, NJ, plan_group_t<R, E, NW, NAX, NJ>, launch_group_t<R, E, NW, NAX, NJ>}
+  {P, NW, NAX, NJ, plan_group_t<R, E, NW, NAX, NJ>, launch_group_t<R, E, NW, NAX, NJ>, \
+   launch_group_batch_t<R, E, NW, NAX, NJ>}
 const GroupVariant kGroupVariants[] = {
     HHG_GROUP_VARIANT(0, double, 1, 11, 1, 2), HHG_GROUP_VARIANT(0, double, 1, 11, 2, 2),
     HHG_GROUP_VARIANT(0, double, 1, 12, 1, 2), HHG_GROUP_VARIANT(0, double, 1, 12, 2, 2),
@@ -674,6 +728,18 @@ bool plan_group(const SolveTables& t, int precision, int sm_count, LaunchShape* 
     return two ? plan_group_t<float, 2, 0, 0, 0>(t, sm_count, out, why, why_len)
                : plan_group_t<float, 1, 0, 0, 0>(t, sm_count, out, why, why_len);
   return plan_group_t<double, 1, 0, 0, 0>(t, sm_count, out, why, why_len);
+}
+
+int launch_group_batch(const LaunchShape& s, const BatchDesc* descs, const int2* items, int nitems, int* counter,
+                       size_t smem, int sm_count, cudaStream_t stream) {
+  if (s.variant >= 0)
+    return kGroupVariants[s.variant].batch(descs, items, nitems, counter, s.threads, smem, sm_count, stream);
+  if (s.kernel == 2)
+    return s.ept == 2 ? launch_group_batch_t<float, 2, 0, 0, 0>(descs, items, nitems, counter, s.threads, smem, sm_count,
+                                                                 stream)
+                      : launch_group_batch_t<float, 1, 0, 0, 0>(descs, items, nitems, counter, s.threads, smem, sm_count,
+                                                                 stream);
+  return launch_group_batch_t<double, 1, 0, 0, 0>(descs, items, nitems, counter, s.threads, smem, sm_count, stream);
 }
 
 void launch_group(const SolveTables& t, const GroupTables& gt, const LaunchShape& s, double2* rho, double2* Jpart,

@@ -79,6 +79,14 @@ def _load(path: str):
         L.SWESim_reset.argtypes = [vp]
         L.SWESim_set_k_rows.argtypes = [vp, ct.c_int, ct.c_int]
         L.SWESim_set_precision.argtypes = [vp, ct.c_int]
+        L.SWEBatch_new.restype = vp
+        L.SWEBatch_add.argtypes = [vp, vp]
+        L.SWEBatch_run.argtypes = [vp]
+        L.SWEBatch_last_ms.argtypes = [vp]
+        L.SWEBatch_last_ms.restype = ct.c_double
+        L.SWEBatch_last_error.argtypes = [vp]
+        L.SWEBatch_last_error.restype = ct.c_char_p
+        L.SWEBatch_delete.argtypes = [vp]
         L.SWESim_get_rho_k.argtypes = [vp, ND_POINTER_1_complex]
         L.SWESim_get_fields.argtypes = [vp, ND_POINTER_1_double, ND_POINTER_1_double, ND_POINTER_1_double]
     _libs[path] = (L, ext)
@@ -221,6 +229,40 @@ class SWE:
         A = np.zeros(3 * n)
         self._call("SWESim_get_fields", t, E, A)
         return t, E.reshape(3, n), A.reshape(3, n)
+
+    def __del__(self):
+        try:
+            self.delete()
+        except Exception:
+            pass
+
+
+class SWEBatch:
+    """Several SWE solves propagated together on one GPU (each from its equilibrium); every solve's
+    current is then read with its own get_current() and equals, bit for bit, what it gives alone."""
+
+    def __init__(self, solves):
+        self.solves = list(solves)
+        if not self.solves:
+            raise SWEError("SWEBatch needs at least one solve")
+        self.lib = self.solves[0].swe_cpp
+        self.ptr = self.lib.SWEBatch_new()
+        for s in self.solves:
+            if self.lib.SWEBatch_add(self.ptr, s.ptr) < 0:
+                raise SWEError("SWEBatch_add failed")
+
+    def run(self):
+        if self.lib.SWEBatch_run(self.ptr) != 0:
+            msg = self.lib.SWEBatch_last_error(self.ptr)
+            raise SWEError(msg.decode() if msg else "SWEBatch_run failed")
+
+    def last_ms(self) -> float:
+        return float(self.lib.SWEBatch_last_ms(self.ptr))
+
+    def delete(self):
+        if self.ptr is not None:
+            self.lib.SWEBatch_delete(self.ptr)
+            self.ptr = None
 
     def __del__(self):
         try:

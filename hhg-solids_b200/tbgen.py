@@ -135,6 +135,10 @@ MODELS = {
     "haldane": (haldane, {}),
     "tmd11_s7": (random_tmd, {"nw": 11, "seed": 7}),
     "tmd6_s1": (random_tmd, {"nw": 6, "seed": 1}),
+    "tmd6_s2": (random_tmd, {"nw": 6, "seed": 2}),
+    "tmd6_s3": (random_tmd, {"nw": 6, "seed": 3}),
+    "tmd11_s1": (random_tmd, {"nw": 11, "seed": 1}),
+    "tmd11_s3": (random_tmd, {"nw": 11, "seed": 3}),
     "tmd11_s2": (random_tmd, {"nw": 11, "seed": 2}),
     "tmd12_s3": (random_tmd, {"nw": 12, "seed": 3}),
     "tmd5_s4": (random_tmd, {"nw": 5, "seed": 4, "window": 5}),

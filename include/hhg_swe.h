@@ -24,6 +24,7 @@ extern "C" {
 
 typedef struct SWESim SWESim;
 typedef struct Settings Settings;
+typedef struct SWEBatch SWEBatch;
 /* std::complex<double> / numpy complex128 layout: {re, im}. */
 typedef struct hhg_cdouble {
   double re, im;
@@ -131,6 +132,20 @@ void SWESim_get_fields(SWESim* swe, double* t, double* E, double* A);
  * clear it at their start: calls whose work overlaps on the GPU (different streams, or different
  * host threads) corrupt each other's result.  Returns 0, or -1 (message in SWESim_last_error). */
 int SWESim_run_simulation_noalloc(SWESim* swe, hhg_cdouble* rho_k, hhg_cdouble* current, void* stream);
+
+/* Batches: several initialised solves (each after SWESim_init, all on one device) propagated
+ * together, each from its equilibrium, with kernels running side by side and the launch sequence
+ * captured in a CUDA graph.  Every solve's current is bit for bit what it gives alone; read it with
+ * SWESim_get_current.  The SWESim objects stay owned by the caller and must outlive the batch. */
+SWEBatch* SWEBatch_new(void);
+/* Appends a solve; returns its index in the batch, or -1. */
+int SWEBatch_add(SWEBatch* batch, SWESim* swe);
+/* Propagates every solve of the batch; returns 0, or -1 (message in SWEBatch_last_error). */
+int SWEBatch_run(SWEBatch* batch);
+/* Device time in milliseconds of the last SWEBatch_run (all solves, first launch to last copy). */
+double SWEBatch_last_ms(SWEBatch* batch);
+const char* SWEBatch_last_error(SWEBatch* batch);
+void SWEBatch_delete(SWEBatch* batch);
 
 /* FP64 FMA / FP32 FMA chain throughput of the current device (TFLOP/s), for roofline denominators. */
 int HHG_measure_peaks(double* fp64_tflops, double* fp32_tflops);
