@@ -49,6 +49,10 @@ WORKLOADS = {
     "c3": dict(model=None, n=None, window=None,
                desc="batched scan: 64 solves, nw in {2,6,11} (seeds 1-3), grids {60,100,150,200}^2, 16 angles "
                     "0-180 deg, I in {0.5,1,1.5,2}e12, lambda in {2000,3000} nm (draws: seed 0)"),
+    "c4": dict(model=None, n=None, window=None,
+               desc="serving: Poisson arrivals at 20 req/s (seed 0), nw in {2,6,11,12} (seeds 1-3), k-grid side "
+                    "even in 60-200, polarisation uniform on the circle, I log-uniform in [3e11,3e12] W/cm^2, "
+                    "C0 pulse, mixed precision, continuous batching (SWEServer)"),
 }
 
 
@@ -72,6 +76,115 @@ def scan_params(n_solves: int = 64, seed: int = 0):
         p["phi_vec"] = np.zeros(3)
         out.append((model, nw, p))
     return out
+
+
+def serve_requests(n: int, rate: float = 20.0, seed: int = 0):
+    """The serving draws: (arrival s, model, nw, param) for n Poisson arrivals."""
+    import numpy as np
+    import tbgen
+
+    rng = np.random.default_rng(seed)
+    models = {2: ["haldane"], 6: ["tmd6_s1", "tmd6_s2", "tmd6_s3"], 11: ["tmd11_s1", "tmd11_s2", "tmd11_s3"],
+              12: ["tmd12_s1", "tmd12_s2", "tmd12_s3"]}
+    t = np.cumsum(rng.exponential(1.0 / rate, n))
+    out = []
+    for i in range(n):
+        nw = int(rng.choice([2, 6, 11, 12]))
+        model = models[nw][int(rng.integers(len(models[nw])))]
+        side = 2 * int(rng.integers(30, 101))
+        th = rng.uniform(0.0, 2.0 * math.pi)
+        p = dict(PULSE, nr1=side, nr2=side, nr3=1, path_tb=tbgen.model_path(model))
+        p["intensity"] = float(math.exp(rng.uniform(math.log(3e11), math.log(3e12))))
+        p["pol_vec"] = np.array([math.cos(th), math.sin(th), 0.0])
+        p["phi_vec"] = np.zeros(3)
+        out.append((float(t[i]), model, nw, p))
+    return out
+
+
+def run_serve(args, local: int):
+    """Serving: requests submitted at their Poisson arrival times to one SWEServer (mixed form,
+    continuous batching); latency = completion - submission.  Beside it the plain FP64 form run
+    sequentially (setup + propagation, one solve after another) on a sample of the same requests."""
+    import numpy as np
+    import tbgen
+    from pySWE import pyswe
+
+    reqs = serve_requests(args.requests)  # generates the model files before the clock starts
+    srv = pyswe.SWEServer(device=local, max_active=args.max_active, chunk_steps=args.chunk)
+    # Warm-up: small requests of every orbital count.
+    warm = []
+    for _ in range(max(1, args.warmup // 3)):
+        for model in ("haldane", "tmd6_s1", "tmd11_s1", "tmd12_s1"):
+            p = dict(reqs[0][3], nr1=20, nr2=20, path_tb=tbgen.model_path(model))
+            s = pyswe.SWE(pyswe.Settings(p), precision="mixed", defer_init=True)
+            warm.append((s, srv.submit(s)))
+    for s, tk in warm:
+        srv.wait(tk)
+        s.delete()
+    base = srv.stats()
+    solves = [None] * len(reqs)
+    tickets = [None] * len(reqs)
+    clocks = ClockSampler(local)
+    clocks.start()
+    t0 = time.perf_counter()
+    for i, (t_arr, model, nw, p) in enumerate(reqs):
+        delay = t0 + t_arr - time.perf_counter()
+        if delay > 0:
+            time.sleep(delay)
+        solves[i] = pyswe.SWE(pyswe.Settings(p), precision="mixed", defer_init=True)
+        tickets[i] = srv.submit(solves[i])
+    for tk in tickets:
+        srv.wait(tk)
+    wall = time.perf_counter() - t0
+    clk = clocks.stop()
+    times = [srv.times(tk) for tk in tickets]
+    lat = np.array([tm["done"] - tm["submit"] for tm in times])
+    queue_wait = np.array([tm["admit"] - tm["submit"] for tm in times])
+    first, last = min(tm["submit"] for tm in times), max(tm["done"] for tm in times)
+    span = last - first
+    st = srv.stats()
+    nt = int(PULSE["tmax"] / PULSE["dt"])
+    ksteps = sum(p["nr1"] * p["nr2"] * nt for _, _, _, p in reqs)
+    J_mixed = [s.get_current()[1:] for s in solves[: args.baseline_sample]]
+    for s in solves:
+        s.delete()
+    srv.close()
+    # Plain FP64, sequential, on the first requests.
+    seq_s, seq_k, errs = 0.0, 0, []
+    for (t_arr, model, nw, p), Jm in zip(reqs[: args.baseline_sample], J_mixed):
+        a = time.perf_counter()
+        s = pyswe.SWE(pyswe.Settings(dict(p)), device=local)
+        s.run_simulation()
+        J = s.get_current()[1:]
+        seq_s += time.perf_counter() - a
+        seq_k += p["nr1"] * p["nr2"] * nt
+        s.delete()
+        errs.append(float(np.linalg.norm(Jm - J) / np.linalg.norm(J)))
+    n = len(reqs)
+
+    def pct(a, q):
+        return float(np.percentile(a, q))
+
+    return {
+        "metric": "solves/h", "value": 3600.0 * n / span, "unit": "solves/h", "n_gpus": 1, "steps": n,
+        "warmup": len(warm), "ms_per_step": 1e3 * span / n, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "c64 commutators/Wannier sums, f64 state/RK/k-sum",
+        "data": "synthetic (seeded TB models and request stream, hhg-solids_b200/tbgen.py)", "impl": "hhg-b200",
+        "config": {"workload": f"c4: {WORKLOADS['c4']['desc']}", "requests": n, "nt": nt,
+                   "max_active": args.max_active, "chunk_steps": args.chunk,
+                   "server": "SWEServer: admission by device-memory footprint, chunked continuous batching, "
+                             "one work-stealing launch per kernel shape per chunk"},
+        "latency_s": {"p50": pct(lat, 50), "p95": pct(lat, 95), "p99": pct(lat, 99), "max": float(lat.max()),
+                      "mean": float(lat.mean())},
+        "queue_wait_s": {"p50": pct(queue_wait, 50), "p99": pct(queue_wait, 99)},
+        "k_pt_rk4_steps_per_s": ksteps / span, "span_s": span, "wall_s": wall,
+        "offered_load_req_per_s": n / reqs[-1][0],
+        "server": {k: (st[k] - base.get(k, 0) if k in ("completed", "chunks", "gpu_ms") else st[k]) for k in st},
+        "fp64_sequential_sample": {"requests": len(errs), "solves_per_hour": 3600.0 * len(errs) / seq_s,
+                                   "k_pt_rk4_steps_per_s": seq_k / seq_s, "s_per_solve": seq_s / len(errs)},
+        "J_rel_l2_mixed_vs_fp64": {"max": max(errs), "median": statistics.median(errs)},
+        "clocks": clk,
+    }
 
 
 def run_scan(args, local: int):
@@ -433,6 +546,10 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"],
                     help="mixed: FP32 Wannier sums and commutators, FP64 state / RK accumulation / k-sum")
+    ap.add_argument("--requests", type=int, default=200, help="c4: requests in the arrival stream")
+    ap.add_argument("--max-active", type=int, default=32, help="c4: most solves running at once")
+    ap.add_argument("--chunk", type=int, default=256, help="c4: RK4 steps per scheduling chunk")
+    ap.add_argument("--baseline-sample", type=int, default=24, help="c4: requests run sequentially in FP64")
     ap.add_argument("--grid", type=int, default=None,
                     help="override the k-grid side (profiling a smaller case of the same kernel)")
     args = ap.parse_args()
@@ -477,9 +594,9 @@ def main():
     lib.HHG_measure_peaks.argtypes = [ct.POINTER(ct.c_double), ct.POINTER(ct.c_double)]
     fp64_peak, fp32_peak = ct.c_double(), ct.c_double()
 
-    if args.workload == "c3":
+    if args.workload in ("c3", "c4"):
         if rank == 0:
-            print(json.dumps(run_scan(args, local)), flush=True)
+            print(json.dumps(run_scan(args, local) if args.workload == "c3" else run_serve(args, local)), flush=True)
         if dist is not None:
             dist.destroy_process_group()
         return

@@ -25,9 +25,7 @@
 #include <string>
 #include <vector>
 
-#include "../kernels/sbe_device.h"
-#include "hhg_swe.h"
-#include "tb_model.hpp"
+#include "swe_sim.hpp"
 
 namespace hhg {
 namespace refarith {
@@ -39,22 +37,12 @@ void efield(int nt, const double* t, double lambda_nm, double tmax_field_fs, dou
 }  // namespace refarith
 }  // namespace hhg
 
-// Defaults of include/settings.h:8-22 of the reference.
-struct Settings {
-  int nr1 = 400, nr2 = 400, nr3 = 1;
-  double tmax = 90.0;
-  double dt = 10.98e-3 / 0.5;
-  int nt = (int)(90.0 / (10.98e-3 / 0.5));
-  double lambda_nm = 3000;
-  double tmax_field = 80.0;
-  double intensity_wcm2 = 5e10;
-  double sx = 0.96, sy = 0.25, sz = 0.0;
-  double phi_x = 0.0, phi_y = 0.0, phi_z = 0.0;
-};
+using hhg::cd;
+using hhg::check_cuda;
+using hhg::d2;
+using hhg::DevBuf;
 
 namespace {
-
-using hhg::cd;
 
 // Setup phase timer, printed to stderr when the environment sets HHG_TRACE=1.
 struct PhaseTrace {
@@ -86,116 +74,8 @@ constexpr double kA2Bohr = 1.0 / 0.5291772;    // include/constants.h:6
 thread_local std::string g_last_error;
 thread_local bool g_has_error = false;
 
-void check_cuda(cudaError_t e, const char* what) {
-  if (e != cudaSuccess) throw std::runtime_error(std::string(what) + ": " + cudaGetErrorString(e));
-}
-
-template <typename T>
-struct DevBuf {
-  T* p = nullptr;
-  size_t n = 0;
-  size_t cap = 0;
-  // Keeps the current allocation when it is large enough (re-initialisation reuses buffers).
-  void alloc(size_t count) {
-    if (count == 0) count = 1;
-    if (p && count <= cap) {
-      n = count;
-      return;
-    }
-    release();
-    check_cuda(cudaMalloc(&p, count * sizeof(T)), "cudaMalloc");
-    n = cap = count;
-  }
-  void upload(const std::vector<T>& v, cudaStream_t s) {
-    alloc(v.size());
-    if (!v.empty()) check_cuda(cudaMemcpyAsync(p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, s), "H2D");
-  }
-  void release() {
-    if (p) cudaFree(p);
-    p = nullptr;
-    n = cap = 0;
-  }
-  ~DevBuf() { release(); }
-};
-
-inline double2 d2(cd z) { return make_double2(z.real(), z.imag()); }
 
 }  // namespace
-
-struct SWESim {
-  std::string path_tb;
-  Settings* settings = nullptr;
-  int device = -1;
-  int req_row0 = 0, req_row1 = -1;  // k-grid row slab requested with SWESim_set_k_rows (-1: all)
-  std::string err;
-  bool has_err = false;
-  bool ready = false;
-
-  hhg::TBModel model;
-  int N1 = 0, N2 = 0, Nk = 0, nw = 0, nw2 = 0, nt = -1;
-  double lat_au[3][3] = {};
-  std::vector<double> Rgrid;  // [Nk][3] Angstrom
-  std::vector<int> site_of_cell;
-  std::vector<double> t, E, A;
-  std::vector<double> es;          // [nt][3][3]
-  std::vector<int2> cell_n, win_n;
-  std::vector<double2> H0, Rtab, V, Q, Xbox, Vd, P, T1, T2;
-  int precision = 0;  // 0 plain FP64, 1 mixed
-  unsigned generation = 0;  // bumped by every successful SWESim_init (batches re-capture on change)
-  int nax = 0, ax_id[3] = {0, 0, 0}, nj = 0, j_id[3] = {0, 0, 0};
-
-  cudaStream_t stream = nullptr;
-  int stream_device = -1;
-  cudaEvent_t ev0 = nullptr, ev1 = nullptr, evm = nullptr;
-  DevBuf<int2> d_cell, d_win;
-  DevBuf<double2> d_H0, d_R, d_V, d_Q, d_Xbox, d_Vd, d_P, d_T1, d_T2, d_rho0, d_rho, d_Jpart, d_J;
-  DevBuf<float2> d_Xbox32, d_Vd32, d_P32, d_T1_32, d_T2_32;
-  hhg::GroupTables gtab{};
-  DevBuf<double> d_es;
-  hhg::SolveTables tab{};
-  hhg::LaunchShape shape{};
-  double2* h_J = nullptr;  // pinned [3][nt]
-  size_t h_J_cap = 0;
-  std::vector<cd> Jhist[3];
-  float last_ms = 0.f, last_prop_ms = 0.f;
-  size_t h2d_bytes = 0;
-  int last_launches = 0;
-
-  ~SWESim() { release(); }
-
-  // Forget the previous setup but keep device buffers, stream, events and the pinned host
-  // buffer for reuse: a restart then costs no cudaFree / cudaFreeHost (both synchronise).
-  void invalidate() {
-    ready = false;
-    for (auto& j : Jhist) j.clear();
-  }
-
-  void release() {
-    d_cell.release();
-    d_win.release();
-    for (auto* b : {&d_H0, &d_R, &d_V, &d_Q, &d_Xbox, &d_Vd, &d_P, &d_T1, &d_T2, &d_rho0, &d_rho, &d_Jpart, &d_J})
-      b->release();
-    for (auto* b : {&d_Xbox32, &d_Vd32, &d_P32, &d_T1_32, &d_T2_32}) b->release();
-    d_es.release();
-    if (h_J) cudaFreeHost(h_J);
-    h_J = nullptr;
-    h_J_cap = 0;
-    if (ev0) cudaEventDestroy(ev0);
-    if (ev1) cudaEventDestroy(ev1);
-    if (evm) cudaEventDestroy(evm);
-    ev0 = ev1 = evm = nullptr;
-    if (stream) cudaStreamDestroy(stream);
-    stream = nullptr;
-    ready = false;
-    for (auto& j : Jhist) j.clear();
-  }
-
-  void init();
-  void run();
-  void reset_state();
-  void test_files();
-  void write_fields_files(const std::string& dir);
-};
 
 namespace {
 
@@ -230,6 +110,7 @@ inline int wrapi(long x, int n) {
 void SWESim::init() {
   PhaseTrace trace;
   invalidate();
+  served = false;
   if (!settings) throw std::runtime_error("SWESim_init: settings not set (call SWESim_set_settings first)");
   if (path_tb.empty()) throw std::runtime_error("SWESim_init: TB path not set (call SWESim_set_path_tb first)");
   model = hhg::parse_tb(path_tb);
@@ -526,6 +407,8 @@ void SWESim::init() {
   tab.N2 = N2;
   tab.Nk = Nk;
   tab.nt = nt;
+  tab.step0 = 0;
+  tab.step1 = nt;
   tab.hermitian = herm ? 1 : 0;
   tab.dt = t[1] - t[0];
   tab.nax = nax;
@@ -568,6 +451,48 @@ void SWESim::init() {
   trace.mark("rho0");
   ready = true;
   ++generation;
+}
+
+size_t SWESim::device_bytes() const {
+  size_t b = d_cell.cap * sizeof(int2) + d_win.cap * sizeof(int2) + d_es.cap * sizeof(double);
+  for (const auto* x : {&d_H0, &d_R, &d_V, &d_Q, &d_Xbox, &d_Vd, &d_P, &d_T1, &d_T2, &d_rho0, &d_rho, &d_Jpart, &d_J})
+    b += x->cap * sizeof(double2);
+  for (const auto* x : {&d_Xbox32, &d_Vd32, &d_P32, &d_T1_32, &d_T2_32}) b += x->cap * sizeof(float2);
+  return b;
+}
+
+size_t SWESim::footprint_estimate() const {
+  if (!settings) throw std::runtime_error("SWESim: settings not set (call SWESim_set_settings first)");
+  if (path_tb.empty()) throw std::runtime_error("SWESim: TB path not set (call SWESim_set_path_tb first)");
+  const hhg::TBModel m = hhg::parse_tb(path_tb);
+  const Settings& s = *settings;
+  const size_t nt_ = (size_t)std::max(2, (int)(s.tmax / s.dt));
+  const size_t N1_ = (size_t)std::max(1, s.nr1), N2_ = (size_t)std::max(1, s.nr2);
+  const size_t w2 = (size_t)m.nw * m.nw, ns = (size_t)std::max(1, m.nsites);
+  int np_ = 2;
+  for (int c = 0; c < m.nsites; ++c) np_ = std::max(np_, std::max(std::abs(m.R[3 * c]), std::abs(m.R[3 * c + 1])));
+  const size_t box = (size_t)(2 * np_ + 1) * (2 * np_ + 1);
+  int dev = device, sms = 148;
+  if (dev < 0) cudaGetDevice(&dev);
+  if (dev >= 0) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const size_t c16 = sizeof(double2);
+  size_t b = 2 * N1_ * N2_ * w2 * c16;                            // rho, rho0
+  b += 4 * (size_t)sms * nt_ * 3 * c16;                           // current partials (up to 4 CTAs per SM)
+  b += nt_ * (3 * c16 + 9 * sizeof(double));                      // J, field table
+  b += nt_ * (ns + hhg::kWindow) * c16;                           // Peierls phases of the listed cells
+  b += nt_ * 2 * (2 * np_ + 1) * c16 * 3 / 2;                     // P, FP64 and FP32
+  b += (4 * box + 4 * ns + 6 * hhg::kWindow) * w2 * c16 * 3 / 2;  // cell tables, both precisions
+  b += (N1_ + N2_) * c16 * 3 / 2 + (size_t(1) << 20);
+  return b;
+}
+
+void SWESim::finish_served(const double2* J) {
+  std::vector<cd> keep[3];
+  for (int a = 0; a < 3; ++a)
+    for (int ti = 0; ti < nt; ++ti) keep[a].push_back(cd(J[(size_t)a * nt + ti].x, J[(size_t)a * nt + ti].y));
+  release();
+  for (int a = 0; a < 3; ++a) Jhist[a] = std::move(keep[a]);
+  served = true;
 }
 
 void SWESim::reset_state() {
@@ -677,198 +602,6 @@ void SWESim::test_files() {
   write_fields_files("fields");
 }
 
-// ------------------------------------------------------------------------------------- batches
-
-// Several initialised solves propagated together.  Solves that run the element-group kernel are
-// grouped by kernel shape; each group is one persistent launch whose CTAs take (solve, virtual CTA)
-// items from a packed work list (longest items first), so uneven solves share the SMs without a
-// static split.  Solves on the thread-per-k-point kernel keep their own launch on their own stream.
-// A solve keeps the tile shape and virtual-CTA split it has alone, so its current is bit for bit
-// the one it gives alone.  The launch sequence (reset to rho0, clear, propagate, reduce, copy the
-// current out) is captured once into a CUDA graph and replayed.
-struct SWEBatch {
-  int device = -1;
-  std::vector<SWESim*> sims;
-  std::vector<cudaStream_t> streams;
-  std::vector<cudaEvent_t> done;
-  cudaStream_t master = nullptr;
-  cudaEvent_t fork = nullptr, ev0 = nullptr, ev1 = nullptr;
-  cudaGraphExec_t graph = nullptr;
-  DevBuf<hhg::BatchDesc> d_desc;
-  DevBuf<int2> d_items;
-  DevBuf<int> d_counters;
-  std::vector<unsigned> generations;
-  bool dirty = true;
-  float last_ms = 0.f;
-  int groups = 0, separate = 0;
-  std::string err;
-  bool has_err = false;
-
-  ~SWEBatch() { release(); }
-  void release() {
-    if (graph) cudaGraphExecDestroy(graph);
-    graph = nullptr;
-    for (auto st : streams) cudaStreamDestroy(st);
-    streams.clear();
-    for (auto e : done) cudaEventDestroy(e);
-    done.clear();
-    for (auto* e : {&fork, &ev0, &ev1})
-      if (*e) cudaEventDestroy(*e);
-    fork = ev0 = ev1 = nullptr;
-    if (master) cudaStreamDestroy(master);
-    master = nullptr;
-  }
-
-  void prepare() {
-    if (sims.empty()) throw std::runtime_error("SWEBatch_run: empty batch");
-    for (SWESim* sim : sims)
-      if (!sim->ready) throw std::runtime_error("SWEBatch_run: a solve of the batch is not initialised");
-    device = sims[0]->device;
-    for (SWESim* sim : sims)
-      if (sim->device != device) throw std::runtime_error("SWEBatch_run: all solves of a batch must be on one device");
-    check_cuda(cudaSetDevice(device), "cudaSetDevice");
-    release();
-    int sms = 0;
-    check_cuda(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device), "cudaDeviceGetAttribute");
-
-    // Kernel-shape classes of the element-group solves; the others run alone.
-    std::map<std::tuple<int, int, int, int, int, int, int, int>, std::vector<int>> classes;
-    std::vector<int> alone;
-    for (int i = 0; i < (int)sims.size(); ++i) {
-      const hhg::LaunchShape& sh = sims[i]->shape;
-      if (sh.kernel == 0) {
-        alone.push_back(i);
-      } else {
-        const hhg::SolveTables& t = sims[i]->tab;
-        classes[std::make_tuple(sh.kernel, sh.variant, sh.ept, sh.threads, sh.group, t.nw, t.nax, t.nj)].push_back(i);
-      }
-    }
-    groups = (int)classes.size();
-    separate = (int)alone.size();
-    // Descriptors and items (per class: solves by decreasing item cost, all items of a solve).
-    std::vector<hhg::BatchDesc> descs(sims.size());
-    std::vector<int2> items;
-    std::vector<std::pair<size_t, size_t>> ranges;  // per class: [first item, end)
-    for (int i = 0; i < (int)sims.size(); ++i) {
-      SWESim* sim = sims[i];
-      hhg::BatchDesc& d = descs[i];
-      std::memset(&d, 0, sizeof d);
-      d.t = sim->tab;
-      d.gt = sim->gtab;
-      d.B = sim->shape.k_per_cta;
-      d.G = sim->shape.group;
-      d.box_sm = sim->shape.box_sm;
-      d.win_sm = sim->shape.win_sm;
-      d.vctas = sim->shape.vctas;
-      d.rho = sim->d_rho.p;
-      d.Jpart = sim->d_Jpart.p;
-    }
-    for (auto& kv : classes) {
-      std::vector<int> members = kv.second;
-      auto cost = [&](int i) {
-        const hhg::LaunchShape& sh = sims[i]->shape;
-        return (double)sh.ntiles / std::max(1, sh.vctas);  // tiles per item
-      };
-      std::stable_sort(members.begin(), members.end(), [&](int a, int b) { return cost(a) > cost(b); });
-      const size_t first = items.size();
-      for (int i : members)
-        for (int v = 0; v < sims[i]->shape.vctas; ++v) items.push_back(make_int2(i, v));
-      ranges.emplace_back(first, items.size());
-    }
-    d_desc.alloc(descs.size());
-    check_cuda(cudaMemcpy(d_desc.p, descs.data(), sizeof(hhg::BatchDesc) * descs.size(), cudaMemcpyHostToDevice), "H2D");
-    d_items.alloc(std::max<size_t>(1, items.size()));
-    if (!items.empty())
-      check_cuda(cudaMemcpy(d_items.p, items.data(), sizeof(int2) * items.size(), cudaMemcpyHostToDevice), "H2D");
-    d_counters.alloc(std::max<size_t>(1, classes.size()));
-
-    check_cuda(cudaStreamCreateWithFlags(&master, cudaStreamNonBlocking), "cudaStreamCreate");
-    for (auto* e : {&fork, &ev0, &ev1}) check_cuda(cudaEventCreate(e), "cudaEventCreate");
-    const size_t nstreams = classes.size() + alone.size();
-    streams.resize(nstreams);
-    done.resize(nstreams);
-    for (size_t q = 0; q < nstreams; ++q) {
-      check_cuda(cudaStreamCreateWithFlags(&streams[q], cudaStreamNonBlocking), "cudaStreamCreate");
-      check_cuda(cudaEventCreateWithFlags(&done[q], cudaEventDisableTiming), "cudaEventCreate");
-    }
-
-    auto reset_and_clear = [&](SWESim* sim, cudaStream_t st) {
-      check_cuda(cudaMemcpyAsync(sim->d_rho.p, sim->d_rho0.p, sizeof(double2) * (size_t)sim->Nk * sim->nw2,
-                                 cudaMemcpyDeviceToDevice, st), "D2D");
-      check_cuda(cudaMemsetAsync(sim->d_Jpart.p, 0, sizeof(double2) * (size_t)sim->shape.vctas * sim->nt * 3, st),
-                 "memset");
-    };
-    auto reduce_and_copy = [&](SWESim* sim, cudaStream_t st) {
-      hhg::launch_reduce_current(sim->d_Jpart.p, sim->shape.vctas, sim->nt, sim->Nk, sim->d_J.p, st);
-      check_cuda(cudaMemcpyAsync(sim->h_J, sim->d_J.p, sizeof(double2) * 3 * (size_t)sim->nt, cudaMemcpyDeviceToHost, st),
-                 "D2H");
-    };
-
-    cudaGraph_t g = nullptr;
-    check_cuda(cudaStreamBeginCapture(master, cudaStreamCaptureModeRelaxed), "cudaStreamBeginCapture");
-    check_cuda(cudaEventRecord(fork, master), "event");
-    size_t q = 0;
-    int ci = 0;
-    for (auto& kv : classes) {
-      cudaStream_t st = streams[q];
-      check_cuda(cudaStreamWaitEvent(st, fork, 0), "cudaStreamWaitEvent");
-      size_t smem = 0;
-      for (int i : kv.second) {
-        reset_and_clear(sims[i], st);
-        smem = std::max(smem, sims[i]->shape.smem);
-      }
-      check_cuda(cudaMemsetAsync(d_counters.p + ci, 0, sizeof(int), st), "memset");
-      const auto& rg = ranges[ci];
-      hhg::launch_group_batch(sims[kv.second[0]]->shape, d_desc.p, d_items.p + rg.first, (int)(rg.second - rg.first),
-                              d_counters.p + ci, smem, sms, st);
-      for (int i : kv.second) reduce_and_copy(sims[i], st);
-      check_cuda(cudaEventRecord(done[q], st), "event");
-      check_cuda(cudaStreamWaitEvent(master, done[q], 0), "cudaStreamWaitEvent");
-      ++q;
-      ++ci;
-    }
-    for (int i : alone) {
-      cudaStream_t st = streams[q];
-      SWESim* sim = sims[i];
-      check_cuda(cudaStreamWaitEvent(st, fork, 0), "cudaStreamWaitEvent");
-      reset_and_clear(sim, st);
-      hhg::launch_propagate(sim->tab, sim->gtab, sim->shape, sim->d_rho.p, sim->d_Jpart.p, sim->d_J.p, st);
-      check_cuda(cudaMemcpyAsync(sim->h_J, sim->d_J.p, sizeof(double2) * 3 * (size_t)sim->nt, cudaMemcpyDeviceToHost, st),
-                 "D2H");
-      check_cuda(cudaEventRecord(done[q], st), "event");
-      check_cuda(cudaStreamWaitEvent(master, done[q], 0), "cudaStreamWaitEvent");
-      ++q;
-    }
-    check_cuda(cudaStreamEndCapture(master, &g), "cudaStreamEndCapture");
-    const cudaError_t ie = cudaGraphInstantiate(&graph, g, 0);
-    cudaGraphDestroy(g);
-    check_cuda(ie, "cudaGraphInstantiate");
-    generations.clear();
-    for (SWESim* sim : sims) generations.push_back(sim->generation);
-    dirty = false;
-  }
-
-  // Every solve from its equilibrium rho0; each SWESim then holds its current as after
-  // SWESim_reset + SWESim_run_simulation.
-  void run() {
-    for (size_t i = 0; i < sims.size() && !dirty; ++i) dirty = !sims[i]->ready || generations[i] != sims[i]->generation;
-    if (dirty) prepare();
-    check_cuda(cudaSetDevice(device), "cudaSetDevice");
-    check_cuda(cudaEventRecord(ev0, master), "event");
-    check_cuda(cudaGraphLaunch(graph, master), "cudaGraphLaunch");
-    check_cuda(cudaEventRecord(ev1, master), "event");
-    check_cuda(cudaStreamSynchronize(master), "SWEBatch_run");
-    check_cuda(cudaEventElapsedTime(&last_ms, ev0, ev1), "event time");
-    for (SWESim* sim : sims) {
-      for (auto& j : sim->Jhist) j.clear();
-      for (int a = 0; a < 3; ++a)
-        for (int ti = 0; ti < sim->nt; ++ti)
-          sim->Jhist[a].push_back(cd(sim->h_J[(size_t)a * sim->nt + ti].x, sim->h_J[(size_t)a * sim->nt + ti].y));
-      sim->last_launches = 2;
-    }
-  }
-};
-
 // ------------------------------------------------------------------------------------- C ABI
 
 namespace {
@@ -935,7 +668,7 @@ void SWESim_restart(SWESim* swe) { guarded(swe, "SWESim_restart", [&] { swe->ini
 
 void SWESim_get_current(SWESim* swe, double* t, hhg_cdouble* jx, hhg_cdouble* jy, hhg_cdouble* jz) {
   guarded(swe, "SWESim_get_current", [&] {
-    if (!swe->ready) throw std::runtime_error("SWESim_get_current: SWESim_init has not succeeded");
+    if (!swe->ready && !swe->served) throw std::runtime_error("SWESim_get_current: SWESim_init has not succeeded");
     if ((int)swe->Jhist[0].size() < swe->nt)
       throw std::runtime_error("SWESim_get_current: run_simulation has not been called");
     hhg_cdouble* out[3] = {jx, jy, jz};
@@ -981,7 +714,7 @@ void Settings_set_phi_vec(Settings* s, double* v) {
 
 const char* SWESim_last_error(SWESim* swe) { return (swe && swe->has_err) ? swe->err.c_str() : nullptr; }
 const char* HHG_last_error(void) { return g_has_error ? g_last_error.c_str() : nullptr; }
-int SWESim_get_nt(SWESim* swe) { return (swe && swe->ready) ? swe->nt : -1; }
+int SWESim_get_nt(SWESim* swe) { return (swe && (swe->ready || swe->served)) ? swe->nt : -1; }
 int SWESim_get_num_orb(SWESim* swe) { return (swe && swe->ready) ? swe->nw : -1; }
 void SWESim_set_device(SWESim* swe, int device) {
   guarded(swe, "SWESim_set_device", [&] { swe->device = device; });
@@ -1049,47 +782,6 @@ int SWESim_run_simulation_noalloc(SWESim* swe, hhg_cdouble* rho_k, hhg_cdouble* 
   return rc;
 }
 
-SWEBatch* SWEBatch_new(void) {
-  try {
-    return new SWEBatch();
-  } catch (...) {
-    return nullptr;
-  }
-}
-
-void SWEBatch_delete(SWEBatch* b) {
-  try {
-    delete b;
-  } catch (...) {
-  }
-}
-
-int SWEBatch_add(SWEBatch* b, SWESim* swe) {
-  if (!b || !swe) return -1;
-  b->sims.push_back(swe);
-  b->dirty = true;
-  return (int)b->sims.size() - 1;
-}
-
-int SWEBatch_run(SWEBatch* b) {
-  if (!b) return -1;
-  try {
-    b->has_err = false;
-    b->run();
-    return 0;
-  } catch (const std::exception& e) {
-    b->err = e.what();
-    b->has_err = true;
-    g_last_error = b->err;
-    g_has_error = true;
-    b->dirty = true;
-    return -1;
-  }
-}
-
-double SWEBatch_last_ms(SWEBatch* b) { return b ? (double)b->last_ms : -1.0; }
-const char* SWEBatch_last_error(SWEBatch* b) { return (b && b->has_err) ? b->err.c_str() : nullptr; }
-
 int HHG_measure_peaks(double* fp64_tflops, double* fp32_tflops) {
   try {
     return hhg::measure_fma_peaks(fp64_tflops, fp32_tflops);
@@ -1099,3 +791,10 @@ int HHG_measure_peaks(double* fp64_tflops, double* fp32_tflops) {
 }
 
 }  // extern "C"
+
+namespace hhg {
+void set_thread_error(const std::string& msg) {
+  g_last_error = msg;
+  g_has_error = true;
+}
+}  // namespace hhg

@@ -14,6 +14,9 @@ struct SolveTables {
   int row0, row1;    // k-grid rows m1 in [row0, row1) are propagated (a slab of a sharded solve);
                      // J is still normalised by the full Nk, so slab currents add up
 
+  int step0, step1;  // one launch propagates steps [step0, step1); 0 and nt for the whole pulse.  A pulse run
+                     // as consecutive chunks gives the same rho and current bit for bit.
+
   int hermitian;     // placed H0 and r are Hermitian-symmetric on the grid: [H,X] = HX - (HX)^+
   double dt;         // au
   int nax, ax_id[3]; // field axes with a non-zero polarisation component
@@ -85,6 +88,9 @@ int launch_group_batch(const LaunchShape& s, const BatchDesc* descs, const int2*
 // If `after_propagate` is non-null it is recorded between the propagation and the reduction.
 int launch_propagate(const SolveTables& t, const GroupTables& gt, const LaunchShape& s, double2* rho, double2* Jpart,
                      double2* J, cudaStream_t stream, cudaEvent_t after_propagate = nullptr);
+// The propagation launch alone (steps [t.step0, t.step1)), without the reduction.
+void launch_propagate_steps(const SolveTables& t, const GroupTables& gt, const LaunchShape& s, double2* rho,
+                            double2* Jpart, cudaStream_t stream);
 
 // Same as launch_propagate, with the current partials in a fixed device array owned by the
 // library instead of a caller buffer (see noalloc.cu).  Returns 0, or -1 with a reason in `why`.

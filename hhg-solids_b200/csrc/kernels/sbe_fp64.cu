@@ -109,8 +109,8 @@ __global__ void __launch_bounds__(kKptMaxThreads) propagate_kpt_kernel(SolveTabl
       sTk[c * nthr + tid] = cmul(t.T1[wrap_mod((long long)m1 * n.x, t.N1)], t.T2[wrap_mod((long long)m2 * n.y, t.N2)]);
     }
 
-    for (int ti0 = 0; ti0 < t.nt; ti0 += kRing) {
-      const int nsteps = min(kRing, t.nt - ti0);
+    for (int ti0 = t.step0; ti0 < t.step1; ti0 += kRing) {
+      const int nsteps = min(kRing, t.step1 - ti0);
       __syncthreads();
       for (int idx = tid; idx < nsteps * ncw; idx += nthr) sQ[idx] = t.Q[(size_t)ti0 * ncw + idx];
       for (int idx = tid; idx < nsteps * 9; idx += nthr) sE[idx] = t.es[(size_t)ti0 * 9 + idx];
@@ -472,8 +472,9 @@ bool plan_propagate(const SolveTables& t, int precision, int sm_count, LaunchSha
   return plan_group(t, precision, sm_count, out, why, why_len);
 }
 
-int launch_propagate(const SolveTables& t, const GroupTables& gt, const LaunchShape& s, double2* rho, double2* Jpart,
-                     double2* J, cudaStream_t stream, cudaEvent_t after_propagate) {
+void launch_propagate_steps(const SolveTables& t, const GroupTables& gt, const LaunchShape& s, double2* rho,
+                            double2* Jpart, cudaStream_t stream) {
+  if (t.step0 >= t.step1) return;
   if (s.kernel == 0) {
     KptKernel kern = kpt_kernel_for(t);
     cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s.smem);
@@ -481,6 +482,11 @@ int launch_propagate(const SolveTables& t, const GroupTables& gt, const LaunchSh
   } else {
     launch_group(t, gt, s, rho, Jpart, stream);
   }
+}
+
+int launch_propagate(const SolveTables& t, const GroupTables& gt, const LaunchShape& s, double2* rho, double2* Jpart,
+                     double2* J, cudaStream_t stream, cudaEvent_t after_propagate) {
+  launch_propagate_steps(t, gt, s, rho, Jpart, stream);
   if (after_propagate) cudaEventRecord(after_propagate, stream);
   const int n = 3 * t.nt;
   reduce_current_kernel<<<(n + 255) / 256, 256, 0, stream>>>(Jpart, s.vctas, t.nt, 1.0 / (double)t.Nk, J);

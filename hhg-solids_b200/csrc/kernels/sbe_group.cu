@@ -352,13 +352,14 @@ __device__ __forceinline__ void group_vctas(const SolveTables& t, const GroupDat
       }
     };
 
-    make_phases(0);
-    if (t.nt > 1) make_phases(1);
+    const int step0 = t.step0, step1 = t.step1;
+    make_phases(step0);
+    if (step0 + 1 < step1) make_phases(step0 + 1);
     __syncthreads();
-    inner_sums(0);
+    inner_sums(step0);
     __syncthreads();
 
-    for (int ti = 0; ti < t.nt; ++ti) {
+    for (int ti = step0; ti < step1; ++ti) {
       const int buf = ti & 1;
       // (1) outer sums over n1 for this k-point: H0(k - A), r_a(k - A), W_a(k)
       V h0[EPT], rk[3][EPT];
@@ -409,8 +410,8 @@ __device__ __forceinline__ void group_vctas(const SolveTables& t, const GroupDat
         }
       }
       // (2) next step's phase factors and inner sums, off this step's critical path
-      if (ti + 2 < t.nt) make_phases(ti + 2);
-      if (ti + 1 < t.nt) inner_sums(ti + 1);
+      if (ti + 2 < step1) make_phases(ti + 2);
+      if (ti + 1 < step1) inner_sums(ti + 1);
 
       // (3) RK4 stages (src/solver.cpp:157-163): fields at t, t+dt/2, t+dt/2, t+dt
       const double* esb = t.es + (size_t)ti * 9;
@@ -528,9 +529,9 @@ __device__ __forceinline__ void group_vctas(const SolveTables& t, const GroupDat
         }
       __syncthreads();
       // Flush a completed ring half: the other half is being written meanwhile.
-      if (s == kJRing - 1 || ti == t.nt - 1) {
-        const int ti0 = ti - s, nsteps = s + 1;
-        const double* half = sJ + (size_t)slot * kJRing * nwarps * 2 * nj;
+      if (s == kJRing - 1 || ti == step1 - 1) {
+        const int ti0 = max(ti - s, step0), nsteps = ti - ti0 + 1;  // a chunk may start inside a ring half
+        const double* half = sJ + ((size_t)slot * kJRing + (ti0 % kJRing)) * nwarps * 2 * nj;
         for (int idx = tid; idx < nsteps * nj; idx += nthr) {
           const int ss = idx / nj, a = idx % nj;
           double re = 0.0, im = 0.0;

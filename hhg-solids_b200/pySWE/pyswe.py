@@ -87,6 +87,19 @@ def _load(path: str):
         L.SWEBatch_last_error.argtypes = [vp]
         L.SWEBatch_last_error.restype = ct.c_char_p
         L.SWEBatch_delete.argtypes = [vp]
+        L.SWEServer_new.argtypes = [ct.c_int, ct.c_longlong, ct.c_int, ct.c_int]
+        L.SWEServer_new.restype = vp
+        L.SWEServer_submit.argtypes = [vp, vp]
+        L.SWEServer_submit.restype = ct.c_longlong
+        L.SWEServer_wait.argtypes = [vp, ct.c_longlong, ct.c_double]
+        L.SWEServer_status.argtypes = [vp, ct.c_longlong]
+        L.SWEServer_times.argtypes = [vp, ct.c_longlong, ND_POINTER_1_double]
+        L.SWEServer_ticket_error.argtypes = [vp, ct.c_longlong]
+        L.SWEServer_ticket_error.restype = ct.c_char_p
+        L.SWEServer_stats.argtypes = [vp, ND_POINTER_1_double, ct.c_int]
+        L.SWEServer_delete.argtypes = [vp]
+        L.HHG_last_error.argtypes = []
+        L.HHG_last_error.restype = ct.c_char_p
         L.SWESim_get_rho_k.argtypes = [vp, ND_POINTER_1_complex]
         L.SWESim_get_fields.argtypes = [vp, ND_POINTER_1_double, ND_POINTER_1_double, ND_POINTER_1_double]
     _libs[path] = (L, ext)
@@ -125,10 +138,11 @@ class Settings:
 
 
 class SWE:
-    """One propagation: setup on construction (SWESim_init), then run_simulation / get_current."""
+    """One propagation: setup on construction (SWESim_init), then run_simulation / get_current.
+    ``defer_init=True`` skips the setup (for a request handed to :class:`SWEServer`)."""
 
     def __init__(self, settings: Settings, device: int | None = None, k_rows: tuple | None = None,
-                 precision: str = "fp64"):
+                 precision: str = "fp64", defer_init: bool = False):
         self.settings = settings
         self.swe_cpp, self._ext = _load(settings.path_lib)
         self.ptr = self.swe_cpp.SWESim_new()
@@ -144,7 +158,8 @@ class SWE:
             self._call("SWESim_set_precision", 1)
         self.set_path_tb(settings.path_tb.encode("UTF-8"))
         self.set_settings(settings.ptr)
-        self.init()
+        if not defer_init:
+            self.init()
 
     def _call(self, name, *args):
         if self.ptr is None:
@@ -267,5 +282,79 @@ class SWEBatch:
     def __del__(self):
         try:
             self.delete()
+        except Exception:
+            pass
+
+
+class SWEServer:
+    """Request loop with continuous batching on one GPU (``SWEServer_*`` of the library).
+
+    ``submit(swe)`` queues a :class:`SWE` (built with ``defer_init=True``, or already set up) and
+    returns a ticket; the server admits requests by device-memory footprint, runs the admitted ones
+    together in chunks of ``chunk_steps`` RK4 steps, and completes each ticket when its pulse ends.
+    ``wait(ticket)`` blocks until then; the solve's current is read with its own ``get_current()``.
+    ``hbm_budget=0`` takes 80 % of the free device memory."""
+
+    def __init__(self, device: int = 0, hbm_budget: int = 0, max_active: int = 32, chunk_steps: int = 256,
+                 path_lib: str | None = None):
+        self.ptr = None
+        self.lib, ext = _load(path_lib or default_library())
+        if not ext:
+            raise SWEError("SWEServer needs this package's library")
+        self.ptr = self.lib.SWEServer_new(int(device), int(hbm_budget), int(max_active), int(chunk_steps))
+        if not self.ptr:
+            msg = self.lib.HHG_last_error()
+            raise SWEError(msg.decode() if msg else "SWEServer_new failed")
+        self._held = {}
+
+    def submit(self, swe: SWE) -> int:
+        t = int(self.lib.SWEServer_submit(self.ptr, swe.ptr))
+        if t < 0:
+            msg = self.lib.HHG_last_error()
+            raise SWEError(msg.decode() if msg else "SWEServer_submit failed")
+        self._held[t] = swe  # the SWESim and its Settings must outlive the request
+        return t
+
+    def wait(self, ticket: int, timeout: float | None = None) -> bool:
+        """True when done, False on timeout; raises SWEError if the request failed."""
+        rc = int(self.lib.SWEServer_wait(self.ptr, int(ticket), -1.0 if timeout is None else float(timeout)))
+        if rc == 1:
+            self._held.pop(ticket, None)
+            return True
+        if rc == 0:
+            return False
+        if rc == -2:
+            raise SWEError(f"unknown ticket {ticket}")
+        msg = self.lib.SWEServer_ticket_error(self.ptr, int(ticket))
+        self._held.pop(ticket, None)
+        raise SWEError(msg.decode() if msg else "request failed")
+
+    _STATES = {0: "queued", 1: "setting up", 2: "running", 3: "done", -1: "failed", -2: "unknown"}
+
+    def status(self, ticket: int) -> str:
+        return self._STATES[int(self.lib.SWEServer_status(self.ptr, int(ticket)))]
+
+    def times(self, ticket: int) -> dict:
+        out = np.zeros(4)
+        self.lib.SWEServer_times(self.ptr, int(ticket), out)
+        return {"submit": out[0], "admit": out[1], "start": out[2], "done": out[3]}
+
+    def stats(self) -> dict:
+        out = np.zeros(9)
+        self.lib.SWEServer_stats(self.ptr, out, 9)
+        keys = ("completed", "failed", "chunks", "gpu_ms", "peak_running", "peak_bytes", "budget_bytes", "queued",
+                "admitted")
+        return {k: (float(v) if k == "gpu_ms" else int(v)) for k, v in zip(keys, out)}
+
+    def close(self):
+        """Serves everything submitted, then stops the server."""
+        if self.ptr is not None:
+            self.lib.SWEServer_delete(self.ptr)
+            self.ptr = None
+            self._held.clear()
+
+    def __del__(self):
+        try:
+            self.close()
         except Exception:
             pass

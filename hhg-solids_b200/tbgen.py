@@ -140,6 +140,8 @@ MODELS = {
     "tmd11_s1": (random_tmd, {"nw": 11, "seed": 1}),
     "tmd11_s3": (random_tmd, {"nw": 11, "seed": 3}),
     "tmd11_s2": (random_tmd, {"nw": 11, "seed": 2}),
+    "tmd12_s1": (random_tmd, {"nw": 12, "seed": 1}),
+    "tmd12_s2": (random_tmd, {"nw": 12, "seed": 2}),
     "tmd12_s3": (random_tmd, {"nw": 12, "seed": 3}),
     "tmd5_s4": (random_tmd, {"nw": 5, "seed": 4, "window": 5}),
 }

@@ -25,6 +25,7 @@ extern "C" {
 typedef struct SWESim SWESim;
 typedef struct Settings Settings;
 typedef struct SWEBatch SWEBatch;
+typedef struct SWEServer SWEServer;
 /* std::complex<double> / numpy complex128 layout: {re, im}. */
 typedef struct hhg_cdouble {
   double re, im;
@@ -146,6 +147,34 @@ int SWEBatch_run(SWEBatch* batch);
 double SWEBatch_last_ms(SWEBatch* batch);
 const char* SWEBatch_last_error(SWEBatch* batch);
 void SWEBatch_delete(SWEBatch* batch);
+
+/* Serving (no counterpart in the reference, whose pol_scan script runs one solve per MPI rank):
+ * a request loop with continuous batching on one device.  A request is a SWESim with its TB path,
+ * settings and precision set; SWESim_init is optional (the server sets it up when it admits it).
+ * Requests are admitted in arrival order while their device memory (an upper bound before setup,
+ * the exact figure after) fits in hbm_budget_bytes beside the running ones and fewer than max_active
+ * are running; a request larger than the budget runs when nothing else does.  Running solves advance
+ * together in chunks of chunk_steps RK4 steps, newly admitted ones joining at the next chunk.  When a
+ * solve finishes, its current is readable with SWESim_get_current and its device memory is returned
+ * (SWESim_init again to reuse the object).  Each result equals, bit for bit, what the same solve
+ * gives alone.  The SWESim and its Settings must outlive the request. */
+/* device: CUDA ordinal; hbm_budget_bytes 0: 80 % of the device memory free at creation. NULL on error (HHG_last_error). */
+SWEServer* SWEServer_new(int device, long long hbm_budget_bytes, int max_active, int chunk_steps);
+/* Queues a request; returns its ticket (>= 0), or -1 (HHG_last_error). */
+long long SWEServer_submit(SWEServer* srv, SWESim* swe);
+/* Blocks until the ticket completes or timeout_s passes (< 0: no limit).
+ * 1 done, -1 failed (SWEServer_ticket_error), 0 timed out, -2 unknown ticket. */
+int SWEServer_wait(SWEServer* srv, long long ticket, double timeout_s);
+/* 0 queued, 1 setting up, 2 running, 3 done, -1 failed, -2 unknown. */
+int SWEServer_status(SWEServer* srv, long long ticket);
+/* Seconds since the server started: submitted, admitted, first chunk, done (0 if not yet). Returns the status. */
+int SWEServer_times(SWEServer* srv, long long ticket, double* out4);
+const char* SWEServer_ticket_error(SWEServer* srv, long long ticket);
+/* Fills up to n of: completed, failed, chunks, GPU ms in chunks, peak running solves, peak reserved
+ * bytes, budget bytes, queued, admitted; returns the count written. */
+int SWEServer_stats(SWEServer* srv, double* out, int n);
+/* Serves every request already submitted, then stops the scheduler and frees the server. */
+void SWEServer_delete(SWEServer* srv);
 
 /* FP64 FMA / FP32 FMA chain throughput of the current device (TFLOP/s), for roofline denominators. */
 int HHG_measure_peaks(double* fp64_tflops, double* fp32_tflops);

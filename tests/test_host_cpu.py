@@ -138,3 +138,21 @@ def test_reference_wrapper_binds_this_library():
         t, jx, jy, jz = swe.get_current()
         assert np.all(t == 0)
     swe.delete()
+
+
+@pytest.mark.skipif(gpu_available(), reason="checks the no-GPU behaviour")
+def test_server_without_gpu_fails_loudly():
+    from pySWE import pyswe
+
+    with pytest.raises(pyswe.SWEError, match="no CUDA device"):
+        pyswe.SWEServer()
+
+
+def test_deferred_request_holds_no_device_state():
+    """A request built for the server (defer_init) only records its settings: no device call."""
+    from pySWE import pyswe
+
+    swe = pyswe.SWE(pyswe.Settings(_param()), precision="mixed", defer_init=True)
+    with pytest.raises(pyswe.SWEError, match="SWESim_init"):
+        swe.get_current()
+    swe.delete()
