@@ -74,7 +74,7 @@ struct SWEBatch {
     check_cuda(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device), "cudaDeviceGetAttribute");
 
     // Kernel-shape classes of the element-group solves; the others run alone.
-    std::map<std::tuple<int, int, int, int, int, int, int, int>, std::vector<int>> classes;
+    std::map<std::tuple<int, int, int, int, int, int, int, int, int>, std::vector<int>> classes;
     std::vector<int> alone;
     for (int i = 0; i < (int)sims.size(); ++i) {
       const hhg::LaunchShape& sh = sims[i]->shape;
@@ -82,7 +82,7 @@ struct SWEBatch {
         alone.push_back(i);
       } else {
         const hhg::SolveTables& t = sims[i]->tab;
-        classes[std::make_tuple(sh.kernel, sh.variant, sh.ept, sh.threads, sh.group, t.nw, t.nax, t.nj)].push_back(i);
+        classes[std::make_tuple(sh.kernel, sh.variant, sh.ept, sh.threads, sh.group, sh.kmode, t.nw, t.nax, t.nj)].push_back(i);
       }
     }
     groups = (int)classes.size();
@@ -421,7 +421,7 @@ struct SWEServer {
   void launch_chunk() {
     int sms = 0;
     check_cuda(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device), "cudaDeviceGetAttribute");
-    std::map<std::tuple<int, int, int, int, int, int, int, int>, std::vector<int>> classes;
+    std::map<std::tuple<int, int, int, int, int, int, int, int, int>, std::vector<int>> classes;
     std::vector<int> alone;
     h_desc.assign(active.size(), hhg::BatchDesc{});
     for (int i = 0; i < (int)active.size(); ++i) {
@@ -445,8 +445,8 @@ struct SWEServer {
       if (sh.kernel == 0)
         alone.push_back(i);
       else
-        classes[std::make_tuple(sh.kernel, sh.variant, sh.ept, sh.threads, sh.group, sim->tab.nw, sim->tab.nax,
-                                sim->tab.nj)].push_back(i);
+        classes[std::make_tuple(sh.kernel, sh.variant, sh.ept, sh.threads, sh.group, sh.kmode, sim->tab.nw,
+                                sim->tab.nax, sim->tab.nj)].push_back(i);
     }
     h_items.clear();
     std::vector<std::pair<size_t, size_t>> ranges;

@@ -128,6 +128,10 @@ void SWESim::init() {
         "SWESim_init: nr1 and nr2 must be even and >= 4 (odd sizes shift the reference's fftshift/ifftshift pair "
         "by one cell; sizes below 4 put its 4x4 current window outside the grid)");
   if (nt < 2) throw std::runtime_error("SWESim_init: tmax/dt must give at least 2 time steps");
+  if (solver == 1 && N1 != N2)
+    throw std::runtime_error(
+        "SWESim_init: the k-space solver needs nr1 == nr2 (its interpolation reads the grid as data[yi*nr1 + xi] "
+        "with yi along the second axis, src/interpolation.cpp:36-37, which scrambles a non-square grid)");
   if (nw > hhg::kMaxOrb) throw std::runtime_error("SWESim_init: more than 16 orbitals is not supported");
   if ((long)N1 * N2 > (1L << 30)) throw std::runtime_error("SWESim_init: grid too large");
   Nk = N1 * N2;
@@ -270,11 +274,85 @@ void SWESim::init() {
       for (int o = 0; o < nw2; ++o) Vd[((size_t)a * hhg::kWindow + w) * nw2 + o] = d2(vw[((size_t)j_id[a] * hhg::kWindow + w) * nw2 + o]);
   const int nwin = (int)win_n.size();
 
-  // Peierls phase e^{i A(t_i).R_c} of every listed cell at every step (src/swe.cpp:225-233), R_c the
-  // cell's supercell position in bohr.
+  // Coordinates the propagation sums over.  The k-space solver interpolates H_eff(k - A) from the
+  // grid read as data[yi*N + xi] with xi along the first fractional coordinate (src/interpolation.cpp:
+  // 17-43): on a square grid that evaluates the model with its cells transposed, n -> (n2, n1).
+  cellp = cell_n;
+  if (solver == 1)
+    for (auto& n : cellp) std::swap(n.x, n.y);
   const int ncw = ncell + nwin;
-  Q.assign((size_t)nt * ncw, make_double2(1.0, 0.0));
-  {
+  // Per-cell factors of every evaluation point.  Real-space solver: the Peierls phase
+  // e^{i A(t_i).R_c} of step i (src/swe.cpp:225-233), R_c the cell's supercell position in bohr.
+  // k-space solver: the bicubic interpolation at k - A_s (src/solver_kspace.cpp:286-305) acts on the
+  // cell (n1', n2') as the factor Cx(n1') Cy(n2'), Cx(q) = sum_a w_a(tx) e^{-2 pi i (ox + a) q / N}
+  // over the Catmull-Rom weights w of the stencil offsets a = -1..2 (src/interpolation.cpp:8-14),
+  // where ox + tx = -N u_A and u_A is the first fractional coordinate of A_s (Cramer solve against
+  // the reciprocal vectors, src/vec3_util.cpp:13-36); Cy likewise from the second.  Points 2i, 2i+1,
+  // 2i+2 are A(t_i), the mean of A(t_i) and A(t_i+1), A(t_i+1) (clamped at the last step).
+  const int npts = solver == 1 ? 2 * nt + 1 : nt;
+  int np_ = 2;
+  for (int c = 0; c < ncell; ++c) np_ = std::max(np_, std::max(std::abs(cellp[c].x), std::abs(cellp[c].y)));
+  const int npw = 2 * np_ + 1;
+  std::vector<double2> Cfac;  // k-space solver: [npts][2][npw] factors Cx, Cy at n = -np..np
+  if (solver == 1) {
+    double bA[3][3];  // reciprocal vectors (1/Angstrom, src/grid.cpp:27-46), then in au
+    {
+      const double(*a)[3] = model.lattice;
+      double cr[3][3];
+      for (int r = 0; r < 3; ++r) {
+        const int p = (r + 1) % 3, q = (r + 2) % 3;
+        cr[r][0] = a[p][1] * a[q][2] - a[p][2] * a[q][1];
+        cr[r][1] = a[p][2] * a[q][0] - a[p][0] * a[q][2];
+        cr[r][2] = a[p][0] * a[q][1] - a[p][1] * a[q][0];
+      }
+      const double vol = a[0][0] * cr[0][0] + a[0][1] * cr[0][1] + a[0][2] * cr[0][2];
+      for (int r = 0; r < 3; ++r)
+        for (int c = 0; c < 3; ++c) bA[r][c] = 2.0 * M_PI / vol * cr[r][c] / kA2Bohr;
+    }
+    double* brows[3] = {bA[0], bA[1], bA[2]};
+    Cfac.assign((size_t)npts * 2 * npw, make_double2(0.0, 0.0));
+    const int N = N1;
+    for (int j = 0; j < npts; ++j) {
+      const int i = std::min(j / 2, nt - 1);
+      double Aj[3];
+      for (int a = 0; a < 3; ++a) {
+        const double* Aa = A.data() + (size_t)a * nt;
+        if (j == 2 * nt || (j % 2 == 1 && i == nt - 1))
+          Aj[a] = Aa[nt - 1];
+        else if (j % 2 == 1)
+          Aj[a] = 0.5 * Aa[i] + 0.5 * Aa[i + 1];
+        else
+          Aj[a] = Aa[j / 2];
+      }
+      double crd[3];
+      hhg::refarith::cramer3(brows, Aj, crd);
+      for (int d = 0; d < 2; ++d) {
+        const double x0 = -crd[d] * (double)N;
+        const double o = std::floor(x0), tt = x0 - o;
+        const double w[4] = {((-0.5 * tt + 1.0) * tt - 0.5) * tt, (1.5 * tt - 2.5) * tt * tt + 1.0,
+                             ((-1.5 * tt + 2.0) * tt + 0.5) * tt, (0.5 * tt - 0.5) * tt * tt};
+        const long ox = (long)o;
+        for (int n = -np_; n <= np_; ++n) {
+          cd acc(0.0, 0.0);
+          for (int a = -1; a <= 2; ++a) {
+            const int m = wrapi((ox + a) * (long)n, N);
+            const double ang = 2.0 * M_PI * (double)m / (double)N;
+            acc += w[a + 1] * cd(std::cos(ang), -std::sin(ang));
+          }
+          Cfac[((size_t)j * 2 + d) * npw + (n + np_)] = d2(acc);
+        }
+      }
+    }
+  }
+  Q.assign((size_t)npts * ncw, make_double2(1.0, 0.0));
+  if (solver == 1) {
+    for (int j = 0; j < npts; ++j)
+      for (int c = 0; c < ncell; ++c) {
+        const cd cx = cd(Cfac[((size_t)j * 2 + 0) * npw + cellp[c].x + np_].x, Cfac[((size_t)j * 2 + 0) * npw + cellp[c].x + np_].y);
+        const cd cy = cd(Cfac[((size_t)j * 2 + 1) * npw + cellp[c].y + np_].x, Cfac[((size_t)j * 2 + 1) * npw + cellp[c].y + np_].y);
+        Q[(size_t)j * ncw + c] = d2(cx * cy);
+      }
+  } else {
     std::vector<double> Rc((size_t)ncw * 3);
     for (int c = 0; c < ncw; ++c) {
       const int2 n = c < ncell ? cell_n[c] : win_n[c - ncell];
@@ -293,33 +371,35 @@ void SWESim::init() {
   // Dense bounding box of the support cells for the separable Wannier sum.
   int b1lo = 0, b1hi = 0, b2lo = 0, b2hi = 0;
   for (int c = 0; c < ncell; ++c) {
-    if (c == 0 || cell_n[c].x < b1lo) b1lo = cell_n[c].x;
-    if (c == 0 || cell_n[c].x > b1hi) b1hi = cell_n[c].x;
-    if (c == 0 || cell_n[c].y < b2lo) b2lo = cell_n[c].y;
-    if (c == 0 || cell_n[c].y > b2hi) b2hi = cell_n[c].y;
+    if (c == 0 || cellp[c].x < b1lo) b1lo = cellp[c].x;
+    if (c == 0 || cellp[c].x > b1hi) b1hi = cellp[c].x;
+    if (c == 0 || cellp[c].y < b2lo) b2lo = cellp[c].y;
+    if (c == 0 || cellp[c].y > b2hi) b2hi = cellp[c].y;
   }
   const int b1n = ncell ? b1hi - b1lo + 1 : 1, b2n = ncell ? b2hi - b2lo + 1 : 1;
   // Box table [1 + nax][b1n][b2n][nw2]: H0, then the field-coupled r of each active axis.
   Xbox.assign((size_t)(1 + nax) * b1n * b2n * nw2, make_double2(0.0, 0.0));
   for (int c = 0; c < ncell; ++c) {
-    const size_t box = (size_t)(cell_n[c].x - b1lo) * b2n + (cell_n[c].y - b2lo);
+    const size_t box = (size_t)(cellp[c].x - b1lo) * b2n + (cellp[c].y - b2lo);
     for (int o = 0; o < nw2; ++o) {
       Xbox[box * nw2 + o] = H0[(size_t)c * nw2 + o];
       for (int a = 0; a < nax; ++a)
         Xbox[((size_t)(1 + a) * b1n * b2n + box) * nw2 + o] = Rtab[((size_t)a * ncell + c) * nw2 + o];
     }
   }
-  // e^{i n A(t_i).a_1}, e^{i n A(t_i).a_2} for |n| <= np.
-  int np_ = 2;
-  for (int c = 0; c < ncell; ++c) np_ = std::max(np_, std::max(std::abs(cell_n[c].x), std::abs(cell_n[c].y)));
-  const int npw = 2 * np_ + 1;
-  P.assign((size_t)nt * 2 * npw, make_double2(1.0, 0.0));
-  for (int ti = 0; ti < nt; ++ti) {
-    const double ax = A[ti], ay = A[nt + ti], az = A[2 * (size_t)nt + ti];
-    for (int d = 0; d < 2; ++d) {
-      const double th = ax * lat_au[d][0] + ay * lat_au[d][1] + az * lat_au[d][2];
-      for (int n = -np_; n <= np_; ++n)
-        P[((size_t)ti * 2 + d) * npw + (n + np_)] = make_double2(std::cos(n * th), std::sin(n * th));
+  // Separable factors per point: e^{i n A(t_i).a_1}, e^{i n A(t_i).a_2} for |n| <= np (real-space
+  // solver), Cx and Cy (k-space solver).
+  if (solver == 1) {
+    P = Cfac;
+  } else {
+    P.assign((size_t)nt * 2 * npw, make_double2(1.0, 0.0));
+    for (int ti = 0; ti < nt; ++ti) {
+      const double ax = A[ti], ay = A[nt + ti], az = A[2 * (size_t)nt + ti];
+      for (int d = 0; d < 2; ++d) {
+        const double th = ax * lat_au[d][0] + ay * lat_au[d][1] + az * lat_au[d][2];
+        for (int n = -np_; n <= np_; ++n)
+          P[((size_t)ti * 2 + d) * npw + (n + np_)] = make_double2(std::cos(n * th), std::sin(n * th));
+      }
     }
   }
   tab.nwin = nwin;
@@ -359,11 +439,12 @@ void SWESim::init() {
 
   trace.mark("tables");
   // Device tables.
-  h2d_bytes = sizeof(int2) * (cell_n.size() + win_n.size()) +
+  h2d_bytes = sizeof(int2) * (cell_n.size() + cellp.size() + win_n.size()) +
               sizeof(double2) * (H0.size() + Rtab.size() + V.size() + Q.size() + Xbox.size() + Vd.size() + P.size() +
                                  T1.size() + T2.size()) +
               sizeof(double) * es.size();
   d_cell.upload(cell_n, stream);
+  d_cellp.upload(cellp, stream);
   d_win.upload(win_n, stream);
   d_H0.upload(H0, stream);
   d_R.upload(Rtab, stream);
@@ -419,7 +500,8 @@ void SWESim::init() {
   }
   tab.es = d_es.p;
   tab.ncell = ncell;
-  tab.cell_n = d_cell.p;
+  tab.cell_n = d_cellp.p;
+  tab.kmode = solver;
   tab.H0 = d_H0.p;
   tab.R = d_R.p;
   tab.win_n = d_win.p;
@@ -443,7 +525,11 @@ void SWESim::init() {
   }
 
   // Equilibrium density matrix (src/swe.cpp:82-90) on the GPU.
-  hhg::launch_rho0_fp64(tab, d_rho0.p, stream);
+  {
+    hhg::SolveTables t0 = tab;  // the model's own cell coordinates
+    t0.cell_n = d_cell.p;
+    hhg::launch_rho0_fp64(t0, d_rho0.p, stream);
+  }
   check_cuda(cudaGetLastError(), "rho0 launch");
   check_cuda(cudaMemcpyAsync(d_rho.p, d_rho0.p, sizeof(double2) * (size_t)Nk * nw2, cudaMemcpyDeviceToDevice, stream),
              "D2D");
@@ -454,7 +540,7 @@ void SWESim::init() {
 }
 
 size_t SWESim::device_bytes() const {
-  size_t b = d_cell.cap * sizeof(int2) + d_win.cap * sizeof(int2) + d_es.cap * sizeof(double);
+  size_t b = (d_cell.cap + d_cellp.cap + d_win.cap) * sizeof(int2) + d_es.cap * sizeof(double);
   for (const auto* x : {&d_H0, &d_R, &d_V, &d_Q, &d_Xbox, &d_Vd, &d_P, &d_T1, &d_T2, &d_rho0, &d_rho, &d_Jpart, &d_J})
     b += x->cap * sizeof(double2);
   for (const auto* x : {&d_Xbox32, &d_Vd32, &d_P32, &d_T1_32, &d_T2_32}) b += x->cap * sizeof(float2);
@@ -753,6 +839,14 @@ void SWESim_set_precision(SWESim* swe, int mode) {
   guarded(swe, "SWESim_set_precision", [&] {
     if (mode != 0 && mode != 1) throw std::runtime_error("SWESim_set_precision: mode must be 0 (plain FP64) or 1 (mixed)");
     swe->precision = mode;
+  });
+}
+
+void SWESim_set_solver(SWESim* swe, int mode) {
+  guarded(swe, "SWESim_set_solver", [&] {
+    if (mode != 0 && mode != 1)
+      throw std::runtime_error("SWESim_set_solver: mode must be 0 (real-space solver) or 1 (k-space solver)");
+    swe->solver = mode;
   });
 }
 

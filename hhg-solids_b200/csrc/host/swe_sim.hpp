@@ -84,13 +84,15 @@ struct SWESim {
   std::vector<int2> cell_n, win_n;
   std::vector<double2> H0, Rtab, V, Q, Xbox, Vd, P, T1, T2;
   int precision = 0;  // 0 plain FP64, 1 mixed
+  int solver = 0;     // 0 the real-space solver (src/solver.cpp), 1 the k-space solver (src/solver_kspace.cpp)
+  std::vector<int2> cellp;  // cell coordinates the propagation sums over (transposed for the k-space solver)
   unsigned generation = 0;  // bumped by every successful SWESim_init (batches re-capture on change)
   int nax = 0, ax_id[3] = {0, 0, 0}, nj = 0, j_id[3] = {0, 0, 0};
 
   cudaStream_t stream = nullptr;
   int stream_device = -1;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr, evm = nullptr;
-  hhg::DevBuf<int2> d_cell, d_win;
+  hhg::DevBuf<int2> d_cell, d_cellp, d_win;
   hhg::DevBuf<double2> d_H0, d_R, d_V, d_Q, d_Xbox, d_Vd, d_P, d_T1, d_T2, d_rho0, d_rho, d_Jpart, d_J;
   hhg::DevBuf<float2> d_Xbox32, d_Vd32, d_P32, d_T1_32, d_T2_32;
   hhg::GroupTables gtab{};
@@ -115,6 +117,7 @@ struct SWESim {
 
   void release() {
     d_cell.release();
+    d_cellp.release();
     d_win.release();
     for (auto* b : {&d_H0, &d_R, &d_V, &d_Q, &d_Xbox, &d_Vd, &d_P, &d_T1, &d_T2, &d_rho0, &d_rho, &d_Jpart, &d_J})
       b->release();

@@ -17,6 +17,11 @@ struct SolveTables {
   int step0, step1;  // one launch propagates steps [step0, step1); 0 and nt for the whole pulse.  A pulse run
                      // as consecutive chunks gives the same rho and current bit for bit.
 
+  int kmode;         // 0: the real-space solver (src/solver.cpp); 1: the k-space solver (src/solver_kspace.cpp),
+                     // whose stages see H at three points per step (t, t + dt/2, t + dt): Q and P are then
+                     // tables of evaluation points 0 .. 2 nt (point 2i + s/2 for stage s of step i) and the
+                     // window carries no phase
+
   int hermitian;     // placed H0 and r are Hermitian-symmetric on the grid: [H,X] = HX - (HX)^+
   double dt;         // au
   int nax, ax_id[3]; // field axes with a non-zero polarisation component
@@ -31,7 +36,8 @@ struct SolveTables {
   int nwin;
   const int2* win_n;    // [nwin]
   const double2* V;     // [nj][nwin][nw2] velocity on the window cells
-  const double2* Q;     // [nt][ncell + nwin] Peierls phase e^{i A(t_i).R_c} of each listed cell
+  const double2* Q;     // [nt][ncell + nwin] Peierls phase e^{i A(t_i).R_c} of each listed cell (k-space
+                        // solver: [2 nt + 1][ncell + nwin] interpolation multipliers, window entries 1)
 
   // Bounding box of the occupied cells (element-group kernel, tables in GroupTables).
   int b1lo, b1n, b2lo, b2n;
@@ -59,6 +65,7 @@ struct LaunchShape {
   int box_sm, win_sm;  // element groups: cell tables staged in shared memory
   int ept;             // element groups: matrix elements per thread
   int variant;         // element groups: compiled shape (-1: runtime-shaped instance)
+  int kmode;           // instance for the k-space solver (SolveTables::kmode)
   size_t smem;     // dynamic shared memory bytes
 };
 

@@ -71,7 +71,7 @@ __device__ __forceinline__ void flush_current(const SolveTables& t, const double
 constexpr int kKptMaxThreads = 512;
 
 // NAXc, NJc: field axes and current axes fixed at compile time (0: read from t).
-template <int NW, int NAXc, int NJc>
+template <int NW, int NAXc, int NJc, bool KM>
 __global__ void __launch_bounds__(kKptMaxThreads) propagate_kpt_kernel(SolveTables t, int vctas, double2* rho,
                                                                        double2* Jpart) {
   constexpr int NW2 = NW * NW;
@@ -82,8 +82,8 @@ __global__ void __launch_bounds__(kKptMaxThreads) propagate_kpt_kernel(SolveTabl
   double2* sR = sH + nc * NW2;                      // [nax][nc][NW2]
   double2* sV = sR + nax * nc * NW2;                // [nj][nwn][NW2]
   double2* sTk = sV + nj * nwn * NW2;               // [ncw][nthr]
-  double2* sQ = sTk + ncw * nthr;                   // [kRing][ncw]
-  double* sE = reinterpret_cast<double*>(sQ + kRing * ncw);  // [kRing][9]
+  double2* sQ = sTk + ncw * nthr;                   // [kRing (k-space solver: 2 kRing + 1)][ncw]
+  double* sE = reinterpret_cast<double*>(sQ + (t.kmode ? 2 * kRing + 1 : kRing) * ncw);  // [kRing][9]
   double* sJ = sE + kRing * 9;                      // [kRing][nwarps][2 nj]
 
   for (int idx = tid; idx < nc * NW2; idx += nthr) sH[idx] = t.H0[idx];
@@ -109,64 +109,81 @@ __global__ void __launch_bounds__(kKptMaxThreads) propagate_kpt_kernel(SolveTabl
       sTk[c * nthr + tid] = cmul(t.T1[wrap_mod((long long)m1 * n.x, t.N1)], t.T2[wrap_mod((long long)m2 * n.y, t.N2)]);
     }
 
+    constexpr bool km = KM;
+    // Hermitian parts of the Wannier sums of one evaluation point: diagonal real, upper triangle
+    // complex.  q = the point's row of per-cell factors.
+    double hd[NW], rd[3][NW];
+    double2 hu[NW2], ru[3][NW2], w[3][NW2];
+    auto box_sums = [&](const double2* q) {
+#pragma unroll
+      for (int i = 0; i < NW; ++i) {
+        hd[i] = 0.0;
+#pragma unroll
+        for (int a = 0; a < 3; ++a) rd[a][i] = 0.0;
+      }
+#pragma unroll
+      for (int e = 0; e < NW2; ++e) {
+        hu[e] = make_double2(0.0, 0.0);
+#pragma unroll
+        for (int a = 0; a < 3; ++a) ru[a][e] = make_double2(0.0, 0.0);
+      }
+#pragma unroll 2
+      for (int c = 0; c < nc; ++c) {
+        const double2 ph = cmul(sTk[c * nthr + tid], q[c]);
+        const double2* hc = sH + c * NW2;
+#pragma unroll
+        for (int i = 0; i < NW; ++i) {
+          hd[i] = fma(ph.x, hc[i * NW + i].x, fma(-ph.y, hc[i * NW + i].y, hd[i]));
+#pragma unroll
+          for (int j = i + 1; j < NW; ++j) hu[i * NW + j] = cfma(ph, hc[i * NW + j], hu[i * NW + j]);
+        }
+#pragma unroll
+        for (int a = 0; a < 3; ++a)
+          if (a < nax) {
+            const double2* rc = sR + (a * nc + c) * NW2;
+#pragma unroll
+            for (int i = 0; i < NW; ++i) {
+              rd[a][i] = fma(ph.x, rc[i * NW + i].x, fma(-ph.y, rc[i * NW + i].y, rd[a][i]));
+#pragma unroll
+              for (int j = i + 1; j < NW; ++j) ru[a][i * NW + j] = cfma(ph, rc[i * NW + j], ru[a][i * NW + j]);
+            }
+          }
+      }
+    };
+    // Window velocity W_a(k): q = the point's factors (Peierls), or none (k-space solver).
+    auto window_sums = [&](const double2* q) {
+#pragma unroll
+      for (int e = 0; e < NW2; ++e)
+#pragma unroll
+        for (int a = 0; a < 3; ++a) w[a][e] = make_double2(0.0, 0.0);
+#pragma unroll 2
+      for (int c = 0; c < nwn; ++c) {
+        const double2 ph = q ? cmul(sTk[(nc + c) * nthr + tid], q[nc + c]) : sTk[(nc + c) * nthr + tid];
+#pragma unroll
+        for (int a = 0; a < 3; ++a)
+          if (a < nj) {
+            const double2* vc = sV + (a * nwn + c) * NW2;
+#pragma unroll
+            for (int e = 0; e < NW2; ++e) w[a][e] = cfma(ph, vc[e], w[a][e]);
+          }
+      }
+    };
+    if (km) window_sums(nullptr);
+
+    const int ppr = km ? 2 : 1;  // evaluation points per step
     for (int ti0 = t.step0; ti0 < t.step1; ti0 += kRing) {
       const int nsteps = min(kRing, t.step1 - ti0);
+      const int nrows = km ? 2 * nsteps + 1 : nsteps;
       __syncthreads();
-      for (int idx = tid; idx < nsteps * ncw; idx += nthr) sQ[idx] = t.Q[(size_t)ti0 * ncw + idx];
+      for (int idx = tid; idx < nrows * ncw; idx += nthr) sQ[idx] = t.Q[(size_t)ppr * ti0 * ncw + idx];
       for (int idx = tid; idx < nsteps * 9; idx += nthr) sE[idx] = t.es[(size_t)ti0 * 9 + idx];
       __syncthreads();
       for (int s = 0; s < nsteps; ++s) {
-        // Wannier sums, Hermitian parts: diagonal real, upper triangle complex.
-        double hd[NW], rd[3][NW];
-        double2 hu[NW2], ru[3][NW2], w[3][NW2];
-#pragma unroll
-        for (int i = 0; i < NW; ++i) {
-          hd[i] = 0.0;
-#pragma unroll
-          for (int a = 0; a < 3; ++a) rd[a][i] = 0.0;
-        }
-#pragma unroll
-        for (int e = 0; e < NW2; ++e) {
-          hu[e] = make_double2(0.0, 0.0);
-#pragma unroll
-          for (int a = 0; a < 3; ++a) {
-            ru[a][e] = make_double2(0.0, 0.0);
-            w[a][e] = make_double2(0.0, 0.0);
-          }
-        }
-        const double2* q = sQ + s * ncw;
-#pragma unroll 2
-        for (int c = 0; c < nc; ++c) {
-          const double2 ph = cmul(sTk[c * nthr + tid], q[c]);
-          const double2* hc = sH + c * NW2;
-#pragma unroll
-          for (int i = 0; i < NW; ++i) {
-            hd[i] = fma(ph.x, hc[i * NW + i].x, fma(-ph.y, hc[i * NW + i].y, hd[i]));
-#pragma unroll
-            for (int j = i + 1; j < NW; ++j) hu[i * NW + j] = cfma(ph, hc[i * NW + j], hu[i * NW + j]);
-          }
-#pragma unroll
-          for (int a = 0; a < 3; ++a)
-            if (a < nax) {
-              const double2* rc = sR + (a * nc + c) * NW2;
-#pragma unroll
-              for (int i = 0; i < NW; ++i) {
-                rd[a][i] = fma(ph.x, rc[i * NW + i].x, fma(-ph.y, rc[i * NW + i].y, rd[a][i]));
-#pragma unroll
-                for (int j = i + 1; j < NW; ++j) ru[a][i * NW + j] = cfma(ph, rc[i * NW + j], ru[a][i * NW + j]);
-              }
-            }
-        }
-#pragma unroll 2
-        for (int c = 0; c < nwn; ++c) {
-          const double2 ph = cmul(sTk[(nc + c) * nthr + tid], q[nc + c]);
-#pragma unroll
-          for (int a = 0; a < 3; ++a)
-            if (a < nj) {
-              const double2* vc = sV + (a * nwn + c) * NW2;
-#pragma unroll
-              for (int e = 0; e < NW2; ++e) w[a][e] = cfma(ph, vc[e], w[a][e]);
-            }
+        if (!km) {
+          box_sums(sQ + s * ncw);
+          window_sums(sQ + s * ncw);
+        } else if (s == 0) {
+          box_sums(sQ);  // point t of the chunk's first step; later steps carry it from stage 4
         }
 
         // Four RK4 stages (src/solver.cpp:157-163), fields at t, t+dt/2, t+dt/2, t+dt.
@@ -175,6 +192,7 @@ __global__ void __launch_bounds__(kKptMaxThreads) propagate_kpt_kernel(SolveTabl
         for (int st = 0; st < 4; ++st) {
           const int f = st == 0 ? 0 : (st == 3 ? 2 : 1);
           const double* es = sE + s * 9 + f * 3;
+          if (km && st > 0 && st != 2) box_sums(sQ + (2 * s + f) * ncw);  // points t + dt/2, t + dt
           double2 H[NW2], X[NW2];
 #pragma unroll
           for (int i = 0; i < NW; ++i) {
@@ -413,19 +431,21 @@ double time_fma(int sms) {
 }
 
 size_t kpt_smem(const SolveTables& t, int threads) {
-  const int ncw = t.ncell + t.nwin;
-  const size_t n2 = (size_t)(t.ncell * t.nw2 * (1 + t.nax) + t.nj * t.nwin * t.nw2 + ncw * threads + kRing * ncw);
+  const int ncw = t.ncell + t.nwin, qrows = t.kmode ? 2 * kRing + 1 : kRing;
+  const size_t n2 = (size_t)(t.ncell * t.nw2 * (1 + t.nax) + t.nj * t.nwin * t.nw2 + ncw * threads + qrows * ncw);
   return n2 * sizeof(double2) + sizeof(double) * (kRing * 9 + kRing * (threads / 32) * 2 * t.nj);
 }
 
 using KptKernel = void (*)(SolveTables, int, double2*, double2*);
-KptKernel kpt_kernel_for(const SolveTables& t) {
+template <bool KM>
+KptKernel kpt_kernel_t(const SolveTables& t) {
   if (t.nw == 2 && t.nj == 2) {
-    if (t.nax == 1) return propagate_kpt_kernel<2, 1, 2>;
-    if (t.nax == 2) return propagate_kpt_kernel<2, 2, 2>;
+    if (t.nax == 1) return propagate_kpt_kernel<2, 1, 2, KM>;
+    if (t.nax == 2) return propagate_kpt_kernel<2, 2, 2, KM>;
   }
-  return t.nw == 1 ? propagate_kpt_kernel<1, 0, 0> : propagate_kpt_kernel<2, 0, 0>;
+  return t.nw == 1 ? propagate_kpt_kernel<1, 0, 0, KM> : propagate_kpt_kernel<2, 0, 0, KM>;
 }
+KptKernel kpt_kernel_for(const SolveTables& t) { return t.kmode ? kpt_kernel_t<true>(t) : kpt_kernel_t<false>(t); }
 
 bool plan_kpt(const SolveTables& t, int sm_count, LaunchShape* out, size_t smem_max) {
   KptKernel kern = kpt_kernel_for(t);
@@ -447,6 +467,7 @@ bool plan_kpt(const SolveTables& t, int sm_count, LaunchShape* out, size_t smem_
   if (balanced >= 64 && balanced < threads) threads = balanced;
   ntiles = (nk_local + threads - 1) / threads;
   out->kernel = 0;
+  out->kmode = t.kmode;
   out->k_per_cta = threads;
   out->group = 1;
   out->threads = threads;

@@ -143,12 +143,13 @@ struct GroupLayout {
     p += (size_t)B * W1;
     tw2 = p;
     p += W2;
+    const size_t ring = t.kmode ? 6 : 3, gbufs = t.kmode ? 4 : 2;
     pw1 = p;
-    p += 3 * (size_t)B * W1;
+    p += ring * (size_t)B * W1;
     pw2 = p;
-    p += 3 * W2;
+    p += ring * W2;
     G = p;
-    p += 2 * (size_t)gg.nbrows * nw2;
+    p += gbufs * (size_t)gg.nbrows * nw2;
     Xbox = p;
     if (box_sm) p += (size_t)gg.nmat * gg.nq1 * gg.W2n * nw2;
     total_cx = (p * sizeof(V) + 15) / 16 * 16 / sizeof(V);
@@ -158,9 +159,9 @@ struct GroupLayout {
     wtw2 = q;
     q += 4;
     wpw1 = q;
-    q += 3 * (size_t)B * 4;
+    q += ring * (size_t)B * 4;
     wpw2 = q;
-    q += 3 * 4;
+    q += ring * 4;
     GW = q;
     q += 2 * (size_t)gg.nwrows * nw2;
     Xwin = q;
@@ -190,7 +191,7 @@ struct GroupData {
 
 // Runs virtual CTAs v_first, v_first + v_step, ... (< vctas) of one solve on this CTA.
 // NWc, NAXc, NJc: orbital count, field axes and current axes fixed at compile time (0: read from t).
-template <typename Real, int EPT, int NWc, int NAXc, int NJc>
+template <typename Real, int EPT, int NWc, int NAXc, int NJc, bool KM>
 __device__ __forceinline__ void group_vctas(const SolveTables& t, const GroupData<Real>& d, int B, int G, int box_sm,
                                             int win_sm, int v_first, int v_step, int vctas, double2* rho,
                                             double2* Jpart) {
@@ -239,6 +240,8 @@ __device__ __forceinline__ void group_vctas(const SolveTables& t, const GroupDat
   const int ntiles = t.N2 * bpc;
   const V vzero = Cx<Real>::make(0, 0);
   const size_t gbuf = (size_t)gg.nbrows * nw2, wbuf = (size_t)gg.nwrows * nw2;
+  constexpr bool km = KM;             // k-space solver: three evaluation points per step
+  const int ring = km ? 6 : 3, gbufs = km ? 4 : 2;
 
   // Constant tables into shared memory (once per launch).
   if (box_sm) {
@@ -279,17 +282,20 @@ __device__ __forceinline__ void group_vctas(const SolveTables& t, const GroupDat
     }
     __syncthreads();
 
-    // Phase factors of step s into ring slot s % 3: p = twiddle x e^{i n A(t_s).a}.
-    auto make_phases = [&](int s) {
+    // Phase factors of evaluation point s into ring slot s % ring: p = twiddle x P(s), with P the
+    // Peierls factor e^{i n A(t_s).a} (real-space solver: one point per step) or the interpolation
+    // multiplier (k-space solver: points t, t + dt/2, t + dt of every step).  The window's factors
+    // are the Peierls ones, or 1 in the k-space solver (made once, `win` false afterwards).
+    auto make_phases = [&](int s, bool win) {
       const V* P1 = d.P + (size_t)s * 2 * npw + t.np;
       const V* P2 = P1 + npw;
       const double2* P1d = d.Pd + (size_t)s * 2 * npw + t.np;
       const double2* P2d = P1d + npw;
-      V* q2 = pw2 + (s % 3) * W2;
-      V* q1 = pw1 + (s % 3) * B * W1;
-      double2* w2 = wpw2 + (s % 3) * 4;
-      double2* w1 = wpw1 + (s % 3) * B * 4;
-      const int nA = W2, nB = nA + B * W1, nC = nB + 4, nD = nC + B * 4;
+      V* q2 = pw2 + (s % ring) * W2;
+      V* q1 = pw1 + (s % ring) * B * W1;
+      double2* w2 = wpw2 + (s % ring) * 4;
+      double2* w1 = wpw1 + (s % ring) * B * 4;
+      const int nA = W2, nB = nA + B * W1, nC = nB + (win ? 4 : 0), nD = nC + (win ? B * 4 : 0);
       for (int idx = tid; idx < nD; idx += nthr) {
         if (idx < nA) {
           q2[idx] = mul(tw2[idx], P2[t.b2lo + idx]);
@@ -298,20 +304,21 @@ __device__ __forceinline__ void group_vctas(const SolveTables& t, const GroupDat
           q1[id1] = mul(tw1[id1], P1[t.b1lo + id1 % W1]);
         } else if (idx < nC) {
           const int q = idx - nB;
-          w2[q] = mul(wtw2[q], P2d[q - 2]);
+          w2[q] = km ? wtw2[q] : mul(wtw2[q], P2d[q - 2]);
         } else {
           const int id1 = idx - nC;
-          w1[id1] = mul(wtw1[id1], P1d[id1 % 4 - 2]);
+          w1[id1] = km ? wtw1[id1] : mul(wtw1[id1], P1d[id1 % 4 - 2]);
         }
       }
     };
-    // Inner sums of step s into buffer s & 1 (rows assigned to groups, elements to threads).
-    auto inner_sums = [&](int s) {
-      const V* q2 = pw2 + (s % 3) * W2;
-      const double2* w2 = wpw2 + (s % 3) * 4;
-      V* Gd = Gb + (s & 1) * gbuf;
+    // Inner sums of point s into buffer s % gbufs (rows assigned to groups, elements to threads);
+    // window rows into buffer s & 1 when `win`.
+    auto inner_sums = [&](int s, bool win) {
+      const V* q2 = pw2 + (s % ring) * W2;
+      const double2* w2 = wpw2 + (s % ring) * 4;
+      V* Gd = Gb + (s % gbufs) * gbuf;
       double2* GWd = GWb + (s & 1) * wbuf;
-      for (int row = g; row < gg.nbrows + gg.nwrows; row += B) {
+      for (int row = g; row < gg.nbrows + (win ? gg.nwrows : 0); row += B) {
         if (row < gg.nbrows) {
           const int mat = row / gg.nq1, qq = row % gg.nq1;
           const V* X = box_sm ? Xbox + (((size_t)mat * gg.nq1 + qq) * W2n) * nw2
@@ -353,65 +360,98 @@ __device__ __forceinline__ void group_vctas(const SolveTables& t, const GroupDat
     };
 
     const int step0 = t.step0, step1 = t.step1;
-    make_phases(step0);
-    if (step0 + 1 < step1) make_phases(step0 + 1);
-    __syncthreads();
-    inner_sums(step0);
-    __syncthreads();
-
-    for (int ti = step0; ti < step1; ++ti) {
-      const int buf = ti & 1;
-      // (1) outer sums over n1 for this k-point: H0(k - A), r_a(k - A), W_a(k)
-      V h0[EPT], rk[3][EPT];
-      double2 wk[3][EPT];
+    // Outer sums over n1 of point s for this k-point: H0(k) and r_a(k) at the point's shift.
+    auto outer_box = [&](int s, V* h0o, V (*rko)[EPT]) {
 #pragma unroll
       for (int u = 0; u < EPT; ++u) {
-        h0[u] = vzero;
+        h0o[u] = vzero;
 #pragma unroll
-        for (int a = 0; a < 3; ++a) {
-          rk[a][u] = vzero;
-          wk[a][u] = make_double2(0.0, 0.0);
-        }
+        for (int a = 0; a < 3; ++a) rko[a][u] = vzero;
       }
-      {
-        const V* p1 = pw1 + (ti % 3) * B * W1 + g * W1;
-        const V* Gd = Gb + buf * gbuf;
-        for (int q1 = 0; q1 < W1n; ++q1) {
-          const V ph = p1[q1];
-          const bool neg = q1 < gg.q1s;  // G(-n1) = G(n1)^+
-          const int row = neg ? (W1n - 1 - q1) - gg.q1s : q1 - gg.q1s;
+      const V* p1 = pw1 + (s % ring) * B * W1 + g * W1;
+      const V* Gd = Gb + (s % gbufs) * gbuf;
+      for (int q1 = 0; q1 < W1n; ++q1) {
+        const V ph = p1[q1];
+        const bool neg = q1 < gg.q1s;  // G(-n1) = G(n1)^+
+        const int row = neg ? (W1n - 1 - q1) - gg.q1s : q1 - gg.q1s;
 #pragma unroll
-          for (int u = 0; u < EPT; ++u)
-            if (actu[u]) {
-              const int el = neg ? eTu[u] : eu[u];
-              V gv = Gd[(size_t)row * nw2 + el];
-              if (neg) gv = conjugate(gv);
-              h0[u] = fmac(ph, gv, h0[u]);
+        for (int u = 0; u < EPT; ++u)
+          if (actu[u]) {
+            const int el = neg ? eTu[u] : eu[u];
+            V gv = Gd[(size_t)row * nw2 + el];
+            if (neg) gv = conjugate(gv);
+            h0o[u] = fmac(ph, gv, h0o[u]);
 #pragma unroll
-              for (int a = 0; a < 3; ++a)
-                if (a < nax) {
-                  V rv = Gd[(size_t)((1 + a) * gg.nq1 + row) * nw2 + el];
-                  if (neg) rv = conjugate(rv);
-                  rk[a][u] = fmac(ph, rv, rk[a][u]);
-                }
-            }
-        }
-        const double2* GWd = GWb + buf * wbuf;
-        const double2* w1 = wpw1 + (ti % 3) * B * 4 + g * 4;
-#pragma unroll
-        for (int q1 = 0; q1 < 4; ++q1) {
-          const double2 ph = w1[q1];
-#pragma unroll
-          for (int u = 0; u < EPT; ++u)
-            if (actu[u])
-#pragma unroll
-              for (int a = 0; a < 3; ++a)
-                if (a < nj) wk[a][u] = fmac(ph, GWd[(size_t)(a * 4 + q1) * nw2 + eu[u]], wk[a][u]);
-        }
+            for (int a = 0; a < 3; ++a)
+              if (a < nax) {
+                V rv = Gd[(size_t)((1 + a) * gg.nq1 + row) * nw2 + el];
+                if (neg) rv = conjugate(rv);
+                rko[a][u] = fmac(ph, rv, rko[a][u]);
+              }
+          }
       }
-      // (2) next step's phase factors and inner sums, off this step's critical path
-      if (ti + 2 < step1) make_phases(ti + 2);
-      if (ti + 1 < step1) inner_sums(ti + 1);
+    };
+    // Outer sum of the window velocity of point s: W_a(k).
+    double2 wk[3][EPT];
+    auto outer_window = [&](int s) {
+#pragma unroll
+      for (int u = 0; u < EPT; ++u)
+#pragma unroll
+        for (int a = 0; a < 3; ++a) wk[a][u] = make_double2(0.0, 0.0);
+      const double2* GWd = GWb + (s & 1) * wbuf;
+      const double2* w1 = wpw1 + (s % ring) * B * 4 + g * 4;
+#pragma unroll
+      for (int q1 = 0; q1 < 4; ++q1) {
+        const double2 ph = w1[q1];
+#pragma unroll
+        for (int u = 0; u < EPT; ++u)
+          if (actu[u])
+#pragma unroll
+            for (int a = 0; a < 3; ++a)
+              if (a < nj) wk[a][u] = fmac(ph, GWd[(size_t)(a * 4 + q1) * nw2 + eu[u]], wk[a][u]);
+      }
+    };
+    // H0(k), r_a(k) of the point of stage 0 (k-space solver: carried from the previous step's stage 3).
+    V hc[EPT], rc[3][EPT];
+    if (!km) {
+      make_phases(step0, true);
+      if (step0 + 1 < step1) make_phases(step0 + 1, true);
+      __syncthreads();
+      inner_sums(step0, true);
+      __syncthreads();
+    } else {
+      // Points 2 step0 .. 2 step0 + 4: phases of all, inner sums of the first three, then the
+      // stage-0 sums of the first step and the (constant) window sum.
+      const int j0 = 2 * step0, jmax = 2 * step1;
+      for (int j = j0; j <= j0 + 4 && j <= jmax; ++j) make_phases(j, j == j0);
+      __syncthreads();
+      for (int j = j0; j <= j0 + 2 && j <= jmax; ++j) inner_sums(j, j == j0);
+      __syncthreads();
+      outer_box(j0, hc, rc);
+      outer_window(j0);
+      __syncthreads();
+    }
+
+    for (int ti = step0; ti < step1; ++ti) {
+      // (1) outer sums: real-space solver, the step's one point (and the window); k-space solver,
+      //     the mid point (stages 2 and 3)
+      V h0[EPT], rk[3][EPT];
+      if (!km) {
+        outer_box(ti, h0, rk);
+        outer_window(ti);
+      } else {
+        outer_box(2 * ti + 1, h0, rk);
+      }
+      // (2) later points' phase factors and inner sums, off this step's critical path
+      if (!km) {
+        if (ti + 2 < step1) make_phases(ti + 2, true);
+        if (ti + 1 < step1) inner_sums(ti + 1, true);
+      } else {
+        if (2 * ti + 5 <= 2 * step1) make_phases(2 * ti + 5, false);
+        if (2 * ti + 6 <= 2 * step1) make_phases(2 * ti + 6, false);
+        if (2 * ti + 3 <= 2 * step1) inner_sums(2 * ti + 3, false);
+        if (2 * ti + 4 <= 2 * step1) inner_sums(2 * ti + 4, false);
+      }
 
       // (3) RK4 stages (src/solver.cpp:157-163): fields at t, t+dt/2, t+dt/2, t+dt
       const double* esb = t.es + (size_t)ti * 9;
@@ -429,15 +469,19 @@ __device__ __forceinline__ void group_vctas(const SolveTables& t, const GroupDat
 #pragma unroll
         for (int a = 0; a < 3; ++a) ea[a] = a < nax ? (Real)esb[f * 3 + t.ax_id[a]] : (Real)0;
         const double cs = (st == 3 ? 1.0 : 0.5) * dt;
+        // k-space solver: stage 1 uses the carried point t, stage 4 the point t + dt (carried on).
+        if (km && st == 3) outer_box(2 * ti + 2, hc, rc);
+        const bool use_c = km && (st == 0 || st == 3);
 #pragma unroll
         for (int u = 0; u < EPT; ++u)
           if (actu[u]) {
-            V hs = h0[u];
+            V hs = use_c ? hc[u] : h0[u];
 #pragma unroll
             for (int a = 0; a < 3; ++a)
               if (a < nax) {
-                hs.x += ea[a] * rk[a][u].x;
-                hs.y += ea[a] * rk[a][u].y;
+                const V rv = use_c ? rc[a][u] : rk[a][u];
+                hs.x += ea[a] * rv.x;
+                hs.y += ea[a] * rv.y;
               }
             double2 x = r[u];
             if (st > 0) {
@@ -564,16 +608,16 @@ __device__ __forceinline__ GroupData<Real> group_data(const GroupTables& gt) {
 }
 
 // One solve: physical CTA b runs virtual CTAs b, b + gridDim.x, ...
-template <typename Real, int EPT, int NWc, int NAXc, int NJc>
+template <typename Real, int EPT, int NWc, int NAXc, int NJc, bool KM = false>
 __global__ void __launch_bounds__(group_threads<EPT>(), 1)
     propagate_group_kernel(SolveTables t, GroupData<Real> d, int B, int G, int box_sm, int win_sm, int vctas,
                            double2* rho, double2* Jpart) {
-  group_vctas<Real, EPT, NWc, NAXc, NJc>(t, d, B, G, box_sm, win_sm, blockIdx.x, gridDim.x, vctas, rho, Jpart);
+  group_vctas<Real, EPT, NWc, NAXc, NJc, KM>(t, d, B, G, box_sm, win_sm, blockIdx.x, gridDim.x, vctas, rho, Jpart);
 }
 
 // Many solves of one kernel shape: persistent CTAs take (solve, virtual CTA) items from a packed
 // work list through an atomic counter.  Which CTA runs an item does not change its result.
-template <typename Real, int EPT, int NWc, int NAXc, int NJc>
+template <typename Real, int EPT, int NWc, int NAXc, int NJc, bool KM = false>
 __global__ void __launch_bounds__(group_threads<EPT>(), 1)
     propagate_group_batch_kernel(const BatchDesc* descs, const int2* items, int nitems, int* counter) {
   __shared__ BatchDesc sd;
@@ -588,7 +632,7 @@ __global__ void __launch_bounds__(group_threads<EPT>(), 1)
     for (int q = threadIdx.x; q < (int)(sizeof(BatchDesc) / sizeof(int)); q += blockDim.x)
       reinterpret_cast<int*>(&sd)[q] = src[q];
     __syncthreads();
-    group_vctas<Real, EPT, NWc, NAXc, NJc>(sd.t, group_data<Real>(sd.gt), sd.B, sd.G, sd.box_sm, sd.win_sm, w.y,
+    group_vctas<Real, EPT, NWc, NAXc, NJc, KM>(sd.t, group_data<Real>(sd.gt), sd.B, sd.G, sd.box_sm, sd.win_sm, w.y,
                                            sd.vctas, sd.vctas, sd.rho, sd.Jpart);
     __syncthreads();
   }
@@ -596,7 +640,7 @@ __global__ void __launch_bounds__(group_threads<EPT>(), 1)
 
 constexpr size_t kSmemMax = 220 * 1024;
 
-template <typename Real, int EPT, int NWc, int NAXc, int NJc>
+template <typename Real, int EPT, int NWc, int NAXc, int NJc, bool KM = false>
 bool plan_group_t(const SolveTables& t, int sm_count, LaunchShape* out, char* why, int why_len) {
   const GroupGeom gg = group_geom(t);
   const int per = (t.nw2 + EPT - 1) / EPT;  // threads needed per k-point
@@ -628,7 +672,7 @@ bool plan_group_t(const SolveTables& t, int sm_count, LaunchShape* out, char* wh
   if (bytes(Bmax, true, true) > kSmemMax) win_sm = 0;
   if (bytes(Bmax, true, win_sm) > kSmemMax) box_sm = 0;
   if (!box_sm && bytes(Bmax, false, true) <= kSmemMax) win_sm = 1;
-  auto kern = propagate_group_kernel<Real, EPT, NWc, NAXc, NJc>;
+  auto kern = propagate_group_kernel<Real, EPT, NWc, NAXc, NJc, KM>;
   const size_t smem_max = bytes(Bmax, box_sm, win_sm);
   cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_max);
   int occ = 0;
@@ -641,6 +685,7 @@ bool plan_group_t(const SolveTables& t, int sm_count, LaunchShape* out, char* wh
   const int best = Bmax;
   const long ntiles = (long)t.N2 * ((rows + best - 1) / best);
   out->kernel = sizeof(Real) == 8 ? 1 : 2;
+  out->kmode = KM ? 1 : 0;
   out->ept = EPT;
   out->k_per_cta = best;
   out->group = G;
@@ -654,7 +699,7 @@ bool plan_group_t(const SolveTables& t, int sm_count, LaunchShape* out, char* wh
   return true;
 }
 
-template <typename Real, int EPT, int NWc, int NAXc, int NJc>
+template <typename Real, int EPT, int NWc, int NAXc, int NJc, bool KM = false>
 void launch_group_t(const SolveTables& t, const GroupTables& gt, const LaunchShape& s, double2* rho, double2* Jpart,
                     cudaStream_t stream) {
   GroupData<Real> d;
@@ -663,15 +708,15 @@ void launch_group_t(const SolveTables& t, const GroupTables& gt, const LaunchSha
   } else {
     d = {gt.Xbox32, gt.P32, gt.T1_32, gt.T2_32, gt.Xwin64, gt.P64, gt.T1_64, gt.T2_64};
   }
-  auto kern = propagate_group_kernel<Real, EPT, NWc, NAXc, NJc>;
+  auto kern = propagate_group_kernel<Real, EPT, NWc, NAXc, NJc, KM>;
   cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s.smem);
   kern<<<s.ctas, s.threads, s.smem, stream>>>(t, d, s.k_per_cta, s.group, s.box_sm, s.win_sm, s.vctas, rho, Jpart);
 }
 
-template <typename Real, int EPT, int NWc, int NAXc, int NJc>
+template <typename Real, int EPT, int NWc, int NAXc, int NJc, bool KM = false>
 int launch_group_batch_t(const BatchDesc* descs, const int2* items, int nitems, int* counter, int threads, size_t smem,
                          int sm_count, cudaStream_t stream) {
-  auto kern = propagate_group_batch_kernel<Real, EPT, NWc, NAXc, NJc>;
+  auto kern = propagate_group_batch_kernel<Real, EPT, NWc, NAXc, NJc, KM>;
   cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   int occ = 0;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, threads, smem);
@@ -718,41 +763,67 @@ const GroupVariant* find_variant(const SolveTables& t, int precision) {
 }  // namespace
 
 bool plan_group(const SolveTables& t, int precision, int sm_count, LaunchShape* out, char* why, int why_len) {
-  if (const GroupVariant* v = find_variant(t, precision)) {
-    out->variant = (int)(v - kGroupVariants);
-    return v->plan(t, sm_count, out, why, why_len);
+  if (!t.kmode) {
+    if (const GroupVariant* v = find_variant(t, precision)) {
+      out->variant = (int)(v - kGroupVariants);
+      return v->plan(t, sm_count, out, why, why_len);
+    }
   }
   out->variant = -1;
   // Runtime-shaped: two elements per thread in the mixed form once a k-point needs more than a warp.
   const bool two = precision == 1 && t.nw2 > 32;
+  if (t.kmode) {
+    if (precision == 1)
+      return two ? plan_group_t<float, 2, 0, 0, 0, true>(t, sm_count, out, why, why_len)
+                 : plan_group_t<float, 1, 0, 0, 0, true>(t, sm_count, out, why, why_len);
+    return plan_group_t<double, 1, 0, 0, 0, true>(t, sm_count, out, why, why_len);
+  }
   if (precision == 1)
     return two ? plan_group_t<float, 2, 0, 0, 0>(t, sm_count, out, why, why_len)
                : plan_group_t<float, 1, 0, 0, 0>(t, sm_count, out, why, why_len);
   return plan_group_t<double, 1, 0, 0, 0>(t, sm_count, out, why, why_len);
 }
 
+namespace {
+template <bool KM>
+int launch_group_batch_generic(const LaunchShape& s, const BatchDesc* descs, const int2* items, int nitems,
+                               int* counter, size_t smem, int sm_count, cudaStream_t stream) {
+  if (s.kernel == 2)
+    return s.ept == 2 ? launch_group_batch_t<float, 2, 0, 0, 0, KM>(descs, items, nitems, counter, s.threads, smem,
+                                                                     sm_count, stream)
+                      : launch_group_batch_t<float, 1, 0, 0, 0, KM>(descs, items, nitems, counter, s.threads, smem,
+                                                                     sm_count, stream);
+  return launch_group_batch_t<double, 1, 0, 0, 0, KM>(descs, items, nitems, counter, s.threads, smem, sm_count,
+                                                      stream);
+}
+template <bool KM>
+void launch_group_generic(const SolveTables& t, const GroupTables& gt, const LaunchShape& s, double2* rho,
+                          double2* Jpart, cudaStream_t stream) {
+  if (s.kernel == 2) {
+    s.ept == 2 ? launch_group_t<float, 2, 0, 0, 0, KM>(t, gt, s, rho, Jpart, stream)
+               : launch_group_t<float, 1, 0, 0, 0, KM>(t, gt, s, rho, Jpart, stream);
+  } else {
+    launch_group_t<double, 1, 0, 0, 0, KM>(t, gt, s, rho, Jpart, stream);
+  }
+}
+}  // namespace
+
 int launch_group_batch(const LaunchShape& s, const BatchDesc* descs, const int2* items, int nitems, int* counter,
                        size_t smem, int sm_count, cudaStream_t stream) {
   if (s.variant >= 0)
     return kGroupVariants[s.variant].batch(descs, items, nitems, counter, s.threads, smem, sm_count, stream);
-  if (s.kernel == 2)
-    return s.ept == 2 ? launch_group_batch_t<float, 2, 0, 0, 0>(descs, items, nitems, counter, s.threads, smem, sm_count,
-                                                                 stream)
-                      : launch_group_batch_t<float, 1, 0, 0, 0>(descs, items, nitems, counter, s.threads, smem, sm_count,
-                                                                 stream);
-  return launch_group_batch_t<double, 1, 0, 0, 0>(descs, items, nitems, counter, s.threads, smem, sm_count, stream);
+  return s.kmode ? launch_group_batch_generic<true>(s, descs, items, nitems, counter, smem, sm_count, stream)
+                 : launch_group_batch_generic<false>(s, descs, items, nitems, counter, smem, sm_count, stream);
 }
 
 void launch_group(const SolveTables& t, const GroupTables& gt, const LaunchShape& s, double2* rho, double2* Jpart,
                   cudaStream_t stream) {
-  if (s.variant >= 0) {
+  if (s.variant >= 0)
     kGroupVariants[s.variant].launch(t, gt, s, rho, Jpart, stream);
-  } else if (s.kernel == 2) {
-    s.ept == 2 ? launch_group_t<float, 2, 0, 0, 0>(t, gt, s, rho, Jpart, stream)
-               : launch_group_t<float, 1, 0, 0, 0>(t, gt, s, rho, Jpart, stream);
-  } else {
-    launch_group_t<double, 1, 0, 0, 0>(t, gt, s, rho, Jpart, stream);
-  }
+  else if (s.kmode)
+    launch_group_generic<true>(t, gt, s, rho, Jpart, stream);
+  else
+    launch_group_generic<false>(t, gt, s, rho, Jpart, stream);
 }
 
 }  // namespace hhg

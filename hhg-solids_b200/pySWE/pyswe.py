@@ -79,6 +79,7 @@ def _load(path: str):
         L.SWESim_reset.argtypes = [vp]
         L.SWESim_set_k_rows.argtypes = [vp, ct.c_int, ct.c_int]
         L.SWESim_set_precision.argtypes = [vp, ct.c_int]
+        L.SWESim_set_solver.argtypes = [vp, ct.c_int]
         L.SWEBatch_new.restype = vp
         L.SWEBatch_add.argtypes = [vp, vp]
         L.SWEBatch_run.argtypes = [vp]
@@ -139,10 +140,12 @@ class Settings:
 
 class SWE:
     """One propagation: setup on construction (SWESim_init), then run_simulation / get_current.
-    ``defer_init=True`` skips the setup (for a request handed to :class:`SWEServer`)."""
+    ``defer_init=True`` skips the setup (for a request handed to :class:`SWEServer`).
+    ``solver="kspace"`` selects the reference's k-space solver (src/solver_kspace.cpp) instead of
+    its real-space one."""
 
     def __init__(self, settings: Settings, device: int | None = None, k_rows: tuple | None = None,
-                 precision: str = "fp64", defer_init: bool = False):
+                 precision: str = "fp64", defer_init: bool = False, solver: str = "rspace"):
         self.settings = settings
         self.swe_cpp, self._ext = _load(settings.path_lib)
         self.ptr = self.swe_cpp.SWESim_new()
@@ -156,6 +159,10 @@ class SWE:
             raise SWEError(f"precision must be 'fp64' or 'mixed', not {precision!r}")
         if precision == "mixed":
             self._call("SWESim_set_precision", 1)
+        if solver not in ("rspace", "kspace"):
+            raise SWEError(f"solver must be 'rspace' or 'kspace', not {solver!r}")
+        if solver == "kspace":
+            self._call("SWESim_set_solver", 1)
         self.set_path_tb(settings.path_tb.encode("UTF-8"))
         self.set_settings(settings.ptr)
         if not defer_init:

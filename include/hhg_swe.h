@@ -98,6 +98,12 @@ int SWESim_last_launches(SWESim* swe);
  * the RK4 accumulation and the current's k-sum in FP64 (error against plain FP64 reported by the
  * tests and bench). */
 void SWESim_set_precision(SWESim* swe, int mode);
+/* Solver (no counterpart in the reference's C ABI, which always drives the real-space solver):
+ * 0 (default) the real-space solver of src/solver.cpp as SWESim::run_simulation drives it;
+ * 1 the k-space solver of src/solver_kspace.cpp (compiled in the reference but reached by none of
+ * its entry points), driven the same way step by step with J taken from the 4x4 window without a
+ * Peierls phase.  The k-space solver needs nr1 == nr2.  Takes effect at the next SWESim_init. */
+void SWESim_set_solver(SWESim* swe, int mode);
 /* Restrict the next SWESim_init to k-grid rows m1 in [row0, row1) (row1 = -1: to the end): one
  * slab of a solve split over several GPUs.  The current stays normalised by the full grid, so the
  * currents of a partition of the rows add up to the full current. */

@@ -63,6 +63,7 @@ def lib():
         L.oracle_rho0.argtypes = [ct.c_char_p, P, dp]
         L.oracle_run.argtypes = [ct.c_char_p, P, ct.c_int, ct.c_int, dp, dp]
         L.oracle_run_steps.argtypes = [ct.c_char_p, P, ct.c_int, ct.c_int, ct.c_int, dp, dp]
+        L.oracle_run_kspace_steps.argtypes = [ct.c_char_p, P, ct.c_int, dp, dp]
         _lib = L
     return _lib
 
@@ -139,6 +140,18 @@ def run(tb: str, param: dict, k_begin: int = 0, k_end: int | None = None, nsteps
     return t, J
 
 
+def run_kspace(tb: str, param: dict, nsteps: int = -1):
+    """The reference's k-space solver (src/solver_kspace.cpp) restated; returns (t, J[3, nt])."""
+    s = settings(param)
+    n = lib().oracle_nt(ct.byref(s))
+    t = np.zeros(n)
+    J = np.zeros((3, n), dtype=np.complex128)
+    got = lib().oracle_run_kspace_steps(tb.encode(), ct.byref(s), int(nsteps), _dp(t), _dp(J))
+    if got != n:
+        raise ValueError(f"oracle_run_kspace_steps failed ({got})")
+    return t, J
+
+
 # ---------------------------------------------------------------- the reference's own build
 
 
@@ -159,6 +172,8 @@ def probe():
         P.probe_fields.argtypes = [ct.c_char_p, ct.c_int, ct.c_int] + [ct.c_double] * 5 + [dp] * 5
         P.probe_operators.argtypes = [ct.c_char_p, ct.c_int, ct.c_int, dp, dp, dp]
         P.probe_rho0.argtypes = [ct.c_char_p, ct.c_int, ct.c_int, dp, dp]
+        P.probe_kspace_run.argtypes = [ct.c_char_p, ct.c_int, ct.c_int] + [ct.c_double] * 5 + [dp, dp, ct.c_int,
+                                                                                              dp, dp]
         _probe = P
     return _probe
 
@@ -239,4 +254,20 @@ def ref_run(tb: str, param: dict, lib_path: str | None = None):
     J = np.zeros((3, n), dtype=np.complex128)
     L.SWESim_get_current(sim, _dp(t), _dp(J[0]), _dp(J[1]), _dp(J[2]))
     L.SWESim_delete(sim)
+    return t, J
+
+
+def ref_kspace_run(tb: str, param: dict, nsteps: int = -1):
+    """The reference's own Solver_kspace, driven step by step (ref_probe.cpp); returns (t, J[3, nt])."""
+    P = probe()
+    n = P.probe_nt(float(param["tmax"]), float(param["dt"]))
+    t = np.zeros(n)
+    J = np.zeros((3, n), dtype=np.complex128)
+    pol = np.ascontiguousarray(param["pol_vec"], dtype=np.float64)
+    phi = np.ascontiguousarray(param["phi_vec"], dtype=np.float64)
+    got = P.probe_kspace_run(tb.encode(), int(param["nr1"]), int(param["nr2"]), float(param["tmax"]),
+                             float(param["dt"]), float(param["intensity"]), float(param["lambda"]),
+                             float(param["tmax_field"]), _dp(pol), _dp(phi), int(nsteps), _dp(t), _dp(J))
+    if got != n:
+        raise ValueError(f"probe_kspace_run failed ({got})")
     return t, J

@@ -12,8 +12,10 @@
 #include "grid.h"
 #include "hamiltonian.h"
 #include "matrix_field.h"
+#include "observable.h"
 #include "rdm.h"
 #include "settings.h"
+#include "solver_kspace.h"
 #include "velocity.h"
 #include "wannier_tb.h"
 
@@ -156,5 +158,75 @@ int probe_rho0(const char* tb, int n1, int n2, cdouble* rho_k, cdouble* Hk) {
   delete w;
   delete s;
   return nw;
+}
+
+// The reference's k-space RK4 solver (src/solver_kspace.cpp), which no reference entry point
+// reaches, driven the way SWESim drives its real-space solver: SWESim::_init's setup
+// (src/swe.cpp:49-93), Solver_kspace::init, then per step step_rk4(ti) followed by the three
+// Observables of src/swe.cpp:203-205 on the real-space rho it leaves behind (no Peierls phase:
+// this solver has none).  First nsteps steps; t (au, nt) and J ([3][nt], zero after nsteps).
+int probe_kspace_run(const char* tb, int n1, int n2, double tmax, double dt, double intensity, double lambda_nm,
+                     double tmax_field, const double* pol, const double* phi, int nsteps, double* t, cdouble* J) {
+  Settings* s = make_settings(n1, n2, tmax, dt, intensity, lambda_nm, tmax_field, pol, phi);
+  WannierTB* w = new WannierTB(tb);
+  s->nt = s->tmax / s->dt;
+  s->num_orb = w->num_orb;
+  s->num_sites = w->num_sites;
+  Grid* g = new Grid(s, w);
+  Hamiltonian* h = new Hamiltonian(s, g, w, WGAUGE, RSPACE);
+  RDM* rho = new RDM(s, g, w, WGAUGE, RSPACE);
+  BerryConnection* r[3];
+  Velocity* v[3];
+  for (int a = 0; a < 3; ++a) r[a] = new BerryConnection(s, g, w, WGAUGE, RSPACE, a);
+  for (int a = 0; a < 3; ++a) v[a] = new Velocity(s, g, w, WGAUGE, RSPACE);
+  for (int a = 0; a < 3; ++a) v[a]->setup(h, r[a], a);
+  MatrixField* U = new MatrixField(s, w);
+  Efield* f = new Efield(s, g, SI);
+  Observable* obs[3];
+  for (int a = 0; a < 3; ++a) obs[a] = new Observable(s, g, rho, v[a]);
+  w->convert_to_au();
+  g->convert_to_au();
+  h->convert_to_au();
+  rho->convert_to_au();
+  for (int a = 0; a < 3; ++a) r[a]->convert_to_au();
+  f->convert_to_au();
+  for (int a = 0; a < 3; ++a) v[a]->convert_to_au();
+  f->init_fields();
+  h->convert_to_k();
+  h->diagonalization_W_KSPACE(U);
+  rho->convert_to_k();
+  h->convert_w_to_h(U);
+  rho->convert_w_to_h(U);
+  rho->calculate_equilibrium(h);
+  h->convert_h_to_w(U);
+  h->convert_to_r();
+  rho->convert_h_to_w(U);
+  rho->convert_to_r();
+  Solver_kspace* ks = new Solver_kspace(s, g, h, rho, r, f, w);
+  ks->init();
+  const int nt = s->nt;
+  const int nrun = (nsteps < 0 || nsteps > nt) ? nt : nsteps;
+  for (int ti = 0; ti < nrun; ++ti) {
+    ks->step_rk4(ti);
+    for (int a = 0; a < 3; ++a) obs[a]->calculate();
+  }
+  for (int i = 0; i < nt; ++i) {
+    t[i] = g->t()[i];
+    for (int a = 0; a < 3; ++a) J[(size_t)a * nt + i] = i < nrun ? obs[a]->get_ptr()[i] : cdouble(0.0, 0.0);
+  }
+  delete ks;
+  for (int a = 0; a < 3; ++a) {
+    delete obs[a];
+    delete v[a];
+    delete r[a];
+  }
+  delete f;
+  delete U;
+  delete rho;
+  delete h;
+  delete g;
+  delete w;
+  delete s;
+  return nt;
 }
 }

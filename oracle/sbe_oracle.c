@@ -570,3 +570,181 @@ int oracle_run_steps(const char* tb, const oracle_settings* s, int k_begin, int 
   tb_free(&m);
   return nt;
 }
+
+/* ---------------------------------------------------------------------------------------------
+ * The reference's k-space RK4 solver (src/solver_kspace.cpp:167-451, src/interpolation.cpp:17-43),
+ * driven per step like the real-space one but without a Peierls phase (it has none): for every
+ * stage, H_eff = H0(k) + E_s . r(k) on the k-grid (the ifftshift + forward FFT of
+ * src/solver_kspace.cpp:122-142, i.e. the DFT over the placed cells), interpolated at k - A_s by
+ * the Catmull-Rom bicubic of src/interpolation.cpp, with A_s = A(t), the mean of A(t) and A(t+dt)
+ * for stages 2 and 3, A(t+dt) (clamped on the last step as the fields are).  The fractional
+ * coordinates come from the reference's Cramer solve against the reciprocal vectors (au); the
+ * interpolation reads data[yi*N1 + xi] with xi along the first coordinate and yi along the second,
+ * as the reference does (on a square grid that is the grid transposed).  The commutator is the
+ * full [H, X].  The reference's R<->k round trip of rho each step is the identity for even N and
+ * is not repeated.  J: the Observables of src/observable.cpp:16-30 on that rho, in Parseval form
+ * with no phase factor. */
+static cplx cubic_at(cplx p0, cplx p1, cplx p2, cplx p3, double t) {
+  /* Catmull-Rom through p1 (t = 0) and p2 (t = 1). */
+  cplx a0 = -0.5 * p0 + 1.5 * p1 - 1.5 * p2 + 0.5 * p3;
+  cplx a1 = p0 - 2.5 * p1 + 2.0 * p2 - 0.5 * p3;
+  cplx a2 = -0.5 * p0 + 0.5 * p2;
+  return ((a0 * t + a1) * t + a2) * t + p1;
+}
+
+static cplx bicubic_at(const cplx* grid, int nw2, int Nx, int Ny, double u, double v, int o) {
+  double x = u * Nx, y = v * Ny;
+  int ix = (int)floor(x), iy = (int)floor(y);
+  double tx = x - (double)ix, ty = y - (double)iy;
+  cplx row[4];
+  for (int b = -1; b <= 2; ++b) {
+    cplx col[4];
+    for (int a = -1; a <= 2; ++a) {
+      int xi = wrap((long)ix + a, Nx), yi = wrap((long)iy + b, Ny);
+      col[a + 1] = grid[((size_t)yi * Nx + xi) * nw2 + o];
+    }
+    row[b + 1] = cubic_at(col[0], col[1], col[2], col[3], tx);
+  }
+  return cubic_at(row[0], row[1], row[2], row[3], ty);
+}
+
+int oracle_run_kspace_steps(const char* tb, const oracle_settings* s, int nsteps, double* t, double* Jout) {
+  tb_model m;
+  if (tb_parse(tb, &m)) return -1;
+  placed_grid g;
+  if (grid_place(&m, s, &g)) {
+    tb_free(&m);
+    return -3;
+  }
+  const int nt = oracle_nt(s);
+  if (nt < 2) {
+    grid_free(&g);
+    tb_free(&m);
+    return -4;
+  }
+  const int nw = g.nw, nw2 = g.nw2, N1 = g.N1, N2 = g.N2, Nk = g.Nk;
+  const double A2au = 1.0 / 0.5291772;
+  double* E = malloc(sizeof(double) * 3 * nt);
+  double* A = malloc(sizeof(double) * 3 * nt);
+  oracle_fields(tb, s, t, E, A);
+  const double dt = t[1] - t[0];
+  double b[3][3], lat[3][3];
+  memcpy(lat, m.lat, sizeof lat);
+  oracle_reciprocal(lat, b);
+  double bau[3][3];
+  for (int r = 0; r < 3; ++r)
+    for (int q = 0; q < 3; ++q) bau[r][q] = b[r][q] / A2au;
+  double* bm[3] = {bau[0], bau[1], bau[2]};
+
+  cell_ref* sup;
+  int ns = list_support(&g, &sup);
+  cplx* vw = malloc(sizeof(cplx) * 3 * 16 * nw2);
+  velocity_window(&m, &g, vw);
+  cplx *T1 = twiddles(N1), *T2 = twiddles(N2);
+  /* H0(k) and r_a(k) on the grid (au). */
+  cplx* h0g = calloc((size_t)Nk * nw2, sizeof(cplx));
+  cplx* rg = calloc(3 * (size_t)Nk * nw2, sizeof(cplx));
+  for (int k = 0; k < Nk; ++k) {
+    const int m1 = k / N2, m2 = k % N2;
+    for (int q = 0; q < ns; ++q) {
+      cplx f = T1[wrap((long)m1 * sup[q].n1, N1)] * T2[wrap((long)m2 * sup[q].n2, N2)];
+      const size_t st = (size_t)sup[q].site * nw2;
+      for (int o = 0; o < nw2; ++o) {
+        h0g[(size_t)k * nw2 + o] += f * (m.hop[st + o] * (1.0 / 27.2114));
+        for (int a = 0; a < 3; ++a) rg[((size_t)a * Nk + k) * nw2 + o] += f * (-m.bc[a][st + o] * A2au);
+      }
+    }
+  }
+  /* Windowed velocity W_a(k) (constant: no phase in this solver). */
+  cplx* Wk = calloc(3 * (size_t)Nk * nw2, sizeof(cplx));
+  for (int k = 0; k < Nk; ++k) {
+    const int m1 = k / N2, m2 = k % N2;
+    for (int w = 0; w < 16; ++w) {
+      cplx f = T1[wrap((long)m1 * (w / 4 - 2), N1)] * T2[wrap((long)m2 * (w % 4 - 2), N2)];
+      for (int a = 0; a < 3; ++a)
+        for (int o = 0; o < nw2; ++o) Wk[((size_t)a * Nk + k) * nw2 + o] += f * vw[((size_t)a * 16 + w) * nw2 + o];
+    }
+  }
+  cplx* rho = malloc(sizeof(cplx) * (size_t)Nk * nw2);
+  {
+    cplx* Hk = malloc(sizeof(cplx) * nw2);
+    cplx* U = malloc(sizeof(cplx) * nw2);
+    double* w = malloc(sizeof(double) * nw);
+    for (int k = 0; k < Nk; ++k) rho0_at(&m, sup, ns, T1, T2, N1, N2, k / N2, k % N2, Hk, U, w, rho + (size_t)k * nw2);
+    free(Hk);
+    free(U);
+    free(w);
+  }
+  cplx* heff = malloc(sizeof(cplx) * (size_t)Nk * nw2);
+  cplx* kn[4];
+  for (int n = 0; n < 4; ++n) kn[n] = malloc(sizeof(cplx) * (size_t)Nk * nw2);
+  cplx* Hs = malloc(sizeof(cplx) * nw2);
+  cplx* X = malloc(sizeof(cplx) * nw2);
+  cplx* J = (cplx*)Jout;
+  for (int i = 0; i < 3 * nt; ++i) J[i] = 0;
+  const int nrun = (nsteps < 0 || nsteps > nt) ? nt : nsteps;
+  for (int ti = 0; ti < nrun; ++ti) {
+    /* src/solver_kspace.cpp:168-229: E and A at t, their end-point mean, t + dt (clamped). */
+    double Es[3][3], As[3][3];
+    for (int a = 0; a < 3; ++a) {
+      const double* Ea = E + (size_t)a * nt;
+      const double* Aa = A + (size_t)a * nt;
+      if (ti < nt - 1) {
+        Es[0][a] = Ea[ti];
+        Es[1][a] = 0.5 * Ea[ti] + 0.5 * Ea[ti + 1];
+        Es[2][a] = Ea[ti + 1];
+        As[0][a] = Aa[ti];
+        As[1][a] = 0.5 * Aa[ti] + 0.5 * Aa[ti + 1];
+        As[2][a] = Aa[ti + 1];
+      } else {
+        Es[0][a] = Es[1][a] = Es[2][a] = Ea[nt - 1];
+        As[0][a] = As[1][a] = As[2][a] = Aa[nt - 1];
+      }
+    }
+    static const double cstage[4] = {0.0, 0.5, 0.5, 1.0};
+    static const int point_of_stage[4] = {0, 1, 1, 2};
+    for (int n = 0; n < 4; ++n) {
+      const int f = point_of_stage[n];
+      for (size_t q = 0; q < (size_t)Nk * nw2; ++q)
+        heff[q] = h0g[q] + Es[f][0] * rg[q] + Es[f][1] * rg[(size_t)Nk * nw2 + q] + Es[f][2] * rg[2 * (size_t)Nk * nw2 + q];
+      for (int k = 0; k < Nk; ++k) {
+        double kv[3], c[3];
+        for (int a = 0; a < 3; ++a) kv[a] = g.K[3 * k + a] / A2au - As[f][a];
+        oracle_cramer3(bm, kv, c);
+        for (int o = 0; o < nw2; ++o) {
+          Hs[o] = bicubic_at(heff, nw2, N1, N2, c[0], c[1], o);
+          X[o] = n == 0 ? rho[(size_t)k * nw2 + o] : rho[(size_t)k * nw2 + o] + cstage[n] * dt * kn[n - 1][(size_t)k * nw2 + o];
+        }
+        rk_stage(nw, Hs, X, kn[n] + (size_t)k * nw2);
+      }
+    }
+    cplx jsum[3] = {0, 0, 0};
+    for (int k = 0; k < Nk; ++k) {
+      cplx* r = rho + (size_t)k * nw2;
+      for (int o = 0; o < nw2; ++o) {
+        const size_t q = (size_t)k * nw2 + o;
+        r[o] = r[o] + (0.1666666666666 * dt) * (kn[0][q] + 2.0 * kn[1][q] + 2.0 * kn[2][q] + kn[3][q]);
+      }
+      for (int a = 0; a < 3; ++a)
+        for (int o = 0; o < nw2; ++o) jsum[a] += Wk[((size_t)a * Nk + k) * nw2 + o] * conj(r[o]);
+    }
+    for (int a = 0; a < 3; ++a) J[(size_t)a * nt + ti] = jsum[a] / (double)Nk;
+  }
+  free(heff);
+  for (int n = 0; n < 4; ++n) free(kn[n]);
+  free(Hs);
+  free(X);
+  free(rho);
+  free(Wk);
+  free(h0g);
+  free(rg);
+  free(T1);
+  free(T2);
+  free(vw);
+  free(E);
+  free(A);
+  free(sup);
+  grid_free(&g);
+  tb_free(&m);
+  return nt;
+}

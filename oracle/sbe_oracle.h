@@ -53,6 +53,13 @@ int oracle_run(const char* tb, const oracle_settings* s, int k_begin, int k_end,
 int oracle_run_steps(const char* tb, const oracle_settings* s, int k_begin, int k_end, int nsteps, double* t,
                      double* J);
 
+/* The reference's k-space solver (src/solver_kspace.cpp, never reached by the reference's own
+ * entry points) driven step by step like the real-space one, without a Peierls phase: per stage,
+ * H0(k) + E_s . r(k) interpolated at k - A_s by the Catmull-Rom bicubic of src/interpolation.cpp
+ * (with its index order), full commutator, RK4; J from the 4x4 window with no phase.  All k-points,
+ * first nsteps steps (< 0: all); t (au) and J ([3][nt]) as in oracle_run.  Returns nt. */
+int oracle_run_kspace_steps(const char* tb, const oracle_settings* s, int nsteps, double* t, double* J);
+
 #ifdef __cplusplus
 }
 #endif

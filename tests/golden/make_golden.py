@@ -3,7 +3,10 @@
 Runs the reference build ``oracle/_ref/libwannier.so`` (compiled from the reference's unmodified
 sources by ``oracle/Makefile``) through the reference's own, unmodified ctypes wrapper
 ``pySWE/pyswe.py`` loaded from the reference checkout, so the fixtures are exactly what a user of
-the reference would get.  Needs the reference checkout (``--ref``); the GPU box never runs this.
+the reference would get.  The ``ks_*`` fixtures come from the reference's k-space solver
+(src/solver_kspace.cpp), which none of its entry points reach: ``oracle/ref_probe.cpp`` drives its
+compiled objects the way SWESim drives the real-space solver.  Needs the reference checkout
+(``--ref``); the GPU box never runs this.
 
     python tests/golden/make_golden.py [--ref /root/reference] [--only NAME ...]
 """
@@ -47,6 +50,12 @@ CASES = {
     "c0": case("haldane", 60),
     "c2_prefix": case("tmd11_s7", 150, tmax=2.2),
     "c1": case("haldane", 200),
+    "ks_haldane_12_pol": case("haldane", 12, tmax=4.0, pol_vec=[0.6, 0.8, 0.0], phi_vec=[0.3, 0.0, 0.0],
+                              solver="kspace"),
+    "ks_tmd6_8": case("tmd6_s1", 8, tmax=1.0, pol_vec=[0.3, 1.0, 0.0], solver="kspace"),
+    "ks_tmd11_10": case("tmd11_s7", 10, tmax=0.5, solver="kspace"),
+    "ks_c0": case("haldane", 60, solver="kspace"),
+    "ks_c1": case("haldane", 200, solver="kspace"),
 }
 
 
@@ -61,18 +70,28 @@ def run_case(pyswe, lib: str, name: str, spec: dict) -> dict:
     p = dict(spec["param"])
     if "lambda_" in p:
         p["lambda"] = p.pop("lambda_")
+    solver = p.pop("solver", "rspace")
     tb = tbgen.model_path(spec["model"])
     param = dict(p, path_lib=lib, path_tb=tb)
     param["pol_vec"] = np.array(p["pol_vec"], dtype=np.float64)
     param["phi_vec"] = np.array(p["phi_vec"], dtype=np.float64)
     t0 = time.time()
-    with open(os.devnull, "w") as devnull, contextlib.redirect_stdout(devnull):
-        settings = pyswe.Settings(param)
-        swe = pyswe.SWE(settings)
-        t_init = time.time() - t0
-        swe.run_simulation()
-        t, jx, jy, jz = swe.get_current()
-        swe.delete()
+    if solver == "kspace":
+        sys.path.insert(0, os.path.join(REPO, "oracle"))
+        import oracle  # noqa: E402
+
+        t, J = oracle.ref_kspace_run(tb, param)
+        jx, jy, jz = J
+        t_init = 0.0
+        p["solver"] = solver
+    else:
+        with open(os.devnull, "w") as devnull, contextlib.redirect_stdout(devnull):
+            settings = pyswe.Settings(param)
+            swe = pyswe.SWE(settings)
+            t_init = time.time() - t0
+            swe.run_simulation()
+            t, jx, jy, jz = swe.get_current()
+            swe.delete()
     t_run = time.time() - t0 - t_init
     out = os.path.join(HERE, f"{name}.npz")
     np.savez_compressed(out, t=np.real(t), J=np.stack([jx, jy, jz]).astype(np.complex128))

@@ -21,7 +21,7 @@ def pyswe():
 
 def run_swe(pyswe, param, device=None):
     s = pyswe.Settings(dict(param))
-    swe = pyswe.SWE(s, device=device)
+    swe = pyswe.SWE(s, device=device, solver=param.get("solver", "rspace"))
     swe.run_simulation()
     t, jx, jy, jz = swe.get_current()
     out = (np.real(t), np.stack([jx, jy, jz]), swe)

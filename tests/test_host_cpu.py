@@ -156,3 +156,12 @@ def test_deferred_request_holds_no_device_state():
     with pytest.raises(pyswe.SWEError, match="SWESim_init"):
         swe.get_current()
     swe.delete()
+
+
+def test_kspace_solver_rejects_non_square_grids():
+    from pySWE import pyswe
+
+    with pytest.raises(pyswe.SWEError, match="nr1 == nr2"):
+        pyswe.SWE(pyswe.Settings(_param(nr1=8, nr2=10)), solver="kspace")
+    with pytest.raises(pyswe.SWEError, match="solver must be"):
+        pyswe.SWE(pyswe.Settings(_param()), solver="fft")

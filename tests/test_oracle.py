@@ -8,7 +8,8 @@ import pytest
 
 from conftest import GOLDEN, golden_names, load_golden, rel_l2
 
-SMALL = [n for n in golden_names() if n not in ("c0", "c1", "c2_prefix")]
+SMALL = [n for n in golden_names() if n not in ("c0", "c1", "c2_prefix") and not n.startswith("ks_")]
+KSPACE_SMALL = [n for n in golden_names() if n.startswith("ks_") and n not in ("ks_c0", "ks_c1")]
 
 
 def test_golden_models_regenerate_bit_for_bit():
@@ -167,3 +168,50 @@ def test_oracle_matches_live_reference(oracle_mod, model, n, tmax, pol):
     assert np.array_equal(t, tr)
     for a in range(2):
         assert rel_l2(J[a], Jr[a]) < 1e-10
+
+
+
+# ------------------------------------------------ the k-space solver (src/solver_kspace.cpp)
+
+
+@pytest.mark.parametrize("name", KSPACE_SMALL)
+def test_kspace_oracle_matches_golden(oracle_mod, name):
+    meta, param, t_ref, J_ref = load_golden(name)
+    t, J = oracle_mod.run_kspace(param["path_tb"], param)
+    assert np.array_equal(t, t_ref)
+    for a in range(3):
+        if np.abs(J_ref[a]).max() == 0:
+            assert np.abs(J[a]).max() == 0
+        else:
+            assert rel_l2(J[a], J_ref[a]) < 1e-10, (name, a, rel_l2(J[a], J_ref[a]))
+
+
+def test_kspace_oracle_matches_golden_c0_prefix(oracle_mod):
+    meta, param, t_ref, J_ref = load_golden("ks_c0")
+    n = 200
+    _, J = oracle_mod.run_kspace(param["path_tb"], param, nsteps=n)
+    assert rel_l2(J[1, :n], J_ref[1, :n]) < 1e-10
+    assert np.abs(J[:, n:]).max() == 0
+
+
+@needs_ref
+@pytest.mark.parametrize("model,n,tmax,pol", [("tmd12_s3", 6, 0.3, [0.5, 0.5, 0.0]), ("haldane", 10, 2.0, [1.0, 0.0, 0.0])])
+def test_kspace_oracle_matches_live_reference(oracle_mod, model, n, tmax, pol):
+    import tbgen
+
+    param = {"nr1": n, "nr2": n, "nr3": 1, "tmax": tmax, "dt": 0.02197, "intensity": 2e12, "lambda": 2000.0,
+             "tmax_field": 80.0, "pol_vec": np.array(pol), "phi_vec": np.zeros(3)}
+    tb = tbgen.model_path(model)
+    _, J_ref = oracle_mod.ref_kspace_run(tb, param)
+    _, J = oracle_mod.run_kspace(tb, param)
+    for a in range(2):
+        assert rel_l2(J[a], J_ref[a]) < 1e-10, (a, rel_l2(J[a], J_ref[a]))
+
+
+@needs_ref
+def test_kspace_solver_is_not_the_real_space_one(oracle_mod):
+    """The two reference solvers differ (no Peierls phase, transposed interpolation); the k-space
+    fixtures are not real-space results under another name."""
+    _, param, _, J_ks = load_golden("ks_haldane_12_pol")
+    _, _, _, J_rs = load_golden("haldane_12_pol")
+    assert rel_l2(J_ks[1], J_rs[1]) > 1e-2
