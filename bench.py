@@ -255,14 +255,15 @@ def workload_param(name: str, rank: int = 0, world: int = 1, grid: int | None = 
     return p
 
 
-def flops_per_kstep(nw: int, window: int, n: int, n_op: int, n_j: int) -> float:
+def flops_per_kstep(nw: int, window: int, n: int, n_op: int, n_j: int, kspace: bool = False) -> float:
     """Algorithmic FP64 flops of one k-point x RK4 step (minimal form):
     4 stages x one complex nw^3 product (Hermitian commutator), the Wannier sum of H0 and the
     field-coupled r as a separable pruned DFT over the window x window cells, the windowed velocity
-    (4x4 pruned DFT) and Tr(W rho), and the RK axpys."""
+    (4x4 pruned DFT) and Tr(W rho), and the RK axpys.  The k-space solver evaluates H at two new
+    points per step (t + dt/2, t + dt) and its window velocity is constant (only Tr(W rho) per step)."""
     f_comm = 32.0 * nw ** 3
-    f_w = 8.0 * nw * nw * n_op * window * (1.0 + window / n)
-    f_j = n_j * 8.0 * nw * nw * (4.0 * (1.0 + 4.0 / n) + 1.0)
+    f_w = 8.0 * nw * nw * n_op * window * (1.0 + window / n) * (2.0 if kspace else 1.0)
+    f_j = n_j * 8.0 * nw * nw * ((0.0 if kspace else 4.0 * (1.0 + 4.0 / n)) + 1.0)
     f_rk = 12.0 * nw * nw
     return f_comm + f_w + f_j + f_rk
 
@@ -326,6 +327,35 @@ class ClockSampler:
 # ---------------------------------------------------------------- the reference's CPU build
 
 
+def _ref_worker_kspace(conn, probe_path, tb, param, nt_sample):
+    """One single-threaded process running the reference's own k-space solver (its compiled
+    Solver_kspace, driven step by step by oracle/ref_probe.cpp: the reference has no entry point for it)."""
+    import ctypes as ct
+
+    import numpy as np
+
+    P = ct.CDLL(probe_path)
+    dp = ct.POINTER(ct.c_double)
+    P.probe_kspace_new.restype = ct.c_void_p
+    P.probe_kspace_new.argtypes = [ct.c_char_p, ct.c_int, ct.c_int] + [ct.c_double] * 5 + [dp, dp]
+    P.probe_kspace_steps.argtypes = [ct.c_void_p, ct.c_int]
+    P.probe_kspace_delete.argtypes = [ct.c_void_p]
+    pol = np.ascontiguousarray(param["pol_vec"], dtype=np.float64)
+    phi = np.ascontiguousarray(param["phi_vec"], dtype=np.float64)
+    h = P.probe_kspace_new(tb.encode(), int(param["nr1"]), int(param["nr2"]), float(param["tmax"]), float(param["dt"]),
+                           float(param["intensity"]), float(param["lambda"]), float(param["tmax_field"]),
+                           pol.ctypes.data_as(dp), phi.ctypes.data_as(dp))
+    conn.send("ready")
+    while True:
+        msg = conn.recv()
+        if msg != "run":
+            break
+        t0 = time.perf_counter()
+        P.probe_kspace_steps(h, int(nt_sample))
+        conn.send(time.perf_counter() - t0)
+    P.probe_kspace_delete(h)
+
+
 def _ref_worker(conn, lib_path, tb, param, nt_sample):
     """One single-threaded reference process (its own SWESim), driven through the reference C ABI."""
     import ctypes as ct
@@ -380,15 +410,15 @@ def _ref_worker(conn, lib_path, tb, param, nt_sample):
 class ReferencePool:
     """`cores` concurrent single-threaded reference solves of the workload's grid and model."""
 
-    def __init__(self, param: dict, nt_sample: int, cores: int):
+    def __init__(self, param: dict, nt_sample: int, cores: int, solver: str = "rspace"):
         import multiprocessing as mp
 
         sys.path.insert(0, os.path.join(REPO, "oracle"))
         import oracle
 
-        lib = oracle.ref_paths()[0]
+        lib = oracle.ref_paths()[0 if solver == "rspace" else 1]
         if not os.path.exists(lib):
-            raise FileNotFoundError("oracle/_ref/libwannier.so (build: make -C oracle with the reference checkout)")
+            raise FileNotFoundError(f"{os.path.relpath(lib, REPO)} (build: make -C oracle with the reference checkout)")
         os.environ["OPENBLAS_NUM_THREADS"] = "1"
         os.environ["OMP_NUM_THREADS"] = "1"
         ctx = mp.get_context("spawn")
@@ -396,7 +426,8 @@ class ReferencePool:
         self.conns, self.procs = [], []
         for _ in range(cores):
             a, b = ctx.Pipe()
-            p = ctx.Process(target=_ref_worker, args=(b, lib, param["path_tb"], param, nt_sample), daemon=True)
+            target = _ref_worker if solver == "rspace" else _ref_worker_kspace
+            p = ctx.Process(target=target, args=(b, lib, param["path_tb"], param, nt_sample), daemon=True)
             p.start()
             self.conns.append(a)
             self.procs.append(p)
@@ -439,14 +470,18 @@ def run_reference_arm(args, rank: int, world: int):
     param = workload_param(args.workload)
     cores = os.cpu_count() or 1
     nt_sample = reference_sample_steps(args.workload)
+    if args.workload in ("c3", "c4"):
+        print(json.dumps({"impl": "reference", "unavailable": "the batched-scan and serving workloads have no "
+                          "reference implementation; their CPU comparison is the c0-c2 arms"}))
+        return
     line = {"metric": "k-pt*RK4-steps/s", "impl": "reference", "unit": "k-pt*RK4-steps/s", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded TB model)",
-            "config": {"workload": f"{args.workload}: {WORKLOADS[args.workload]['desc']}",
+            "config": {"workload": f"{args.workload}: {WORKLOADS[args.workload]['desc']}", "solver": args.solver,
                        "sample": f"{cores} concurrent single-threaded processes x {nt_sample} RK4 steps",
                        "l2": "n/a (CPU)"}}
     try:
-        pool = ReferencePool(param, nt_sample, cores)
+        pool = ReferencePool(param, nt_sample, cores, args.solver)
     except Exception as e:  # noqa: BLE001
         print(json.dumps({"impl": "reference", "unavailable": f"reference CPU build not runnable: {e}"}))
         return
@@ -465,13 +500,13 @@ def run_reference_arm(args, rank: int, world: int):
     print(json.dumps(line), flush=True)
 
 
-def cpu_baseline(workload: str) -> dict:
+def cpu_baseline(workload: str, solver: str = "rspace") -> dict:
     """Reference CPU build on the host cores, bounded sample (one warm and one timed round)."""
     param = workload_param(workload)
     cores = os.cpu_count() or 1
     nt_sample = reference_sample_steps(workload)
     try:
-        pool = ReferencePool(param, nt_sample, cores)
+        pool = ReferencePool(param, nt_sample, cores, solver)
     except Exception as e:  # noqa: BLE001
         return {"value": None, "unit": "k-pt*RK4-steps/s", "cores": cores, "kind": "reference",
                 "sample": f"unavailable: {e}"}
@@ -546,6 +581,8 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"],
                     help="mixed: FP32 Wannier sums and commutators, FP64 state / RK accumulation / k-sum")
+    ap.add_argument("--solver", default="rspace", choices=["rspace", "kspace"],
+                    help="kspace: the reference's k-space solver (src/solver_kspace.cpp) instead of its real-space one")
     ap.add_argument("--requests", type=int, default=200, help="c4: requests in the arrival stream")
     ap.add_argument("--max-active", type=int, default=32, help="c4: most solves running at once")
     ap.add_argument("--chunk", type=int, default=256, help="c4: RK4 steps per scheduling chunk")
@@ -604,7 +641,7 @@ def main():
     param = workload_param(args.workload, rank, world, args.grid)
     w = WORKLOADS[args.workload]
     settings = pyswe.Settings(dict(param))
-    swe = pyswe.SWE(settings, device=local, precision=args.precision)
+    swe = pyswe.SWE(settings, device=local, precision=args.precision, solver=args.solver)
     nk = param["nr1"] * param["nr2"]
     nt = settings.nt
     nw = swe.num_orb()
@@ -660,7 +697,7 @@ def main():
         swe.reset()
         swe.run_simulation()
         J_mixed = swe.get_current()[1:]
-        ref = pyswe.SWE(pyswe.Settings(dict(param)), device=local)
+        ref = pyswe.SWE(pyswe.Settings(dict(param)), device=local, solver=args.solver)
         ref.run_simulation()
         J_fp64 = ref.get_current()[1:]
         fp64_ms = ref.last_kernel_ms()
@@ -672,7 +709,7 @@ def main():
     if rank != 0:
         return
 
-    fpk = flops_per_kstep(nw, w["window"], param["nr1"], n_op, n_j)
+    fpk = flops_per_kstep(nw, w["window"], param["nr1"], n_op, n_j, kspace=args.solver == "kspace")
     prop_mean = statistics.mean(prop_ms)
     achieved = fpk * nk * nt / (prop_mean * 1e-3) / 1e12
     traffic, traffic_src = load_traffic(args.workload)
@@ -693,12 +730,12 @@ def main():
         "config": {"workload": f"{args.workload}: {WORKLOADS[args.workload]['desc']}"
                    + (f" (grid overridden to {args.grid}x{args.grid})" if args.grid else ""),
                    "k_grid": [param["nr1"], param["nr2"]],
-                   "nt": nt, "num_orb": nw, "precision": args.precision, "parallelism": f"replicas x{world}" if world > 1 else "single",
+                   "nt": nt, "num_orb": nw, "precision": args.precision, "solver": args.solver, "parallelism": f"replicas x{world}" if world > 1 else "single",
                    "l2": "flushed between timed solves (256 MiB write)", "launch": shape},
         "solves_per_hour": 3600.0 * world * args.steps / (total_ms * 1e-3),
         "roofline": {"bound": "fp64", "achieved": achieved, "peak": fp64_peak.value, "unit": "TFLOP/s",
                      "frac": achieved / fp64_peak.value if fp64_peak.value > 0 else None, "traffic": traffic,
-                     "kernel": "propagate_fp64_kernel", "flops_per_kstep": fpk,
+                     "kernel": shape.get("kernel_name"), "flops_per_kstep": fpk,
                      "peak_source": "live FP64 FMA-chain probe on this GPU (HHG_measure_peaks); "
                                     "MEASURED_PEAKS.json has no FP64 figure",
                      "fp32_peak": fp32_peak.value, "kernel_ms": prop_mean, "traffic_source": traffic_src},
@@ -711,7 +748,7 @@ def main():
     if mixed:
         line["mixed_vs_fp64"] = mixed
     if world == 1 and not args.no_cpu_baseline and not args.grid:
-        line["cpu_baseline"] = cpu_baseline(args.workload)
+        line["cpu_baseline"] = cpu_baseline(args.workload, args.solver)
     print(json.dumps(line), flush=True)
 
 

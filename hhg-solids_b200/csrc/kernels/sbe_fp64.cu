@@ -18,6 +18,7 @@
 //   state in registers; per-cell phases e^{-ik.R_c} (per thread, fixed) x e^{iA.R_c} (per step).
 // propagate_group_kernel    (any nw <= 16, FP64 or mixed precision): in sbe_group.cu.
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 
 #include "sbe_device.h"
@@ -489,7 +490,11 @@ bool plan_propagate(const SolveTables& t, int precision, int sm_count, LaunchSha
     snprintf(why, why_len, "num_orb=%d outside the supported range 1..%d", t.nw, kMaxOrb);
     return false;
   }
-  if (precision == 0 && t.hermitian && t.nw <= 2 && plan_kpt(t, sm_count, out, kSmemMax)) return true;
+  // Tuning override: HHG_KERNEL=group runs the element-group kernel where the thread-per-k-point
+  // one would be chosen.
+  const char* force = std::getenv("HHG_KERNEL");
+  const bool force_group = force && std::strcmp(force, "group") == 0;
+  if (!force_group && precision == 0 && t.hermitian && t.nw <= 2 && plan_kpt(t, sm_count, out, kSmemMax)) return true;
   return plan_group(t, precision, sm_count, out, why, why_len);
 }
 

@@ -228,8 +228,10 @@ class SWE:
     def launch_shape(self) -> dict:
         c, t, k = ct.c_int(), ct.c_int(), ct.c_int()
         s = ct.c_longlong()
-        self.swe_cpp.SWESim_launch_shape(self.ptr, ct.byref(c), ct.byref(t), ct.byref(k), ct.byref(s))
-        return {"ctas": c.value, "threads": t.value, "k_per_cta": k.value, "smem_bytes": s.value}
+        kind = int(self.swe_cpp.SWESim_launch_shape(self.ptr, ct.byref(c), ct.byref(t), ct.byref(k), ct.byref(s)))
+        names = {0: "propagate_kpt_kernel", 1: "propagate_group_kernel<double>", 2: "propagate_group_kernel<float>"}
+        return {"ctas": c.value, "threads": t.value, "k_per_cta": k.value, "smem_bytes": s.value,
+                "kernel_name": names.get(kind, "none")}
 
     def last_launches(self) -> int:
         return int(self.swe_cpp.SWESim_last_launches(self.ptr))
