@@ -78,7 +78,7 @@ struct SWEBatch {
     std::vector<int> alone;
     for (int i = 0; i < (int)sims.size(); ++i) {
       const hhg::LaunchShape& sh = sims[i]->shape;
-      if (sh.kernel == 0) {
+      if (sh.kernel == 0 || sh.kernel == 3) {
         alone.push_back(i);
       } else {
         const hhg::SolveTables& t = sims[i]->tab;
@@ -442,7 +442,7 @@ struct SWEServer {
       d.rho = sim->d_rho.p;
       d.Jpart = sim->d_Jpart.p;
       const hhg::LaunchShape& sh = sim->shape;
-      if (sh.kernel == 0)
+      if (sh.kernel == 0 || sh.kernel == 3)
         alone.push_back(i);
       else
         classes[std::make_tuple(sh.kernel, sh.variant, sh.ept, sh.threads, sh.group, sh.kmode, sim->tab.nw,

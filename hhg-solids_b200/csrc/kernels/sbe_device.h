@@ -55,7 +55,8 @@ struct GroupTables {
 };
 
 struct LaunchShape {
-  int kernel;      // 0: thread per k-point (FP64, nw <= 2, Hermitian); 1: element groups FP64; 2: element groups mixed
+  int kernel;      // 0: thread per k-point (FP64, nw <= 2, Hermitian); 1: element groups FP64; 2: element groups mixed;
+                   // 3: column tiles, thread per k-point (FP64, nw <= 2, Hermitian)
   int k_per_cta;   // k-points per CTA
   int group;       // threads per k-point
   int threads;     // threads per CTA
@@ -85,6 +86,10 @@ bool plan_propagate(const SolveTables& t, int precision, int sm_count, LaunchSha
 bool plan_group(const SolveTables& t, int precision, int sm_count, LaunchShape* out, char* why, int why_len);
 void launch_group(const SolveTables& t, const GroupTables& gt, const LaunchShape& s, double2* rho, double2* Jpart,
                   cudaStream_t stream);
+// Column-tile kernel (nw <= 2, Hermitian, FP64): false if the solve does not suit it.
+bool plan_kcol(const SolveTables& t, int sm_count, LaunchShape* out, size_t smem_max);
+void launch_kcol(const SolveTables& t, const GroupTables& gt, const LaunchShape& s, double2* rho, double2* Jpart,
+                 cudaStream_t stream);
 // Persistent work-stealing launch over (solve, virtual CTA) items of solves sharing the kernel shape of
 // `s` (same variant, threads); smem = the largest member's.  Returns the grid size.
 int launch_group_batch(const LaunchShape& s, const BatchDesc* descs, const int2* items, int nitems, int* counter,

@@ -69,7 +69,7 @@ __device__ __forceinline__ void flush_current(const SolveTables& t, const double
 
 // ------------------------------------------------------------------ thread per k-point (nw <= 2)
 
-constexpr int kKptMaxThreads = 512;
+constexpr int kKptMaxThreads = 288;
 
 // NAXc, NJc: field axes and current axes fixed at compile time (0: read from t).
 template <int NW, int NAXc, int NJc, bool KM>
@@ -128,7 +128,7 @@ __global__ void __launch_bounds__(kKptMaxThreads) propagate_kpt_kernel(SolveTabl
 #pragma unroll
         for (int a = 0; a < 3; ++a) ru[a][e] = make_double2(0.0, 0.0);
       }
-#pragma unroll 2
+#pragma unroll 4
       for (int c = 0; c < nc; ++c) {
         const double2 ph = cmul(sTk[c * nthr + tid], q[c]);
         const double2* hc = sH + c * NW2;
@@ -157,9 +157,13 @@ __global__ void __launch_bounds__(kKptMaxThreads) propagate_kpt_kernel(SolveTabl
       for (int e = 0; e < NW2; ++e)
 #pragma unroll
         for (int a = 0; a < 3; ++a) w[a][e] = make_double2(0.0, 0.0);
-#pragma unroll 2
+#pragma unroll 4
       for (int c = 0; c < nwn; ++c) {
-        const double2 ph = q ? cmul(sTk[(nc + c) * nthr + tid], q[nc + c]) : sTk[(nc + c) * nthr + tid];
+        double2 ph;
+        if constexpr (KM)
+          ph = sTk[(nc + c) * nthr + tid];
+        else
+          ph = cmul(sTk[(nc + c) * nthr + tid], q[nc + c]);
 #pragma unroll
         for (int a = 0; a < 3; ++a)
           if (a < nj) {
@@ -490,11 +494,22 @@ bool plan_propagate(const SolveTables& t, int precision, int sm_count, LaunchSha
     snprintf(why, why_len, "num_orb=%d outside the supported range 1..%d", t.nw, kMaxOrb);
     return false;
   }
-  // Tuning override: HHG_KERNEL=group runs the element-group kernel where the thread-per-k-point
-  // one would be chosen.
+  // Tuning override: HHG_KERNEL=group / kpt / kcol forces that kernel where a thread-per-k-point one
+  // would be chosen.
   const char* force = std::getenv("HHG_KERNEL");
   const bool force_group = force && std::strcmp(force, "group") == 0;
-  if (!force_group && precision == 0 && t.hermitian && t.nw <= 2 && plan_kpt(t, sm_count, out, kSmemMax)) return true;
+  const bool force_kpt = force && std::strcmp(force, "kpt") == 0;
+  const bool force_kcol = force && std::strcmp(force, "kcol") == 0;
+  if (!force_group && precision == 0 && t.hermitian && t.nw <= 2) {
+    // Column tiles when there are enough columns to fill the GPU, else one k-point per thread in
+    // consecutive-k tiles.
+    LaunchShape kc{};
+    if (!force_kpt && plan_kcol(t, sm_count, &kc, kSmemMax) && (force_kcol || kc.ntiles >= sm_count)) {
+      *out = kc;
+      return true;
+    }
+    if (plan_kpt(t, sm_count, out, kSmemMax)) return true;
+  }
   return plan_group(t, precision, sm_count, out, why, why_len);
 }
 
@@ -505,6 +520,8 @@ void launch_propagate_steps(const SolveTables& t, const GroupTables& gt, const L
     KptKernel kern = kpt_kernel_for(t);
     cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s.smem);
     kern<<<s.ctas, s.threads, s.smem, stream>>>(t, s.vctas, rho, Jpart);
+  } else if (s.kernel == 3) {
+    launch_kcol(t, gt, s, rho, Jpart, stream);
   } else {
     launch_group(t, gt, s, rho, Jpart, stream);
   }

@@ -1,0 +1,371 @@
+// Column-tile FP64 propagation for nw <= 2 with a Hermitian placement (the 2-orbital configurations).
+//
+// Same propagation as propagate_kpt_kernel (the k-space-resident RK4 of src/solver.cpp:86-181 with
+// the current of src/observable.cpp:16-30, or the k-space solver of src/solver_kspace.cpp), with the
+// Wannier sums in separable form shared by a k-grid column:
+//
+//   H(k) = sum_n1 e^{-2 pi i m1 n1 / N1} G(n1),   G(n1) = P1(n1) sum_n2 e^{-2 pi i m2 n2 / N2} P2(n2) X(n1, n2)
+//
+// (P = the per-point factors: Peierls powers e^{i n A.a}, or the k-space solver's interpolation
+// factors) and likewise for the current window.  A CTA owns R consecutive rows m1 of one column m2,
+// one thread per k-point with its state in registers.  Every kRing steps the CTA computes the
+// column's G for all points of the chunk into shared memory (one pair of barriers per chunk); per
+// step each thread then sums b1n box rows and 4 window rows with its own row twiddles, instead of
+// every cell of the support and window.
+#include <cstdio>
+#include <cstdlib>
+
+#include "sbe_device.h"
+
+namespace hhg {
+namespace {
+
+__device__ __forceinline__ double2 kc_mul(double2 a, double2 b) {
+  return make_double2(fma(a.x, b.x, -a.y * b.y), fma(a.x, b.y, a.y * b.x));
+}
+__device__ __forceinline__ double2 kc_fma(double2 a, double2 b, double2 c) {
+  c.x = fma(a.x, b.x, c.x);
+  c.x = fma(-a.y, b.y, c.x);
+  c.y = fma(a.x, b.y, c.y);
+  c.y = fma(a.y, b.x, c.y);
+  return c;
+}
+__device__ __forceinline__ double kc_warp_sum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+__device__ __forceinline__ int kc_wrap(long long x, int n) {
+  int r = (int)(x % n);
+  return r < 0 ? r + n : r;
+}
+
+constexpr int kKcolMaxThreads = 256;
+
+// Shared-memory layout (complex double units unless noted), shared by host planning and kernel.
+struct KcolLayout {
+  size_t t1, G, GW, p2, total_cx, E_d, J_d;
+  __host__ __device__ KcolLayout(const SolveTables& t, int threads) {
+    const size_t nmat = 1 + t.nax, nw2 = t.nw2, pts = t.kmode ? 2 * kRing + 1 : kRing;
+    size_t p = 0;
+    t1 = p;
+    p += (size_t)(t.b1n + 4) * threads;          // per-thread row twiddles: box rows, window rows
+    G = p;
+    p += pts * t.b1n * nmat * nw2;               // column sums of the chunk's points
+    GW = p;
+    p += (t.kmode ? 1 : kRing) * 4 * (size_t)t.nj * nw2;  // window column sums (constant: k-space solver)
+    p2 = p;
+    p += pts * (size_t)(t.b2n + 4);              // column factors of each point
+    total_cx = p;
+    E_d = 0;
+    J_d = kRing * 9;
+  }
+  __host__ __device__ size_t bytes(int threads) const {
+    return total_cx * sizeof(double2) + (J_d + (size_t)kRing * (threads / 32) * 2 * 3) * sizeof(double);
+  }
+};
+
+template <int NW, int NAXc, int NJc, bool KM>
+__global__ void __launch_bounds__(kKcolMaxThreads) propagate_kcol_kernel(SolveTables t, GroupTables gt, int R,
+                                                                         int vctas, double2* rho, double2* Jpart) {
+  constexpr int NW2 = NW * NW;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  const int nax = NAXc ? NAXc : t.nax, nj = NJc ? NJc : t.nj, nmat = 1 + nax;
+  const int b1n = t.b1n, b2n = t.b2n, npw = 2 * t.np + 1;
+  const int nthr = blockDim.x, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarps = nthr >> 5;
+  const KcolLayout L(t, nthr);
+  double2* sm = reinterpret_cast<double2*>(smraw);
+  double2* sT1 = sm + L.t1;
+  double2* sG = sm + L.G;
+  double2* sGW = sm + L.GW;
+  double2* sp2 = sm + L.p2;
+  double* sE = reinterpret_cast<double*>(sm + L.total_cx) + L.E_d;
+  double* sJ = reinterpret_cast<double*>(sm + L.total_cx) + L.J_d;
+  const double2* X = gt.Xbox64;  // [nmat][b1n][b2n][NW2]
+  const double2* V = gt.Xwin64;  // [nj][4][4][NW2]
+  const double2* P = gt.P64;     // [points][2][npw]
+  const int ppr = KM ? 2 : 1, cstride = b2n + 4;
+  const double dt = t.dt;
+  const double prefac = 0.1666666666666 * dt;
+  const int rows = t.row1 - t.row0, tpc = (rows + R - 1) / R, ntiles = t.N2 * tpc;
+
+  double hd[NW], rd[3][NW];
+  double2 hu[NW2], ru[3][NW2], w[3][NW2];
+  // Box sums of chunk point pt (Hermitian parts: diagonal real, upper triangle complex).
+  auto box_sums = [&](int pt) {
+#pragma unroll
+    for (int i = 0; i < NW; ++i) {
+      hd[i] = 0.0;
+#pragma unroll
+      for (int a = 0; a < 3; ++a) rd[a][i] = 0.0;
+    }
+#pragma unroll
+    for (int e = 0; e < NW2; ++e) {
+      hu[e] = make_double2(0.0, 0.0);
+#pragma unroll
+      for (int a = 0; a < 3; ++a) ru[a][e] = make_double2(0.0, 0.0);
+    }
+#pragma unroll 4
+    for (int q1 = 0; q1 < b1n; ++q1) {
+      const double2 tw = sT1[q1 * nthr + tid];
+      const double2* g = sG + ((size_t)pt * b1n + q1) * nmat * NW2;
+#pragma unroll
+      for (int i = 0; i < NW; ++i) {
+        hd[i] = fma(tw.x, g[i * NW + i].x, fma(-tw.y, g[i * NW + i].y, hd[i]));
+#pragma unroll
+        for (int j = i + 1; j < NW; ++j) hu[i * NW + j] = kc_fma(tw, g[i * NW + j], hu[i * NW + j]);
+      }
+#pragma unroll
+      for (int a = 0; a < 3; ++a)
+        if (a < nax) {
+          const double2* ga = g + (1 + a) * NW2;
+#pragma unroll
+          for (int i = 0; i < NW; ++i) {
+            rd[a][i] = fma(tw.x, ga[i * NW + i].x, fma(-tw.y, ga[i * NW + i].y, rd[a][i]));
+#pragma unroll
+            for (int j = i + 1; j < NW; ++j) ru[a][i * NW + j] = kc_fma(tw, ga[i * NW + j], ru[a][i * NW + j]);
+          }
+        }
+    }
+  };
+  // Window velocity W_a(k) from the column sums of slot s.
+  auto window_sums = [&](int s) {
+#pragma unroll
+    for (int e = 0; e < NW2; ++e)
+#pragma unroll
+      for (int a = 0; a < 3; ++a) w[a][e] = make_double2(0.0, 0.0);
+#pragma unroll
+    for (int w1 = 0; w1 < 4; ++w1) {
+      const double2 tw = sT1[(b1n + w1) * nthr + tid];
+      const double2* g = sGW + ((size_t)s * 4 + w1) * nj * NW2;
+#pragma unroll
+      for (int a = 0; a < 3; ++a)
+        if (a < nj)
+#pragma unroll
+          for (int e = 0; e < NW2; ++e) w[a][e] = kc_fma(tw, g[a * NW2 + e], w[a][e]);
+    }
+  };
+
+  // Virtual CTA v owns tiles v, v + vctas, ... and its own row of current partials.
+  for (int v = blockIdx.x; v < vctas; v += gridDim.x)
+  for (int tile = v; tile < ntiles; tile += vctas) {
+    const int m2 = tile / tpc, m1r = t.row0 + (tile % tpc) * R + tid;
+    const bool kval = tid < R && m1r < t.row1;
+    const int m1 = kval ? m1r : t.row0;
+    const size_t k = (size_t)m1 * t.N2 + m2;
+    double2 r[NW2];
+#pragma unroll
+    for (int e = 0; e < NW2; ++e) r[e] = kval ? rho[k * NW2 + e] : make_double2(0.0, 0.0);
+    for (int q = 0; q < b1n; ++q) sT1[q * nthr + tid] = t.T1[kc_wrap((long long)m1 * (t.b1lo + q), t.N1)];
+    for (int q = 0; q < 4; ++q) sT1[(b1n + q) * nthr + tid] = t.T1[kc_wrap((long long)m1 * (q - 2), t.N1)];
+
+    for (int ti0 = t.step0; ti0 < t.step1; ti0 += kRing) {
+      const int nsteps = min(kRing, t.step1 - ti0);
+      const int npts = KM ? 2 * nsteps + 1 : nsteps, j0 = ppr * ti0;
+      __syncthreads();  // the previous chunk's readers are done
+      // (a) column factors of each point: box n2 = b2lo + q, then window n2 = -2..1
+      for (int idx = tid; idx < npts * cstride; idx += nthr) {
+        const int s = idx / cstride, q = idx % cstride;
+        const int n2 = q < b2n ? t.b2lo + q : q - b2n - 2;
+        const double2 tw = t.T2[kc_wrap((long long)m2 * n2, t.N2)];
+        sp2[idx] = (KM && q >= b2n) ? tw : kc_mul(tw, P[((size_t)(j0 + s) * 2 + 1) * npw + t.np + n2]);
+      }
+      for (int idx = tid; idx < nsteps * 9; idx += nthr) sE[idx] = t.es[(size_t)ti0 * 9 + idx];
+      __syncthreads();
+      // (b) the column's sums G(n1) of each point, times the row factor P1(n1)
+      const int nG = npts * b1n * nmat * NW2;
+      for (int idx = tid; idx < nG; idx += nthr) {
+        const int e = idx % NW2;
+        int rest = idx / NW2;
+        const int mat = rest % nmat;
+        rest /= nmat;
+        const int q1 = rest % b1n, s = rest / b1n;
+        const double2* x = X + ((size_t)(mat * b1n + q1) * b2n) * NW2 + e;
+        const double2* p2 = sp2 + s * cstride;
+        double2 acc = make_double2(0.0, 0.0);
+        for (int q2 = 0; q2 < b2n; ++q2) acc = kc_fma(p2[q2], x[(size_t)q2 * NW2], acc);
+        sG[idx] = kc_mul(P[(size_t)(j0 + s) * 2 * npw + t.np + t.b1lo + q1], acc);
+      }
+      const bool win_now = !KM || ti0 == t.step0;  // the k-space solver's window sums are constant
+      if (win_now) {
+        const int nW = (KM ? 1 : nsteps) * 4 * nj * NW2;
+        for (int idx = tid; idx < nW; idx += nthr) {
+          const int e = idx % NW2;
+          int rest = idx / NW2;
+          const int a = rest % nj;
+          rest /= nj;
+          const int w1 = rest % 4, s = rest / 4;
+          const double2* vv = V + ((size_t)(a * 4 + w1) * 4) * NW2 + e;
+          const double2* p2 = sp2 + s * cstride + b2n;
+          double2 acc = make_double2(0.0, 0.0);
+#pragma unroll
+          for (int w2 = 0; w2 < 4; ++w2) acc = kc_fma(p2[w2], vv[(size_t)w2 * NW2], acc);
+          sGW[idx] = KM ? acc : kc_mul(P[(size_t)(j0 + s) * 2 * npw + t.np + (w1 - 2)], acc);
+        }
+      }
+      __syncthreads();
+      if (KM && ti0 == t.step0) window_sums(0);
+
+      for (int s = 0; s < nsteps; ++s) {
+        if (!KM) {
+          box_sums(s);
+          window_sums(s);
+        } else if (s == 0) {
+          box_sums(0);  // point t of the chunk's first step; later steps carry it from stage 4
+        }
+        // Four RK4 stages (src/solver.cpp:157-163), fields at t, t+dt/2, t+dt/2, t+dt.
+        double2 K[NW2], S[NW2];
+#pragma unroll
+        for (int st = 0; st < 4; ++st) {
+          const int f = st == 0 ? 0 : (st == 3 ? 2 : 1);
+          const double* es = sE + s * 9 + f * 3;
+          if (KM && st > 0 && st != 2) box_sums(2 * s + f);  // points t + dt/2, t + dt
+          double2 H[NW2], Xm[NW2];
+#pragma unroll
+          for (int i = 0; i < NW; ++i) {
+            double d = hd[i];
+#pragma unroll
+            for (int a = 0; a < 3; ++a)
+              if (a < nax) d = fma(es[t.ax_id[a]], rd[a][i], d);
+            H[i * NW + i] = make_double2(d, 0.0);
+#pragma unroll
+            for (int j = i + 1; j < NW; ++j) {
+              double2 u = hu[i * NW + j];
+#pragma unroll
+              for (int a = 0; a < 3; ++a)
+                if (a < nax) {
+                  const double ea = es[t.ax_id[a]];
+                  u.x = fma(ea, ru[a][i * NW + j].x, u.x);
+                  u.y = fma(ea, ru[a][i * NW + j].y, u.y);
+                }
+              H[i * NW + j] = u;
+              H[j * NW + i] = make_double2(u.x, -u.y);
+            }
+          }
+          const double cs = (st == 3 ? 1.0 : 0.5) * dt;
+#pragma unroll
+          for (int e = 0; e < NW2; ++e)
+            Xm[e] = st == 0 ? r[e] : make_double2(r[e].x + cs * K[e].x, r[e].y + cs * K[e].y);
+          double2 HX[NW2];
+#pragma unroll
+          for (int i = 0; i < NW; ++i)
+#pragma unroll
+            for (int j = 0; j < NW; ++j) {
+              double2 acc = make_double2(0.0, 0.0);
+#pragma unroll
+              for (int l = 0; l < NW; ++l) acc = kc_fma(H[i * NW + l], Xm[l * NW + j], acc);
+              HX[i * NW + j] = acc;
+            }
+#pragma unroll
+          for (int i = 0; i < NW; ++i)
+#pragma unroll
+            for (int j = 0; j < NW; ++j) {
+              // k = -i (HX - (HX)^+)
+              const double cx = HX[i * NW + j].x - HX[j * NW + i].x, cy = HX[i * NW + j].y + HX[j * NW + i].y;
+              K[i * NW + j] = make_double2(cy, -cx);
+            }
+          const double wgt = st == 3 ? 1.0 : 2.0;
+#pragma unroll
+          for (int e = 0; e < NW2; ++e)
+            S[e] = st == 0 ? K[e] : make_double2(S[e].x + wgt * K[e].x, S[e].y + wgt * K[e].y);
+        }
+#pragma unroll
+        for (int e = 0; e < NW2; ++e) r[e] = make_double2(r[e].x + prefac * S[e].x, r[e].y + prefac * S[e].y);
+
+        // Current partials.
+#pragma unroll
+        for (int a = 0; a < 3; ++a)
+          if (a < nj) {
+            double re = 0.0, im = 0.0;
+            if (kval) {
+#pragma unroll
+              for (int e = 0; e < NW2; ++e) {
+                re = fma(w[a][e].x, r[e].x, fma(w[a][e].y, r[e].y, re));
+                im = fma(w[a][e].y, r[e].x, fma(-w[a][e].x, r[e].y, im));
+              }
+            }
+            re = kc_warp_sum(re);
+            im = kc_warp_sum(im);
+            if (lane == 0) {
+              sJ[(s * nwarps + warp) * 2 * nj + 2 * a] = re;
+              sJ[(s * nwarps + warp) * 2 * nj + 2 * a + 1] = im;
+            }
+          }
+      }
+      __syncthreads();
+      // Add the chunk's per-warp partials into this virtual CTA's row.
+      for (int idx = tid; idx < nsteps * nj; idx += nthr) {
+        const int s = idx / nj, a = idx % nj;
+        double re = 0.0, im = 0.0;
+        for (int q = 0; q < nwarps; ++q) {
+          re += sJ[(s * nwarps + q) * 2 * nj + 2 * a];
+          im += sJ[(s * nwarps + q) * 2 * nj + 2 * a + 1];
+        }
+        double2* dst = Jpart + ((size_t)v * t.nt + ti0 + s) * 3 + t.j_id[a];
+        const double2 old = *dst;
+        *dst = make_double2(old.x + re, old.y + im);
+      }
+    }
+    if (kval) {
+#pragma unroll
+      for (int e = 0; e < NW2; ++e) rho[k * NW2 + e] = r[e];
+    }
+  }
+}
+
+using KcolKernel = void (*)(SolveTables, GroupTables, int, int, double2*, double2*);
+
+template <bool KM>
+KcolKernel kcol_kernel_t(const SolveTables& t) {
+  if (t.nw == 2 && t.nj == 2) {
+    if (t.nax == 1) return propagate_kcol_kernel<2, 1, 2, KM>;
+    if (t.nax == 2) return propagate_kcol_kernel<2, 2, 2, KM>;
+  }
+  return t.nw == 1 ? propagate_kcol_kernel<1, 0, 0, KM> : propagate_kcol_kernel<2, 0, 0, KM>;
+}
+KcolKernel kcol_kernel_for(const SolveTables& t) { return t.kmode ? kcol_kernel_t<true>(t) : kcol_kernel_t<false>(t); }
+
+}  // namespace
+
+bool plan_kcol(const SolveTables& t, int sm_count, LaunchShape* out, size_t smem_max) {
+  if (t.nw > 2 || !t.hermitian) return false;
+  const int rows = t.row1 - t.row0;
+  // Rows per tile: equal parts of at most 128 rows (measured on the 200x200 grid: 100-row tiles,
+  // four resident CTAs per SM, beat whole 200-row columns by 16 % and 50-row tiles by 30 %).
+  int parts = (rows + 127) / 128;
+  if (const char* e = std::getenv("HHG_KCOL_PARTS")) parts = std::max(parts, std::atoi(e));  // tuning override
+  const int R = (rows + parts - 1) / parts;
+  const int threads = (R + 31) / 32 * 32;
+  const long ntiles = (long)t.N2 * ((rows + R - 1) / R);
+  const KcolLayout L(t, threads);
+  const size_t smem = L.bytes(threads);
+  if (smem > smem_max || threads > kKcolMaxThreads) return false;
+  KcolKernel kern = kcol_kernel_for(t);
+  cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  int occ = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, threads, smem);
+  if (occ < 1) return false;
+  const long slots = (long)occ * sm_count;
+  out->kernel = 3;
+  out->kmode = t.kmode;
+  out->k_per_cta = R;
+  out->group = 1;
+  out->threads = threads;
+  out->ntiles = (int)ntiles;
+  out->ctas = (int)(ntiles < slots ? ntiles : slots);
+  out->vctas = out->ctas;
+  out->box_sm = out->win_sm = 0;
+  out->ept = 1;
+  out->variant = -1;
+  out->smem = smem;
+  return true;
+}
+
+void launch_kcol(const SolveTables& t, const GroupTables& gt, const LaunchShape& s, double2* rho, double2* Jpart,
+                 cudaStream_t stream) {
+  KcolKernel kern = kcol_kernel_for(t);
+  cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s.smem);
+  kern<<<s.ctas, s.threads, s.smem, stream>>>(t, gt, s.k_per_cta, s.vctas, rho, Jpart);
+}
+
+}  // namespace hhg
