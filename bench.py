@@ -561,8 +561,10 @@ def mixed_report(J_mixed, J_fp64, param, fp64_ms, mixed_ms):
             "fp64_ms_per_solve": fp64_ms, "mixed_ms_per_solve": mixed_ms, "speedup_vs_fp64": fp64_ms / mixed_ms}
 
 
-def load_traffic(workload: str):
-    path = os.path.join(REPO, "profiles", f"propagate_fp64_{workload}_traffic.json")
+def load_traffic(workload: str, kernel: str):
+    """DRAM bytes per launch of this kernel on this workload, from a committed ncu capture summary."""
+    short = (kernel or "").split("<")[0].replace("_kernel", "")
+    path = os.path.join(REPO, "profiles", f"{short}_{workload}_traffic.json")
     if not os.path.exists(path):
         return None, None
     with open(path) as f:
@@ -712,7 +714,8 @@ def main():
     fpk = flops_per_kstep(nw, w["window"], param["nr1"], n_op, n_j, kspace=args.solver == "kspace")
     prop_mean = statistics.mean(prop_ms)
     achieved = fpk * nk * nt / (prop_mean * 1e-3) / 1e12
-    traffic, traffic_src = load_traffic(args.workload)
+    traffic, traffic_src = (load_traffic(args.workload, shape.get("kernel_name"))
+                            if args.solver == "rspace" and args.precision == "fp64" and not args.grid else (None, None))
     line = {
         "metric": "k-pt*RK4-steps/s",
         "value": value,
