@@ -116,6 +116,14 @@ void launch_reduce_current(const double2* Jpart, int vctas, int nt, int Nk, doub
 // rho0(k) = U f U^+ of H(k) = sum_cells e^{-ik.R} H0 (no field), one warp per k-point.
 int launch_rho0_fp64(const SolveTables& t, double2* rho, cudaStream_t stream);
 
+// S[b] = fftshift(fft(ifftshift(gradient(J[b], h)))) for `count` signals of length n (device
+// buffers; scratch holds count*n values).  Returns the number of FFT passes, or -1.
+int spectrum_device(const double2* J, int n, int count, double h, double2* S, double2* scratch, cudaStream_t stream);
+// I[b][(h-1)/2], h = 1, 3, ..., 2 nh - 1: |S|^2 summed over the harmonic-order window (h - 1/2, h + 1/2)
+// of the order axis linspace(-n pi/tmax, n pi/tmax, n) / (2 pi 300 / lambda_nm).
+int harmonics_device(const double2* S, int n, int count, double tmax, double lambda_nm, int nh, double* I,
+                     cudaStream_t stream);
+
 // FMA-chain throughput probe (TFLOP/s) on the current device.
 int measure_fma_peaks(double* fp64_tflops, double* fp32_tflops);
 

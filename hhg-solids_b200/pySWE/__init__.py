@@ -1,2 +1,2 @@
 """ctypes API of the hhg-b200 SBE propagator, with the classes of the reference's pySWE."""
-from .pyswe import SWE, SWEBatch, SWEServer, Settings, SWEError, default_library  # noqa: F401
+from .pyswe import SWE, SWEBatch, SWEServer, Settings, SWEError, default_library, harmonic_intensities, spectrum  # noqa: F401

@@ -99,6 +99,11 @@ def _load(path: str):
         L.SWEServer_ticket_error.restype = ct.c_char_p
         L.SWEServer_stats.argtypes = [vp, ND_POINTER_1_double, ct.c_int]
         L.SWEServer_delete.argtypes = [vp]
+        L.SWESim_get_spectrum.argtypes = [vp, ct.c_double, ND_POINTER_1_complex, ND_POINTER_1_complex,
+                                           ND_POINTER_1_complex]
+        L.HHG_spectrum.argtypes = [ND_POINTER_1_complex, ct.c_int, ct.c_int, ct.c_double, ND_POINTER_1_complex]
+        L.HHG_harmonic_intensities.argtypes = [ND_POINTER_1_complex, ct.c_int, ct.c_int, ct.c_double, ct.c_double,
+                                               ct.c_int, ND_POINTER_1_double]
         L.HHG_last_error.argtypes = []
         L.HHG_last_error.restype = ct.c_char_p
         L.SWESim_get_rho_k.argtypes = [vp, ND_POINTER_1_complex]
@@ -247,6 +252,14 @@ class SWE:
         self._call("SWESim_get_rho_k", out)
         return out.reshape(nk, nw * nw)
 
+    def get_spectrum(self, spacing: float | None = None):
+        """(hhg_x, hhg_y, hhg_z) = fftshift(fft(ifftshift(gradient(J, dt)))) per axis, computed on the
+        GPU: the spectra of the reference's scripts/pol_scan.py:34-40 (dt = the settings' dt in fs)."""
+        n = self.settings.nt
+        out = [np.zeros(n, dtype=np.complex128) for _ in range(3)]
+        self._call("SWESim_get_spectrum", float(spacing or 0.0), out[0], out[1], out[2])
+        return out
+
     def get_fields(self):
         n = self.settings.nt
         t = np.zeros(n)
@@ -368,3 +381,33 @@ class SWEServer:
             self.close()
         except Exception:
             pass
+
+
+def _check(lib, rc, name):
+    if rc != 0:
+        msg = lib.HHG_last_error()
+        raise SWEError(msg.decode() if msg else f"{name} failed")
+
+
+def spectrum(J, spacing: float, path_lib: str | None = None):
+    """fftshift(fft(ifftshift(gradient(J, spacing)))) along the last axis of J, on the GPU."""
+    lib, _ = _load(path_lib or default_library())
+    J = np.ascontiguousarray(J, dtype=np.complex128)
+    shape = J.shape
+    flat = J.reshape(-1, shape[-1])
+    out = np.zeros_like(flat)
+    _check(lib, lib.HHG_spectrum(flat.reshape(-1), flat.shape[1], flat.shape[0], float(spacing), out.reshape(-1)),
+           "HHG_spectrum")
+    return out.reshape(shape)
+
+
+def harmonic_intensities(S, tmax: float, lam: float, n_harmonics: int, path_lib: str | None = None):
+    """|S|^2 summed over the odd harmonic orders 1, 3, ..., 2 n - 1 (windows of +-1/2 on pol_scan's
+    order axis), on the GPU; returns [..., n_harmonics]."""
+    lib, _ = _load(path_lib or default_library())
+    S = np.ascontiguousarray(S, dtype=np.complex128)
+    flat = S.reshape(-1, S.shape[-1])
+    out = np.zeros((flat.shape[0], int(n_harmonics)))
+    _check(lib, lib.HHG_harmonic_intensities(flat.reshape(-1), flat.shape[1], flat.shape[0], float(tmax), float(lam),
+                                             int(n_harmonics), out.reshape(-1)), "HHG_harmonic_intensities")
+    return out.reshape(S.shape[:-1] + (int(n_harmonics),))

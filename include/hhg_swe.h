@@ -182,6 +182,19 @@ int SWEServer_stats(SWEServer* srv, double* out, int n);
 /* Serves every request already submitted, then stops the scheduler and frees the server. */
 void SWEServer_delete(SWEServer* srv);
 
+/* HHG spectra on the device (the post-processing of the reference's scripts/pol_scan.py:34-40, which
+ * runs it in numpy; no C counterpart).  S = fftshift(fft(ifftshift(gradient(J, spacing)))) with
+ * numpy's conventions, from a batched mixed-radix FFT kernel (any length). */
+/* Spectra of the solve's current as SWESim_get_current returns it (x, y, z; nt values each; NULL
+ * skips an axis); spacing <= 0 takes the settings' dt in fs, as pol_scan does. */
+void SWESim_get_spectrum(SWESim* swe, double spacing, hhg_cdouble* sx, hhg_cdouble* sy, hhg_cdouble* sz);
+/* count signals of n samples each (host arrays [count][n]); returns 0 or -1 (HHG_last_error). */
+int HHG_spectrum(const hhg_cdouble* J, int n, int count, double spacing, hhg_cdouble* S);
+/* I[count][nh]: |S|^2 summed over each odd harmonic order h = 1, 3, ..., 2 nh - 1, within
+ * (h - 1/2, h + 1/2) on pol_scan's order axis linspace(-n pi/tmax, n pi/tmax, n) / (2 pi 300 / lambda_nm). */
+int HHG_harmonic_intensities(const hhg_cdouble* S, int n, int count, double tmax_fs, double lambda_nm, int nh,
+                             double* I);
+
 /* FP64 FMA / FP32 FMA chain throughput of the current device (TFLOP/s), for roofline denominators. */
 int HHG_measure_peaks(double* fp64_tflops, double* fp32_tflops);
 

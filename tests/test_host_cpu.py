@@ -165,3 +165,11 @@ def test_kspace_solver_rejects_non_square_grids():
         pyswe.SWE(pyswe.Settings(_param(nr1=8, nr2=10)), solver="kspace")
     with pytest.raises(pyswe.SWEError, match="solver must be"):
         pyswe.SWE(pyswe.Settings(_param()), solver="fft")
+
+
+@pytest.mark.skipif(gpu_available(), reason="checks the no-GPU behaviour")
+def test_spectrum_without_gpu_fails_loudly():
+    from pySWE import pyswe
+
+    with pytest.raises(pyswe.SWEError, match="no CUDA device"):
+        pyswe.spectrum(np.zeros((3, 16), dtype=complex), 0.1)
