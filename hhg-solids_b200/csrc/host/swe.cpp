@@ -114,6 +114,28 @@ void SWESim::init() {
   if (!settings) throw std::runtime_error("SWESim_init: settings not set (call SWESim_set_settings first)");
   if (path_tb.empty()) throw std::runtime_error("SWESim_init: TB path not set (call SWESim_set_path_tb first)");
   model = hhg::parse_tb(path_tb);
+  // Optional Wannier90 reading (off by default, where the model is read exactly as the reference
+  // reads it, src/wannier_tb.cpp:36-49,74,102): the file's orbital order and the degeneracy weights.
+  if (tb_flags & 2)
+    for (int st = 0; st < model.nsites; ++st) {
+      auto transpose = [&](std::vector<cd>& v) {
+        for (int i = 0; i < model.nw; ++i)
+          for (int j = i + 1; j < model.nw; ++j)
+            std::swap(v[((size_t)st * model.nw + i) * model.nw + j], v[((size_t)st * model.nw + j) * model.nw + i]);
+      };
+      transpose(model.hop);
+      for (auto& b : model.bc) transpose(b);
+    }
+  if (tb_flags & 1)
+    for (int st = 0; st < model.nsites; ++st) {
+      const int dg = model.degeneracy[st];
+      if (dg <= 0) throw std::runtime_error("SWESim_init: degeneracy " + std::to_string(dg) + " in the TB file");
+      const size_t nwsq = (size_t)model.nw * model.nw;
+      for (size_t o = 0; o < nwsq; ++o) {
+        model.hop[st * nwsq + o] /= (double)dg;
+        for (auto& b : model.bc) b[st * nwsq + o] /= (double)dg;
+      }
+    }
   trace.mark("parse");
   Settings& s = *settings;
   nt = (int)(s.tmax / s.dt);
@@ -839,6 +861,13 @@ void SWESim_set_precision(SWESim* swe, int mode) {
   guarded(swe, "SWESim_set_precision", [&] {
     if (mode != 0 && mode != 1) throw std::runtime_error("SWESim_set_precision: mode must be 0 (plain FP64) or 1 (mixed)");
     swe->precision = mode;
+  });
+}
+
+void SWESim_set_tb_convention(SWESim* swe, int flags) {
+  guarded(swe, "SWESim_set_tb_convention", [&] {
+    if (flags < 0 || flags > 3) throw std::runtime_error("SWESim_set_tb_convention: flags must be in 0..3");
+    swe->tb_flags = flags;
   });
 }
 

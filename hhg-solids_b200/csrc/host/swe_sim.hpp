@@ -85,6 +85,8 @@ struct SWESim {
   std::vector<double2> H0, Rtab, V, Q, Xbox, Vd, P, T1, T2;
   int precision = 0;  // 0 plain FP64, 1 mixed
   int solver = 0;     // 0 the real-space solver (src/solver.cpp), 1 the k-space solver (src/solver_kspace.cpp)
+  int tb_flags = 0;   // TB reading: 0 as the reference; bit 0 divide by the degeneracies, bit 1 keep the file's
+                      // orbital order (line "m n" at [m-1][n-1])
   std::vector<int2> cellp;  // cell coordinates the propagation sums over (transposed for the k-space solver)
   unsigned generation = 0;  // bumped by every successful SWESim_init (batches re-capture on change)
   int nax = 0, ax_id[3] = {0, 0, 0}, nj = 0, j_id[3] = {0, 0, 0};

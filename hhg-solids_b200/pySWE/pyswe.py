@@ -80,6 +80,7 @@ def _load(path: str):
         L.SWESim_set_k_rows.argtypes = [vp, ct.c_int, ct.c_int]
         L.SWESim_set_precision.argtypes = [vp, ct.c_int]
         L.SWESim_set_solver.argtypes = [vp, ct.c_int]
+        L.SWESim_set_tb_convention.argtypes = [vp, ct.c_int]
         L.SWEBatch_new.restype = vp
         L.SWEBatch_add.argtypes = [vp, vp]
         L.SWEBatch_run.argtypes = [vp]
@@ -147,10 +148,14 @@ class SWE:
     """One propagation: setup on construction (SWESim_init), then run_simulation / get_current.
     ``defer_init=True`` skips the setup (for a request handed to :class:`SWEServer`).
     ``solver="kspace"`` selects the reference's k-space solver (src/solver_kspace.cpp) instead of
-    its real-space one."""
+    its real-space one.  ``tb_convention="faithful"`` reads the TB file as Wannier90 defines it
+    (degeneracy weights applied, orbital order kept) instead of as the reference does."""
+
+    _TB = {"reference": 0, "faithful": 3, "degeneracy": 1, "untransposed": 2}
 
     def __init__(self, settings: Settings, device: int | None = None, k_rows: tuple | None = None,
-                 precision: str = "fp64", defer_init: bool = False, solver: str = "rspace"):
+                 precision: str = "fp64", defer_init: bool = False, solver: str = "rspace",
+                 tb_convention: str = "reference"):
         self.settings = settings
         self.swe_cpp, self._ext = _load(settings.path_lib)
         self.ptr = self.swe_cpp.SWESim_new()
@@ -168,6 +173,10 @@ class SWE:
             raise SWEError(f"solver must be 'rspace' or 'kspace', not {solver!r}")
         if solver == "kspace":
             self._call("SWESim_set_solver", 1)
+        if tb_convention not in self._TB:
+            raise SWEError(f"tb_convention must be one of {sorted(self._TB)}, not {tb_convention!r}")
+        if self._TB[tb_convention]:
+            self._call("SWESim_set_tb_convention", self._TB[tb_convention])
         self.set_path_tb(settings.path_tb.encode("UTF-8"))
         self.set_settings(settings.ptr)
         if not defer_init:

@@ -37,8 +37,9 @@ def _cells(half: int):
     return [(n1, n2) for n1 in range(-half, half + 1) for n2 in range(-half, half + 1)]
 
 
-def write_tb(path: str, comment: str, lattice: np.ndarray, cells, H: dict, X: dict) -> str:
-    """Write a model; ``H[cell]`` is the stored nw x nw complex matrix, ``X[cell]`` is (3, nw, nw).
+def write_tb(path: str, comment: str, lattice: np.ndarray, cells, H: dict, X: dict, degeneracy: dict | None = None) -> str:
+    """Write a model; ``H[cell]`` is the stored nw x nw complex matrix, ``X[cell]`` is (3, nw, nw),
+    ``degeneracy[cell]`` the Wigner-Seitz weight written in the header (1 when omitted).
 
     Returns the sha256 of the file."""
     nw = next(iter(H.values())).shape[0]
@@ -47,7 +48,7 @@ def write_tb(path: str, comment: str, lattice: np.ndarray, cells, H: dict, X: di
         lines.append(" ".join(f"{v:.18e}" for v in row))
     lines.append(str(nw))
     lines.append(str(len(cells)))
-    deg = ["1"] * len(cells)
+    deg = [str(int((degeneracy or {}).get(c, 1))) for c in cells]
     for i in range(0, len(deg), 15):
         lines.append(" ".join(deg[i : i + 15]))
     lines.append("")
@@ -130,6 +131,55 @@ def random_tmd(path: str, nw: int = 11, seed: int = 7, window: int = 7, a: float
                     cells, H, X)
 
 
+def _deg_model(nw: int, seed: int, window: int, a: float):
+    """A random model with Wannier90-style degeneracies (2 on the edge of the cell window, 4 at its
+    corners), as (cells, stored H, stored X, degeneracy)."""
+    rng = np.random.default_rng(seed)
+    half = window // 2
+    cells = _cells(half)
+    H, X, deg = {}, {}, {}
+    for c in cells:
+        mc = (-c[0], -c[1])
+        deg[c] = (2 if abs(c[0]) == half else 1) * (2 if abs(c[1]) == half else 1)
+        if c in H:
+            continue
+        if c == (0, 0):
+            G = (rng.standard_normal((nw, nw)) + 1j * rng.standard_normal((nw, nw))) * 0.4
+            H[c] = (G + G.conj().T) / 2 + np.diag(rng.uniform(-3.0, 3.0, nw))
+            X[c] = np.zeros((3, nw, nw), dtype=np.complex128)
+            for ax in range(2):
+                P = (rng.standard_normal((nw, nw)) + 1j * rng.standard_normal((nw, nw))) * 0.2
+                X[c][ax] = (P + P.conj().T) / 2
+        else:
+            s = 0.4 * math.exp(-math.hypot(c[0], c[1]) / 1.2)
+            H[c] = (rng.standard_normal((nw, nw)) + 1j * rng.standard_normal((nw, nw))) * s
+            H[mc] = H[c].conj().T
+            X[c] = np.zeros((3, nw, nw), dtype=np.complex128)
+            X[mc] = np.zeros((3, nw, nw), dtype=np.complex128)
+            for ax in range(2):
+                X[c][ax] = (rng.standard_normal((nw, nw)) + 1j * rng.standard_normal((nw, nw))) * 0.5 * s
+                X[mc][ax] = X[c][ax].conj().T
+    return cells, H, X, deg
+
+
+def tmd_deg(path: str, nw: int = 6, seed: int = 5, window: int = 5, a: float = 2.5) -> str:
+    """A model file with non-unit degeneracies, read as Wannier90 defines them with
+    SWE(..., tb_convention="faithful")."""
+    cells, H, X, deg = _deg_model(nw, seed, window, a)
+    return write_tb(path, f"synthetic {nw}-orbital model with degeneracies, seed {seed} (hhg-b200 tbgen)",
+                    _lattice(a), cells, H, X, deg)
+
+
+def tmd_deg_equiv(path: str, nw: int = 6, seed: int = 5, window: int = 5, a: float = 2.5) -> str:
+    """The same model rewritten so that the reference's own reading (transposed blocks, degeneracies
+    ignored) gives the faithful reading of tmd_deg: stored blocks M^T / degeneracy, unit degeneracies."""
+    cells, H, X, deg = _deg_model(nw, seed, window, a)
+    H2 = {c: H[c].T / deg[c] for c in cells}
+    X2 = {c: np.stack([X[c][ax].T for ax in range(3)]) / deg[c] for c in cells}
+    return write_tb(path, f"synthetic {nw}-orbital model, degeneracies applied, seed {seed} (hhg-b200 tbgen)",
+                    _lattice(a), cells, H2, X2)
+
+
 # name -> (generator, kwargs)
 MODELS = {
     "haldane": (haldane, {}),
@@ -144,6 +194,8 @@ MODELS = {
     "tmd12_s2": (random_tmd, {"nw": 12, "seed": 2}),
     "tmd12_s3": (random_tmd, {"nw": 12, "seed": 3}),
     "tmd5_s4": (random_tmd, {"nw": 5, "seed": 4, "window": 5}),
+    "tmd6_deg": (tmd_deg, {}),
+    "tmd6_deg_equiv": (tmd_deg_equiv, {}),
 }
 
 

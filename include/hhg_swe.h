@@ -98,6 +98,11 @@ int SWESim_last_launches(SWESim* swe);
  * the RK4 accumulation and the current's k-sum in FP64 (error against plain FP64 reported by the
  * tests and bench). */
 void SWESim_set_precision(SWESim* swe, int mode);
+/* TB-file reading (no counterpart in the reference, which always transposes each block and ignores
+ * the degeneracy line, src/wannier_tb.cpp:36-49,74,102): flags 0 (default) read as the reference
+ * does; bit 0 divides each R block (H and positions) by its degeneracy, as Wannier90 defines the
+ * file; bit 1 stores line "m n" at [m-1][n-1].  Takes effect at the next SWESim_init. */
+void SWESim_set_tb_convention(SWESim* swe, int flags);
 /* Solver (no counterpart in the reference's C ABI, which always drives the real-space solver):
  * 0 (default) the real-space solver of src/solver.cpp as SWESim::run_simulation drives it;
  * 1 the k-space solver of src/solver_kspace.cpp (compiled in the reference but reached by none of

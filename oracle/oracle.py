@@ -23,6 +23,7 @@ class OracleSettings(ct.Structure):
         ("tmax", ct.c_double), ("dt", ct.c_double), ("intensity", ct.c_double),
         ("lambda_nm", ct.c_double), ("tmax_field", ct.c_double),
         ("pol", ct.c_double * 3), ("phi", ct.c_double * 3),
+        ("tb_flags", ct.c_int),
     ]
 
 
@@ -36,6 +37,7 @@ def settings(param: dict) -> OracleSettings:
     for i in range(3):
         s.pol[i] = float(param["pol_vec"][i])
         s.phi[i] = float(param["phi_vec"][i])
+    s.tb_flags = {"reference": 0, "faithful": 3}[param.get("tb_convention", "reference")]
     return s
 
 

@@ -25,12 +25,35 @@ typedef struct {
   int (*R)[3];
   cplx* hop; /* [site][n][m] = H_mn (transposed as in src/wannier_tb.cpp:74) */
   cplx* bc[3];
+  int* deg;
 } tb_model;
+
+/* The optional Wannier90 reading (not the reference's): bit 1 undoes the transpose, bit 0 divides
+ * each R block by its degeneracy. */
+static void tb_apply_flags(tb_model* m, int flags) {
+  const int nw = m->nw, nw2 = nw * nw;
+  for (int s = 0; s < m->nsites; ++s) {
+    cplx* blocks[4] = {m->hop + (size_t)s * nw2, m->bc[0] + (size_t)s * nw2, m->bc[1] + (size_t)s * nw2,
+                       m->bc[2] + (size_t)s * nw2};
+    for (int b = 0; b < 4; ++b) {
+      if (flags & 2)
+        for (int i = 0; i < nw; ++i)
+          for (int j = i + 1; j < nw; ++j) {
+            cplx t = blocks[b][i * nw + j];
+            blocks[b][i * nw + j] = blocks[b][j * nw + i];
+            blocks[b][j * nw + i] = t;
+          }
+      if ((flags & 1) && m->deg[s] > 0)
+        for (int o = 0; o < nw2; ++o) blocks[b][o] /= (double)m->deg[s];
+    }
+  }
+}
 
 static void tb_free(tb_model* m) {
   free(m->R);
   free(m->hop);
   for (int a = 0; a < 3; ++a) free(m->bc[a]);
+  free(m->deg);
   memset(m, 0, sizeof(*m));
 }
 
@@ -62,7 +85,17 @@ static int tb_parse(const char* path, tb_model* m) {
     return -2;
   }
   int ndeg = (m->nsites - 1) / 15 + 1;
-  for (int i = 0; i < ndeg; ++i) read_line(f, line, sizeof line); /* degeneracies: parsed, never applied */
+  m->deg = calloc((size_t)m->nsites, sizeof(int));
+  int nd = 0;
+  for (int i = 0; i < ndeg; ++i) { /* degeneracies: the reference parses and never applies them */
+    read_line(f, line, sizeof line);
+    char* p = line;
+    int used = 0, v = 0;
+    while (nd < m->nsites && sscanf(p, "%d%n", &v, &used) == 1) {
+      m->deg[nd++] = v;
+      p += used;
+    }
+  }
   read_line(f, line, sizeof line);
   const int nw = m->nw, nw2 = nw * nw;
   m->R = calloc((size_t)m->nsites, sizeof(*m->R));
@@ -172,6 +205,7 @@ int oracle_fields(const char* tb, const oracle_settings* s, double* t, double* E
 int oracle_place(const char* tb, const oracle_settings* s, double* Hout, double* r3out) {
   tb_model m;
   if (tb_parse(tb, &m)) return -1;
+  tb_apply_flags(&m, s->tb_flags);
   placed_grid g;
   if (grid_place(&m, s, &g)) {
     tb_free(&m);
@@ -265,6 +299,7 @@ static void velocity_window(const tb_model* m, const placed_grid* g, cplx* v3w) 
 int oracle_velocity_window(const char* tb, const oracle_settings* s, double* v3w) {
   tb_model m;
   if (tb_parse(tb, &m)) return -1;
+  tb_apply_flags(&m, s->tb_flags);
   placed_grid g;
   if (grid_place(&m, s, &g)) {
     tb_free(&m);
@@ -373,6 +408,7 @@ static void rho0_at(const tb_model* m, const cell_ref* sup, int ns, const cplx* 
 int oracle_rho0(const char* tb, const oracle_settings* s, double* rho_out) {
   tb_model m;
   if (tb_parse(tb, &m)) return -1;
+  tb_apply_flags(&m, s->tb_flags);
   placed_grid g;
   if (grid_place(&m, s, &g)) {
     tb_free(&m);
@@ -417,6 +453,7 @@ int oracle_run_steps(const char* tb, const oracle_settings* s, int k_begin, int 
                      double* Jout) {
   tb_model m;
   if (tb_parse(tb, &m)) return -1;
+  tb_apply_flags(&m, s->tb_flags);
   placed_grid g;
   if (grid_place(&m, s, &g)) {
     tb_free(&m);
@@ -611,6 +648,7 @@ static cplx bicubic_at(const cplx* grid, int nw2, int Nx, int Ny, double u, doub
 int oracle_run_kspace_steps(const char* tb, const oracle_settings* s, int nsteps, double* t, double* Jout) {
   tb_model m;
   if (tb_parse(tb, &m)) return -1;
+  tb_apply_flags(&m, s->tb_flags);
   placed_grid g;
   if (grid_place(&m, s, &g)) {
     tb_free(&m);

@@ -28,6 +28,8 @@ typedef struct {
   int nr1, nr2, nr3;
   double tmax, dt, intensity, lambda_nm, tmax_field;
   double pol[3], phi[3];
+  int tb_flags; /* 0: read the TB file as the reference does; bit 0: divide by the degeneracies;
+                   bit 1: keep the file's orbital order (an option the reference does not have) */
 } oracle_settings;
 
 /* nt = (int)(tmax / dt)  (src/swe.cpp:52). */

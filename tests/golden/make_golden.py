@@ -50,6 +50,7 @@ CASES = {
     "c0": case("haldane", 60),
     "c2_prefix": case("tmd11_s7", 150, tmax=2.2),
     "c1": case("haldane", 200),
+    "w90_tmd6_deg_8": case("tmd6_deg_equiv", 8, tmax=1.0, pol_vec=[0.6, 0.8, 0.0], intensity=2e12),
     "ks_haldane_12_pol": case("haldane", 12, tmax=4.0, pol_vec=[0.6, 0.8, 0.0], phi_vec=[0.3, 0.0, 0.0],
                               solver="kspace"),
     "ks_tmd6_8": case("tmd6_s1", 8, tmax=1.0, pol_vec=[0.3, 1.0, 0.0], solver="kspace"),

@@ -261,3 +261,18 @@ def test_runtime_shaped_kernel_instance(pyswe, oracle_mod, precision, tol):
     s.delete()
     _, Jo = oracle_mod.run(tb, param)
     assert rel_l2(J, Jo) < tol
+
+
+
+def test_faithful_tb_reading_on_gpu(pyswe):
+    import tbgen
+
+    _, param, _, J_ref = load_golden("w90_tmd6_deg_8")
+    p = dict(param, path_tb=tbgen.model_path("tmd6_deg"))
+    for precision in ("fp64", "mixed"):
+        s = pyswe.SWE(pyswe.Settings(p), tb_convention="faithful", precision=precision)
+        s.run_simulation()
+        J = s.get_current()[1:]
+        s.delete()
+        for a in range(2):
+            assert rel_l2(J[a], J_ref[a]) < (1e-10 if precision == "fp64" else 1e-5)

@@ -215,3 +215,20 @@ def test_kspace_solver_is_not_the_real_space_one(oracle_mod):
     _, param, _, J_ks = load_golden("ks_haldane_12_pol")
     _, _, _, J_rs = load_golden("haldane_12_pol")
     assert rel_l2(J_ks[1], J_rs[1]) > 1e-2
+
+
+
+# ------------------------------------------------ faithful Wannier90 reading (an option, not the reference's)
+
+
+def test_faithful_tb_reading_equals_the_reference_on_the_equivalent_file(oracle_mod):
+    """tmd6_deg read with degeneracy weights and the file's orbital order equals what the reference
+    computes from tmd6_deg_equiv (the same model rewritten for the reference's reading)."""
+    import tbgen
+
+    _, param, t_ref, J_ref = load_golden("w90_tmd6_deg_8")
+    _, J = oracle_mod.run(tbgen.model_path("tmd6_deg"), dict(param, tb_convention="faithful"))
+    for a in range(2):
+        assert rel_l2(J[a], J_ref[a]) < 1e-10
+    _, J0 = oracle_mod.run(tbgen.model_path("tmd6_deg"), param)  # the reference's own reading differs
+    assert rel_l2(J0[1], J_ref[1]) > 1e-3
