@@ -131,7 +131,7 @@ def run_serve(args, local: int):
         delay = t0 + t_arr - time.perf_counter()
         if delay > 0:
             time.sleep(delay)
-        solves[i] = pyswe.SWE(pyswe.Settings(p), precision="mixed", defer_init=True)
+        solves[i] = pyswe.SWE(pyswe.Settings(p), precision="mixed", defer_init=True, autotune=args.autotune)
         tickets[i] = srv.submit(solves[i])
     for tk in tickets:
         srv.wait(tk)
@@ -153,7 +153,7 @@ def run_serve(args, local: int):
     seq_s, seq_k, errs = 0.0, 0, []
     for (t_arr, model, nw, p), Jm in zip(reqs[: args.baseline_sample], J_mixed):
         a = time.perf_counter()
-        s = pyswe.SWE(pyswe.Settings(dict(p)), device=local)
+        s = pyswe.SWE(pyswe.Settings(dict(p)), device=local, autotune=args.autotune)
         s.run_simulation()
         J = s.get_current()[1:]
         seq_s += time.perf_counter() - a
@@ -195,7 +195,8 @@ def run_scan(args, local: int):
     draws = scan_params()
     kpts = sum(p["nr1"] * p["nr2"] for _, _, p in draws)
     t0 = time.perf_counter()
-    mixed = [pyswe.SWE(pyswe.Settings(dict(p)), device=local, precision="mixed") for _, _, p in draws]
+    mixed = [pyswe.SWE(pyswe.Settings(dict(p)), device=local, precision="mixed", autotune=args.autotune)
+             for _, _, p in draws]
     setup_s = time.perf_counter() - t0
     nt = mixed[0].settings.nt
     batch = pyswe.SWEBatch(mixed)
@@ -215,7 +216,7 @@ def run_scan(args, local: int):
     # Plain FP64, 64 sequential solves.
     seq_ms, errs = 0.0, []
     for (model, nw, p), Jm in zip(draws, J_mixed):
-        s = pyswe.SWE(pyswe.Settings(dict(p)), device=local)
+        s = pyswe.SWE(pyswe.Settings(dict(p)), device=local, autotune=args.autotune)
         s.run_simulation()
         seq_ms += s.last_kernel_ms()
         J = s.get_current()[1:]
@@ -585,6 +586,7 @@ def main():
                     help="mixed: FP32 Wannier sums and commutators, FP64 state / RK accumulation / k-sum")
     ap.add_argument("--solver", default="rspace", choices=["rspace", "kspace"],
                     help="kspace: the reference's k-space solver (src/solver_kspace.cpp) instead of its real-space one")
+    ap.add_argument("--autotune", action="store_true", help="time candidate tile shapes at setup (SWESim_set_autotune)")
     ap.add_argument("--requests", type=int, default=200, help="c4: requests in the arrival stream")
     ap.add_argument("--max-active", type=int, default=32, help="c4: most solves running at once")
     ap.add_argument("--chunk", type=int, default=256, help="c4: RK4 steps per scheduling chunk")
@@ -643,7 +645,7 @@ def main():
     param = workload_param(args.workload, rank, world, args.grid)
     w = WORKLOADS[args.workload]
     settings = pyswe.Settings(dict(param))
-    swe = pyswe.SWE(settings, device=local, precision=args.precision, solver=args.solver)
+    swe = pyswe.SWE(settings, device=local, precision=args.precision, solver=args.solver, autotune=args.autotune)
     nk = param["nr1"] * param["nr2"]
     nt = settings.nt
     nw = swe.num_orb()
@@ -699,7 +701,7 @@ def main():
         swe.reset()
         swe.run_simulation()
         J_mixed = swe.get_current()[1:]
-        ref = pyswe.SWE(pyswe.Settings(dict(param)), device=local, solver=args.solver)
+        ref = pyswe.SWE(pyswe.Settings(dict(param)), device=local, solver=args.solver, autotune=args.autotune)
         ref.run_simulation()
         J_fp64 = ref.get_current()[1:]
         fp64_ms = ref.last_kernel_ms()
@@ -733,7 +735,8 @@ def main():
         "config": {"workload": f"{args.workload}: {WORKLOADS[args.workload]['desc']}"
                    + (f" (grid overridden to {args.grid}x{args.grid})" if args.grid else ""),
                    "k_grid": [param["nr1"], param["nr2"]],
-                   "nt": nt, "num_orb": nw, "precision": args.precision, "solver": args.solver, "parallelism": f"replicas x{world}" if world > 1 else "single",
+                   "nt": nt, "num_orb": nw, "precision": args.precision, "solver": args.solver,
+                   "autotune": args.autotune, "parallelism": f"replicas x{world}" if world > 1 else "single",
                    "l2": "flushed between timed solves (256 MiB write)", "launch": shape},
         "solves_per_hour": 3600.0 * world * args.steps / (total_ms * 1e-3),
         "roofline": {"bound": "fp64", "achieved": achieved, "peak": fp64_peak.value, "unit": "TFLOP/s",

@@ -19,6 +19,7 @@
 #include <fstream>
 #include <functional>
 #include <map>
+#include <mutex>
 #include <memory>
 #include <sstream>
 #include <stdexcept>
@@ -106,6 +107,93 @@ inline int wrapi(long x, int n) {
 }
 
 }  // namespace
+
+namespace {
+
+bool autotune_env() {
+  const char* e = std::getenv("HHG_AUTOTUNE");
+  return e && e[0] == '1';
+}
+
+// Tile hints measured by tune_tiles, per device and solve shape: every solve of the same shape in
+// this process uses the same tiles (so batches and servers stay bit-identical to solo runs).
+std::mutex g_tune_mutex;
+std::map<std::vector<int>, int> g_tune_cache;
+
+}  // namespace
+
+// Autotuner: times the propagation of the first steps under each candidate tile shape and keeps
+// the fastest (element-group kernels: k-points per CTA from the largest that fits down to half of
+// it; column tiles: 1 to 3 parts per column).  The state is reset to rho0 afterwards.
+void SWESim::tune_tiles(int sms) {
+  const std::vector<int> key = {device, shape.kernel, shape.variant, precision, nw, tab.nax, tab.nj, N1, N2,
+                                tab.row1 - tab.row0, tab.kmode, tab.hermitian, tab.b1n, tab.b2n};
+  int hint = -1;
+  {
+    std::lock_guard<std::mutex> lk(g_tune_mutex);
+    auto it = g_tune_cache.find(key);
+    if (it != g_tune_cache.end()) hint = it->second;
+  }
+  char why[256] = {0};
+  if (hint < 0) {
+    std::vector<int> hints;
+    if (shape.kernel == 3) {
+      hints = {1, 2, 3};
+    } else if (shape.kernel == 1 || shape.kernel == 2) {
+      const int B = shape.k_per_cta;
+      for (int b : {B, (3 * B + 3) / 4, (2 * B + 2) / 3, (B + 1) / 2}) hints.push_back(b);
+    }
+    const int steps = std::min(nt, 128);
+    DevBuf<double2> scratch;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    check_cuda(cudaEventCreate(&e0), "cudaEventCreate");
+    check_cuda(cudaEventCreate(&e1), "cudaEventCreate");
+    float best_ms = 0.f;
+    std::vector<std::pair<int, int>> seen;  // (k_per_cta, threads) already timed
+    for (int h : hints) {
+      hhg::LaunchShape cand{};
+      if (!hhg::plan_propagate(tab, precision, sms, &cand, why, sizeof why, h)) continue;
+      bool dup = false;
+      for (auto& p : seen) dup = dup || (p.first == cand.k_per_cta && p.second == cand.threads);
+      if (dup) continue;
+      seen.emplace_back(cand.k_per_cta, cand.threads);
+      scratch.alloc((size_t)cand.vctas * nt * 3);
+      hhg::SolveTables tt = tab;
+      tt.step1 = steps;
+      float ms = 0.f;
+      for (int rep = 0; rep < 3; ++rep) {
+        check_cuda(cudaMemcpyAsync(d_rho.p, d_rho0.p, sizeof(double2) * (size_t)Nk * nw2, cudaMemcpyDeviceToDevice,
+                                   stream), "D2D");
+        check_cuda(cudaEventRecord(e0, stream), "event");
+        hhg::launch_propagate_steps(tt, gtab, cand, d_rho.p, scratch.p, stream);
+        check_cuda(cudaEventRecord(e1, stream), "event");
+        check_cuda(cudaEventSynchronize(e1), "autotune");
+        float m = 0.f;
+        check_cuda(cudaEventElapsedTime(&m, e0, e1), "event time");
+        if (rep > 0) ms = rep == 1 ? m : std::min(ms, m);  // first run warms up
+      }
+      check_cuda(cudaGetLastError(), "autotune launch");
+      if (hint < 0 || ms < best_ms) {
+        best_ms = ms;
+        hint = h;
+      }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (hint < 0) hint = 0;
+    std::lock_guard<std::mutex> lk(g_tune_mutex);
+    g_tune_cache.emplace(key, hint);  // the first measurement of a shape wins
+    hint = g_tune_cache[key];
+  }
+  if (hint > 0) {
+    hhg::LaunchShape tuned{};
+    if (hhg::plan_propagate(tab, precision, sms, &tuned, why, sizeof why, hint)) shape = tuned;
+  }
+  d_Jpart.alloc((size_t)shape.vctas * nt * 3);
+  check_cuda(cudaMemcpyAsync(d_rho.p, d_rho0.p, sizeof(double2) * (size_t)Nk * nw2, cudaMemcpyDeviceToDevice, stream),
+             "D2D");
+  check_cuda(cudaStreamSynchronize(stream), "autotune");
+}
 
 void SWESim::init() {
   PhaseTrace trace;
@@ -557,6 +645,10 @@ void SWESim::init() {
              "D2D");
   check_cuda(cudaStreamSynchronize(stream), "init");
   trace.mark("rho0");
+  if (autotune || autotune_env()) {
+    tune_tiles(sms);
+    trace.mark("autotune");
+  }
   ready = true;
   ++generation;
 }
@@ -862,6 +954,10 @@ void SWESim_set_precision(SWESim* swe, int mode) {
     if (mode != 0 && mode != 1) throw std::runtime_error("SWESim_set_precision: mode must be 0 (plain FP64) or 1 (mixed)");
     swe->precision = mode;
   });
+}
+
+void SWESim_set_autotune(SWESim* swe, int on) {
+  guarded(swe, "SWESim_set_autotune", [&] { swe->autotune = on != 0; });
 }
 
 void SWESim_set_tb_convention(SWESim* swe, int flags) {

@@ -85,6 +85,7 @@ struct SWESim {
   std::vector<double2> H0, Rtab, V, Q, Xbox, Vd, P, T1, T2;
   int precision = 0;  // 0 plain FP64, 1 mixed
   int solver = 0;     // 0 the real-space solver (src/solver.cpp), 1 the k-space solver (src/solver_kspace.cpp)
+  bool autotune = false;  // time candidate tile shapes at SWESim_init (also HHG_AUTOTUNE=1)
   int tb_flags = 0;   // TB reading: 0 as the reference; bit 0 divide by the degeneracies, bit 1 keep the file's
                       // orbital order (line "m n" at [m-1][n-1])
   std::vector<int2> cellp;  // cell coordinates the propagation sums over (transposed for the k-space solver)
@@ -147,6 +148,7 @@ struct SWESim {
   // Keeps J[3][nt] as the current record (as run() does) and returns every device buffer.
   void finish_served(const double2* J);
 
+  void tune_tiles(int sms);
   void init();
   void run();
   void reset_state();

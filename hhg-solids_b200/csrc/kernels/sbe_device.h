@@ -82,12 +82,17 @@ struct BatchDesc {
 // Picks kernel and launch shape for a solve on the current device; false (with a reason) if it
 // cannot run it.  precision 0: plain FP64; 1: mixed (FP32 commutators and Wannier sums, FP64 state,
 // RK accumulation and current sum).
-bool plan_propagate(const SolveTables& t, int precision, int sm_count, LaunchShape* out, char* why, int why_len);
-bool plan_group(const SolveTables& t, int precision, int sm_count, LaunchShape* out, char* why, int why_len);
+// tile_hint > 0 asks for smaller tiles than the default (element groups: k-points per CTA; column
+// tiles: parts per column); the autotuner of swe.cpp passes the measured best.  Result bits depend
+// on the tile shape only through the order of the final k-sum.
+bool plan_propagate(const SolveTables& t, int precision, int sm_count, LaunchShape* out, char* why, int why_len,
+                    int tile_hint = 0);
+bool plan_group(const SolveTables& t, int precision, int sm_count, LaunchShape* out, char* why, int why_len,
+                int tile_hint = 0);
 void launch_group(const SolveTables& t, const GroupTables& gt, const LaunchShape& s, double2* rho, double2* Jpart,
                   cudaStream_t stream);
 // Column-tile kernel (nw <= 2, Hermitian, FP64): false if the solve does not suit it.
-bool plan_kcol(const SolveTables& t, int sm_count, LaunchShape* out, size_t smem_max);
+bool plan_kcol(const SolveTables& t, int sm_count, LaunchShape* out, size_t smem_max, int parts_hint = 0);
 void launch_kcol(const SolveTables& t, const GroupTables& gt, const LaunchShape& s, double2* rho, double2* Jpart,
                  cudaStream_t stream);
 // Persistent work-stealing launch over (solve, virtual CTA) items of solves sharing the kernel shape of

@@ -488,7 +488,8 @@ bool plan_kpt(const SolveTables& t, int sm_count, LaunchShape* out, size_t smem_
 
 }  // namespace
 
-bool plan_propagate(const SolveTables& t, int precision, int sm_count, LaunchShape* out, char* why, int why_len) {
+bool plan_propagate(const SolveTables& t, int precision, int sm_count, LaunchShape* out, char* why, int why_len,
+                    int tile_hint) {
   const size_t kSmemMax = 220 * 1024;
   if (t.nw < 1 || t.nw > kMaxOrb) {
     snprintf(why, why_len, "num_orb=%d outside the supported range 1..%d", t.nw, kMaxOrb);
@@ -500,17 +501,19 @@ bool plan_propagate(const SolveTables& t, int precision, int sm_count, LaunchSha
   const bool force_group = force && std::strcmp(force, "group") == 0;
   const bool force_kpt = force && std::strcmp(force, "kpt") == 0;
   const bool force_kcol = force && std::strcmp(force, "kcol") == 0;
-  if (!force_group && precision == 0 && t.hermitian && t.nw <= 2) {
+  // nw <= 2 runs the FP64 thread-per-k-point kernels in both precisions: with 2x2 matrices the FP32
+  // element-group kernel is several times slower, so the mixed form gains nothing there.
+  if (!force_group && t.hermitian && t.nw <= 2) {
     // Column tiles when there are enough columns to fill the GPU, else one k-point per thread in
     // consecutive-k tiles.
     LaunchShape kc{};
-    if (!force_kpt && plan_kcol(t, sm_count, &kc, kSmemMax) && (force_kcol || kc.ntiles >= sm_count)) {
+    if (!force_kpt && plan_kcol(t, sm_count, &kc, kSmemMax, tile_hint) && (force_kcol || kc.ntiles >= sm_count)) {
       *out = kc;
       return true;
     }
     if (plan_kpt(t, sm_count, out, kSmemMax)) return true;
   }
-  return plan_group(t, precision, sm_count, out, why, why_len);
+  return plan_group(t, precision, sm_count, out, why, why_len, tile_hint);
 }
 
 void launch_propagate_steps(const SolveTables& t, const GroupTables& gt, const LaunchShape& s, double2* rho,

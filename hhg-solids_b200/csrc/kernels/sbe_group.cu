@@ -641,7 +641,7 @@ __global__ void __launch_bounds__(group_threads<EPT>(), 1)
 constexpr size_t kSmemMax = 220 * 1024;
 
 template <typename Real, int EPT, int NWc, int NAXc, int NJc, bool KM = false>
-bool plan_group_t(const SolveTables& t, int sm_count, LaunchShape* out, char* why, int why_len) {
+bool plan_group_t(const SolveTables& t, int sm_count, LaunchShape* out, char* why, int why_len, int tile_hint) {
   const GroupGeom gg = group_geom(t);
   const int per = (t.nw2 + EPT - 1) / EPT;  // threads needed per k-point
   int G;
@@ -669,20 +669,20 @@ bool plan_group_t(const SolveTables& t, int sm_count, LaunchShape* out, char* wh
     snprintf(why, why_len, "model (%d orbitals, %dx%d cell box) does not fit in shared memory", t.nw, t.b1n, t.b2n);
     return false;
   }
-  if (bytes(Bmax, true, true) > kSmemMax) win_sm = 0;
-  if (bytes(Bmax, true, win_sm) > kSmemMax) box_sm = 0;
-  if (!box_sm && bytes(Bmax, false, true) <= kSmemMax) win_sm = 1;
+  // B = the largest count that fits, unless a tile hint (the autotuner's choice) asks for fewer: the
+  // tile shape is a property of the kernel shape, the model and the hint, the same alone and in a batch.
+  const int best = tile_hint > 0 ? std::max(step, std::min(Bmax, tile_hint / step * step)) : Bmax;
+  if (bytes(best, true, true) > kSmemMax) win_sm = 0;
+  if (bytes(best, true, win_sm) > kSmemMax) box_sm = 0;
+  if (!box_sm && bytes(best, false, true) <= kSmemMax) win_sm = 1;
   auto kern = propagate_group_kernel<Real, EPT, NWc, NAXc, NJc, KM>;
-  const size_t smem_max = bytes(Bmax, box_sm, win_sm);
+  const size_t smem_max = bytes(best, box_sm, win_sm);
   cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_max);
   int occ = 0;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, Bmax * G, smem_max);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, best * G, smem_max);
   if (occ < 1) occ = 1;
   const long slots = (long)occ * sm_count;
-  // B = the largest count that fits: the tile shape is then a property of the kernel shape and the
-  // model, the same alone and in a batch.
   const int rows = t.row1 - t.row0;
-  const int best = Bmax;
   const long ntiles = (long)t.N2 * ((rows + best - 1) / best);
   out->kernel = sizeof(Real) == 8 ? 1 : 2;
   out->kmode = KM ? 1 : 0;
@@ -729,7 +729,7 @@ int launch_group_batch_t(const BatchDesc* descs, const int2* items, int nitems, 
 // Compiled shapes: (orbitals, field axes, current axes) of the configurations this library is built
 // for, each in plain FP64 (one element per thread) and mixed precision (two elements per thread);
 // any other shape runs the runtime-shaped instance.
-using PlanFn = bool (*)(const SolveTables&, int, LaunchShape*, char*, int);
+using PlanFn = bool (*)(const SolveTables&, int, LaunchShape*, char*, int, int);
 using LaunchFn = void (*)(const SolveTables&, const GroupTables&, const LaunchShape&, double2*, double2*, cudaStream_t);
 using BatchFn = int (*)(const BatchDesc*, const int2*, int, int*, int, size_t, int, cudaStream_t);
 struct GroupVariant {
@@ -762,11 +762,12 @@ const GroupVariant* find_variant(const SolveTables& t, int precision) {
 
 }  // namespace
 
-bool plan_group(const SolveTables& t, int precision, int sm_count, LaunchShape* out, char* why, int why_len) {
+bool plan_group(const SolveTables& t, int precision, int sm_count, LaunchShape* out, char* why, int why_len,
+                int tile_hint) {
   if (!t.kmode) {
     if (const GroupVariant* v = find_variant(t, precision)) {
       out->variant = (int)(v - kGroupVariants);
-      return v->plan(t, sm_count, out, why, why_len);
+      return v->plan(t, sm_count, out, why, why_len, tile_hint);
     }
   }
   out->variant = -1;
@@ -774,14 +775,14 @@ bool plan_group(const SolveTables& t, int precision, int sm_count, LaunchShape* 
   const bool two = precision == 1 && t.nw2 > 32;
   if (t.kmode) {
     if (precision == 1)
-      return two ? plan_group_t<float, 2, 0, 0, 0, true>(t, sm_count, out, why, why_len)
-                 : plan_group_t<float, 1, 0, 0, 0, true>(t, sm_count, out, why, why_len);
-    return plan_group_t<double, 1, 0, 0, 0, true>(t, sm_count, out, why, why_len);
+      return two ? plan_group_t<float, 2, 0, 0, 0, true>(t, sm_count, out, why, why_len, tile_hint)
+                 : plan_group_t<float, 1, 0, 0, 0, true>(t, sm_count, out, why, why_len, tile_hint);
+    return plan_group_t<double, 1, 0, 0, 0, true>(t, sm_count, out, why, why_len, tile_hint);
   }
   if (precision == 1)
-    return two ? plan_group_t<float, 2, 0, 0, 0>(t, sm_count, out, why, why_len)
-               : plan_group_t<float, 1, 0, 0, 0>(t, sm_count, out, why, why_len);
-  return plan_group_t<double, 1, 0, 0, 0>(t, sm_count, out, why, why_len);
+    return two ? plan_group_t<float, 2, 0, 0, 0>(t, sm_count, out, why, why_len, tile_hint)
+               : plan_group_t<float, 1, 0, 0, 0>(t, sm_count, out, why, why_len, tile_hint);
+  return plan_group_t<double, 1, 0, 0, 0>(t, sm_count, out, why, why_len, tile_hint);
 }
 
 namespace {

@@ -13,6 +13,7 @@
 // step each thread then sums b1n box rows and 4 window rows with its own row twiddles, instead of
 // every cell of the support and window.
 #include <cstdio>
+#include <algorithm>
 #include <cstdlib>
 
 #include "sbe_device.h"
@@ -327,12 +328,13 @@ KcolKernel kcol_kernel_for(const SolveTables& t) { return t.kmode ? kcol_kernel_
 
 }  // namespace
 
-bool plan_kcol(const SolveTables& t, int sm_count, LaunchShape* out, size_t smem_max) {
+bool plan_kcol(const SolveTables& t, int sm_count, LaunchShape* out, size_t smem_max, int parts_hint) {
   if (t.nw > 2 || !t.hermitian) return false;
   const int rows = t.row1 - t.row0;
   // Rows per tile: equal parts of at most 128 rows (measured on the 200x200 grid: 100-row tiles,
   // four resident CTAs per SM, beat whole 200-row columns by 16 % and 50-row tiles by 30 %).
   int parts = (rows + 127) / 128;
+  if (parts_hint > 0) parts = std::max((rows + kKcolMaxThreads - 1) / kKcolMaxThreads, parts_hint);
   if (const char* e = std::getenv("HHG_KCOL_PARTS")) parts = std::max(parts, std::atoi(e));  // tuning override
   const int R = (rows + parts - 1) / parts;
   const int threads = (R + 31) / 32 * 32;

@@ -81,6 +81,7 @@ def _load(path: str):
         L.SWESim_set_precision.argtypes = [vp, ct.c_int]
         L.SWESim_set_solver.argtypes = [vp, ct.c_int]
         L.SWESim_set_tb_convention.argtypes = [vp, ct.c_int]
+        L.SWESim_set_autotune.argtypes = [vp, ct.c_int]
         L.SWEBatch_new.restype = vp
         L.SWEBatch_add.argtypes = [vp, vp]
         L.SWEBatch_run.argtypes = [vp]
@@ -149,13 +150,14 @@ class SWE:
     ``defer_init=True`` skips the setup (for a request handed to :class:`SWEServer`).
     ``solver="kspace"`` selects the reference's k-space solver (src/solver_kspace.cpp) instead of
     its real-space one.  ``tb_convention="faithful"`` reads the TB file as Wannier90 defines it
-    (degeneracy weights applied, orbital order kept) instead of as the reference does."""
+    (degeneracy weights applied, orbital order kept) instead of as the reference does.
+    ``autotune=True`` times a few tile shapes at setup and keeps the fastest."""
 
     _TB = {"reference": 0, "faithful": 3, "degeneracy": 1, "untransposed": 2}
 
     def __init__(self, settings: Settings, device: int | None = None, k_rows: tuple | None = None,
                  precision: str = "fp64", defer_init: bool = False, solver: str = "rspace",
-                 tb_convention: str = "reference"):
+                 tb_convention: str = "reference", autotune: bool = False):
         self.settings = settings
         self.swe_cpp, self._ext = _load(settings.path_lib)
         self.ptr = self.swe_cpp.SWESim_new()
@@ -177,6 +179,8 @@ class SWE:
             raise SWEError(f"tb_convention must be one of {sorted(self._TB)}, not {tb_convention!r}")
         if self._TB[tb_convention]:
             self._call("SWESim_set_tb_convention", self._TB[tb_convention])
+        if autotune:
+            self._call("SWESim_set_autotune", 1)
         self.set_path_tb(settings.path_tb.encode("UTF-8"))
         self.set_settings(settings.ptr)
         if not defer_init:

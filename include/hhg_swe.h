@@ -98,6 +98,12 @@ int SWESim_last_launches(SWESim* swe);
  * the RK4 accumulation and the current's k-sum in FP64 (error against plain FP64 reported by the
  * tests and bench). */
 void SWESim_set_precision(SWESim* swe, int mode);
+/* Autotuning of the tile shape (no counterpart in the reference): when on (or with the environment
+ * variable HHG_AUTOTUNE=1), SWESim_init times the first steps of the pulse under a few candidate tile
+ * shapes (k-points per CTA, rows per column tile) and keeps the fastest; the choice is cached per
+ * device and solve shape for the rest of the process.  Results change only by the rounding of the
+ * current's k-sum order.  Takes effect at the next SWESim_init. */
+void SWESim_set_autotune(SWESim* swe, int on);
 /* TB-file reading (no counterpart in the reference, which always transposes each block and ignores
  * the degeneracy line, src/wannier_tb.cpp:36-49,74,102): flags 0 (default) read as the reference
  * does; bit 0 divides each R block (H and positions) by its degeneracy, as Wannier90 defines the
