@@ -586,6 +586,7 @@ def main():
                     help="mixed: FP32 Wannier sums and commutators, FP64 state / RK accumulation / k-sum")
     ap.add_argument("--solver", default="rspace", choices=["rspace", "kspace"],
                     help="kspace: the reference's k-space solver (src/solver_kspace.cpp) instead of its real-space one")
+    ap.add_argument("--batch", type=int, default=1, help="mixed: also time this many solves of the workload as one SWEBatch")
     ap.add_argument("--autotune", action="store_true", help="time candidate tile shapes at setup (SWESim_set_autotune)")
     ap.add_argument("--requests", type=int, default=200, help="c4: requests in the arrival stream")
     ap.add_argument("--max-active", type=int, default=32, help="c4: most solves running at once")
@@ -627,6 +628,7 @@ def main():
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         return float(t.item())
 
+    import numpy as np
     from pySWE import pyswe
 
     import ctypes as ct
@@ -707,6 +709,29 @@ def main():
         fp64_ms = ref.last_kernel_ms()
         ref.delete()
         mixed = mixed_report(J_mixed, J_fp64, param, fp64_ms, total_ms / args.steps)
+        if args.batch > 1:
+            # The batched mixed form: args.batch solves of this configuration (polarisation angles
+            # spread over the half circle) in one SWEBatch, against the plain FP64 solve's throughput.
+            solves = []
+            for i in range(args.batch):
+                pi = dict(param)
+                ang = math.pi * i / args.batch
+                pi["pol_vec"] = np.array([math.sin(ang), math.cos(ang), 0.0])
+                solves.append(pyswe.SWE(pyswe.Settings(pi), device=local, precision="mixed", solver=args.solver,
+                                        autotune=args.autotune))
+            batch = pyswe.SWEBatch(solves)
+            batch.run()
+            bms = []
+            for _ in range(2):
+                batch.run()
+                bms.append(batch.last_ms())
+            batch.delete()
+            for s in solves:
+                s.delete()
+            per_solve = statistics.mean(bms) / args.batch
+            mixed["batched"] = {"solves": args.batch, "ms_per_batch": statistics.mean(bms), "ms_per_solve": per_solve,
+                                "k_pt_rk4_steps_per_s": nk * nt / (per_solve * 1e-3),
+                                "throughput_vs_fp64_solo": fp64_ms / per_solve}
     swe.delete()
     if dist is not None:
         dist.destroy_process_group()

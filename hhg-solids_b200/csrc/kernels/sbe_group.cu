@@ -583,7 +583,9 @@ __device__ __forceinline__ void group_vctas(const SolveTables& t, const GroupDat
             re += half[(ss * nwarps + w) * 2 * nj + 2 * a];
             im += half[(ss * nwarps + w) * 2 * nj + 2 * a + 1];
           }
-          double2* dst = Jpart + ((size_t)v * t.nt + ti0 + ss) * 3 + t.j_id[a];
+          // (selects, not an indexed read: an indexed read of the descriptor would move it to local memory)
+          const int ja = a == 0 ? t.j_id[0] : (a == 1 ? t.j_id[1] : t.j_id[2]);
+          double2* dst = Jpart + ((size_t)v * t.nt + ti0 + ss) * 3 + ja;
           const double2 old = *dst;
           *dst = make_double2(old.x + re, old.y + im);
         }
@@ -620,20 +622,19 @@ __global__ void __launch_bounds__(group_threads<EPT>(), 1)
 template <typename Real, int EPT, int NWc, int NAXc, int NJc, bool KM = false>
 __global__ void __launch_bounds__(group_threads<EPT>(), 1)
     propagate_group_batch_kernel(const BatchDesc* descs, const int2* items, int nitems, int* counter) {
-  __shared__ BatchDesc sd;
   __shared__ int s_item;
   for (;;) {
     if (threadIdx.x == 0) s_item = atomicAdd(counter, 1);
     __syncthreads();
     const int it = s_item;
+    __syncthreads();  // s_item is rewritten by the next iteration
     if (it >= nitems) break;
     const int2 w = items[it];  // (solve, virtual CTA)
-    const int* src = reinterpret_cast<const int*>(descs + w.x);
-    for (int q = threadIdx.x; q < (int)(sizeof(BatchDesc) / sizeof(int)); q += blockDim.x)
-      reinterpret_cast<int*>(&sd)[q] = src[q];
-    __syncthreads();
-    group_vctas<Real, EPT, NWc, NAXc, NJc, KM>(sd.t, group_data<Real>(sd.gt), sd.B, sd.G, sd.box_sm, sd.win_sm, w.y,
-                                           sd.vctas, sd.vctas, sd.rho, sd.Jpart);
+    // The descriptor in registers (read-only, uniform across the CTA): the hot loop reads its fields
+    // every step, which would be shared-memory loads if it stayed in shared memory.
+    const BatchDesc dsc = descs[w.x];
+    group_vctas<Real, EPT, NWc, NAXc, NJc, KM>(dsc.t, group_data<Real>(dsc.gt), dsc.B, dsc.G, dsc.box_sm, dsc.win_sm,
+                                               w.y, dsc.vctas, dsc.vctas, dsc.rho, dsc.Jpart);
     __syncthreads();
   }
 }
