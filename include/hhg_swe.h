@@ -144,7 +144,8 @@ void SWESim_get_fields(SWESim* swe, double* t, double* E, double* A);
  *
  * It calls no cudaMalloc / cudaFree: the current partials go to a fixed 32 MiB array of device
  * memory that the library holds on each device it is used on until the process exits.  Solves
- * that need more (CTAs x nt x 48 bytes > 32 MiB, e.g. nt above about 4700 when a solve fills all 148 SMs) are
+ * that need more (virtual CTAs x nt x 48 bytes > 32 MiB: an element-group solve on 148 CTAs up to nt of about
+ * 4700; a 200x200 2-orbital solve on 400 column tiles up to about 1740) are
  * rejected with -1 and a message.  The first call on a device looks up that array's address, so
  * make it before capturing the stream into a graph.  All calls on a device share the array and
  * clear it at their start: calls whose work overlaps on the GPU (different streams, or different
