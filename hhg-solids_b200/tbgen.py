@@ -194,6 +194,8 @@ MODELS = {
     "tmd12_s2": (random_tmd, {"nw": 12, "seed": 2}),
     "tmd12_s3": (random_tmd, {"nw": 12, "seed": 3}),
     "tmd5_s4": (random_tmd, {"nw": 5, "seed": 4, "window": 5}),
+    "tmd16_s1": (random_tmd, {"nw": 16, "seed": 1, "window": 5}),
+    "tmd1_s2": (random_tmd, {"nw": 1, "seed": 2, "window": 5}),
     "tmd6_deg": (tmd_deg, {}),
     "tmd6_deg_equiv": (tmd_deg_equiv, {}),
 }
