@@ -22,6 +22,7 @@
 #include <cstring>
 
 #include "sbe_device.h"
+#include "sbe_herm2.cuh"
 
 namespace hhg {
 namespace {
@@ -191,64 +192,70 @@ __global__ void __launch_bounds__(kKptMaxThreads) propagate_kpt_kernel(SolveTabl
           box_sums(sQ);  // point t of the chunk's first step; later steps carry it from stage 4
         }
 
-        // Four RK4 stages (src/solver.cpp:157-163), fields at t, t+dt/2, t+dt/2, t+dt.
-        double2 K[NW2], S[NW2];
+        if constexpr (NW == 2) {
+          herm2_rk4_step<NAXc>(r, hd, hu, rd, ru, nax, t.ax_id, sE + s * 9, dt, prefac, [&](int fpt) {
+            if (km) box_sums(sQ + (2 * s + fpt) * ncw);  // the k-space solver's points t + dt/2, t + dt
+          });
+        } else {
+          // Four RK4 stages (src/solver.cpp:157-163), fields at t, t+dt/2, t+dt/2, t+dt.
+          double2 K[NW2], S[NW2];
 #pragma unroll
-        for (int st = 0; st < 4; ++st) {
-          const int f = st == 0 ? 0 : (st == 3 ? 2 : 1);
-          const double* es = sE + s * 9 + f * 3;
-          if (km && st > 0 && st != 2) box_sums(sQ + (2 * s + f) * ncw);  // points t + dt/2, t + dt
-          double2 H[NW2], X[NW2];
+          for (int st = 0; st < 4; ++st) {
+            const int f = st == 0 ? 0 : (st == 3 ? 2 : 1);
+            const double* es = sE + s * 9 + f * 3;
+            if (km && st > 0 && st != 2) box_sums(sQ + (2 * s + f) * ncw);  // points t + dt/2, t + dt
+            double2 H[NW2], X[NW2];
 #pragma unroll
-          for (int i = 0; i < NW; ++i) {
-            double d = hd[i];
-#pragma unroll
-            for (int a = 0; a < 3; ++a)
-              if (a < nax) d = fma(es[t.ax_id[a]], rd[a][i], d);
-            H[i * NW + i] = make_double2(d, 0.0);
-#pragma unroll
-            for (int j = i + 1; j < NW; ++j) {
-              double2 u = hu[i * NW + j];
+            for (int i = 0; i < NW; ++i) {
+              double d = hd[i];
 #pragma unroll
               for (int a = 0; a < 3; ++a)
-                if (a < nax) {
-                  const double ea = es[t.ax_id[a]];
-                  u.x = fma(ea, ru[a][i * NW + j].x, u.x);
-                  u.y = fma(ea, ru[a][i * NW + j].y, u.y);
-                }
-              H[i * NW + j] = u;
-              H[j * NW + i] = cconj(u);
+                if (a < nax) d = fma(es[t.ax_id[a]], rd[a][i], d);
+              H[i * NW + i] = make_double2(d, 0.0);
+#pragma unroll
+              for (int j = i + 1; j < NW; ++j) {
+                double2 u = hu[i * NW + j];
+#pragma unroll
+                for (int a = 0; a < 3; ++a)
+                  if (a < nax) {
+                    const double ea = es[t.ax_id[a]];
+                    u.x = fma(ea, ru[a][i * NW + j].x, u.x);
+                    u.y = fma(ea, ru[a][i * NW + j].y, u.y);
+                  }
+                H[i * NW + j] = u;
+                H[j * NW + i] = cconj(u);
+              }
             }
+            const double cs = (st == 3 ? 1.0 : 0.5) * dt;
+#pragma unroll
+            for (int e = 0; e < NW2; ++e)
+              X[e] = st == 0 ? r[e] : make_double2(r[e].x + cs * K[e].x, r[e].y + cs * K[e].y);
+            double2 HX[NW2];
+#pragma unroll
+            for (int i = 0; i < NW; ++i)
+#pragma unroll
+              for (int j = 0; j < NW; ++j) {
+                double2 acc = make_double2(0.0, 0.0);
+#pragma unroll
+                for (int l = 0; l < NW; ++l) acc = cfma(H[i * NW + l], X[l * NW + j], acc);
+                HX[i * NW + j] = acc;
+              }
+#pragma unroll
+            for (int i = 0; i < NW; ++i)
+#pragma unroll
+              for (int j = 0; j < NW; ++j) {
+                // k = -i (HX - (HX)^+)
+                const double cx = HX[i * NW + j].x - HX[j * NW + i].x, cy = HX[i * NW + j].y + HX[j * NW + i].y;
+                K[i * NW + j] = make_double2(cy, -cx);
+              }
+            const double wgt = st == 3 ? 1.0 : 2.0;
+#pragma unroll
+            for (int e = 0; e < NW2; ++e)
+              S[e] = st == 0 ? K[e] : make_double2(S[e].x + wgt * K[e].x, S[e].y + wgt * K[e].y);
           }
-          const double cs = (st == 3 ? 1.0 : 0.5) * dt;
 #pragma unroll
-          for (int e = 0; e < NW2; ++e)
-            X[e] = st == 0 ? r[e] : make_double2(r[e].x + cs * K[e].x, r[e].y + cs * K[e].y);
-          double2 HX[NW2];
-#pragma unroll
-          for (int i = 0; i < NW; ++i)
-#pragma unroll
-            for (int j = 0; j < NW; ++j) {
-              double2 acc = make_double2(0.0, 0.0);
-#pragma unroll
-              for (int l = 0; l < NW; ++l) acc = cfma(H[i * NW + l], X[l * NW + j], acc);
-              HX[i * NW + j] = acc;
-            }
-#pragma unroll
-          for (int i = 0; i < NW; ++i)
-#pragma unroll
-            for (int j = 0; j < NW; ++j) {
-              // k = -i (HX - (HX)^+)
-              const double cx = HX[i * NW + j].x - HX[j * NW + i].x, cy = HX[i * NW + j].y + HX[j * NW + i].y;
-              K[i * NW + j] = make_double2(cy, -cx);
-            }
-          const double wgt = st == 3 ? 1.0 : 2.0;
-#pragma unroll
-          for (int e = 0; e < NW2; ++e)
-            S[e] = st == 0 ? K[e] : make_double2(S[e].x + wgt * K[e].x, S[e].y + wgt * K[e].y);
+          for (int e = 0; e < NW2; ++e) r[e] = make_double2(r[e].x + prefac * S[e].x, r[e].y + prefac * S[e].y);
         }
-#pragma unroll
-        for (int e = 0; e < NW2; ++e) r[e] = make_double2(r[e].x + prefac * S[e].x, r[e].y + prefac * S[e].y);
 
         // Current partials.
 #pragma unroll
