@@ -402,8 +402,7 @@ void SWESim::init() {
   const int npts = solver == 1 ? 2 * nt + 1 : nt;
   int np_ = 2;
   for (int c = 0; c < ncell; ++c) np_ = std::max(np_, std::max(std::abs(cellp[c].x), std::abs(cellp[c].y)));
-  const int npw = 2 * np_ + 1;
-  std::vector<double2> Cfac;  // k-space solver: [npts][2][npw] factors Cx, Cy at n = -np..np
+  std::vector<double> x0;  // k-space solver: [npts][2] stencil offsets -N u_d(A_j)
   if (solver == 1) {
     double bA[3][3];  // reciprocal vectors (1/Angstrom, src/grid.cpp:27-46), then in au
     {
@@ -420,7 +419,7 @@ void SWESim::init() {
         for (int c = 0; c < 3; ++c) bA[r][c] = 2.0 * M_PI / vol * cr[r][c] / kA2Bohr;
     }
     double* brows[3] = {bA[0], bA[1], bA[2]};
-    Cfac.assign((size_t)npts * 2 * npw, make_double2(0.0, 0.0));
+    x0.assign((size_t)npts * 2, 0.0);
     const int N = N1;
     for (int j = 0; j < npts; ++j) {
       const int i = std::min(j / 2, nt - 1);
@@ -436,46 +435,16 @@ void SWESim::init() {
       }
       double crd[3];
       hhg::refarith::cramer3(brows, Aj, crd);
-      for (int d = 0; d < 2; ++d) {
-        const double x0 = -crd[d] * (double)N;
-        const double o = std::floor(x0), tt = x0 - o;
-        const double w[4] = {((-0.5 * tt + 1.0) * tt - 0.5) * tt, (1.5 * tt - 2.5) * tt * tt + 1.0,
-                             ((-1.5 * tt + 2.0) * tt + 0.5) * tt, (0.5 * tt - 0.5) * tt * tt};
-        const long ox = (long)o;
-        for (int n = -np_; n <= np_; ++n) {
-          cd acc(0.0, 0.0);
-          for (int a = -1; a <= 2; ++a) {
-            const int m = wrapi((ox + a) * (long)n, N);
-            const double ang = 2.0 * M_PI * (double)m / (double)N;
-            acc += w[a + 1] * cd(std::cos(ang), -std::sin(ang));
-          }
-          Cfac[((size_t)j * 2 + d) * npw + (n + np_)] = d2(acc);
-        }
-      }
+      for (int d = 0; d < 2; ++d) x0[(size_t)2 * j + d] = -crd[d] * (double)N;  // stencil offset o + t
     }
   }
-  Q.assign((size_t)npts * ncw, make_double2(1.0, 0.0));
-  if (solver == 1) {
-    for (int j = 0; j < npts; ++j)
-      for (int c = 0; c < ncell; ++c) {
-        const cd cx = cd(Cfac[((size_t)j * 2 + 0) * npw + cellp[c].x + np_].x, Cfac[((size_t)j * 2 + 0) * npw + cellp[c].x + np_].y);
-        const cd cy = cd(Cfac[((size_t)j * 2 + 1) * npw + cellp[c].y + np_].x, Cfac[((size_t)j * 2 + 1) * npw + cellp[c].y + np_].y);
-        Q[(size_t)j * ncw + c] = d2(cx * cy);
-      }
-  } else {
-    std::vector<double> Rc((size_t)ncw * 3);
-    for (int c = 0; c < ncw; ++c) {
-      const int2 n = c < ncell ? cell_n[c] : win_n[c - ncell];
-      const int cc = cell_of(n.x, n.y);
-      for (int a = 0; a < 3; ++a) Rc[3 * c + a] = Rgrid[3 * (size_t)cc + a] * kA2Bohr;
-    }
-    for (int ti = 0; ti < nt; ++ti) {
-      const double ax = A[ti], ay = A[nt + ti], az = A[2 * (size_t)nt + ti];
-      for (int c = 0; c < ncw; ++c) {
-        const double th = ax * Rc[3 * c] + ay * Rc[3 * c + 1] + az * Rc[3 * c + 2];
-        Q[(size_t)ti * ncw + c] = make_double2(std::cos(th), std::sin(th));
-      }
-    }
+  // (The tables themselves are built on the device below, from A, the cell positions Rc and the
+  // stencil offsets x0.)
+  Rc.assign((size_t)ncw * 3, 0.0);
+  for (int c = 0; c < ncw; ++c) {
+    const int2 n = c < ncell ? cell_n[c] : win_n[c - ncell];
+    const int cc = cell_of(n.x, n.y);
+    for (int a = 0; a < 3; ++a) Rc[3 * c + a] = Rgrid[3 * (size_t)cc + a] * kA2Bohr;
   }
 
   // Dense bounding box of the support cells for the separable Wannier sum.
@@ -497,21 +466,9 @@ void SWESim::init() {
         Xbox[((size_t)(1 + a) * b1n * b2n + box) * nw2 + o] = Rtab[((size_t)a * ncell + c) * nw2 + o];
     }
   }
-  // Separable factors per point: e^{i n A(t_i).a_1}, e^{i n A(t_i).a_2} for |n| <= np (real-space
-  // solver), Cx and Cy (k-space solver).
-  if (solver == 1) {
-    P = Cfac;
-  } else {
-    P.assign((size_t)nt * 2 * npw, make_double2(1.0, 0.0));
-    for (int ti = 0; ti < nt; ++ti) {
-      const double ax = A[ti], ay = A[nt + ti], az = A[2 * (size_t)nt + ti];
-      for (int d = 0; d < 2; ++d) {
-        const double th = ax * lat_au[d][0] + ay * lat_au[d][1] + az * lat_au[d][2];
-        for (int n = -np_; n <= np_; ++n)
-          P[((size_t)ti * 2 + d) * npw + (n + np_)] = make_double2(std::cos(n * th), std::sin(n * th));
-      }
-    }
-  }
+  npts_ = npts;
+  ncw_ = ncw;
+  x0_ = std::move(x0);
   tab.nwin = nwin;
   tab.b1lo = b1lo;
   tab.b1n = b1n;
@@ -550,19 +507,31 @@ void SWESim::init() {
   trace.mark("tables");
   // Device tables.
   h2d_bytes = sizeof(int2) * (cell_n.size() + cellp.size() + win_n.size()) +
-              sizeof(double2) * (H0.size() + Rtab.size() + V.size() + Q.size() + Xbox.size() + Vd.size() + P.size() +
-                                 T1.size() + T2.size()) +
-              sizeof(double) * es.size();
+              sizeof(double2) * (H0.size() + Rtab.size() + V.size() + Xbox.size() + Vd.size() + T1.size() + T2.size()) +
+              sizeof(double) * (es.size() + A.size() + Rc.size() + x0_.size());
   d_cell.upload(cell_n, stream);
   d_cellp.upload(cellp, stream);
   d_win.upload(win_n, stream);
   d_H0.upload(H0, stream);
   d_R.upload(Rtab, stream);
   d_V.upload(V, stream);
-  d_Q.upload(Q, stream);
+  // Factor tables of every evaluation point, built on the device.
+  {
+    const int npw = 2 * tab.np + 1;
+    d_A.upload(A, stream);
+    d_Rc.upload(Rc, stream);
+    d_Q.alloc((size_t)npts_ * ncw_);
+    d_P.alloc((size_t)npts_ * 2 * npw);
+    if (solver == 1) {
+      d_x0.upload(x0_, stream);
+      hhg::launch_interp_tables(d_x0.p, N1, tab.np, npts_, d_cellp.p, (int)cellp.size(), ncw_, d_P.p, d_Q.p, stream);
+    } else {
+      hhg::launch_peierls_tables(d_A.p, d_Rc.p, lat_au, nt, ncw_, tab.np, d_Q.p, d_P.p, stream);
+    }
+    check_cuda(cudaGetLastError(), "table kernels");
+  }
   d_Xbox.upload(Xbox, stream);
   d_Vd.upload(Vd, stream);
-  d_P.upload(P, stream);
   d_T1.upload(T1, stream);
   d_T2.upload(T2, stream);
   d_es.upload(es, stream);
@@ -575,10 +544,11 @@ void SWESim::init() {
     };
     d_Xbox32.upload(to32(Xbox), stream);
     d_Vd32.upload(to32(Vd), stream);
-    d_P32.upload(to32(P), stream);
+    d_P32.alloc(d_P.n);
+    hhg::launch_to_float2(d_P.p, d_P.n, d_P32.p, stream);
     d_T1_32.upload(to32(T1), stream);
     d_T2_32.upload(to32(T2), stream);
-    h2d_bytes += sizeof(float2) * (Xbox.size() + Vd.size() + P.size() + T1.size() + T2.size());
+    h2d_bytes += sizeof(float2) * (Xbox.size() + Vd.size() + T1.size() + T2.size());
     check_cuda(cudaStreamSynchronize(stream), "H2D");  // the host vectors above are temporaries
   }
   gtab = hhg::GroupTables{d_Xbox.p, d_Vd.p, d_P.p, d_T1.p, d_T2.p,
@@ -654,7 +624,8 @@ void SWESim::init() {
 }
 
 size_t SWESim::device_bytes() const {
-  size_t b = (d_cell.cap + d_cellp.cap + d_win.cap) * sizeof(int2) + d_es.cap * sizeof(double);
+  size_t b = (d_cell.cap + d_cellp.cap + d_win.cap) * sizeof(int2) +
+             (d_es.cap + d_A.cap + d_Rc.cap + d_x0.cap) * sizeof(double);
   for (const auto* x : {&d_H0, &d_R, &d_V, &d_Q, &d_Xbox, &d_Vd, &d_P, &d_T1, &d_T2, &d_rho0, &d_rho, &d_Jpart, &d_J})
     b += x->cap * sizeof(double2);
   for (const auto* x : {&d_Xbox32, &d_Vd32, &d_P32, &d_T1_32, &d_T2_32}) b += x->cap * sizeof(float2);

@@ -82,7 +82,9 @@ struct SWESim {
   std::vector<double> t, E, A;
   std::vector<double> es;          // [nt][3][3]
   std::vector<int2> cell_n, win_n;
-  std::vector<double2> H0, Rtab, V, Q, Xbox, Vd, P, T1, T2;
+  std::vector<double2> H0, Rtab, V, Xbox, Vd, T1, T2;
+  std::vector<double> Rc, x0_;  // listed cells' positions (bohr); k-space stencil offsets
+  int npts_ = 0, ncw_ = 0;      // evaluation points, listed cells
   int precision = 0;  // 0 plain FP64, 1 mixed
   int solver = 0;     // 0 the real-space solver (src/solver.cpp), 1 the k-space solver (src/solver_kspace.cpp)
   bool autotune = false;  // time candidate tile shapes at SWESim_init (also HHG_AUTOTUNE=1)
@@ -99,7 +101,7 @@ struct SWESim {
   hhg::DevBuf<double2> d_H0, d_R, d_V, d_Q, d_Xbox, d_Vd, d_P, d_T1, d_T2, d_rho0, d_rho, d_Jpart, d_J;
   hhg::DevBuf<float2> d_Xbox32, d_Vd32, d_P32, d_T1_32, d_T2_32;
   hhg::GroupTables gtab{};
-  hhg::DevBuf<double> d_es;
+  hhg::DevBuf<double> d_es, d_A, d_Rc, d_x0;
   hhg::SolveTables tab{};
   hhg::LaunchShape shape{};
   double2* h_J = nullptr;  // pinned [3][nt]
@@ -126,6 +128,9 @@ struct SWESim {
       b->release();
     for (auto* b : {&d_Xbox32, &d_Vd32, &d_P32, &d_T1_32, &d_T2_32}) b->release();
     d_es.release();
+    d_A.release();
+    d_Rc.release();
+    d_x0.release();
     if (h_J) cudaFreeHost(h_J);
     h_J = nullptr;
     h_J_cap = 0;

@@ -129,6 +129,16 @@ int spectrum_device(const double2* J, int n, int count, double h, double2* S, do
 int harmonics_device(const double2* S, int n, int count, double tmax, double lambda_nm, int nh, double* I,
                      cudaStream_t stream);
 
+// Per-step factor tables on the device (tables.cu).  A [3][nt] (au), Rc [ncw][3] (bohr), lat the first
+// two lattice vectors (bohr): Q [nt][ncw] Peierls phases, P [nt][2][2np+1] separable powers.
+void launch_peierls_tables(const double* A, const double* Rc, const double lat[2][3], int nt, int ncw, int np,
+                           double2* Q, double2* P, cudaStream_t stream);
+// k-space solver: x0 [npts][2] stencil offsets -N u_d; P [npts][2][2np+1] interpolation factors,
+// Q [npts][ncw] their products on the (transposed) cells, 1 on the window cells.
+void launch_interp_tables(const double* x0, int N, int np, int npts, const int2* cellp, int ncell, int ncw, double2* P,
+                          double2* Q, cudaStream_t stream);
+void launch_to_float2(const double2* in, size_t n, float2* out, cudaStream_t stream);
+
 // FMA-chain throughput probe (TFLOP/s) on the current device.
 int measure_fma_peaks(double* fp64_tflops, double* fp32_tflops);
 
