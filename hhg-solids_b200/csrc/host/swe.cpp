@@ -326,12 +326,15 @@ void SWESim::init() {
   for (int c = 0; c < Nk; ++c)
     if (site_of_cell[c] >= 0) placed.push_back(c);
   std::vector<cd> vw((size_t)3 * hhg::kWindow * nw2, cd(0, 0));
-  for (int a = 0; a < 3; ++a)
+  for (int a = 0; a < 3; ++a) {
+    bool r_nonzero = false;  // an axis without position elements has no convolution term
+    for (const cd& z : model.bc[a]) r_nonzero = r_nonzero || z != cd(0, 0);
     for (int w = 0; w < hhg::kWindow; ++w) {
       const int n1 = w / 4 - 2, n2 = w % 4 - 2;
       const int c = cell_of(n1, n2);
       std::vector<cd> acc(nw2, cd(0, 0));
       for (int q : placed) {
+        if (!r_nonzero) break;
         const int q1 = q / N2 - N1 / 2, q2 = q % N2 - N2 / 2;
         const int d = cell_of(n1 - q1, n2 - q2);
         const int sd = site_of_cell[d];
@@ -341,10 +344,13 @@ void SWESim::init() {
         const cd* Hq = model.hop.data() + (size_t)sq * nw2;
         const cd* rd = model.bc[a].data() + (size_t)sd * nw2;
         const cd* Hd = model.hop.data() + (size_t)sd * nw2;
+        // The products written out: the same arithmetic as std::complex's operator* on finite
+        // values, without its out-of-line NaN handling.
+        auto mul = [](cd x, cd y) { return cd(x.real() * y.real() - x.imag() * y.imag(), x.real() * y.imag() + x.imag() * y.real()); };
         for (int i = 0; i < nw; ++i)
           for (int j = 0; j < nw; ++j) {
             cd sum(0, 0);
-            for (int k = 0; k < nw; ++k) sum += (-rq[i * nw + k]) * Hd[k * nw + j] - Hq[i * nw + k] * (-rd[k * nw + j]);
+            for (int k = 0; k < nw; ++k) sum += mul(-rq[i * nw + k], Hd[k * nw + j]) - mul(Hq[i * nw + k], -rd[k * nw + j]);
             acc[i * nw + j] += sum;
           }
       }
@@ -355,6 +361,7 @@ void SWESim::init() {
         vw[((size_t)a * hhg::kWindow + w) * nw2 + o] = cd(0, 1) * (Ra * h - acc[o]);
       }
     }
+  }
   nj = 0;
   for (int a = 0; a < 3; ++a) {
     bool nz = false;

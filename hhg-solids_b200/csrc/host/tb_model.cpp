@@ -7,6 +7,7 @@
 // 101-102).  Unlike the reference, malformed files raise an error instead of reading garbage.
 #include "tb_model.hpp"
 
+#include <cstdlib>
 #include <fstream>
 #include <sstream>
 #include <stdexcept>
@@ -33,6 +34,28 @@ struct LineReader {
     std::ostringstream os;
     os << "TB file " << path << " line " << lineno << ": " << msg;
     throw std::runtime_error(os.str());
+  }
+};
+
+// Numbers of one line, read with strtol / strtod (the conversions istream's operator>> uses, so the
+// values are the same; a per-line istringstream made setup parse-bound for large models).
+struct Fields {
+  const char* p;
+  bool ok = true;
+  explicit Fields(const std::string& s) : p(s.c_str()) {}
+  long integer() {
+    char* end = nullptr;
+    const long v = std::strtol(p, &end, 10);
+    ok = ok && end != p;
+    p = end;
+    return v;
+  }
+  double real() {
+    char* end = nullptr;
+    const double v = std::strtod(p, &end);
+    ok = ok && end != p;
+    p = end;
+    return v;
   }
 };
 
@@ -69,13 +92,18 @@ TBModel parse_tb(const std::string& path) {
   m.hop.assign((size_t)m.nsites * nw2, cd(0, 0));
   for (int a = 0; a < 3; ++a) m.bc[a].assign((size_t)m.nsites * nw2, cd(0, 0));
   for (int s = 0; s < m.nsites; ++s) {
-    std::istringstream is(rd.next("R cell"));
-    if (!(is >> m.R[3 * s] >> m.R[3 * s + 1] >> m.R[3 * s + 2])) rd.fail("bad R cell line");
+    {
+      const std::string line = rd.next("R cell");
+      Fields f(line);
+      for (int a = 0; a < 3; ++a) m.R[3 * s + a] = (int)f.integer();
+      if (!f.ok) rd.fail("bad R cell line");
+    }
     for (int q = 0; q < nw2; ++q) {
-      std::istringstream ls(rd.next("hopping"));
-      int o1, o2;
-      double re, im;
-      if (!(ls >> o1 >> o2 >> re >> im) || o1 < 1 || o1 > nw || o2 < 1 || o2 > nw) rd.fail("bad hopping line");
+      const std::string line = rd.next("hopping");
+      Fields f(line);
+      const long o1 = f.integer(), o2 = f.integer();
+      const double re = f.real(), im = f.real();
+      if (!f.ok || o1 < 1 || o1 > nw || o2 < 1 || o2 > nw) rd.fail("bad hopping line");
       m.hop[(size_t)s * nw2 + (o2 - 1) * nw + (o1 - 1)] = cd(re, im);
     }
     rd.next("separator");
@@ -83,12 +111,12 @@ TBModel parse_tb(const std::string& path) {
   for (int s = 0; s < m.nsites; ++s) {
     rd.next("position block header");
     for (int q = 0; q < nw2; ++q) {
-      std::istringstream ls(rd.next("position element"));
-      int o1, o2;
+      const std::string line = rd.next("position element");
+      Fields f(line);
+      const long o1 = f.integer(), o2 = f.integer();
       double v[6];
-      if (!(ls >> o1 >> o2 >> v[0] >> v[1] >> v[2] >> v[3] >> v[4] >> v[5]) || o1 < 1 || o1 > nw || o2 < 1 ||
-          o2 > nw)
-        rd.fail("bad position line");
+      for (double& x : v) x = f.real();
+      if (!f.ok || o1 < 1 || o1 > nw || o2 < 1 || o2 > nw) rd.fail("bad position line");
       for (int a = 0; a < 3; ++a) m.bc[a][(size_t)s * nw2 + (o2 - 1) * nw + (o1 - 1)] = cd(v[2 * a], v[2 * a + 1]);
     }
     std::string sep;
