@@ -100,6 +100,15 @@ constexpr int group_threads() {
 }
 constexpr int kJRing = 16;          // steps per current-partial flush
 
+// Threads per k-point for nw2 elements at ept per thread: the next power of two up to a warp,
+// whole warps beyond it.
+__host__ __device__ constexpr int group_size(int nw2, int ept) {
+  const int per = (nw2 + ept - 1) / ept;
+  int g = 1;
+  while (g < per && g < 32) g <<= 1;
+  return per <= 32 ? g : (per + 31) / 32 * 32;
+}
+
 // Geometry shared by host planning and the kernel.
 struct GroupGeom {
   int W1n, W2n;   // cell box
@@ -191,14 +200,18 @@ struct GroupData {
 
 // Runs virtual CTAs v_first, v_first + v_step, ... (< vctas) of one solve on this CTA.
 // NWc, NAXc, NJc: orbital count, field axes and current axes fixed at compile time (0: read from t).
-template <typename Real, int EPT, int NWc, int NAXc, int NJc, bool KM>
-__device__ __forceinline__ void group_vctas(const SolveTables& t, const GroupData<Real>& d, int B, int G, int box_sm,
+// WBc > 0: a square WBc x WBc cell box with Hermitian halving, fixed at compile time, so that the
+// Wannier-sum loops unroll with constant offsets.
+template <typename Real, int EPT, int NWc, int NAXc, int NJc, bool KM, int WBc = 0>
+__device__ __forceinline__ void group_vctas(const SolveTables& t, const GroupData<Real>& d, int B, int G_in, int box_sm,
                                             int win_sm, int v_first, int v_step, int vctas, double2* rho,
                                             double2* Jpart) {
   using V = typename Cx<Real>::T;
   extern __shared__ __align__(16) unsigned char smraw[];
   const GroupGeom gg = group_geom(t);
   const int nw = NWc ? NWc : t.nw, nw2 = nw * nw, nax = NAXc ? NAXc : t.nax, nj = NJc ? NJc : t.nj;
+  constexpr int Gc = NWc ? group_size(NWc * NWc, EPT) : 0;
+  const int G = Gc ? Gc : G_in;
   const int nthr = blockDim.x, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarps = (nthr + 31) >> 5;
   const int g = tid / G, e0 = tid % G;
   // This thread owns elements e0 + u*G, u < EPT.
@@ -212,7 +225,10 @@ __device__ __forceinline__ void group_vctas(const SolveTables& t, const GroupDat
     ju[u] = actu[u] ? eu[u] % nw : 0;
     eTu[u] = ju[u] * nw + iu[u];
   }
-  const int W1n = gg.W1n, W2n = gg.W2n, W1 = W1n, W2 = W2n;
+  constexpr bool kBox = WBc > 0;
+  const int W1n = kBox ? WBc : gg.W1n, W2n = kBox ? WBc : gg.W2n, W1 = W1n, W2 = W2n;
+  const int q1s = kBox ? (WBc - 1) / 2 : gg.q1s, nq1 = kBox ? WBc - (WBc - 1) / 2 : gg.nq1;
+  const int nmat = NAXc ? 1 + NAXc : gg.nmat, nbrows = nmat * nq1, nwrows = NJc ? 4 * NJc : gg.nwrows;
   const GroupLayout<Real> L(t, gg, B, nwarps, box_sm, win_sm);
   V* sm = reinterpret_cast<V*>(smraw);
   double2* dsm = reinterpret_cast<double2*>(sm + L.total_cx);
@@ -239,16 +255,16 @@ __device__ __forceinline__ void group_vctas(const SolveTables& t, const GroupDat
   const int bpc = (rows + B - 1) / B;
   const int ntiles = t.N2 * bpc;
   const V vzero = Cx<Real>::make(0, 0);
-  const size_t gbuf = (size_t)gg.nbrows * nw2, wbuf = (size_t)gg.nwrows * nw2;
+  const size_t gbuf = (size_t)nbrows * nw2, wbuf = (size_t)nwrows * nw2;
   constexpr bool km = KM;             // k-space solver: three evaluation points per step
   const int ring = km ? 6 : 3, gbufs = km ? 4 : 2;
 
   // Constant tables into shared memory (once per launch).
   if (box_sm) {
-    const size_t n = (size_t)gg.nq1 * W2n * nw2;
-    for (int mat = 0; mat < gg.nmat; ++mat)
+    const size_t n = (size_t)nq1 * W2n * nw2;
+    for (int mat = 0; mat < nmat; ++mat)
       for (size_t idx = tid; idx < n; idx += nthr)
-        sm[L.Xbox + mat * n + idx] = d.Xbox[((size_t)mat * W1n + gg.q1s) * W2n * nw2 + idx];
+        sm[L.Xbox + mat * n + idx] = d.Xbox[((size_t)mat * W1n + q1s) * W2n * nw2 + idx];
   }
   if (win_sm)
     for (size_t idx = tid; idx < (size_t)nj * 16 * nw2; idx += nthr) dsm[L.Xwin + idx] = d.Xwin[idx];
@@ -318,14 +334,15 @@ __device__ __forceinline__ void group_vctas(const SolveTables& t, const GroupDat
       const double2* w2 = wpw2 + (s % ring) * 4;
       V* Gd = Gb + (s % gbufs) * gbuf;
       double2* GWd = GWb + (s & 1) * wbuf;
-      for (int row = g; row < gg.nbrows + (win ? gg.nwrows : 0); row += B) {
-        if (row < gg.nbrows) {
-          const int mat = row / gg.nq1, qq = row % gg.nq1;
-          const V* X = box_sm ? Xbox + (((size_t)mat * gg.nq1 + qq) * W2n) * nw2
-                              : Xbox + (((size_t)mat * W1n + gg.q1s + qq) * W2n) * nw2;
+      for (int row = g; row < nbrows + (win ? nwrows : 0); row += B) {
+        if (row < nbrows) {
+          const int mat = row / nq1, qq = row % nq1;
+          const V* X = box_sm ? Xbox + (((size_t)mat * nq1 + qq) * W2n) * nw2
+                              : Xbox + (((size_t)mat * W1n + q1s + qq) * W2n) * nw2;
           V acc[EPT];
 #pragma unroll
           for (int u = 0; u < EPT; ++u) acc[u] = vzero;
+#pragma unroll(kBox ? (WBc + 3) / 4 : 1)
           for (int q0 = 0; q0 < W2n; q0 += 4) {
             V xv[4][EPT];
 #pragma unroll
@@ -343,7 +360,7 @@ __device__ __forceinline__ void group_vctas(const SolveTables& t, const GroupDat
           for (int u = 0; u < EPT; ++u)
             if (actu[u]) Gd[(size_t)row * nw2 + eu[u]] = acc[u];
         } else {
-          const int wr = row - gg.nbrows;  // a * 4 + q1
+          const int wr = row - nbrows;  // a * 4 + q1
           const double2* X = Xwin + (size_t)wr * 4 * nw2;
 #pragma unroll
           for (int u = 0; u < EPT; ++u)
@@ -370,10 +387,11 @@ __device__ __forceinline__ void group_vctas(const SolveTables& t, const GroupDat
       }
       const V* p1 = pw1 + (s % ring) * B * W1 + g * W1;
       const V* Gd = Gb + (s % gbufs) * gbuf;
+#pragma unroll(kBox ? WBc : 1)
       for (int q1 = 0; q1 < W1n; ++q1) {
         const V ph = p1[q1];
-        const bool neg = q1 < gg.q1s;  // G(-n1) = G(n1)^+
-        const int row = neg ? (W1n - 1 - q1) - gg.q1s : q1 - gg.q1s;
+        const bool neg = q1 < q1s;  // G(-n1) = G(n1)^+
+        const int row = neg ? (W1n - 1 - q1) - q1s : q1 - q1s;
 #pragma unroll
         for (int u = 0; u < EPT; ++u)
           if (actu[u]) {
@@ -384,7 +402,7 @@ __device__ __forceinline__ void group_vctas(const SolveTables& t, const GroupDat
 #pragma unroll
             for (int a = 0; a < 3; ++a)
               if (a < nax) {
-                V rv = Gd[(size_t)((1 + a) * gg.nq1 + row) * nw2 + el];
+                V rv = Gd[(size_t)((1 + a) * nq1 + row) * nw2 + el];
                 if (neg) rv = conjugate(rv);
                 rko[a][u] = fmac(ph, rv, rko[a][u]);
               }
@@ -610,16 +628,16 @@ __device__ __forceinline__ GroupData<Real> group_data(const GroupTables& gt) {
 }
 
 // One solve: physical CTA b runs virtual CTAs b, b + gridDim.x, ...
-template <typename Real, int EPT, int NWc, int NAXc, int NJc, bool KM = false>
+template <typename Real, int EPT, int NWc, int NAXc, int NJc, bool KM = false, int WBc = 0>
 __global__ void __launch_bounds__(group_threads<EPT>(), 1)
     propagate_group_kernel(SolveTables t, GroupData<Real> d, int B, int G, int box_sm, int win_sm, int vctas,
                            double2* rho, double2* Jpart) {
-  group_vctas<Real, EPT, NWc, NAXc, NJc, KM>(t, d, B, G, box_sm, win_sm, blockIdx.x, gridDim.x, vctas, rho, Jpart);
+  group_vctas<Real, EPT, NWc, NAXc, NJc, KM, WBc>(t, d, B, G, box_sm, win_sm, blockIdx.x, gridDim.x, vctas, rho, Jpart);
 }
 
 // Many solves of one kernel shape: persistent CTAs take (solve, virtual CTA) items from a packed
 // work list through an atomic counter.  Which CTA runs an item does not change its result.
-template <typename Real, int EPT, int NWc, int NAXc, int NJc, bool KM = false>
+template <typename Real, int EPT, int NWc, int NAXc, int NJc, bool KM = false, int WBc = 0>
 __global__ void __launch_bounds__(group_threads<EPT>(), 1)
     propagate_group_batch_kernel(const BatchDesc* descs, const int2* items, int nitems, int* counter) {
   __shared__ int s_item;
@@ -633,7 +651,7 @@ __global__ void __launch_bounds__(group_threads<EPT>(), 1)
     // The descriptor in registers (read-only, uniform across the CTA): the hot loop reads its fields
     // every step, which would be shared-memory loads if it stayed in shared memory.
     const BatchDesc dsc = descs[w.x];
-    group_vctas<Real, EPT, NWc, NAXc, NJc, KM>(dsc.t, group_data<Real>(dsc.gt), dsc.B, dsc.G, dsc.box_sm, dsc.win_sm,
+    group_vctas<Real, EPT, NWc, NAXc, NJc, KM, WBc>(dsc.t, group_data<Real>(dsc.gt), dsc.B, dsc.G, dsc.box_sm, dsc.win_sm,
                                                w.y, dsc.vctas, dsc.vctas, dsc.rho, dsc.Jpart);
     __syncthreads();
   }
@@ -641,17 +659,10 @@ __global__ void __launch_bounds__(group_threads<EPT>(), 1)
 
 constexpr size_t kSmemMax = 220 * 1024;
 
-template <typename Real, int EPT, int NWc, int NAXc, int NJc, bool KM = false>
+template <typename Real, int EPT, int NWc, int NAXc, int NJc, bool KM = false, int WBc = 0>
 bool plan_group_t(const SolveTables& t, int sm_count, LaunchShape* out, char* why, int why_len, int tile_hint) {
   const GroupGeom gg = group_geom(t);
-  const int per = (t.nw2 + EPT - 1) / EPT;  // threads needed per k-point
-  int G;
-  if (per <= 32) {
-    G = 1;
-    while (G < per) G <<= 1;
-  } else {
-    G = (per + 31) / 32 * 32;
-  }
+  const int G = group_size(t.nw2, EPT);
   const int step = G < 32 ? 32 / G : 1;  // whole warps per CTA
   int Bmax = group_threads<EPT>() / G;
   if (G > 32 && Bmax > 15) Bmax = 15;  // one named barrier per group, ids 1..15
@@ -676,7 +687,7 @@ bool plan_group_t(const SolveTables& t, int sm_count, LaunchShape* out, char* wh
   if (bytes(best, true, true) > kSmemMax) win_sm = 0;
   if (bytes(best, true, win_sm) > kSmemMax) box_sm = 0;
   if (!box_sm && bytes(best, false, true) <= kSmemMax) win_sm = 1;
-  auto kern = propagate_group_kernel<Real, EPT, NWc, NAXc, NJc, KM>;
+  auto kern = propagate_group_kernel<Real, EPT, NWc, NAXc, NJc, KM, WBc>;
   const size_t smem_max = bytes(best, box_sm, win_sm);
   cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_max);
   int occ = 0;
@@ -700,7 +711,7 @@ bool plan_group_t(const SolveTables& t, int sm_count, LaunchShape* out, char* wh
   return true;
 }
 
-template <typename Real, int EPT, int NWc, int NAXc, int NJc, bool KM = false>
+template <typename Real, int EPT, int NWc, int NAXc, int NJc, bool KM = false, int WBc = 0>
 void launch_group_t(const SolveTables& t, const GroupTables& gt, const LaunchShape& s, double2* rho, double2* Jpart,
                     cudaStream_t stream) {
   GroupData<Real> d;
@@ -709,15 +720,15 @@ void launch_group_t(const SolveTables& t, const GroupTables& gt, const LaunchSha
   } else {
     d = {gt.Xbox32, gt.P32, gt.T1_32, gt.T2_32, gt.Xwin64, gt.P64, gt.T1_64, gt.T2_64};
   }
-  auto kern = propagate_group_kernel<Real, EPT, NWc, NAXc, NJc, KM>;
+  auto kern = propagate_group_kernel<Real, EPT, NWc, NAXc, NJc, KM, WBc>;
   cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s.smem);
   kern<<<s.ctas, s.threads, s.smem, stream>>>(t, d, s.k_per_cta, s.group, s.box_sm, s.win_sm, s.vctas, rho, Jpart);
 }
 
-template <typename Real, int EPT, int NWc, int NAXc, int NJc, bool KM = false>
+template <typename Real, int EPT, int NWc, int NAXc, int NJc, bool KM = false, int WBc = 0>
 int launch_group_batch_t(const BatchDesc* descs, const int2* items, int nitems, int* counter, int threads, size_t smem,
                          int sm_count, cudaStream_t stream) {
-  auto kern = propagate_group_batch_kernel<Real, EPT, NWc, NAXc, NJc, KM>;
+  auto kern = propagate_group_batch_kernel<Real, EPT, NWc, NAXc, NJc, KM, WBc>;
   cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   int occ = 0;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, threads, smem);
@@ -734,30 +745,43 @@ using PlanFn = bool (*)(const SolveTables&, int, LaunchShape*, char*, int, int);
 using LaunchFn = void (*)(const SolveTables&, const GroupTables&, const LaunchShape&, double2*, double2*, cudaStream_t);
 using BatchFn = int (*)(const BatchDesc*, const int2*, int, int*, int, size_t, int, cudaStream_t);
 struct GroupVariant {
-  int precision, nw, nax, nj;
+  int precision, nw, nax, nj, wb;  // wb > 0: square wb x wb cell box with Hermitian halving
   PlanFn plan;
   LaunchFn launch;
   BatchFn batch;
 };
-#define HHG_GROUP_VARIANT(P, R, E, NW, NAX, NJ) \
-  {P, NW, NAX, NJ, plan_group_t<R, E, NW, NAX, NJ>, launch_group_t<R, E, NW, NAX, NJ>, \
-   launch_group_batch_t<R, E, NW, NAX, NJ>}
+#define HHG_GROUP_VARIANT(P, R, E, NW, NAX, NJ, WB)                                                \
+  {P, NW, NAX, NJ, WB, plan_group_t<R, E, NW, NAX, NJ, false, WB>, launch_group_t<R, E, NW, NAX, NJ, false, WB>, \
+   launch_group_batch_t<R, E, NW, NAX, NJ, false, WB>}
+// Listed before the any-box variants of the same shape, which they take precedence over.
 const GroupVariant kGroupVariants[] = {
-    HHG_GROUP_VARIANT(0, double, 1, 11, 1, 2), HHG_GROUP_VARIANT(0, double, 1, 11, 2, 2),
-    HHG_GROUP_VARIANT(0, double, 1, 12, 1, 2), HHG_GROUP_VARIANT(0, double, 1, 12, 2, 2),
-    HHG_GROUP_VARIANT(0, double, 1, 6, 1, 2),  HHG_GROUP_VARIANT(0, double, 1, 6, 2, 2),
-    HHG_GROUP_VARIANT(1, float, 2, 11, 1, 2),  HHG_GROUP_VARIANT(1, float, 2, 11, 2, 2),
-    HHG_GROUP_VARIANT(1, float, 2, 12, 1, 2),  HHG_GROUP_VARIANT(1, float, 2, 12, 2, 2),
-    HHG_GROUP_VARIANT(1, float, 1, 6, 1, 2),   HHG_GROUP_VARIANT(1, float, 1, 6, 2, 2),
-    HHG_GROUP_VARIANT(1, float, 1, 2, 1, 2),   HHG_GROUP_VARIANT(1, float, 1, 2, 2, 2),
+    HHG_GROUP_VARIANT(0, double, 1, 11, 1, 2, 7), HHG_GROUP_VARIANT(0, double, 1, 11, 2, 2, 7),
+    HHG_GROUP_VARIANT(0, double, 1, 12, 1, 2, 7), HHG_GROUP_VARIANT(0, double, 1, 12, 2, 2, 7),
+    HHG_GROUP_VARIANT(1, float, 2, 11, 1, 2, 7),  HHG_GROUP_VARIANT(1, float, 2, 11, 2, 2, 7),
+    HHG_GROUP_VARIANT(1, float, 2, 12, 1, 2, 7),  HHG_GROUP_VARIANT(1, float, 2, 12, 2, 2, 7),
+    HHG_GROUP_VARIANT(0, double, 1, 11, 1, 2, 0), HHG_GROUP_VARIANT(0, double, 1, 11, 2, 2, 0),
+    HHG_GROUP_VARIANT(0, double, 1, 12, 1, 2, 0), HHG_GROUP_VARIANT(0, double, 1, 12, 2, 2, 0),
+    HHG_GROUP_VARIANT(0, double, 1, 6, 1, 2, 0),  HHG_GROUP_VARIANT(0, double, 1, 6, 2, 2, 0),
+    HHG_GROUP_VARIANT(1, float, 2, 11, 1, 2, 0),  HHG_GROUP_VARIANT(1, float, 2, 11, 2, 2, 0),
+    HHG_GROUP_VARIANT(1, float, 2, 12, 1, 2, 0),  HHG_GROUP_VARIANT(1, float, 2, 12, 2, 2, 0),
+    HHG_GROUP_VARIANT(1, float, 1, 6, 1, 2, 0),   HHG_GROUP_VARIANT(1, float, 1, 6, 2, 2, 0),
+    HHG_GROUP_VARIANT(1, float, 1, 2, 1, 2, 0),   HHG_GROUP_VARIANT(1, float, 1, 2, 2, 2, 0),
 };
 #undef HHG_GROUP_VARIANT
 
 const GroupVariant* find_variant(const SolveTables& t, int precision) {
   if (const char* env = std::getenv("HHG_GROUP_GENERIC"))
     if (env[0] == '1') return nullptr;  // tuning override: runtime-shaped instance
-  for (const GroupVariant& v : kGroupVariants)
-    if (v.precision == precision && v.nw == t.nw && v.nax == t.nax && v.nj == t.nj) return &v;
+  const bool any_box = [] {
+    const char* env = std::getenv("HHG_GROUP_ANYBOX");  // tuning override: skip the fixed-box variants
+    return env && env[0] == '1';
+  }();
+  const GroupGeom gg = group_geom(t);
+  for (const GroupVariant& v : kGroupVariants) {
+    if (v.precision != precision || v.nw != t.nw || v.nax != t.nax || v.nj != t.nj) continue;
+    if (v.wb > 0 && (any_box || !gg.half || t.b1n != v.wb || t.b2n != v.wb)) continue;
+    return &v;
+  }
   return nullptr;
 }
 
