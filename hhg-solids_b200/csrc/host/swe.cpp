@@ -903,7 +903,7 @@ long long SWESim_h2d_bytes(SWESim* swe) { return swe ? (long long)swe->h2d_bytes
 int SWESim_launch_shape(SWESim* swe, int* ctas, int* threads, int* k_per_cta, long long* smem) {
   if (!swe || !swe->ready) return -1;
   if (ctas) *ctas = swe->shape.ctas;
-  if (threads) *threads = swe->shape.k_per_cta * swe->shape.group;
+  if (threads) *threads = swe->shape.threads;
   if (k_per_cta) *k_per_cta = swe->shape.k_per_cta;
   if (smem) *smem = (long long)swe->shape.smem;
   return swe->shape.kernel;

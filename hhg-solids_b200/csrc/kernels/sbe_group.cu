@@ -142,12 +142,13 @@ struct GroupLayout {
   using V = typename Cx<Real>::T;
   size_t groups, tw1, tw2, pw1, pw2, G, Xbox, total_cx;
   size_t wtw1, wtw2, wpw1, wpw2, GW, Xwin, total_dcx, sJ_doubles;
+  // kstride: complex values per k-point in the per-k-point area (3 nw2, or three padded tiles).
   __host__ __device__ GroupLayout(const SolveTables& t, const GroupGeom& gg, int B, int nwarps, bool box_sm,
-                                  bool win_sm) {
+                                  bool win_sm, int kstride) {
     const size_t nw2 = t.nw2, W1 = gg.W1n, W2 = gg.W2n;
     size_t p = 0;
     groups = p;
-    p += (size_t)B * 3 * nw2;
+    p += (size_t)B * kstride;
     tw1 = p;
     p += (size_t)B * W1;
     tw2 = p;
@@ -202,7 +203,14 @@ struct GroupData {
 // NWc, NAXc, NJc: orbital count, field axes and current axes fixed at compile time (0: read from t).
 // WBc > 0: a square WBc x WBc cell box with Hermitian halving, fixed at compile time, so that the
 // Wannier-sum loops unroll with constant offsets.
-template <typename Real, int EPT, int NWc, int NAXc, int NJc, bool KM, int WBc = 0>
+// KP (k-point pairs; mixed form, Hermitian, compile-time orbital count): a group of threads holds two
+// k-points, thread e0 owning element e0 of both, so each load of an inner Wannier sum G(n1) or of a
+// window row serves two k-points; the commutator's product H X is formed in 2x2 register tiles from
+// a column-major H and a row-major X padded to an even side NP (one 16-byte load of two H values
+// and one of two X values per four complex multiply-adds), then read back by the element owners.
+// Rows are NP + 2 values apart, an odd number of 16-byte units, which spreads the transposed
+// accesses of the owners over the banks.
+template <typename Real, int EPT, int NWc, int NAXc, int NJc, bool KM, int WBc = 0, bool KP = false>
 __device__ __forceinline__ void group_vctas(const SolveTables& t, const GroupData<Real>& d, int B, int G_in, int box_sm,
                                             int win_sm, int v_first, int v_step, int vctas, double2* rho,
                                             double2* Jpart) {
@@ -210,16 +218,21 @@ __device__ __forceinline__ void group_vctas(const SolveTables& t, const GroupDat
   extern __shared__ __align__(16) unsigned char smraw[];
   const GroupGeom gg = group_geom(t);
   const int nw = NWc ? NWc : t.nw, nw2 = nw * nw, nax = NAXc ? NAXc : t.nax, nj = NJc ? NJc : t.nj;
-  constexpr int Gc = NWc ? group_size(NWc * NWc, EPT) : 0;
+  static_assert(!KP || (EPT == 2 && NWc > 0 && sizeof(Real) == 4 && !KM), "k-point pairs: mixed form, fixed shape");
+  constexpr int KPG = KP ? 2 : 1;                      // k-points per thread group
+  constexpr int EU = KP ? 1 : EPT;                     // distinct elements per thread
+  constexpr int NP = KP ? (NWc + 1) / 2 * 2 : 1;       // padded side of the tile layout
+  constexpr int NS = NP + 2;                           // its row stride: an odd number of 16-byte units
+  constexpr int Gc = NWc ? group_size(NWc * NWc, EU) : 0;
   const int G = Gc ? Gc : G_in;
   const int nthr = blockDim.x, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarps = (nthr + 31) >> 5;
-  const int g = tid / G, e0 = tid % G;
-  // This thread owns elements e0 + u*G, u < EPT.
+  const int g = tid / G, e0 = tid % G, ngroups = B / KPG;
+  // Slot u of this thread: element e0 + u*G of k-point g, or (KP) element e0 of k-point 2g + u.
   int eu[EPT], iu[EPT], ju[EPT], eTu[EPT];
   bool actu[EPT];
 #pragma unroll
   for (int u = 0; u < EPT; ++u) {
-    eu[u] = e0 + u * G;
+    eu[u] = KP ? e0 : e0 + u * G;
     actu[u] = eu[u] < nw2;
     iu[u] = actu[u] ? eu[u] / nw : 0;
     ju[u] = actu[u] ? eu[u] % nw : 0;
@@ -229,10 +242,11 @@ __device__ __forceinline__ void group_vctas(const SolveTables& t, const GroupDat
   const int W1n = kBox ? WBc : gg.W1n, W2n = kBox ? WBc : gg.W2n, W1 = W1n, W2 = W2n;
   const int q1s = kBox ? (WBc - 1) / 2 : gg.q1s, nq1 = kBox ? WBc - (WBc - 1) / 2 : gg.nq1;
   const int nmat = NAXc ? 1 + NAXc : gg.nmat, nbrows = nmat * nq1, nwrows = NJc ? 4 * NJc : gg.nwrows;
-  const GroupLayout<Real> L(t, gg, B, nwarps, box_sm, win_sm);
+  const int kstride = KP ? 3 * NP * NS : 3 * nw2;
+  const GroupLayout<Real> L(t, gg, B, nwarps, box_sm, win_sm, kstride);
   V* sm = reinterpret_cast<V*>(smraw);
   double2* dsm = reinterpret_cast<double2*>(sm + L.total_cx);
-  V* Hs = sm + L.groups + (size_t)g * 3 * nw2;
+  V* Hs = sm + L.groups + (size_t)g * KPG * kstride;
   V* Xs = Hs + nw2;
   V* HXs = Xs + nw2;
   V* tw1 = sm + L.tw1;
@@ -268,21 +282,24 @@ __device__ __forceinline__ void group_vctas(const SolveTables& t, const GroupDat
   }
   if (win_sm)
     for (size_t idx = tid; idx < (size_t)nj * 16 * nw2; idx += nthr) dsm[L.Xwin + idx] = d.Xwin[idx];
+  // Tile layout: the padding rows and columns are never written and must read as zero.
+  if (KP)
+    for (size_t idx = tid; idx < (size_t)B * kstride; idx += nthr) sm[L.groups + idx] = vzero;
 
   // Virtual CTA v owns tiles v, v + vctas, ... and its own row of current partials, so the result
   // does not depend on how many physical CTAs share the work.
   for (int v = v_first; v < vctas; v += v_step)
   for (int tile = v; tile < ntiles; tile += vctas) {
     const int m2 = tile / bpc, m10 = t.row0 + (tile % bpc) * B;
-    const int m1 = m10 + g;
-    const bool kval = m1 < t.row1;
-    const size_t k = (size_t)m1 * t.N2 + m2;
     bool own[EPT];
+    size_t kk[EPT];
     double2 r[EPT];
 #pragma unroll
     for (int u = 0; u < EPT; ++u) {
-      own[u] = actu[u] && kval;
-      r[u] = own[u] ? rho[k * nw2 + eu[u]] : make_double2(0.0, 0.0);
+      const int m1 = m10 + (KP ? KPG * g + u : g);
+      kk[u] = (size_t)m1 * t.N2 + m2;
+      own[u] = actu[u] && m1 < t.row1;
+      r[u] = own[u] ? rho[kk[u] * nw2 + eu[u]] : make_double2(0.0, 0.0);
     }
 
     // Twiddles e^{-2 pi i m n / N} of the box offsets, and (FP64) of the window offsets -2..1.
@@ -334,36 +351,36 @@ __device__ __forceinline__ void group_vctas(const SolveTables& t, const GroupDat
       const double2* w2 = wpw2 + (s % ring) * 4;
       V* Gd = Gb + (s % gbufs) * gbuf;
       double2* GWd = GWb + (s & 1) * wbuf;
-      for (int row = g; row < nbrows + (win ? nwrows : 0); row += B) {
+      for (int row = g; row < nbrows + (win ? nwrows : 0); row += ngroups) {
         if (row < nbrows) {
           const int mat = row / nq1, qq = row % nq1;
           const V* X = box_sm ? Xbox + (((size_t)mat * nq1 + qq) * W2n) * nw2
                               : Xbox + (((size_t)mat * W1n + q1s + qq) * W2n) * nw2;
           V acc[EPT];
 #pragma unroll
-          for (int u = 0; u < EPT; ++u) acc[u] = vzero;
+          for (int u = 0; u < EU; ++u) acc[u] = vzero;
 #pragma unroll(kBox ? (WBc + 3) / 4 : 1)
           for (int q0 = 0; q0 < W2n; q0 += 4) {
             V xv[4][EPT];
 #pragma unroll
             for (int q = 0; q < 4; ++q)
 #pragma unroll
-              for (int u = 0; u < EPT; ++u)
+              for (int u = 0; u < EU; ++u)
                 if (q0 + q < W2n && actu[u]) xv[q][u] = X[(size_t)(q0 + q) * nw2 + eu[u]];
 #pragma unroll
             for (int q = 0; q < 4; ++q)
 #pragma unroll
-              for (int u = 0; u < EPT; ++u)
+              for (int u = 0; u < EU; ++u)
                 if (q0 + q < W2n && actu[u]) acc[u] = fmac(q2[q0 + q], xv[q][u], acc[u]);
           }
 #pragma unroll
-          for (int u = 0; u < EPT; ++u)
+          for (int u = 0; u < EU; ++u)
             if (actu[u]) Gd[(size_t)row * nw2 + eu[u]] = acc[u];
         } else {
           const int wr = row - nbrows;  // a * 4 + q1
           const double2* X = Xwin + (size_t)wr * 4 * nw2;
 #pragma unroll
-          for (int u = 0; u < EPT; ++u)
+          for (int u = 0; u < EU; ++u)
             if (actu[u]) {
               double2 xv[4], wacc = make_double2(0.0, 0.0);
 #pragma unroll
@@ -385,28 +402,47 @@ __device__ __forceinline__ void group_vctas(const SolveTables& t, const GroupDat
 #pragma unroll
         for (int a = 0; a < 3; ++a) rko[a][u] = vzero;
       }
-      const V* p1 = pw1 + (s % ring) * B * W1 + g * W1;
+      const V* p1 = pw1 + (s % ring) * B * W1 + g * KPG * W1;
       const V* Gd = Gb + (s % gbufs) * gbuf;
 #pragma unroll(kBox ? WBc : 1)
       for (int q1 = 0; q1 < W1n; ++q1) {
         const V ph = p1[q1];
         const bool neg = q1 < q1s;  // G(-n1) = G(n1)^+
         const int row = neg ? (W1n - 1 - q1) - q1s : q1 - q1s;
-#pragma unroll
-        for (int u = 0; u < EPT; ++u)
-          if (actu[u]) {
-            const int el = neg ? eTu[u] : eu[u];
+        if constexpr (KP) {
+          const V ph1 = p1[W1 + q1];
+          if (actu[0]) {
+            const int el = neg ? eTu[0] : eu[0];
             V gv = Gd[(size_t)row * nw2 + el];
             if (neg) gv = conjugate(gv);
-            h0o[u] = fmac(ph, gv, h0o[u]);
+            h0o[0] = fmac(ph, gv, h0o[0]);
+            h0o[1] = fmac(ph1, gv, h0o[1]);
 #pragma unroll
             for (int a = 0; a < 3; ++a)
               if (a < nax) {
                 V rv = Gd[(size_t)((1 + a) * nq1 + row) * nw2 + el];
                 if (neg) rv = conjugate(rv);
-                rko[a][u] = fmac(ph, rv, rko[a][u]);
+                rko[a][0] = fmac(ph, rv, rko[a][0]);
+                rko[a][1] = fmac(ph1, rv, rko[a][1]);
               }
           }
+        } else {
+#pragma unroll
+          for (int u = 0; u < EPT; ++u)
+            if (actu[u]) {
+              const int el = neg ? eTu[u] : eu[u];
+              V gv = Gd[(size_t)row * nw2 + el];
+              if (neg) gv = conjugate(gv);
+              h0o[u] = fmac(ph, gv, h0o[u]);
+#pragma unroll
+              for (int a = 0; a < 3; ++a)
+                if (a < nax) {
+                  V rv = Gd[(size_t)((1 + a) * nq1 + row) * nw2 + el];
+                  if (neg) rv = conjugate(rv);
+                  rko[a][u] = fmac(ph, rv, rko[a][u]);
+                }
+            }
+        }
       }
     };
     // Outer sum of the window velocity of point s: W_a(k).
@@ -417,16 +453,28 @@ __device__ __forceinline__ void group_vctas(const SolveTables& t, const GroupDat
 #pragma unroll
         for (int a = 0; a < 3; ++a) wk[a][u] = make_double2(0.0, 0.0);
       const double2* GWd = GWb + (s & 1) * wbuf;
-      const double2* w1 = wpw1 + (s % ring) * B * 4 + g * 4;
+      const double2* w1 = wpw1 + (s % ring) * B * 4 + g * KPG * 4;
 #pragma unroll
       for (int q1 = 0; q1 < 4; ++q1) {
         const double2 ph = w1[q1];
-#pragma unroll
-        for (int u = 0; u < EPT; ++u)
-          if (actu[u])
+        if constexpr (KP) {
+          const double2 ph1 = w1[4 + q1];
+          if (actu[0])
 #pragma unroll
             for (int a = 0; a < 3; ++a)
-              if (a < nj) wk[a][u] = fmac(ph, GWd[(size_t)(a * 4 + q1) * nw2 + eu[u]], wk[a][u]);
+              if (a < nj) {
+                const double2 gw = GWd[(size_t)(a * 4 + q1) * nw2 + eu[0]];
+                wk[a][0] = fmac(ph, gw, wk[a][0]);
+                wk[a][1] = fmac(ph1, gw, wk[a][1]);
+              }
+        } else {
+#pragma unroll
+          for (int u = 0; u < EPT; ++u)
+            if (actu[u])
+#pragma unroll
+              for (int a = 0; a < 3; ++a)
+                if (a < nj) wk[a][u] = fmac(ph, GWd[(size_t)(a * 4 + q1) * nw2 + eu[u]], wk[a][u]);
+        }
       }
     };
     // H0(k), r_a(k) of the point of stage 0 (k-space solver: carried from the previous step's stage 3).
@@ -506,12 +554,49 @@ __device__ __forceinline__ void group_vctas(const SolveTables& t, const GroupDat
               x.x = r[u].x + cs * (double)K[u].x;
               x.y = r[u].y + cs * (double)K[u].y;
             }
-            Hs[eu[u]] = hs;
-            Xs[eu[u]] = Cx<Real>::make((Real)x.x, (Real)x.y);
+            if constexpr (KP) {
+              V* base = Hs + u * kstride;
+              base[ju[u] * NS + iu[u]] = hs;                                        // H column-major
+              base[NP * NS + iu[u] * NS + ju[u]] = Cx<Real>::make((Real)x.x, (Real)x.y);  // X row-major
+            } else {
+              Hs[eu[u]] = hs;
+              Xs[eu[u]] = Cx<Real>::make((Real)x.x, (Real)x.y);
+            }
           }
         group_sync(g, G);
         V hx[EPT];
-        if (t.hermitian) {
+        if constexpr (KP) {
+          // 2x2 tiles of H X: tile p of the pair's 2 (NP/2)^2 covers rows 2ti, 2ti+1, columns 2tj, 2tj+1.
+          constexpr int NT = NP / 2;
+          if (e0 < KPG * NT * NT) {
+            const int pk = e0 / (NT * NT), pt = e0 % (NT * NT), ti = pt / NT, tj = pt % NT;
+            V* base = Hs + pk * kstride;
+            const float4* HT4 = reinterpret_cast<const float4*>(base) + ti;
+            const float4* XP4 = reinterpret_cast<const float4*>(base + NP * NS) + tj;
+            V c00 = vzero, c01 = vzero, c10 = vzero, c11 = vzero;
+#pragma unroll
+            for (int l = 0; l < NWc; ++l) {
+              const float4 hv = HT4[l * (NS / 2)], xv = XP4[l * (NS / 2)];
+              const V h0v = Cx<Real>::make(hv.x, hv.y), h1v = Cx<Real>::make(hv.z, hv.w);
+              const V x0v = Cx<Real>::make(xv.x, xv.y), x1v = Cx<Real>::make(xv.z, xv.w);
+              c00 = fmac(h0v, x0v, c00);
+              c01 = fmac(h0v, x1v, c01);
+              c10 = fmac(h1v, x0v, c10);
+              c11 = fmac(h1v, x1v, c11);
+            }
+            float4* HX4 = reinterpret_cast<float4*>(base + 2 * NP * NS);
+            HX4[(2 * ti) * (NS / 2) + tj] = make_float4(c00.x, c00.y, c01.x, c01.y);
+            HX4[(2 * ti + 1) * (NS / 2) + tj] = make_float4(c10.x, c10.y, c11.x, c11.y);
+          }
+          group_sync(g, G);
+#pragma unroll
+          for (int u = 0; u < EPT; ++u)
+            if (actu[u]) {
+              const V* HXP = Hs + u * kstride + 2 * NP * NS;
+              const V hv = HXP[iu[u] * NS + ju[u]], ht = HXP[ju[u] * NS + iu[u]];
+              K[u] = Cx<Real>::make(hv.y + ht.y, -(hv.x - ht.x));  // -i (HX - (HX)^+)
+            }
+        } else if (t.hermitian) {
 #pragma unroll
           for (int u = 0; u < EPT; ++u) {
             hx[u] = vzero;
@@ -611,7 +696,7 @@ __device__ __forceinline__ void group_vctas(const SolveTables& t, const GroupDat
     }
 #pragma unroll
     for (int u = 0; u < EPT; ++u)
-      if (own[u]) rho[k * nw2 + eu[u]] = r[u];
+      if (own[u]) rho[kk[u] * nw2 + eu[u]] = r[u];
     __syncthreads();
   }
 }
@@ -628,16 +713,16 @@ __device__ __forceinline__ GroupData<Real> group_data(const GroupTables& gt) {
 }
 
 // One solve: physical CTA b runs virtual CTAs b, b + gridDim.x, ...
-template <typename Real, int EPT, int NWc, int NAXc, int NJc, bool KM = false, int WBc = 0>
+template <typename Real, int EPT, int NWc, int NAXc, int NJc, bool KM = false, int WBc = 0, bool KP = false>
 __global__ void __launch_bounds__(group_threads<EPT>(), 1)
     propagate_group_kernel(SolveTables t, GroupData<Real> d, int B, int G, int box_sm, int win_sm, int vctas,
                            double2* rho, double2* Jpart) {
-  group_vctas<Real, EPT, NWc, NAXc, NJc, KM, WBc>(t, d, B, G, box_sm, win_sm, blockIdx.x, gridDim.x, vctas, rho, Jpart);
+  group_vctas<Real, EPT, NWc, NAXc, NJc, KM, WBc, KP>(t, d, B, G, box_sm, win_sm, blockIdx.x, gridDim.x, vctas, rho, Jpart);
 }
 
 // Many solves of one kernel shape: persistent CTAs take (solve, virtual CTA) items from a packed
 // work list through an atomic counter.  Which CTA runs an item does not change its result.
-template <typename Real, int EPT, int NWc, int NAXc, int NJc, bool KM = false, int WBc = 0>
+template <typename Real, int EPT, int NWc, int NAXc, int NJc, bool KM = false, int WBc = 0, bool KP = false>
 __global__ void __launch_bounds__(group_threads<EPT>(), 1)
     propagate_group_batch_kernel(const BatchDesc* descs, const int2* items, int nitems, int* counter) {
   __shared__ int s_item;
@@ -651,7 +736,7 @@ __global__ void __launch_bounds__(group_threads<EPT>(), 1)
     // The descriptor in registers (read-only, uniform across the CTA): the hot loop reads its fields
     // every step, which would be shared-memory loads if it stayed in shared memory.
     const BatchDesc dsc = descs[w.x];
-    group_vctas<Real, EPT, NWc, NAXc, NJc, KM, WBc>(dsc.t, group_data<Real>(dsc.gt), dsc.B, dsc.G, dsc.box_sm, dsc.win_sm,
+    group_vctas<Real, EPT, NWc, NAXc, NJc, KM, WBc, KP>(dsc.t, group_data<Real>(dsc.gt), dsc.B, dsc.G, dsc.box_sm, dsc.win_sm,
                                                w.y, dsc.vctas, dsc.vctas, dsc.rho, dsc.Jpart);
     __syncthreads();
   }
@@ -659,21 +744,23 @@ __global__ void __launch_bounds__(group_threads<EPT>(), 1)
 
 constexpr size_t kSmemMax = 220 * 1024;
 
-template <typename Real, int EPT, int NWc, int NAXc, int NJc, bool KM = false, int WBc = 0>
+template <typename Real, int EPT, int NWc, int NAXc, int NJc, bool KM = false, int WBc = 0, bool KP = false>
 bool plan_group_t(const SolveTables& t, int sm_count, LaunchShape* out, char* why, int why_len, int tile_hint) {
   const GroupGeom gg = group_geom(t);
-  const int G = group_size(t.nw2, EPT);
-  const int step = G < 32 ? 32 / G : 1;  // whole warps per CTA
-  int Bmax = group_threads<EPT>() / G;
-  if (G > 32 && Bmax > 15) Bmax = 15;  // one named barrier per group, ids 1..15
+  constexpr int KPG = KP ? 2 : 1;  // k-points per thread group
+  const int G = group_size(t.nw2, KP ? 1 : EPT);
+  const int step = (G < 32 ? 32 / G : 1) * KPG;  // whole warps (and whole groups) per CTA
+  int Bmax = group_threads<EPT>() / G * KPG;
+  if (G > 32 && Bmax > 15 * KPG) Bmax = 15 * KPG;  // one named barrier per group, ids 1..15
   Bmax = Bmax / step * step;
+  const int kstride = KP ? 3 * ((t.nw + 1) / 2 * 2) * ((t.nw + 1) / 2 * 2 + 2) : 3 * t.nw2;
   if (Bmax < 1) {
     snprintf(why, why_len, "num_orb=%d needs %d threads per k-point", t.nw, G);
     return false;
   }
   // Shared-memory placement of the tables: both, box only, none.
   auto bytes = [&](int B, bool bs, bool ws) {
-    return GroupLayout<Real>(t, gg, B, (B * G + 31) / 32, bs, ws).bytes();
+    return GroupLayout<Real>(t, gg, B, (B / KPG * G + 31) / 32, bs, ws, kstride).bytes();
   };
   int box_sm = 1, win_sm = 1;
   while (Bmax > step && bytes(Bmax, false, false) > kSmemMax) Bmax -= step;
@@ -687,11 +774,11 @@ bool plan_group_t(const SolveTables& t, int sm_count, LaunchShape* out, char* wh
   if (bytes(best, true, true) > kSmemMax) win_sm = 0;
   if (bytes(best, true, win_sm) > kSmemMax) box_sm = 0;
   if (!box_sm && bytes(best, false, true) <= kSmemMax) win_sm = 1;
-  auto kern = propagate_group_kernel<Real, EPT, NWc, NAXc, NJc, KM, WBc>;
+  auto kern = propagate_group_kernel<Real, EPT, NWc, NAXc, NJc, KM, WBc, KP>;
   const size_t smem_max = bytes(best, box_sm, win_sm);
   cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_max);
   int occ = 0;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, best * G, smem_max);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, best / KPG * G, smem_max);
   if (occ < 1) occ = 1;
   const long slots = (long)occ * sm_count;
   const int rows = t.row1 - t.row0;
@@ -701,7 +788,7 @@ bool plan_group_t(const SolveTables& t, int sm_count, LaunchShape* out, char* wh
   out->ept = EPT;
   out->k_per_cta = best;
   out->group = G;
-  out->threads = best * G;
+  out->threads = best / KPG * G;
   out->ntiles = (int)ntiles;
   out->ctas = (int)(ntiles < slots ? ntiles : slots);
   out->vctas = out->ctas;
@@ -711,7 +798,7 @@ bool plan_group_t(const SolveTables& t, int sm_count, LaunchShape* out, char* wh
   return true;
 }
 
-template <typename Real, int EPT, int NWc, int NAXc, int NJc, bool KM = false, int WBc = 0>
+template <typename Real, int EPT, int NWc, int NAXc, int NJc, bool KM = false, int WBc = 0, bool KP = false>
 void launch_group_t(const SolveTables& t, const GroupTables& gt, const LaunchShape& s, double2* rho, double2* Jpart,
                     cudaStream_t stream) {
   GroupData<Real> d;
@@ -720,15 +807,15 @@ void launch_group_t(const SolveTables& t, const GroupTables& gt, const LaunchSha
   } else {
     d = {gt.Xbox32, gt.P32, gt.T1_32, gt.T2_32, gt.Xwin64, gt.P64, gt.T1_64, gt.T2_64};
   }
-  auto kern = propagate_group_kernel<Real, EPT, NWc, NAXc, NJc, KM, WBc>;
+  auto kern = propagate_group_kernel<Real, EPT, NWc, NAXc, NJc, KM, WBc, KP>;
   cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s.smem);
   kern<<<s.ctas, s.threads, s.smem, stream>>>(t, d, s.k_per_cta, s.group, s.box_sm, s.win_sm, s.vctas, rho, Jpart);
 }
 
-template <typename Real, int EPT, int NWc, int NAXc, int NJc, bool KM = false, int WBc = 0>
+template <typename Real, int EPT, int NWc, int NAXc, int NJc, bool KM = false, int WBc = 0, bool KP = false>
 int launch_group_batch_t(const BatchDesc* descs, const int2* items, int nitems, int* counter, int threads, size_t smem,
                          int sm_count, cudaStream_t stream) {
-  auto kern = propagate_group_batch_kernel<Real, EPT, NWc, NAXc, NJc, KM, WBc>;
+  auto kern = propagate_group_batch_kernel<Real, EPT, NWc, NAXc, NJc, KM, WBc, KP>;
   cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   int occ = 0;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, threads, smem);
@@ -746,15 +833,18 @@ using LaunchFn = void (*)(const SolveTables&, const GroupTables&, const LaunchSh
 using BatchFn = int (*)(const BatchDesc*, const int2*, int, int*, int, size_t, int, cudaStream_t);
 struct GroupVariant {
   int precision, nw, nax, nj, wb;  // wb > 0: square wb x wb cell box with Hermitian halving
+  bool kp;                          // k-point pairs
   PlanFn plan;
   LaunchFn launch;
   BatchFn batch;
 };
-#define HHG_GROUP_VARIANT(P, R, E, NW, NAX, NJ, WB)                                                \
-  {P, NW, NAX, NJ, WB, plan_group_t<R, E, NW, NAX, NJ, false, WB>, launch_group_t<R, E, NW, NAX, NJ, false, WB>, \
-   launch_group_batch_t<R, E, NW, NAX, NJ, false, WB>}
+#define HHG_GROUP_VARIANT_KP(P, R, E, NW, NAX, NJ, WB, KP)                                        \
+  {P, NW, NAX, NJ, WB, KP, plan_group_t<R, E, NW, NAX, NJ, false, WB, KP>,                          \
+   launch_group_t<R, E, NW, NAX, NJ, false, WB, KP>, launch_group_batch_t<R, E, NW, NAX, NJ, false, WB, KP>}
+#define HHG_GROUP_VARIANT(P, R, E, NW, NAX, NJ, WB) HHG_GROUP_VARIANT_KP(P, R, E, NW, NAX, NJ, WB, false)
 // Listed before the any-box variants of the same shape, which they take precedence over.
 const GroupVariant kGroupVariants[] = {
+    HHG_GROUP_VARIANT_KP(1, float, 2, 11, 1, 2, 7, true), HHG_GROUP_VARIANT_KP(1, float, 2, 11, 2, 2, 7, true),
     HHG_GROUP_VARIANT(0, double, 1, 11, 1, 2, 7), HHG_GROUP_VARIANT(0, double, 1, 11, 2, 2, 7),
     HHG_GROUP_VARIANT(0, double, 1, 12, 1, 2, 7), HHG_GROUP_VARIANT(0, double, 1, 12, 2, 2, 7),
     HHG_GROUP_VARIANT(1, float, 2, 11, 1, 2, 7),  HHG_GROUP_VARIANT(1, float, 2, 11, 2, 2, 7),
@@ -768,6 +858,7 @@ const GroupVariant kGroupVariants[] = {
     HHG_GROUP_VARIANT(1, float, 1, 2, 1, 2, 0),   HHG_GROUP_VARIANT(1, float, 1, 2, 2, 2, 0),
 };
 #undef HHG_GROUP_VARIANT
+#undef HHG_GROUP_VARIANT_KP
 
 const GroupVariant* find_variant(const SolveTables& t, int precision) {
   if (const char* env = std::getenv("HHG_GROUP_GENERIC"))
@@ -776,10 +867,15 @@ const GroupVariant* find_variant(const SolveTables& t, int precision) {
     const char* env = std::getenv("HHG_GROUP_ANYBOX");  // tuning override: skip the fixed-box variants
     return env && env[0] == '1';
   }();
+  const bool no_pair = [] {
+    const char* env = std::getenv("HHG_GROUP_NOPAIR");  // tuning override: skip the k-point-pair variants
+    return env && env[0] == '1';
+  }();
   const GroupGeom gg = group_geom(t);
   for (const GroupVariant& v : kGroupVariants) {
     if (v.precision != precision || v.nw != t.nw || v.nax != t.nax || v.nj != t.nj) continue;
     if (v.wb > 0 && (any_box || !gg.half || t.b1n != v.wb || t.b2n != v.wb)) continue;
+    if (v.kp && no_pair) continue;
     return &v;
   }
   return nullptr;
