@@ -43,6 +43,7 @@ bool persistent_batch_mode() {
 struct SWEBatch {
   int device = -1;
   std::vector<SWESim*> sims;
+  std::vector<int> launches;  // per solve: kernel launches of one run (propagation and reduction)
   std::vector<cudaStream_t> streams;
   std::vector<cudaEvent_t> done;
   cudaStream_t master = nullptr;
@@ -91,7 +92,7 @@ struct SWEBatch {
     std::vector<int> alone;
     for (int i = 0; i < (int)sims.size(); ++i) {
       const hhg::LaunchShape& sh = sims[i]->shape;
-      if (sh.kernel == 0 || sh.kernel == 3 || streams_only) {
+      if (sh.kernel == 0 || sh.kernel == 3 || sh.pre_chunk > 0 || streams_only) {
         alone.push_back(i);
       } else {
         const hhg::SolveTables& t = sims[i]->tab;
@@ -159,6 +160,7 @@ struct SWEBatch {
                  "D2H");
     };
 
+    launches.assign(sims.size(), 0);
     cudaGraph_t g = nullptr;
     check_cuda(cudaStreamBeginCapture(master, cudaStreamCaptureModeRelaxed), "cudaStreamBeginCapture");
     check_cuda(cudaEventRecord(fork, master), "event");
@@ -176,6 +178,7 @@ struct SWEBatch {
       const auto& rg = ranges[ci];
       hhg::launch_group_batch(sims[kv.second[0]]->shape, d_desc.p, d_items.p + rg.first, (int)(rg.second - rg.first),
                               d_counters.p + ci, smem, sms, st);
+      for (int i : kv.second) launches[i] = 2;  // the shared launch and the solve's reduction
       for (int i : kv.second) reduce_and_copy(sims[i], st);
       check_cuda(cudaEventRecord(done[q], st), "event");
       check_cuda(cudaStreamWaitEvent(master, done[q], 0), "cudaStreamWaitEvent");
@@ -187,7 +190,7 @@ struct SWEBatch {
       SWESim* sim = sims[i];
       check_cuda(cudaStreamWaitEvent(st, fork, 0), "cudaStreamWaitEvent");
       reset_and_clear(sim, st);
-      hhg::launch_propagate(sim->tab, sim->gtab, sim->shape, sim->d_rho.p, sim->d_Jpart.p, sim->d_J.p, st);
+      launches[i] = hhg::launch_propagate(sim->tab, sim->gtab, sim->shape, sim->d_rho.p, sim->d_Jpart.p, sim->d_J.p, st);
       check_cuda(cudaMemcpyAsync(sim->h_J, sim->d_J.p, sizeof(double2) * 3 * (size_t)sim->nt, cudaMemcpyDeviceToHost, st),
                  "D2H");
       check_cuda(cudaEventRecord(done[q], st), "event");
@@ -214,12 +217,13 @@ struct SWEBatch {
     check_cuda(cudaEventRecord(ev1, master), "event");
     check_cuda(cudaStreamSynchronize(master), "SWEBatch_run");
     check_cuda(cudaEventElapsedTime(&last_ms, ev0, ev1), "event time");
-    for (SWESim* sim : sims) {
+    for (size_t i = 0; i < sims.size(); ++i) {
+      SWESim* sim = sims[i];
       for (auto& j : sim->Jhist) j.clear();
       for (int a = 0; a < 3; ++a)
         for (int ti = 0; ti < sim->nt; ++ti)
           sim->Jhist[a].push_back(cd(sim->h_J[(size_t)a * sim->nt + ti].x, sim->h_J[(size_t)a * sim->nt + ti].y));
-      sim->last_launches = 2;
+      sim->last_launches = launches[i];
     }
   }
 };
@@ -457,7 +461,7 @@ struct SWEServer {
       d.rho = sim->d_rho.p;
       d.Jpart = sim->d_Jpart.p;
       const hhg::LaunchShape& sh = sim->shape;
-      if (sh.kernel == 0 || sh.kernel == 3 || !persistent)
+      if (sh.kernel == 0 || sh.kernel == 3 || sh.pre_chunk > 0 || !persistent)
         alone.push_back(i);
       else
         classes[std::make_tuple(sh.kernel, sh.variant, sh.ept, sh.threads, sh.group, sh.kmode, sim->tab.nw,

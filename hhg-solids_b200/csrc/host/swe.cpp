@@ -559,7 +559,7 @@ void SWESim::init() {
     check_cuda(cudaStreamSynchronize(stream), "H2D");  // the host vectors above are temporaries
   }
   gtab = hhg::GroupTables{d_Xbox.p, d_Vd.p, d_P.p, d_T1.p, d_T2.p,
-                          d_Xbox32.p, d_Vd32.p, d_P32.p, d_T1_32.p, d_T2_32.p};
+                          d_Xbox32.p, d_Vd32.p, d_P32.p, d_T1_32.p, d_T2_32.p, nullptr};
   d_rho0.alloc((size_t)Nk * nw2);
   d_rho.alloc((size_t)Nk * nw2);
   d_J.alloc((size_t)3 * nt);
@@ -604,6 +604,12 @@ void SWESim::init() {
   if (!hhg::plan_propagate(tab, precision, sms, &shape, why, sizeof why)) throw std::runtime_error(std::string("SWESim_init: ") + why);
   trace.mark("plan");
   d_Jpart.alloc((size_t)shape.vctas * nt * 3);
+  // Scratch of the precomputed inner sums (independent of the tile shape, so autotuning keeps it).
+  gtab.pre = nullptr;
+  if (shape.pre_bytes > 0) {
+    d_pre.alloc((shape.pre_bytes + sizeof(double2) - 1) / sizeof(double2));
+    gtab.pre = d_pre.p;
+  }
   if (!h_J || h_J_cap < (size_t)3 * nt) {
     if (h_J) cudaFreeHost(h_J);
     h_J = nullptr;
@@ -633,7 +639,8 @@ void SWESim::init() {
 size_t SWESim::device_bytes() const {
   size_t b = (d_cell.cap + d_cellp.cap + d_win.cap) * sizeof(int2) +
              (d_es.cap + d_A.cap + d_Rc.cap + d_x0.cap) * sizeof(double);
-  for (const auto* x : {&d_H0, &d_R, &d_V, &d_Q, &d_Xbox, &d_Vd, &d_P, &d_T1, &d_T2, &d_rho0, &d_rho, &d_Jpart, &d_J})
+  for (const auto* x : {&d_H0, &d_R, &d_V, &d_Q, &d_Xbox, &d_Vd, &d_P, &d_T1, &d_T2, &d_rho0, &d_rho, &d_Jpart, &d_J,
+                        &d_pre})
     b += x->cap * sizeof(double2);
   for (const auto* x : {&d_Xbox32, &d_Vd32, &d_P32, &d_T1_32, &d_T2_32}) b += x->cap * sizeof(float2);
   return b;
@@ -661,6 +668,8 @@ size_t SWESim::footprint_estimate() const {
   b += nt_ * 2 * (2 * np_ + 1) * c16 * 3 / 2;                     // P, FP64 and FP32
   b += (4 * box + 4 * ns + 6 * hhg::kWindow) * w2 * c16 * 3 / 2;  // cell tables, both precisions
   b += (N1_ + N2_) * c16 * 3 / 2 + (size_t(1) << 20);
+  // Precomputed inner sums: 64 steps x N2 columns x (box rows of H0 and r_a, window rows) x nw2.
+  b += std::min<size_t>(64, nt_) * N2_ * ((size_t)4 * (np_ + 1) + 12) * w2 * c16;
   return b;
 }
 

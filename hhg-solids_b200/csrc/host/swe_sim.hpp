@@ -99,6 +99,7 @@ struct SWESim {
   cudaEvent_t ev0 = nullptr, ev1 = nullptr, evm = nullptr;
   hhg::DevBuf<int2> d_cell, d_cellp, d_win;
   hhg::DevBuf<double2> d_H0, d_R, d_V, d_Q, d_Xbox, d_Vd, d_P, d_T1, d_T2, d_rho0, d_rho, d_Jpart, d_J;
+  hhg::DevBuf<double2> d_pre;  // precomputed inner sums (element-group shapes with pre_chunk > 0)
   hhg::DevBuf<float2> d_Xbox32, d_Vd32, d_P32, d_T1_32, d_T2_32;
   hhg::GroupTables gtab{};
   hhg::DevBuf<double> d_es, d_A, d_Rc, d_x0;

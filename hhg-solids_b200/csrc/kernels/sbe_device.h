@@ -52,6 +52,7 @@ struct SolveTables {
 struct GroupTables {
   const double2 *Xbox64, *Xwin64, *P64, *T1_64, *T2_64;
   const float2 *Xbox32, *Xwin32, *P32, *T1_32, *T2_32;
+  void* pre;  // scratch of LaunchShape::pre_bytes for precomputed inner sums (shapes with pre_chunk > 0)
 };
 
 struct LaunchShape {
@@ -68,6 +69,9 @@ struct LaunchShape {
   int variant;         // element groups: compiled shape (-1: runtime-shaped instance)
   int kmode;           // instance for the k-space solver (SolveTables::kmode)
   size_t smem;     // dynamic shared memory bytes
+  int pre_chunk;     // element groups: > 0 when the inner Wannier sums of every column are precomputed
+                     // by a separate kernel, this many steps per launch pair
+  size_t pre_bytes;  // scratch those sums need (GroupTables::pre)
 };
 
 // One solve of a batched element-group launch (device memory).
@@ -89,8 +93,8 @@ bool plan_propagate(const SolveTables& t, int precision, int sm_count, LaunchSha
                     int tile_hint = 0);
 bool plan_group(const SolveTables& t, int precision, int sm_count, LaunchShape* out, char* why, int why_len,
                 int tile_hint = 0);
-void launch_group(const SolveTables& t, const GroupTables& gt, const LaunchShape& s, double2* rho, double2* Jpart,
-                  cudaStream_t stream);
+int launch_group(const SolveTables& t, const GroupTables& gt, const LaunchShape& s, double2* rho, double2* Jpart,
+                 cudaStream_t stream);
 // Column-tile kernel (nw <= 2, Hermitian, FP64): false if the solve does not suit it.
 bool plan_kcol(const SolveTables& t, int sm_count, LaunchShape* out, size_t smem_max, int parts_hint = 0);
 void launch_kcol(const SolveTables& t, const GroupTables& gt, const LaunchShape& s, double2* rho, double2* Jpart,
@@ -105,9 +109,9 @@ int launch_group_batch(const LaunchShape& s, const BatchDesc* descs, const int2*
 // If `after_propagate` is non-null it is recorded between the propagation and the reduction.
 int launch_propagate(const SolveTables& t, const GroupTables& gt, const LaunchShape& s, double2* rho, double2* Jpart,
                      double2* J, cudaStream_t stream, cudaEvent_t after_propagate = nullptr);
-// The propagation launch alone (steps [t.step0, t.step1)), without the reduction.
-void launch_propagate_steps(const SolveTables& t, const GroupTables& gt, const LaunchShape& s, double2* rho,
-                            double2* Jpart, cudaStream_t stream);
+// The propagation launches alone (steps [t.step0, t.step1)), without the reduction; returns their number.
+int launch_propagate_steps(const SolveTables& t, const GroupTables& gt, const LaunchShape& s, double2* rho,
+                           double2* Jpart, cudaStream_t stream);
 
 // Same as launch_propagate, with the current partials in a fixed device array owned by the
 // library instead of a caller buffer (see noalloc.cu).  Returns 0, or -1 with a reason in `why`.

@@ -523,27 +523,29 @@ bool plan_propagate(const SolveTables& t, int precision, int sm_count, LaunchSha
   return plan_group(t, precision, sm_count, out, why, why_len, tile_hint);
 }
 
-void launch_propagate_steps(const SolveTables& t, const GroupTables& gt, const LaunchShape& s, double2* rho,
-                            double2* Jpart, cudaStream_t stream) {
-  if (t.step0 >= t.step1) return;
+int launch_propagate_steps(const SolveTables& t, const GroupTables& gt, const LaunchShape& s, double2* rho,
+                           double2* Jpart, cudaStream_t stream) {
+  if (t.step0 >= t.step1) return 0;
   if (s.kernel == 0) {
     KptKernel kern = kpt_kernel_for(t);
     cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s.smem);
     kern<<<s.ctas, s.threads, s.smem, stream>>>(t, s.vctas, rho, Jpart);
-  } else if (s.kernel == 3) {
-    launch_kcol(t, gt, s, rho, Jpart, stream);
-  } else {
-    launch_group(t, gt, s, rho, Jpart, stream);
+    return 1;
   }
+  if (s.kernel == 3) {
+    launch_kcol(t, gt, s, rho, Jpart, stream);
+    return 1;
+  }
+  return launch_group(t, gt, s, rho, Jpart, stream);
 }
 
 int launch_propagate(const SolveTables& t, const GroupTables& gt, const LaunchShape& s, double2* rho, double2* Jpart,
                      double2* J, cudaStream_t stream, cudaEvent_t after_propagate) {
-  launch_propagate_steps(t, gt, s, rho, Jpart, stream);
+  const int launches = launch_propagate_steps(t, gt, s, rho, Jpart, stream);
   if (after_propagate) cudaEventRecord(after_propagate, stream);
   const int n = 3 * t.nt;
   reduce_current_kernel<<<(n + 255) / 256, 256, 0, stream>>>(Jpart, s.vctas, t.nt, 1.0 / (double)t.Nk, J);
-  return 2;
+  return launches + 1;
 }
 
 void launch_reduce_current(const double2* Jpart, int vctas, int nt, int Nk, double2* J, cudaStream_t stream) {

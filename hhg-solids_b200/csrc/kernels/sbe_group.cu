@@ -158,6 +158,7 @@ struct GroupLayout {
     p += ring * (size_t)B * W1;
     pw2 = p;
     p += ring * W2;
+    p = (p * sizeof(V) + 15) / 16 * 16 / sizeof(V);  // 16-byte copies land in G
     G = p;
     p += gbufs * (size_t)gg.nbrows * nw2;
     Xbox = p;
@@ -197,7 +198,17 @@ struct GroupData {
   const double2* Pd;
   const double2* T1d;
   const double2* T2d;
+  const V* Gpre;          // precomputed inner sums [step in chunk][N2][nbrows][nw2] (or null)
+  const double2* GWpre;   // and of the window rows [step in chunk][N2][nwrows][nw2]
 };
+
+// 16-byte asynchronous copy global -> shared (completes at cp_async_wait_all).
+__device__ __forceinline__ void cp_async16(void* dst_smem, const void* src_gmem) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(dst_smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d), "l"(src_gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
 
 // Runs virtual CTAs v_first, v_first + v_step, ... (< vctas) of one solve on this CTA.
 // NWc, NAXc, NJc: orbital count, field axes and current axes fixed at compile time (0: read from t).
@@ -210,7 +221,10 @@ struct GroupData {
 // and one of two X values per four complex multiply-adds), then read back by the element owners.
 // Rows are NP + 2 values apart, an odd number of 16-byte units, which spreads the transposed
 // accesses of the owners over the banks.
-template <typename Real, int EPT, int NWc, int NAXc, int NJc, bool KM, int WBc = 0, bool KP = false>
+// PG: the inner sums of every evaluation point come precomputed (group_sums_kernel) and are copied
+// into shared memory with cp.async one step ahead, instead of being formed by every CTA of the column.
+template <typename Real, int EPT, int NWc, int NAXc, int NJc, bool KM, int WBc = 0, bool KP = false,
+          bool PG = false>
 __device__ __forceinline__ void group_vctas(const SolveTables& t, const GroupData<Real>& d, int B, int G_in, int box_sm,
                                             int win_sm, int v_first, int v_step, int vctas, double2* rho,
                                             double2* Jpart) {
@@ -219,6 +233,7 @@ __device__ __forceinline__ void group_vctas(const SolveTables& t, const GroupDat
   const GroupGeom gg = group_geom(t);
   const int nw = NWc ? NWc : t.nw, nw2 = nw * nw, nax = NAXc ? NAXc : t.nax, nj = NJc ? NJc : t.nj;
   static_assert(!KP || (EPT == 2 && NWc > 0 && sizeof(Real) == 4 && !KM), "k-point pairs: mixed form, fixed shape");
+  static_assert(!PG || !KM, "precomputed sums: real-space solver");
   constexpr int KPG = KP ? 2 : 1;                      // k-points per thread group
   constexpr int EU = KP ? 1 : EPT;                     // distinct elements per thread
   constexpr int NP = KP ? (NWc + 1) / 2 * 2 : 1;       // padded side of the tile layout
@@ -394,6 +409,22 @@ __device__ __forceinline__ void group_vctas(const SolveTables& t, const GroupDat
     };
 
     const int step0 = t.step0, step1 = t.step1;
+    // Precomputed inner sums of point s (box rows into buffer s % gbufs, window rows into s & 1).
+    auto fetch_sums = [&](int s) {
+      const size_t blk = (size_t)(s - step0) * t.N2 + m2;
+      const char* src = reinterpret_cast<const char*>(d.Gpre + blk * gbuf);
+      char* dst = reinterpret_cast<char*>(Gb + (s % gbufs) * gbuf);
+      const double2* wsrc = d.GWpre + blk * wbuf;
+      double2* wdst = GWb + (s & 1) * wbuf;
+      const int nA = (int)(gbuf * sizeof(V) / 16), nB = (int)wbuf;
+      for (int idx = tid; idx < nA + nB; idx += nthr) {
+        if (idx < nA)
+          cp_async16(dst + (size_t)idx * 16, src + (size_t)idx * 16);
+        else
+          cp_async16(wdst + (idx - nA), wsrc + (idx - nA));
+      }
+      cp_async_commit();
+    };
     // Outer sums over n1 of point s for this k-point: H0(k) and r_a(k) at the point's shift.
     auto outer_box = [&](int s, V* h0o, V (*rko)[EPT]) {
 #pragma unroll
@@ -483,7 +514,12 @@ __device__ __forceinline__ void group_vctas(const SolveTables& t, const GroupDat
       make_phases(step0, true);
       if (step0 + 1 < step1) make_phases(step0 + 1, true);
       __syncthreads();
-      inner_sums(step0, true);
+      if constexpr (PG) {
+        fetch_sums(step0);
+        cp_async_wait_all();
+      } else {
+        inner_sums(step0, true);
+      }
       __syncthreads();
     } else {
       // Points 2 step0 .. 2 step0 + 4: phases of all, inner sums of the first three, then the
@@ -511,7 +547,11 @@ __device__ __forceinline__ void group_vctas(const SolveTables& t, const GroupDat
       // (2) later points' phase factors and inner sums, off this step's critical path
       if (!km) {
         if (ti + 2 < step1) make_phases(ti + 2, true);
-        if (ti + 1 < step1) inner_sums(ti + 1, true);
+        if constexpr (PG) {
+          if (ti + 1 < step1) fetch_sums(ti + 1);
+        } else {
+          if (ti + 1 < step1) inner_sums(ti + 1, true);
+        }
       } else {
         if (2 * ti + 5 <= 2 * step1) make_phases(2 * ti + 5, false);
         if (2 * ti + 6 <= 2 * step1) make_phases(2 * ti + 6, false);
@@ -674,6 +714,7 @@ __device__ __forceinline__ void group_vctas(const SolveTables& t, const GroupDat
             dst[1] = im;
           }
         }
+      if constexpr (PG) cp_async_wait_all();  // the next step's sums, before the barrier publishes them
       __syncthreads();
       // Flush a completed ring half: the other half is being written meanwhile.
       if (s == kJRing - 1 || ti == step1 - 1) {
@@ -701,23 +742,68 @@ __device__ __forceinline__ void group_vctas(const SolveTables& t, const GroupDat
   }
 }
 
+constexpr int kMaxPreBox = 64;  // widest cell box of the precomputed-sum shapes
+constexpr int kPreChunk = 64;   // steps per precompute + propagate launch pair
+
+// Inner Wannier sums of every column for the steps [t.step0, t.step1) of the real-space solver:
+// block (s, m2) forms the box rows G_e = sum_q p2(q) X(mat, q1s + qq, q)_e and the window rows with
+// the operations (and their order) of group_vctas's inner_sums, into [s - t.step0][m2][row][nw2].
+template <typename Real>
+__global__ void __launch_bounds__(256) group_sums_kernel(SolveTables t, GroupData<Real> d, int q1s, int nq1,
+                                                         int nbrows, int nwrows, typename Cx<Real>::T* Gpre,
+                                                         double2* GWpre) {
+  using V = typename Cx<Real>::T;
+  __shared__ V q2[kMaxPreBox];
+  __shared__ double2 w2[4];
+  const int sl = blockIdx.x / t.N2, m2 = blockIdx.x % t.N2, s = t.step0 + sl;
+  const int npw = 2 * t.np + 1, W1n = t.b1n, W2n = t.b2n, nw2 = t.nw2;
+  const V* P2 = d.P + (size_t)s * 2 * npw + t.np + npw;
+  const double2* P2d = d.Pd + (size_t)s * 2 * npw + t.np + npw;
+  for (int idx = threadIdx.x; idx < W2n + 4; idx += blockDim.x) {
+    if (idx < W2n) {
+      q2[idx] = mul(d.T2[wrap_mod((long long)m2 * (t.b2lo + idx), t.N2)], P2[t.b2lo + idx]);
+    } else {
+      const int q = idx - W2n;
+      w2[q] = mul(d.T2d[wrap_mod((long long)m2 * (q - 2), t.N2)], P2d[q - 2]);
+    }
+  }
+  __syncthreads();
+  V* G = Gpre + (size_t)blockIdx.x * nbrows * nw2;
+  for (int idx = threadIdx.x; idx < nbrows * nw2; idx += blockDim.x) {
+    const int row = idx / nw2, e = idx % nw2, mat = row / nq1, qq = row % nq1;
+    const V* X = d.Xbox + ((size_t)(mat * W1n + q1s + qq) * W2n) * nw2;
+    V acc = Cx<Real>::make(0, 0);
+    for (int q = 0; q < W2n; ++q) acc = fmac(q2[q], X[(size_t)q * nw2 + e], acc);
+    G[idx] = acc;
+  }
+  double2* GW = GWpre + (size_t)blockIdx.x * nwrows * nw2;
+  for (int idx = threadIdx.x; idx < nwrows * nw2; idx += blockDim.x) {
+    const int wr = idx / nw2, e = idx % nw2;
+    const double2* X = d.Xwin + (size_t)wr * 4 * nw2;
+    double2 acc = make_double2(0.0, 0.0);
+    for (int q = 0; q < 4; ++q) acc = fmac(w2[q], X[(size_t)q * nw2 + e], acc);
+    GW[idx] = acc;
+  }
+}
+
 template <typename Real>
 __device__ __forceinline__ GroupData<Real> group_data(const GroupTables& gt) {
   GroupData<Real> d;
   if constexpr (sizeof(Real) == 8) {
-    d = {gt.Xbox64, gt.P64, gt.T1_64, gt.T2_64, gt.Xwin64, gt.P64, gt.T1_64, gt.T2_64};
+    d = {gt.Xbox64, gt.P64, gt.T1_64, gt.T2_64, gt.Xwin64, gt.P64, gt.T1_64, gt.T2_64, nullptr, nullptr};
   } else {
-    d = {gt.Xbox32, gt.P32, gt.T1_32, gt.T2_32, gt.Xwin64, gt.P64, gt.T1_64, gt.T2_64};
+    d = {gt.Xbox32, gt.P32, gt.T1_32, gt.T2_32, gt.Xwin64, gt.P64, gt.T1_64, gt.T2_64, nullptr, nullptr};
   }
   return d;
 }
 
 // One solve: physical CTA b runs virtual CTAs b, b + gridDim.x, ...
-template <typename Real, int EPT, int NWc, int NAXc, int NJc, bool KM = false, int WBc = 0, bool KP = false>
+template <typename Real, int EPT, int NWc, int NAXc, int NJc, bool KM = false, int WBc = 0, bool KP = false,
+          bool PG = false>
 __global__ void __launch_bounds__(group_threads<EPT>(), 1)
     propagate_group_kernel(SolveTables t, GroupData<Real> d, int B, int G, int box_sm, int win_sm, int vctas,
                            double2* rho, double2* Jpart) {
-  group_vctas<Real, EPT, NWc, NAXc, NJc, KM, WBc, KP>(t, d, B, G, box_sm, win_sm, blockIdx.x, gridDim.x, vctas, rho, Jpart);
+  group_vctas<Real, EPT, NWc, NAXc, NJc, KM, WBc, KP, PG>(t, d, B, G, box_sm, win_sm, blockIdx.x, gridDim.x, vctas, rho, Jpart);
 }
 
 // Many solves of one kernel shape: persistent CTAs take (solve, virtual CTA) items from a packed
@@ -744,7 +830,8 @@ __global__ void __launch_bounds__(group_threads<EPT>(), 1)
 
 constexpr size_t kSmemMax = 220 * 1024;
 
-template <typename Real, int EPT, int NWc, int NAXc, int NJc, bool KM = false, int WBc = 0, bool KP = false>
+template <typename Real, int EPT, int NWc, int NAXc, int NJc, bool KM = false, int WBc = 0, bool KP = false,
+          bool PG = false>
 bool plan_group_t(const SolveTables& t, int sm_count, LaunchShape* out, char* why, int why_len, int tile_hint) {
   const GroupGeom gg = group_geom(t);
   constexpr int KPG = KP ? 2 : 1;  // k-points per thread group
@@ -774,7 +861,21 @@ bool plan_group_t(const SolveTables& t, int sm_count, LaunchShape* out, char* wh
   if (bytes(best, true, true) > kSmemMax) win_sm = 0;
   if (bytes(best, true, win_sm) > kSmemMax) box_sm = 0;
   if (!box_sm && bytes(best, false, true) <= kSmemMax) win_sm = 1;
-  auto kern = propagate_group_kernel<Real, EPT, NWc, NAXc, NJc, KM, WBc, KP>;
+  out->pre_chunk = 0;
+  out->pre_bytes = 0;
+  if constexpr (PG) {
+    // The tables are read by the precompute kernel only; the propagation copies finished sums.
+    box_sm = win_sm = 0;
+    const size_t gbytes = (size_t)gg.nbrows * t.nw2 * sizeof(typename Cx<Real>::T);
+    const size_t wbytes = (size_t)gg.nwrows * t.nw2 * sizeof(double2);
+    if (gbytes % 16 != 0 || gg.W2n > kMaxPreBox) {
+      snprintf(why, why_len, "precomputed sums need 16-byte rows and a box of at most %d cells", kMaxPreBox);
+      return false;
+    }
+    out->pre_chunk = std::min(kPreChunk, t.nt);
+    out->pre_bytes = (size_t)out->pre_chunk * t.N2 * (gbytes + wbytes);
+  }
+  auto kern = propagate_group_kernel<Real, EPT, NWc, NAXc, NJc, KM, WBc, KP, PG>;
   const size_t smem_max = bytes(best, box_sm, win_sm);
   cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_max);
   int occ = 0;
@@ -798,18 +899,46 @@ bool plan_group_t(const SolveTables& t, int sm_count, LaunchShape* out, char* wh
   return true;
 }
 
-template <typename Real, int EPT, int NWc, int NAXc, int NJc, bool KM = false, int WBc = 0, bool KP = false>
-void launch_group_t(const SolveTables& t, const GroupTables& gt, const LaunchShape& s, double2* rho, double2* Jpart,
-                    cudaStream_t stream) {
+template <typename Real, int EPT, int NWc, int NAXc, int NJc, bool KM = false, int WBc = 0, bool KP = false,
+          bool PG = false>
+int launch_group_t(const SolveTables& t, const GroupTables& gt, const LaunchShape& s, double2* rho, double2* Jpart,
+                   cudaStream_t stream) {
+  using V = typename Cx<Real>::T;
   GroupData<Real> d;
   if constexpr (sizeof(Real) == 8) {
-    d = {gt.Xbox64, gt.P64, gt.T1_64, gt.T2_64, gt.Xwin64, gt.P64, gt.T1_64, gt.T2_64};
+    d = {gt.Xbox64, gt.P64, gt.T1_64, gt.T2_64, gt.Xwin64, gt.P64, gt.T1_64, gt.T2_64, nullptr, nullptr};
   } else {
-    d = {gt.Xbox32, gt.P32, gt.T1_32, gt.T2_32, gt.Xwin64, gt.P64, gt.T1_64, gt.T2_64};
+    d = {gt.Xbox32, gt.P32, gt.T1_32, gt.T2_32, gt.Xwin64, gt.P64, gt.T1_64, gt.T2_64, nullptr, nullptr};
   }
-  auto kern = propagate_group_kernel<Real, EPT, NWc, NAXc, NJc, KM, WBc, KP>;
-  cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s.smem);
-  kern<<<s.ctas, s.threads, s.smem, stream>>>(t, d, s.k_per_cta, s.group, s.box_sm, s.win_sm, s.vctas, rho, Jpart);
+  if constexpr (PG) {
+    // Without its scratch the shape runs the in-kernel sums (tables read from global memory).
+    if (!gt.pre || s.pre_chunk <= 0) return launch_group_t<Real, EPT, NWc, NAXc, NJc, KM, WBc, KP, false>(t, gt, s, rho, Jpart, stream);
+    const GroupGeom gg = group_geom(t);
+    const size_t gbuf = (size_t)gg.nbrows * t.nw2, wbuf = (size_t)gg.nwrows * t.nw2;
+    V* Gpre = static_cast<V*>(gt.pre);
+    double2* GWpre = reinterpret_cast<double2*>(static_cast<char*>(gt.pre) + (size_t)s.pre_chunk * t.N2 * gbuf * sizeof(V));
+    d.Gpre = Gpre;
+    d.GWpre = GWpre;
+    auto kern = propagate_group_kernel<Real, EPT, NWc, NAXc, NJc, KM, WBc, KP, true>;
+    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s.smem);
+    int launches = 0;
+    for (int c0 = t.step0; c0 < t.step1; c0 += s.pre_chunk) {
+      SolveTables tc = t;
+      tc.step0 = c0;
+      tc.step1 = std::min(c0 + s.pre_chunk, t.step1);
+      group_sums_kernel<Real><<<(tc.step1 - c0) * t.N2, 256, 0, stream>>>(tc, d, gg.q1s, gg.nq1, gg.nbrows, gg.nwrows,
+                                                                          Gpre, GWpre);
+      kern<<<s.ctas, s.threads, s.smem, stream>>>(tc, d, s.k_per_cta, s.group, s.box_sm, s.win_sm, s.vctas, rho, Jpart);
+      launches += 2;
+    }
+    (void)wbuf;
+    return launches;
+  } else {
+    auto kern = propagate_group_kernel<Real, EPT, NWc, NAXc, NJc, KM, WBc, KP, false>;
+    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s.smem);
+    kern<<<s.ctas, s.threads, s.smem, stream>>>(t, d, s.k_per_cta, s.group, s.box_sm, s.win_sm, s.vctas, rho, Jpart);
+    return 1;
+  }
 }
 
 template <typename Real, int EPT, int NWc, int NAXc, int NJc, bool KM = false, int WBc = 0, bool KP = false>
@@ -829,22 +958,28 @@ int launch_group_batch_t(const BatchDesc* descs, const int2* items, int nitems, 
 // for, each in plain FP64 (one element per thread) and mixed precision (two elements per thread);
 // any other shape runs the runtime-shaped instance.
 using PlanFn = bool (*)(const SolveTables&, int, LaunchShape*, char*, int, int);
-using LaunchFn = void (*)(const SolveTables&, const GroupTables&, const LaunchShape&, double2*, double2*, cudaStream_t);
+using LaunchFn = int (*)(const SolveTables&, const GroupTables&, const LaunchShape&, double2*, double2*, cudaStream_t);
 using BatchFn = int (*)(const BatchDesc*, const int2*, int, int*, int, size_t, int, cudaStream_t);
 struct GroupVariant {
   int precision, nw, nax, nj, wb;  // wb > 0: square wb x wb cell box with Hermitian halving
   bool kp;                          // k-point pairs
+  bool pg;                          // precomputed inner sums
   PlanFn plan;
   LaunchFn launch;
   BatchFn batch;
 };
-#define HHG_GROUP_VARIANT_KP(P, R, E, NW, NAX, NJ, WB, KP)                                        \
-  {P, NW, NAX, NJ, WB, KP, plan_group_t<R, E, NW, NAX, NJ, false, WB, KP>,                          \
-   launch_group_t<R, E, NW, NAX, NJ, false, WB, KP>, launch_group_batch_t<R, E, NW, NAX, NJ, false, WB, KP>}
-#define HHG_GROUP_VARIANT(P, R, E, NW, NAX, NJ, WB) HHG_GROUP_VARIANT_KP(P, R, E, NW, NAX, NJ, WB, false)
-// Listed before the any-box variants of the same shape, which they take precedence over.
+#define HHG_GROUP_VARIANT_X(P, R, E, NW, NAX, NJ, WB, KP, PG)                                      \
+  {P, NW, NAX, NJ, WB, KP, PG, plan_group_t<R, E, NW, NAX, NJ, false, WB, KP, PG>,                  \
+   launch_group_t<R, E, NW, NAX, NJ, false, WB, KP, PG>, launch_group_batch_t<R, E, NW, NAX, NJ, false, WB, KP>}
+#define HHG_GROUP_VARIANT(P, R, E, NW, NAX, NJ, WB) HHG_GROUP_VARIANT_X(P, R, E, NW, NAX, NJ, WB, false, false)
+// Listed in order of preference: a solve runs the first one that matches it.  (The persistent batch
+// launch of a precomputed-sum shape runs its in-kernel-sum instance.)
 const GroupVariant kGroupVariants[] = {
-    HHG_GROUP_VARIANT_KP(1, float, 2, 11, 1, 2, 7, true), HHG_GROUP_VARIANT_KP(1, float, 2, 11, 2, 2, 7, true),
+    HHG_GROUP_VARIANT_X(1, float, 2, 11, 1, 2, 7, true, true),  HHG_GROUP_VARIANT_X(1, float, 2, 11, 2, 2, 7, true, true),
+    HHG_GROUP_VARIANT_X(1, float, 2, 11, 1, 2, 7, true, false), HHG_GROUP_VARIANT_X(1, float, 2, 11, 2, 2, 7, true, false),
+    HHG_GROUP_VARIANT_X(0, double, 1, 11, 1, 2, 7, false, true), HHG_GROUP_VARIANT_X(0, double, 1, 11, 2, 2, 7, false, true),
+    HHG_GROUP_VARIANT_X(0, double, 1, 12, 1, 2, 7, false, true), HHG_GROUP_VARIANT_X(0, double, 1, 12, 2, 2, 7, false, true),
+    HHG_GROUP_VARIANT_X(1, float, 2, 12, 1, 2, 7, false, true),  HHG_GROUP_VARIANT_X(1, float, 2, 12, 2, 2, 7, false, true),
     HHG_GROUP_VARIANT(0, double, 1, 11, 1, 2, 7), HHG_GROUP_VARIANT(0, double, 1, 11, 2, 2, 7),
     HHG_GROUP_VARIANT(0, double, 1, 12, 1, 2, 7), HHG_GROUP_VARIANT(0, double, 1, 12, 2, 2, 7),
     HHG_GROUP_VARIANT(1, float, 2, 11, 1, 2, 7),  HHG_GROUP_VARIANT(1, float, 2, 11, 2, 2, 7),
@@ -858,7 +993,7 @@ const GroupVariant kGroupVariants[] = {
     HHG_GROUP_VARIANT(1, float, 1, 2, 1, 2, 0),   HHG_GROUP_VARIANT(1, float, 1, 2, 2, 2, 0),
 };
 #undef HHG_GROUP_VARIANT
-#undef HHG_GROUP_VARIANT_KP
+#undef HHG_GROUP_VARIANT_X
 
 const GroupVariant* find_variant(const SolveTables& t, int precision) {
   if (const char* env = std::getenv("HHG_GROUP_GENERIC"))
@@ -871,11 +1006,16 @@ const GroupVariant* find_variant(const SolveTables& t, int precision) {
     const char* env = std::getenv("HHG_GROUP_NOPAIR");  // tuning override: skip the k-point-pair variants
     return env && env[0] == '1';
   }();
+  const bool no_pre = [] {
+    const char* env = std::getenv("HHG_GROUP_NOPRE");  // tuning override: skip the precomputed-sum variants
+    return env && env[0] == '1';
+  }();
   const GroupGeom gg = group_geom(t);
   for (const GroupVariant& v : kGroupVariants) {
     if (v.precision != precision || v.nw != t.nw || v.nax != t.nax || v.nj != t.nj) continue;
     if (v.wb > 0 && (any_box || !gg.half || t.b1n != v.wb || t.b2n != v.wb)) continue;
     if (v.kp && no_pair) continue;
+    if (v.pg && no_pre) continue;
     return &v;
   }
   return nullptr;
@@ -919,14 +1059,12 @@ int launch_group_batch_generic(const LaunchShape& s, const BatchDesc* descs, con
                                                       stream);
 }
 template <bool KM>
-void launch_group_generic(const SolveTables& t, const GroupTables& gt, const LaunchShape& s, double2* rho,
-                          double2* Jpart, cudaStream_t stream) {
-  if (s.kernel == 2) {
-    s.ept == 2 ? launch_group_t<float, 2, 0, 0, 0, KM>(t, gt, s, rho, Jpart, stream)
-               : launch_group_t<float, 1, 0, 0, 0, KM>(t, gt, s, rho, Jpart, stream);
-  } else {
-    launch_group_t<double, 1, 0, 0, 0, KM>(t, gt, s, rho, Jpart, stream);
-  }
+int launch_group_generic(const SolveTables& t, const GroupTables& gt, const LaunchShape& s, double2* rho,
+                         double2* Jpart, cudaStream_t stream) {
+  if (s.kernel == 2)
+    return s.ept == 2 ? launch_group_t<float, 2, 0, 0, 0, KM>(t, gt, s, rho, Jpart, stream)
+                      : launch_group_t<float, 1, 0, 0, 0, KM>(t, gt, s, rho, Jpart, stream);
+  return launch_group_t<double, 1, 0, 0, 0, KM>(t, gt, s, rho, Jpart, stream);
 }
 }  // namespace
 
@@ -938,14 +1076,11 @@ int launch_group_batch(const LaunchShape& s, const BatchDesc* descs, const int2*
                  : launch_group_batch_generic<false>(s, descs, items, nitems, counter, smem, sm_count, stream);
 }
 
-void launch_group(const SolveTables& t, const GroupTables& gt, const LaunchShape& s, double2* rho, double2* Jpart,
-                  cudaStream_t stream) {
-  if (s.variant >= 0)
-    kGroupVariants[s.variant].launch(t, gt, s, rho, Jpart, stream);
-  else if (s.kmode)
-    launch_group_generic<true>(t, gt, s, rho, Jpart, stream);
-  else
-    launch_group_generic<false>(t, gt, s, rho, Jpart, stream);
+int launch_group(const SolveTables& t, const GroupTables& gt, const LaunchShape& s, double2* rho, double2* Jpart,
+                 cudaStream_t stream) {
+  if (s.variant >= 0) return kGroupVariants[s.variant].launch(t, gt, s, rho, Jpart, stream);
+  if (s.kmode) return launch_group_generic<true>(t, gt, s, rho, Jpart, stream);
+  return launch_group_generic<false>(t, gt, s, rho, Jpart, stream);
 }
 
 }  // namespace hhg
