@@ -253,7 +253,11 @@ void SWESim::init() {
   if (stream && device != stream_device) release();  // device changed: start over
   check_cuda(cudaSetDevice(device), "cudaSetDevice");
   if (!stream) {
-    check_cuda(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking), "cudaStreamCreate");
+    // Highest priority: a solve set up while a server runs others gets its table and rho0 kernels
+    // onto the SMs as soon as blocks of the running launches retire, instead of behind them.
+    int least = 0, greatest = 0;
+    check_cuda(cudaDeviceGetStreamPriorityRange(&least, &greatest), "cudaDeviceGetStreamPriorityRange");
+    check_cuda(cudaStreamCreateWithPriority(&stream, cudaStreamNonBlocking, greatest), "cudaStreamCreate");
     check_cuda(cudaEventCreate(&ev0), "cudaEventCreate");
     check_cuda(cudaEventCreate(&ev1), "cudaEventCreate");
     check_cuda(cudaEventCreate(&evm), "cudaEventCreate");

@@ -100,6 +100,10 @@ constexpr int group_threads() {
 }
 constexpr int kJRing = 16;          // steps per current-partial flush
 
+// Row stride (complex values) of the k-point-pair tile layout of side np (even): an odd number of
+// 16-byte units, so that the owners' transposed accesses spread over the banks.
+__host__ __device__ constexpr int tile_stride(int np) { return (np / 2) % 2 == 1 ? np : np + 2; }
+
 // Threads per k-point for nw2 elements at ept per thread: the next power of two up to a warp,
 // whole warps beyond it.
 __host__ __device__ constexpr int group_size(int nw2, int ept) {
@@ -219,7 +223,7 @@ __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wai
 // window row serves two k-points; the commutator's product H X is formed in 2x2 register tiles from
 // a column-major H and a row-major X padded to an even side NP (one 16-byte load of two H values
 // and one of two X values per four complex multiply-adds), then read back by the element owners.
-// Rows are NP + 2 values apart, an odd number of 16-byte units, which spreads the transposed
+// Rows are an odd number of 16-byte units apart (tile_stride), which spreads the transposed
 // accesses of the owners over the banks.
 // PG: the inner sums of every evaluation point come precomputed (group_sums_kernel) and are copied
 // into shared memory with cp.async one step ahead, instead of being formed by every CTA of the column.
@@ -237,7 +241,7 @@ __device__ __forceinline__ void group_vctas(const SolveTables& t, const GroupDat
   constexpr int KPG = KP ? 2 : 1;                      // k-points per thread group
   constexpr int EU = KP ? 1 : EPT;                     // distinct elements per thread
   constexpr int NP = KP ? (NWc + 1) / 2 * 2 : 1;       // padded side of the tile layout
-  constexpr int NS = NP + 2;                           // its row stride: an odd number of 16-byte units
+  constexpr int NS = tile_stride(NP);                  // its row stride: an odd number of 16-byte units
   constexpr int Gc = NWc ? group_size(NWc * NWc, EU) : 0;
   const int G = Gc ? Gc : G_in;
   const int nthr = blockDim.x, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarps = (nthr + 31) >> 5;
@@ -840,7 +844,7 @@ bool plan_group_t(const SolveTables& t, int sm_count, LaunchShape* out, char* wh
   int Bmax = group_threads<EPT>() / G * KPG;
   if (G > 32 && Bmax > 15 * KPG) Bmax = 15 * KPG;  // one named barrier per group, ids 1..15
   Bmax = Bmax / step * step;
-  const int kstride = KP ? 3 * ((t.nw + 1) / 2 * 2) * ((t.nw + 1) / 2 * 2 + 2) : 3 * t.nw2;
+  const int kstride = KP ? 3 * ((t.nw + 1) / 2 * 2) * tile_stride((t.nw + 1) / 2 * 2) : 3 * t.nw2;
   if (Bmax < 1) {
     snprintf(why, why_len, "num_orb=%d needs %d threads per k-point", t.nw, G);
     return false;
@@ -976,6 +980,9 @@ struct GroupVariant {
 // launch of a precomputed-sum shape runs its in-kernel-sum instance.)
 const GroupVariant kGroupVariants[] = {
     HHG_GROUP_VARIANT_X(1, float, 2, 11, 1, 2, 7, true, true),  HHG_GROUP_VARIANT_X(1, float, 2, 11, 2, 2, 7, true, true),
+    HHG_GROUP_VARIANT_X(1, float, 2, 12, 1, 2, 7, true, true),  HHG_GROUP_VARIANT_X(1, float, 2, 12, 2, 2, 7, true, true),
+    HHG_GROUP_VARIANT_X(1, float, 2, 6, 1, 2, 7, true, true),   HHG_GROUP_VARIANT_X(1, float, 2, 6, 2, 2, 7, true, true),
+    HHG_GROUP_VARIANT_X(0, double, 1, 6, 1, 2, 7, false, true), HHG_GROUP_VARIANT_X(0, double, 1, 6, 2, 2, 7, false, true),
     HHG_GROUP_VARIANT_X(1, float, 2, 11, 1, 2, 7, true, false), HHG_GROUP_VARIANT_X(1, float, 2, 11, 2, 2, 7, true, false),
     HHG_GROUP_VARIANT_X(0, double, 1, 11, 1, 2, 7, false, true), HHG_GROUP_VARIANT_X(0, double, 1, 11, 2, 2, 7, false, true),
     HHG_GROUP_VARIANT_X(0, double, 1, 12, 1, 2, 7, false, true), HHG_GROUP_VARIANT_X(0, double, 1, 12, 2, 2, 7, false, true),
