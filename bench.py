@@ -269,6 +269,17 @@ def flops_per_kstep(nw: int, window: int, n: int, n_op: int, n_j: int, kspace: b
     return f_comm + f_w + f_j + f_rk
 
 
+def flops_split_mixed(nw: int, window: int, n: int, n_op: int, n_j: int, kspace: bool = False):
+    """(FP64, FP32) parts of flops_per_kstep in the mixed form: the commutators and the Wannier sums
+    run in FP32; the windowed velocity, Tr(W rho) and the RK accumulation stay in FP64.  (For nw <= 2
+    the mixed form runs the FP64 kernels, so everything counts as FP64.)"""
+    total = flops_per_kstep(nw, window, n, n_op, n_j, kspace)
+    if nw <= 2:
+        return total, 0.0
+    f32 = 32.0 * nw ** 3 + 8.0 * nw * nw * n_op * window * (1.0 + window / n) * (2.0 if kspace else 1.0)
+    return total - f32, f32
+
+
 class ClockSampler:
     """nvidia-smi samples of SM clock and throttle reasons during the timed region."""
 
@@ -564,7 +575,10 @@ def mixed_report(J_mixed, J_fp64, param, fp64_ms, mixed_ms):
 
 def load_traffic(workload: str, kernel: str):
     """DRAM bytes per launch of this kernel on this workload, from a committed ncu capture summary."""
-    short = (kernel or "").split("<")[0].replace("_kernel", "")
+    name = kernel or ""
+    short = name.split("<")[0].replace("_kernel", "")
+    if "<" in name:  # element-group kernels: one file per arithmetic type
+        short += "_" + name.split("<")[1].split(",")[0].rstrip(">").strip()
     path = os.path.join(REPO, "profiles", f"{short}_{workload}_traffic.json")
     if not os.path.exists(path):
         return None, None
@@ -742,7 +756,17 @@ def main():
     prop_mean = statistics.mean(prop_ms)
     achieved = fpk * nk * nt / (prop_mean * 1e-3) / 1e12
     traffic, traffic_src = (load_traffic(args.workload, shape.get("kernel_name"))
-                            if args.solver == "rspace" and args.precision == "fp64" and not args.grid else (None, None))
+                            if args.solver == "rspace" and not args.grid else (None, None))
+    # The peak the kernel is held to: the FP64 FMA-chain peak, or in the mixed form the rate at which
+    # both pipes would finish their own parts (FP64 flops at the FP64 peak plus FP32 flops at the
+    # FP32 peak, one after the other).
+    bound, peak, split = "fp64", fp64_peak.value, None
+    if args.precision == "mixed":
+        f64, f32 = flops_split_mixed(nw, w["window"], param["nr1"], n_op, n_j, kspace=args.solver == "kspace")
+        if f32 > 0 and fp64_peak.value > 0 and fp32_peak.value > 0:
+            bound = "fp64+fp32"
+            peak = (f64 + f32) / (f64 / fp64_peak.value + f32 / fp32_peak.value)
+            split = {"fp64_flops_per_kstep": f64, "fp32_flops_per_kstep": f32}
     line = {
         "metric": "k-pt*RK4-steps/s",
         "value": value,
@@ -764,11 +788,11 @@ def main():
                    "autotune": args.autotune, "parallelism": f"replicas x{world}" if world > 1 else "single",
                    "l2": "flushed between timed solves (256 MiB write)", "launch": shape},
         "solves_per_hour": 3600.0 * world * args.steps / (total_ms * 1e-3),
-        "roofline": {"bound": "fp64", "achieved": achieved, "peak": fp64_peak.value, "unit": "TFLOP/s",
-                     "frac": achieved / fp64_peak.value if fp64_peak.value > 0 else None, "traffic": traffic,
-                     "kernel": shape.get("kernel_name"), "flops_per_kstep": fpk,
-                     "peak_source": "live FP64 FMA-chain probe on this GPU (HHG_measure_peaks); "
-                                    "MEASURED_PEAKS.json has no FP64 figure",
+        "roofline": {"bound": bound, "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                     "frac": achieved / peak if peak > 0 else None, "traffic": traffic,
+                     "kernel": shape.get("kernel_name"), "flops_per_kstep": fpk, "flops_split": split,
+                     "peak_source": "live FP64 / FP32 FMA-chain probes on this GPU (HHG_measure_peaks); "
+                                    "MEASURED_PEAKS.json has no FP64 or FP32 figure",
                      "fp32_peak": fp32_peak.value, "kernel_ms": prop_mean, "traffic_source": traffic_src},
         "gpu_launches": launches,
         "clocks": clk,

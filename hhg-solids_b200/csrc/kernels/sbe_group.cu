@@ -22,6 +22,7 @@
 #include <cstdio>
 #include <algorithm>
 #include <cstdlib>
+#include <stdexcept>
 
 #include "sbe_device.h"
 
@@ -92,11 +93,11 @@ __device__ __forceinline__ void group_sync(int g, int G) {
   }
 }
 
-// Upper bound on threads per CTA: 640 (96 registers per thread) with one element per thread, 512
-// (128 registers) with two.
-template <int EPT>
+// Upper bound on threads per CTA: 640 (96 registers per thread) with one element per thread, 768
+// (80 registers) when the inner sums come precomputed, 512 (128 registers) with two.
+template <int EPT, bool PG = false>
 constexpr int group_threads() {
-  return EPT == 1 ? 640 : 512;
+  return EPT == 1 ? (PG ? 768 : 640) : 512;
 }
 constexpr int kJRing = 16;          // steps per current-partial flush
 
@@ -804,7 +805,7 @@ __device__ __forceinline__ GroupData<Real> group_data(const GroupTables& gt) {
 // One solve: physical CTA b runs virtual CTAs b, b + gridDim.x, ...
 template <typename Real, int EPT, int NWc, int NAXc, int NJc, bool KM = false, int WBc = 0, bool KP = false,
           bool PG = false>
-__global__ void __launch_bounds__(group_threads<EPT>(), 1)
+__global__ void __launch_bounds__(group_threads<EPT, PG>(), 1)
     propagate_group_kernel(SolveTables t, GroupData<Real> d, int B, int G, int box_sm, int win_sm, int vctas,
                            double2* rho, double2* Jpart) {
   group_vctas<Real, EPT, NWc, NAXc, NJc, KM, WBc, KP, PG>(t, d, B, G, box_sm, win_sm, blockIdx.x, gridDim.x, vctas, rho, Jpart);
@@ -841,7 +842,7 @@ bool plan_group_t(const SolveTables& t, int sm_count, LaunchShape* out, char* wh
   constexpr int KPG = KP ? 2 : 1;  // k-points per thread group
   const int G = group_size(t.nw2, KP ? 1 : EPT);
   const int step = (G < 32 ? 32 / G : 1) * KPG;  // whole warps (and whole groups) per CTA
-  int Bmax = group_threads<EPT>() / G * KPG;
+  int Bmax = group_threads<EPT, PG>() / G * KPG;
   if (G > 32 && Bmax > 15 * KPG) Bmax = 15 * KPG;  // one named barrier per group, ids 1..15
   Bmax = Bmax / step * step;
   const int kstride = KP ? 3 * ((t.nw + 1) / 2 * 2) * tile_stride((t.nw + 1) / 2 * 2) : 3 * t.nw2;
@@ -915,8 +916,8 @@ int launch_group_t(const SolveTables& t, const GroupTables& gt, const LaunchShap
     d = {gt.Xbox32, gt.P32, gt.T1_32, gt.T2_32, gt.Xwin64, gt.P64, gt.T1_64, gt.T2_64, nullptr, nullptr};
   }
   if constexpr (PG) {
-    // Without its scratch the shape runs the in-kernel sums (tables read from global memory).
-    if (!gt.pre || s.pre_chunk <= 0) return launch_group_t<Real, EPT, NWc, NAXc, NJc, KM, WBc, KP, false>(t, gt, s, rho, Jpart, stream);
+    if (!gt.pre || s.pre_chunk <= 0)
+      throw std::runtime_error("element-group launch: a precomputed-sum shape needs its scratch (GroupTables::pre)");
     const GroupGeom gg = group_geom(t);
     const size_t gbuf = (size_t)gg.nbrows * t.nw2, wbuf = (size_t)gg.nwrows * t.nw2;
     V* Gpre = static_cast<V*>(gt.pre);
@@ -984,6 +985,8 @@ const GroupVariant kGroupVariants[] = {
     HHG_GROUP_VARIANT_X(1, float, 2, 6, 1, 2, 7, true, true),   HHG_GROUP_VARIANT_X(1, float, 2, 6, 2, 2, 7, true, true),
     HHG_GROUP_VARIANT_X(0, double, 1, 6, 1, 2, 7, false, true), HHG_GROUP_VARIANT_X(0, double, 1, 6, 2, 2, 7, false, true),
     HHG_GROUP_VARIANT_X(1, float, 2, 11, 1, 2, 7, true, false), HHG_GROUP_VARIANT_X(1, float, 2, 11, 2, 2, 7, true, false),
+    HHG_GROUP_VARIANT_X(1, float, 2, 12, 1, 2, 7, true, false), HHG_GROUP_VARIANT_X(1, float, 2, 12, 2, 2, 7, true, false),
+    HHG_GROUP_VARIANT_X(1, float, 2, 6, 1, 2, 7, true, false),  HHG_GROUP_VARIANT_X(1, float, 2, 6, 2, 2, 7, true, false),
     HHG_GROUP_VARIANT_X(0, double, 1, 11, 1, 2, 7, false, true), HHG_GROUP_VARIANT_X(0, double, 1, 11, 2, 2, 7, false, true),
     HHG_GROUP_VARIANT_X(0, double, 1, 12, 1, 2, 7, false, true), HHG_GROUP_VARIANT_X(0, double, 1, 12, 2, 2, 7, false, true),
     HHG_GROUP_VARIANT_X(1, float, 2, 12, 1, 2, 7, false, true),  HHG_GROUP_VARIANT_X(1, float, 2, 12, 2, 2, 7, false, true),
