@@ -25,6 +25,7 @@
 #include <stdexcept>
 
 #include "sbe_device.h"
+#include "warp_reduce.cuh"
 
 namespace hhg {
 namespace {
@@ -74,11 +75,6 @@ __device__ __forceinline__ V add(V a, V b) {
   return a;
 }
 
-__device__ __forceinline__ double warp_sum(double v) {
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-  return v;
-}
 
 __device__ __forceinline__ int wrap_mod(long long x, int n) {
   int r = (int)(x % n);
@@ -700,25 +696,21 @@ __device__ __forceinline__ void group_vctas(const SolveTables& t, const GroupDat
 
       // (4) current partials, summed over k in FP64
       const int slot = (ti / kJRing) & 1, s = ti % kJRing;
+      {
+        double re[3] = {0.0, 0.0, 0.0}, im[3] = {0.0, 0.0, 0.0};
 #pragma unroll
-      for (int a = 0; a < 3; ++a)
-        if (a < nj) {
-          double re = 0.0, im = 0.0;
+        for (int a = 0; a < 3; ++a)
+          if (a < nj) {
 #pragma unroll
-          for (int u = 0; u < EPT; ++u)
-            if (own[u]) {
-              const double wx = wk[a][u].x, wy = wk[a][u].y;
-              re = fma(wx, r[u].x, fma(wy, r[u].y, re));
-              im = fma(wy, r[u].x, fma(-wx, r[u].y, im));
-            }
-          re = warp_sum(re);
-          im = warp_sum(im);
-          if (lane == 0) {
-            double* dst = sJ + (((size_t)slot * kJRing + s) * nwarps + warp) * 2 * nj + 2 * a;
-            dst[0] = re;
-            dst[1] = im;
+            for (int u = 0; u < EPT; ++u)
+              if (own[u]) {
+                const double wx = wk[a][u].x, wy = wk[a][u].y;
+                re[a] = fma(wx, r[u].x, fma(wy, r[u].y, re[a]));
+                im[a] = fma(wy, r[u].x, fma(-wx, r[u].y, im[a]));
+              }
           }
-        }
+        warp_store_current(re, im, nj, lane, sJ + (((size_t)slot * kJRing + s) * nwarps + warp) * 2 * nj);
+      }
       if constexpr (PG) cp_async_wait_all();  // the next step's sums, before the barrier publishes them
       __syncthreads();
       // Flush a completed ring half: the other half is being written meanwhile.
