@@ -182,7 +182,8 @@ def run_serve(args, local: int):
         "queue_wait_s": {"p50": pct(queue_wait, 50), "p99": pct(queue_wait, 99)},
         "k_pt_rk4_steps_per_s": ksteps / span, "span_s": span, "wall_s": wall,
         "offered_load_req_per_s": n / reqs[-1][0],
-        "server": {k: (st[k] - base.get(k, 0) if k in ("completed", "chunks", "gpu_ms") else st[k]) for k in st},
+        "server": {k: (st[k] - base.get(k, 0) if k in ("completed", "chunks", "gpu_ms", "gap_ms", "setup_ms", "finish_ms")
+                       else st[k]) for k in st},
         "fp64_sequential_sample": {"requests": len(errs), "solves_per_hour": 3600.0 * len(errs) / seq_s,
                                    "k_pt_rk4_steps_per_s": seq_k / seq_s, "s_per_solve": seq_s / len(errs)},
         "J_rel_l2_mixed_vs_fp64": {"max": max(errs), "median": statistics.median(errs)},

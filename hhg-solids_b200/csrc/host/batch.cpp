@@ -156,11 +156,12 @@ struct SWEBatch {
     };
     auto reduce_and_copy = [&](SWESim* sim, cudaStream_t st) {
       hhg::launch_reduce_current(sim->d_Jpart.p, sim->shape.vctas, sim->nt, sim->Nk, sim->d_J.p, st);
-      check_cuda(cudaMemcpyAsync(sim->h_J, sim->d_J.p, sizeof(double2) * 3 * (size_t)sim->nt, cudaMemcpyDeviceToHost, st),
+      check_cuda(cudaMemcpyAsync(sim->host_J(), sim->d_J.p, sizeof(double2) * 3 * (size_t)sim->nt, cudaMemcpyDeviceToHost, st),
                  "D2H");
     };
 
     launches.assign(sims.size(), 0);
+    for (SWESim* sim : sims) sim->host_J();  // pinned current buffers, before the capture
     cudaGraph_t g = nullptr;
     check_cuda(cudaStreamBeginCapture(master, cudaStreamCaptureModeRelaxed), "cudaStreamBeginCapture");
     check_cuda(cudaEventRecord(fork, master), "event");
@@ -191,7 +192,7 @@ struct SWEBatch {
       check_cuda(cudaStreamWaitEvent(st, fork, 0), "cudaStreamWaitEvent");
       reset_and_clear(sim, st);
       launches[i] = hhg::launch_propagate(sim->tab, sim->gtab, sim->shape, sim->d_rho.p, sim->d_Jpart.p, sim->d_J.p, st);
-      check_cuda(cudaMemcpyAsync(sim->h_J, sim->d_J.p, sizeof(double2) * 3 * (size_t)sim->nt, cudaMemcpyDeviceToHost, st),
+      check_cuda(cudaMemcpyAsync(sim->host_J(), sim->d_J.p, sizeof(double2) * 3 * (size_t)sim->nt, cudaMemcpyDeviceToHost, st),
                  "D2H");
       check_cuda(cudaEventRecord(done[q], st), "event");
       check_cuda(cudaStreamWaitEvent(master, done[q], 0), "cudaStreamWaitEvent");
@@ -284,6 +285,8 @@ struct SWEServer {
   std::vector<cudaStream_t> streams;
   std::vector<cudaEvent_t> stream_done;
   cudaEvent_t chunk_begin = nullptr, chunk_end = nullptr, uploaded = nullptr;
+  cudaEvent_t ends[2] = {nullptr, nullptr};  // chunk_end alternates between these (GPU gaps between chunks)
+  bool have_prev_end = false;
   DevBuf<hhg::BatchDesc> d_desc;
   DevBuf<int2> d_items;
   DevBuf<int> d_counters;
@@ -297,6 +300,9 @@ struct SWEServer {
   int peak_active = 0;
   size_t peak_bytes = 0;
   double gpu_ms = 0.0;
+  double gap_ms = 0.0;    // GPU time between the end of a chunk and the start of the next one
+  double setup_ms = 0.0;  // host time setting up admitted solves
+  double finish_ms = 0.0; // host time completing finished solves
 
   double now() const { return std::chrono::duration<double>(Clock::now() - t0).count(); }
 
@@ -309,7 +315,8 @@ struct SWEServer {
     }
     check_cuda(cudaStreamCreateWithFlags(&master, cudaStreamNonBlocking), "cudaStreamCreate");
     check_cuda(cudaEventCreate(&chunk_begin), "cudaEventCreate");
-    check_cuda(cudaEventCreateWithFlags(&chunk_end, cudaEventBlockingSync), "cudaEventCreate");
+    for (auto* e : {&ends[0], &ends[1]}) check_cuda(cudaEventCreateWithFlags(e, cudaEventBlockingSync), "cudaEventCreate");
+    chunk_end = ends[0];
     check_cuda(cudaEventCreateWithFlags(&uploaded, cudaEventDisableTiming), "cudaEventCreate");
     thr = std::thread([this] { loop(); });
   }
@@ -323,7 +330,7 @@ struct SWEServer {
     if (thr.joinable()) thr.join();
     for (auto st : streams) cudaStreamDestroy(st);
     for (auto e : stream_done) cudaEventDestroy(e);
-    for (auto e : {chunk_begin, chunk_end, uploaded})
+    for (auto e : {chunk_begin, ends[0], ends[1], uploaded})
       if (e) cudaEventDestroy(e);
     if (master) cudaStreamDestroy(master);
     if (h_J) cudaFreeHost(h_J);
@@ -388,6 +395,7 @@ struct SWEServer {
       t->state = 1;
       t->t_admit = now();
     }
+    const auto s0 = Clock::now();
     try {
       if (!sim->ready) {
         sim->device = device;
@@ -400,6 +408,7 @@ struct SWEServer {
       check_cuda(cudaStreamSynchronize(sim->stream), "setup");
       for (auto& j : sim->Jhist) j.clear();
       const size_t actual = sim->device_bytes();
+      setup_ms += std::chrono::duration<double, std::milli>(Clock::now() - s0).count();
       std::lock_guard<std::mutex> lk(mu);
       used = used - t->reserved + actual;
       t->reserved = actual;
@@ -523,6 +532,7 @@ struct SWEServer {
       check_cuda(cudaEventRecord(stream_done[u], streams[u]), "event");
       check_cuda(cudaStreamWaitEvent(master, stream_done[u], 0), "cudaStreamWaitEvent");
     }
+    chunk_end = ends[chunks % 2];
     check_cuda(cudaEventRecord(chunk_end, master), "event");
     ++chunks;
   }
@@ -531,6 +541,15 @@ struct SWEServer {
     check_cuda(cudaEventSynchronize(chunk_end), "chunk");
     float ms = 0.f;
     if (cudaEventElapsedTime(&ms, chunk_begin, chunk_end) == cudaSuccess) gpu_ms += ms;
+    const cudaEvent_t prev_end = chunk_end == ends[0] ? ends[1] : ends[0];
+    if (have_prev_end && cudaEventElapsedTime(&ms, prev_end, chunk_begin) == cudaSuccess) gap_ms += ms;
+    have_prev_end = true;
+    const auto f0 = Clock::now();
+    struct AddFinish {
+      double& acc;
+      Clock::time_point t;
+      ~AddFinish() { acc += std::chrono::duration<double, std::milli>(Clock::now() - t).count(); }
+    } add_finish{finish_ms, f0};
     std::vector<Ticket*> finished, still;
     for (Ticket* t : active) {
       t->step = t->step1;
@@ -763,10 +782,11 @@ const char* SWEServer_ticket_error(SWEServer* srv, long long ticket) {
 int SWEServer_stats(SWEServer* srv, double* out, int n) {
   if (!srv || !out) return -1;
   std::lock_guard<std::mutex> lk(srv->mu);
-  const double v[9] = {(double)srv->completed, (double)srv->failed, (double)srv->chunks, srv->gpu_ms,
-                       (double)srv->peak_active, (double)srv->peak_bytes, (double)srv->budget,
-                       (double)srv->queue.size(), (double)srv->admitted};
-  const int m = n < 9 ? n : 9;
+  const double v[12] = {(double)srv->completed, (double)srv->failed, (double)srv->chunks, srv->gpu_ms,
+                        (double)srv->peak_active, (double)srv->peak_bytes, (double)srv->budget,
+                        (double)srv->queue.size(), (double)srv->admitted, srv->gap_ms, srv->setup_ms,
+                        srv->finish_ms};
+  const int m = n < 12 ? n : 12;
   for (int i = 0; i < m; ++i) out[i] = v[i];
   return m;
 }

@@ -258,6 +258,12 @@ void SWESim::init() {
     int least = 0, greatest = 0;
     check_cuda(cudaDeviceGetStreamPriorityRange(&least, &greatest), "cudaDeviceGetStreamPriorityRange");
     check_cuda(cudaStreamCreateWithPriority(&stream, cudaStreamNonBlocking, greatest), "cudaStreamCreate");
+    // Device buffers come from the device's stream-ordered pool, which keeps freed memory for reuse.
+    cudaMemPool_t pool = nullptr;
+    check_cuda(cudaDeviceGetDefaultMemPool(&pool, device), "cudaDeviceGetDefaultMemPool");
+    uint64_t keep = UINT64_MAX;
+    check_cuda(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep), "cudaMemPoolSetAttribute");
+    bind_buffers(stream);
     check_cuda(cudaEventCreate(&ev0), "cudaEventCreate");
     check_cuda(cudaEventCreate(&ev1), "cudaEventCreate");
     check_cuda(cudaEventCreate(&evm), "cudaEventCreate");
@@ -614,12 +620,6 @@ void SWESim::init() {
     d_pre.alloc((shape.pre_bytes + sizeof(double2) - 1) / sizeof(double2));
     gtab.pre = d_pre.p;
   }
-  if (!h_J || h_J_cap < (size_t)3 * nt) {
-    if (h_J) cudaFreeHost(h_J);
-    h_J = nullptr;
-    check_cuda(cudaMallocHost(&h_J, sizeof(double2) * 3 * (size_t)nt), "cudaMallocHost");
-    h_J_cap = (size_t)3 * nt;
-  }
 
   // Equilibrium density matrix (src/swe.cpp:82-90) on the GPU.
   {
@@ -677,6 +677,19 @@ size_t SWESim::footprint_estimate() const {
   return b;
 }
 
+// The pinned [3][nt] host copy of the current, allocated at the first run rather than at setup: a
+// solve set up by a server while others run never needs it (page-locking allocations can wait for
+// the device).
+double2* SWESim::host_J() {
+  if (!h_J || h_J_cap < (size_t)3 * nt) {
+    if (h_J) cudaFreeHost(h_J);
+    h_J = nullptr;
+    check_cuda(cudaMallocHost(&h_J, sizeof(double2) * 3 * (size_t)nt), "cudaMallocHost");
+    h_J_cap = (size_t)3 * nt;
+  }
+  return h_J;
+}
+
 void SWESim::finish_served(const double2* J) {
   std::vector<cd> keep[3];
   for (int a = 0; a < 3; ++a)
@@ -702,7 +715,7 @@ void SWESim::run() {
   last_launches = hhg::launch_propagate(tab, gtab, shape, d_rho.p, d_Jpart.p, d_J.p, stream, evm);
   check_cuda(cudaGetLastError(), "propagate launch");
   check_cuda(cudaEventRecord(ev1, stream), "event");
-  check_cuda(cudaMemcpyAsync(h_J, d_J.p, sizeof(double2) * 3 * (size_t)nt, cudaMemcpyDeviceToHost, stream), "D2H");
+  check_cuda(cudaMemcpyAsync(host_J(), d_J.p, sizeof(double2) * 3 * (size_t)nt, cudaMemcpyDeviceToHost, stream), "D2H");
   check_cuda(cudaStreamSynchronize(stream), "run_simulation");
   check_cuda(cudaEventElapsedTime(&last_ms, ev0, ev1), "event time");
   check_cuda(cudaEventElapsedTime(&last_prop_ms, ev0, evm), "event time");

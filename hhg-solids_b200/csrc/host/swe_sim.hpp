@@ -35,6 +35,11 @@ struct DevBuf {
   T* p = nullptr;
   size_t n = 0;
   size_t cap = 0;
+  // Set: allocations are stream-ordered on this stream, from the device's memory pool (no device-wide
+  // synchronisation, so a server can set solves up and retire them while others run).  The buffer
+  // may then be used on other streams only after the host has synchronised with this one.
+  cudaStream_t astream = nullptr;
+  bool pooled = false;
   // Keeps the current allocation when it is large enough (re-initialisation reuses buffers).
   void alloc(size_t count) {
     if (count == 0) count = 1;
@@ -43,17 +48,31 @@ struct DevBuf {
       return;
     }
     release();
-    check_cuda(cudaMalloc(&p, count * sizeof(T)), "cudaMalloc");
+    if (astream) {
+      check_cuda(cudaMallocAsync(reinterpret_cast<void**>(&p), count * sizeof(T), astream), "cudaMallocAsync");
+      pooled = true;
+    } else {
+      check_cuda(cudaMalloc(&p, count * sizeof(T)), "cudaMalloc");
+      pooled = false;
+    }
     n = cap = count;
   }
   void upload(const std::vector<T>& v, cudaStream_t s) {
     alloc(v.size());
     if (!v.empty()) check_cuda(cudaMemcpyAsync(p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, s), "H2D");
   }
+  // A pooled buffer is returned in the order of its stream: every use of it on any stream must have
+  // completed (the owners release only after synchronising).
   void release() {
-    if (p) cudaFree(p);
+    if (p) {
+      if (pooled)
+        cudaFreeAsync(p, astream);
+      else
+        cudaFree(p);
+    }
     p = nullptr;
     n = cap = 0;
+    pooled = false;
   }
   ~DevBuf() { release(); }
 };
@@ -105,7 +124,7 @@ struct SWESim {
   hhg::DevBuf<double> d_es, d_A, d_Rc, d_x0;
   hhg::SolveTables tab{};
   hhg::LaunchShape shape{};
-  double2* h_J = nullptr;  // pinned [3][nt]
+  double2* h_J = nullptr;  // pinned [3][nt] (host_J())
   size_t h_J_cap = 0;
   std::vector<hhg::cd> Jhist[3];
   float last_ms = 0.f, last_prop_ms = 0.f;
@@ -121,6 +140,14 @@ struct SWESim {
     for (auto& j : Jhist) j.clear();
   }
 
+  // Stream-ordered allocation of every device buffer on `s` (nullptr: plain cudaMalloc).
+  void bind_buffers(cudaStream_t s) {
+    for (auto* b : {&d_cell, &d_cellp, &d_win}) b->astream = s;
+    for (auto* b : {&d_H0, &d_R, &d_V, &d_Q, &d_Xbox, &d_Vd, &d_P, &d_T1, &d_T2, &d_rho0, &d_rho, &d_Jpart, &d_J, &d_pre})
+      b->astream = s;
+    for (auto* b : {&d_Xbox32, &d_Vd32, &d_P32, &d_T1_32, &d_T2_32}) b->astream = s;
+    for (auto* b : {&d_es, &d_A, &d_Rc, &d_x0}) b->astream = s;
+  }
   void release() {
     d_cell.release();
     d_cellp.release();
@@ -132,6 +159,8 @@ struct SWESim {
     d_A.release();
     d_Rc.release();
     d_x0.release();
+    d_pre.release();
+    bind_buffers(nullptr);
     if (h_J) cudaFreeHost(h_J);
     h_J = nullptr;
     h_J_cap = 0;
@@ -152,6 +181,7 @@ struct SWESim {
   // Upper bound of the device memory init() allocates for the current settings (parses the TB file).
   size_t footprint_estimate() const;
   // Keeps J[3][nt] as the current record (as run() does) and returns every device buffer.
+  double2* host_J();
   void finish_served(const double2* J);
 
   void tune_tiles(int sms);

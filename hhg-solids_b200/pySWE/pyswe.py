@@ -376,11 +376,11 @@ class SWEServer:
         return {"submit": out[0], "admit": out[1], "start": out[2], "done": out[3]}
 
     def stats(self) -> dict:
-        out = np.zeros(9)
-        self.lib.SWEServer_stats(self.ptr, out, 9)
+        out = np.zeros(12)
+        self.lib.SWEServer_stats(self.ptr, out, 12)
         keys = ("completed", "failed", "chunks", "gpu_ms", "peak_running", "peak_bytes", "budget_bytes", "queued",
-                "admitted")
-        return {k: (float(v) if k == "gpu_ms" else int(v)) for k, v in zip(keys, out)}
+                "admitted", "gap_ms", "setup_ms", "finish_ms")
+        return {k: (float(v) if k.endswith("_ms") else int(v)) for k, v in zip(keys, out)}
 
     def close(self):
         """Serves everything submitted, then stops the server."""

@@ -189,7 +189,8 @@ int SWEServer_status(SWEServer* srv, long long ticket);
 int SWEServer_times(SWEServer* srv, long long ticket, double* out4);
 const char* SWEServer_ticket_error(SWEServer* srv, long long ticket);
 /* Fills up to n of: completed, failed, chunks, GPU ms in chunks, peak running solves, peak reserved
- * bytes, budget bytes, queued, admitted; returns the count written. */
+ * bytes, budget bytes, queued, admitted, GPU ms between chunks, host ms setting up admitted solves,
+ * host ms completing finished ones; returns the count written. */
 int SWEServer_stats(SWEServer* srv, double* out, int n);
 /* Serves every request already submitted, then stops the scheduler and frees the server. */
 void SWEServer_delete(SWEServer* srv);
