@@ -14,6 +14,12 @@
 //    needs one CTA barrier; the phase factors of step t+2 are prepared two steps ahead in a
 //    three-slot ring.
 //  * the constant cell tables are copied to shared memory once per launch when they fit.
+//  * shapes with a Hermitian 7x7 cell box (TMD-like models of 6, 11 and 12 orbitals) are compiled with the
+//    box fixed (WBc), and may take the inner sums precomputed (PG): group_sums_kernel forms the sums
+//    of every column for a chunk of 64 steps, once per column instead of once per CTA of the column,
+//    and the propagation copies each step's block into shared memory with cp.async one step ahead.
+//  * in the mixed form such shapes hold two k-points per thread group (KP), each thread owning one
+//    element of both, and form the commutator's product in 2x2 register tiles.
 //
 // Precision.  Real = double: everything FP64 (the plain form).  Real = float (the mixed form): the
 // Wannier sums of H0 and r, the field coupling and the RK4 commutators in complex FP32; the state rho,
