@@ -967,14 +967,18 @@ struct GroupVariant {
   int precision, nw, nax, nj, wb;  // wb > 0: square wb x wb cell box with Hermitian halving
   bool kp;                          // k-point pairs
   bool pg;                          // precomputed inner sums
+  bool km;                          // k-space solver instance
   PlanFn plan;
   LaunchFn launch;
   BatchFn batch;
 };
 #define HHG_GROUP_VARIANT_X(P, R, E, NW, NAX, NJ, WB, KP, PG)                                      \
-  {P, NW, NAX, NJ, WB, KP, PG, plan_group_t<R, E, NW, NAX, NJ, false, WB, KP, PG>,                  \
+  {P, NW, NAX, NJ, WB, KP, PG, false, plan_group_t<R, E, NW, NAX, NJ, false, WB, KP, PG>,           \
    launch_group_t<R, E, NW, NAX, NJ, false, WB, KP, PG>, launch_group_batch_t<R, E, NW, NAX, NJ, false, WB, KP>}
 #define HHG_GROUP_VARIANT(P, R, E, NW, NAX, NJ, WB) HHG_GROUP_VARIANT_X(P, R, E, NW, NAX, NJ, WB, false, false)
+#define HHG_GROUP_VARIANT_KM(P, R, E, NW, NAX, NJ, WB)                                             \
+  {P, NW, NAX, NJ, WB, false, false, true, plan_group_t<R, E, NW, NAX, NJ, true, WB>,              \
+   launch_group_t<R, E, NW, NAX, NJ, true, WB>, launch_group_batch_t<R, E, NW, NAX, NJ, true, WB>}
 // Listed in order of preference: a solve runs the first one that matches it.  (The persistent batch
 // launch of a precomputed-sum shape runs its in-kernel-sum instance.)
 const GroupVariant kGroupVariants[] = {
@@ -999,9 +1003,15 @@ const GroupVariant kGroupVariants[] = {
     HHG_GROUP_VARIANT(1, float, 2, 12, 1, 2, 0),  HHG_GROUP_VARIANT(1, float, 2, 12, 2, 2, 0),
     HHG_GROUP_VARIANT(1, float, 1, 6, 1, 2, 0),   HHG_GROUP_VARIANT(1, float, 1, 6, 2, 2, 0),
     HHG_GROUP_VARIANT(1, float, 1, 2, 1, 2, 0),   HHG_GROUP_VARIANT(1, float, 1, 2, 2, 2, 0),
+    // k-space solver (three evaluation points per step): the compiled 7x7 box only.
+    HHG_GROUP_VARIANT_KM(0, double, 1, 11, 1, 2, 7), HHG_GROUP_VARIANT_KM(0, double, 1, 11, 2, 2, 7),
+    HHG_GROUP_VARIANT_KM(0, double, 1, 12, 1, 2, 7), HHG_GROUP_VARIANT_KM(0, double, 1, 12, 2, 2, 7),
+    HHG_GROUP_VARIANT_KM(1, float, 2, 11, 1, 2, 7),  HHG_GROUP_VARIANT_KM(1, float, 2, 11, 2, 2, 7),
+    HHG_GROUP_VARIANT_KM(1, float, 2, 12, 1, 2, 7),  HHG_GROUP_VARIANT_KM(1, float, 2, 12, 2, 2, 7),
 };
 #undef HHG_GROUP_VARIANT
 #undef HHG_GROUP_VARIANT_X
+#undef HHG_GROUP_VARIANT_KM
 
 const GroupVariant* find_variant(const SolveTables& t, int precision) {
   if (const char* env = std::getenv("HHG_GROUP_GENERIC"))
@@ -1021,6 +1031,7 @@ const GroupVariant* find_variant(const SolveTables& t, int precision) {
   const GroupGeom gg = group_geom(t);
   for (const GroupVariant& v : kGroupVariants) {
     if (v.precision != precision || v.nw != t.nw || v.nax != t.nax || v.nj != t.nj) continue;
+    if (v.km != (t.kmode != 0)) continue;
     if (v.wb > 0 && (any_box || !gg.half || t.b1n != v.wb || t.b2n != v.wb)) continue;
     if (v.kp && no_pair) continue;
     if (v.pg && no_pre) continue;
@@ -1033,11 +1044,9 @@ const GroupVariant* find_variant(const SolveTables& t, int precision) {
 
 bool plan_group(const SolveTables& t, int precision, int sm_count, LaunchShape* out, char* why, int why_len,
                 int tile_hint) {
-  if (!t.kmode) {
-    if (const GroupVariant* v = find_variant(t, precision)) {
-      out->variant = (int)(v - kGroupVariants);
-      return v->plan(t, sm_count, out, why, why_len, tile_hint);
-    }
+  if (const GroupVariant* v = find_variant(t, precision)) {
+    out->variant = (int)(v - kGroupVariants);
+    return v->plan(t, sm_count, out, why, why_len, tile_hint);
   }
   out->variant = -1;
   // Runtime-shaped: two elements per thread in the mixed form once a k-point needs more than a warp.
