@@ -240,7 +240,6 @@ __device__ __forceinline__ void group_vctas(const SolveTables& t, const GroupDat
   const GroupGeom gg = group_geom(t);
   const int nw = NWc ? NWc : t.nw, nw2 = nw * nw, nax = NAXc ? NAXc : t.nax, nj = NJc ? NJc : t.nj;
   static_assert(!KP || (EPT == 2 && NWc > 0 && sizeof(Real) == 4 && !KM), "k-point pairs: mixed form, fixed shape");
-  static_assert(!PG || !KM, "precomputed sums: real-space solver");
   constexpr int KPG = KP ? 2 : 1;                      // k-points per thread group
   constexpr int EU = KP ? 1 : EPT;                     // distinct elements per thread
   constexpr int NP = KP ? (NWc + 1) / 2 * 2 : 1;       // padded side of the tile layout
@@ -417,13 +416,15 @@ __device__ __forceinline__ void group_vctas(const SolveTables& t, const GroupDat
 
     const int step0 = t.step0, step1 = t.step1;
     // Precomputed inner sums of point s (box rows into buffer s % gbufs, window rows into s & 1).
-    auto fetch_sums = [&](int s) {
-      const size_t blk = (size_t)(s - step0) * t.N2 + m2;
+    // The k-space solver's points are 2 step0 ... 2 step1 and its window rows are the same for all
+    // of them (one block per column).
+    auto fetch_sums = [&](int s, bool win) {
+      const size_t blk = (size_t)(s - (km ? 2 * step0 : step0)) * t.N2 + m2;
       const char* src = reinterpret_cast<const char*>(d.Gpre + blk * gbuf);
       char* dst = reinterpret_cast<char*>(Gb + (s % gbufs) * gbuf);
-      const double2* wsrc = d.GWpre + blk * wbuf;
+      const double2* wsrc = d.GWpre + (km ? (size_t)m2 : blk) * wbuf;
       double2* wdst = GWb + (s & 1) * wbuf;
-      const int nA = (int)(gbuf * sizeof(V) / 16), nB = (int)wbuf;
+      const int nA = (int)(gbuf * sizeof(V) / 16), nB = win ? (int)wbuf : 0;
       for (int idx = tid; idx < nA + nB; idx += nthr) {
         if (idx < nA)
           cp_async16(dst + (size_t)idx * 16, src + (size_t)idx * 16);
@@ -522,7 +523,7 @@ __device__ __forceinline__ void group_vctas(const SolveTables& t, const GroupDat
       if (step0 + 1 < step1) make_phases(step0 + 1, true);
       __syncthreads();
       if constexpr (PG) {
-        fetch_sums(step0);
+        fetch_sums(step0, true);
         cp_async_wait_all();
       } else {
         inner_sums(step0, true);
@@ -534,7 +535,13 @@ __device__ __forceinline__ void group_vctas(const SolveTables& t, const GroupDat
       const int j0 = 2 * step0, jmax = 2 * step1;
       for (int j = j0; j <= j0 + 4 && j <= jmax; ++j) make_phases(j, j == j0);
       __syncthreads();
-      for (int j = j0; j <= j0 + 2 && j <= jmax; ++j) inner_sums(j, j == j0);
+      for (int j = j0; j <= j0 + 2 && j <= jmax; ++j) {
+        if constexpr (PG)
+          fetch_sums(j, j == j0);
+        else
+          inner_sums(j, j == j0);
+      }
+      if constexpr (PG) cp_async_wait_all();
       __syncthreads();
       outer_box(j0, hc, rc);
       outer_window(j0);
@@ -555,15 +562,20 @@ __device__ __forceinline__ void group_vctas(const SolveTables& t, const GroupDat
       if (!km) {
         if (ti + 2 < step1) make_phases(ti + 2, true);
         if constexpr (PG) {
-          if (ti + 1 < step1) fetch_sums(ti + 1);
+          if (ti + 1 < step1) fetch_sums(ti + 1, true);
         } else {
           if (ti + 1 < step1) inner_sums(ti + 1, true);
         }
       } else {
         if (2 * ti + 5 <= 2 * step1) make_phases(2 * ti + 5, false);
         if (2 * ti + 6 <= 2 * step1) make_phases(2 * ti + 6, false);
-        if (2 * ti + 3 <= 2 * step1) inner_sums(2 * ti + 3, false);
-        if (2 * ti + 4 <= 2 * step1) inner_sums(2 * ti + 4, false);
+        if constexpr (PG) {
+          if (2 * ti + 3 <= 2 * step1) fetch_sums(2 * ti + 3, false);
+          if (2 * ti + 4 <= 2 * step1) fetch_sums(2 * ti + 4, false);
+        } else {
+          if (2 * ti + 3 <= 2 * step1) inner_sums(2 * ti + 3, false);
+          if (2 * ti + 4 <= 2 * step1) inner_sums(2 * ti + 4, false);
+        }
       }
 
       // (3) RK4 stages (src/solver.cpp:157-163): fields at t, t+dt/2, t+dt/2, t+dt
@@ -748,9 +760,11 @@ __device__ __forceinline__ void group_vctas(const SolveTables& t, const GroupDat
 constexpr int kMaxPreBox = 64;  // widest cell box of the precomputed-sum shapes
 constexpr int kPreChunk = 64;   // steps per precompute + propagate launch pair
 
-// Inner Wannier sums of every column for the steps [t.step0, t.step1) of the real-space solver:
-// block (s, m2) forms the box rows G_e = sum_q p2(q) X(mat, q1s + qq, q)_e and the window rows with
-// the operations (and their order) of group_vctas's inner_sums, into [s - t.step0][m2][row][nw2].
+// Inner Wannier sums of every column for the steps [t.step0, t.step1): block (s, m2) forms the box
+// rows G_e = sum_q p2(q) X(mat, q1s + qq, q)_e and the window rows with the operations (and their
+// order) of group_vctas's inner_sums, into [s - t.step0][m2][row][nw2].  For the k-space solver the
+// points are 2 step0 ... 2 step1 and the window rows, the same for every point, are written once per
+// column ([m2][row][nw2], by the blocks of the first point).
 template <typename Real>
 __global__ void __launch_bounds__(256) group_sums_kernel(SolveTables t, GroupData<Real> d, int q1s, int nq1,
                                                          int nbrows, int nwrows, typename Cx<Real>::T* Gpre,
@@ -758,7 +772,7 @@ __global__ void __launch_bounds__(256) group_sums_kernel(SolveTables t, GroupDat
   using V = typename Cx<Real>::T;
   __shared__ V q2[kMaxPreBox];
   __shared__ double2 w2[4];
-  const int sl = blockIdx.x / t.N2, m2 = blockIdx.x % t.N2, s = t.step0 + sl;
+  const int sl = blockIdx.x / t.N2, m2 = blockIdx.x % t.N2, s = (t.kmode ? 2 * t.step0 : t.step0) + sl;
   const int npw = 2 * t.np + 1, W1n = t.b1n, W2n = t.b2n, nw2 = t.nw2;
   const V* P2 = d.P + (size_t)s * 2 * npw + t.np + npw;
   const double2* P2d = d.Pd + (size_t)s * 2 * npw + t.np + npw;
@@ -767,7 +781,8 @@ __global__ void __launch_bounds__(256) group_sums_kernel(SolveTables t, GroupDat
       q2[idx] = mul(d.T2[wrap_mod((long long)m2 * (t.b2lo + idx), t.N2)], P2[t.b2lo + idx]);
     } else {
       const int q = idx - W2n;
-      w2[q] = mul(d.T2d[wrap_mod((long long)m2 * (q - 2), t.N2)], P2d[q - 2]);
+      const double2 tw = d.T2d[wrap_mod((long long)m2 * (q - 2), t.N2)];
+      w2[q] = t.kmode ? tw : mul(tw, P2d[q - 2]);
     }
   }
   __syncthreads();
@@ -779,7 +794,8 @@ __global__ void __launch_bounds__(256) group_sums_kernel(SolveTables t, GroupDat
     for (int q = 0; q < W2n; ++q) acc = fmac(q2[q], X[(size_t)q * nw2 + e], acc);
     G[idx] = acc;
   }
-  double2* GW = GWpre + (size_t)blockIdx.x * nwrows * nw2;
+  if (t.kmode && sl > 0) return;
+  double2* GW = GWpre + (size_t)(t.kmode ? m2 : blockIdx.x) * nwrows * nw2;
   for (int idx = threadIdx.x; idx < nwrows * nw2; idx += blockDim.x) {
     const int wr = idx / nw2, e = idx % nw2;
     const double2* X = d.Xwin + (size_t)wr * 4 * nw2;
@@ -876,7 +892,8 @@ bool plan_group_t(const SolveTables& t, int sm_count, LaunchShape* out, char* wh
       return false;
     }
     out->pre_chunk = std::min(kPreChunk, t.nt);
-    out->pre_bytes = (size_t)out->pre_chunk * t.N2 * (gbytes + wbytes);
+    out->pre_bytes = KM ? (size_t)(2 * out->pre_chunk + 1) * t.N2 * gbytes + (size_t)t.N2 * wbytes
+                        : (size_t)out->pre_chunk * t.N2 * (gbytes + wbytes);
   }
   auto kern = propagate_group_kernel<Real, EPT, NWc, NAXc, NJc, KM, WBc, KP, PG>;
   const size_t smem_max = bytes(best, box_sm, win_sm);
@@ -919,7 +936,8 @@ int launch_group_t(const SolveTables& t, const GroupTables& gt, const LaunchShap
     const GroupGeom gg = group_geom(t);
     const size_t gbuf = (size_t)gg.nbrows * t.nw2, wbuf = (size_t)gg.nwrows * t.nw2;
     V* Gpre = static_cast<V*>(gt.pre);
-    double2* GWpre = reinterpret_cast<double2*>(static_cast<char*>(gt.pre) + (size_t)s.pre_chunk * t.N2 * gbuf * sizeof(V));
+    const size_t npts_max = KM ? 2 * (size_t)s.pre_chunk + 1 : (size_t)s.pre_chunk;
+    double2* GWpre = reinterpret_cast<double2*>(static_cast<char*>(gt.pre) + npts_max * t.N2 * gbuf * sizeof(V));
     d.Gpre = Gpre;
     d.GWpre = GWpre;
     auto kern = propagate_group_kernel<Real, EPT, NWc, NAXc, NJc, KM, WBc, KP, true>;
@@ -929,8 +947,9 @@ int launch_group_t(const SolveTables& t, const GroupTables& gt, const LaunchShap
       SolveTables tc = t;
       tc.step0 = c0;
       tc.step1 = std::min(c0 + s.pre_chunk, t.step1);
-      group_sums_kernel<Real><<<(tc.step1 - c0) * t.N2, 256, 0, stream>>>(tc, d, gg.q1s, gg.nq1, gg.nbrows, gg.nwrows,
-                                                                          Gpre, GWpre);
+      const int npts = KM ? 2 * (tc.step1 - c0) + 1 : tc.step1 - c0;
+      group_sums_kernel<Real><<<npts * t.N2, 256, 0, stream>>>(tc, d, gg.q1s, gg.nq1, gg.nbrows, gg.nwrows, Gpre,
+                                                               GWpre);
       kern<<<s.ctas, s.threads, s.smem, stream>>>(tc, d, s.k_per_cta, s.group, s.box_sm, s.win_sm, s.vctas, rho, Jpart);
       launches += 2;
     }
@@ -976,9 +995,9 @@ struct GroupVariant {
   {P, NW, NAX, NJ, WB, KP, PG, false, plan_group_t<R, E, NW, NAX, NJ, false, WB, KP, PG>,           \
    launch_group_t<R, E, NW, NAX, NJ, false, WB, KP, PG>, launch_group_batch_t<R, E, NW, NAX, NJ, false, WB, KP>}
 #define HHG_GROUP_VARIANT(P, R, E, NW, NAX, NJ, WB) HHG_GROUP_VARIANT_X(P, R, E, NW, NAX, NJ, WB, false, false)
-#define HHG_GROUP_VARIANT_KM(P, R, E, NW, NAX, NJ, WB)                                             \
-  {P, NW, NAX, NJ, WB, false, false, true, plan_group_t<R, E, NW, NAX, NJ, true, WB>,              \
-   launch_group_t<R, E, NW, NAX, NJ, true, WB>, launch_group_batch_t<R, E, NW, NAX, NJ, true, WB>}
+#define HHG_GROUP_VARIANT_KM(P, R, E, NW, NAX, NJ, WB, PG)                                         \
+  {P, NW, NAX, NJ, WB, false, PG, true, plan_group_t<R, E, NW, NAX, NJ, true, WB, false, PG>,      \
+   launch_group_t<R, E, NW, NAX, NJ, true, WB, false, PG>, launch_group_batch_t<R, E, NW, NAX, NJ, true, WB>}
 // Listed in order of preference: a solve runs the first one that matches it.  (The persistent batch
 // launch of a precomputed-sum shape runs its in-kernel-sum instance.)
 const GroupVariant kGroupVariants[] = {
@@ -1004,10 +1023,14 @@ const GroupVariant kGroupVariants[] = {
     HHG_GROUP_VARIANT(1, float, 1, 6, 1, 2, 0),   HHG_GROUP_VARIANT(1, float, 1, 6, 2, 2, 0),
     HHG_GROUP_VARIANT(1, float, 1, 2, 1, 2, 0),   HHG_GROUP_VARIANT(1, float, 1, 2, 2, 2, 0),
     // k-space solver (three evaluation points per step): the compiled 7x7 box only.
-    HHG_GROUP_VARIANT_KM(0, double, 1, 11, 1, 2, 7), HHG_GROUP_VARIANT_KM(0, double, 1, 11, 2, 2, 7),
-    HHG_GROUP_VARIANT_KM(0, double, 1, 12, 1, 2, 7), HHG_GROUP_VARIANT_KM(0, double, 1, 12, 2, 2, 7),
-    HHG_GROUP_VARIANT_KM(1, float, 2, 11, 1, 2, 7),  HHG_GROUP_VARIANT_KM(1, float, 2, 11, 2, 2, 7),
-    HHG_GROUP_VARIANT_KM(1, float, 2, 12, 1, 2, 7),  HHG_GROUP_VARIANT_KM(1, float, 2, 12, 2, 2, 7),
+    HHG_GROUP_VARIANT_KM(0, double, 1, 11, 1, 2, 7, true), HHG_GROUP_VARIANT_KM(0, double, 1, 11, 2, 2, 7, true),
+    HHG_GROUP_VARIANT_KM(0, double, 1, 12, 1, 2, 7, true), HHG_GROUP_VARIANT_KM(0, double, 1, 12, 2, 2, 7, true),
+    HHG_GROUP_VARIANT_KM(1, float, 2, 11, 1, 2, 7, true),  HHG_GROUP_VARIANT_KM(1, float, 2, 11, 2, 2, 7, true),
+    HHG_GROUP_VARIANT_KM(1, float, 2, 12, 1, 2, 7, true),  HHG_GROUP_VARIANT_KM(1, float, 2, 12, 2, 2, 7, true),
+    HHG_GROUP_VARIANT_KM(0, double, 1, 11, 1, 2, 7, false), HHG_GROUP_VARIANT_KM(0, double, 1, 11, 2, 2, 7, false),
+    HHG_GROUP_VARIANT_KM(0, double, 1, 12, 1, 2, 7, false), HHG_GROUP_VARIANT_KM(0, double, 1, 12, 2, 2, 7, false),
+    HHG_GROUP_VARIANT_KM(1, float, 2, 11, 1, 2, 7, false),  HHG_GROUP_VARIANT_KM(1, float, 2, 11, 2, 2, 7, false),
+    HHG_GROUP_VARIANT_KM(1, float, 2, 12, 1, 2, 7, false),  HHG_GROUP_VARIANT_KM(1, float, 2, 12, 2, 2, 7, false),
 };
 #undef HHG_GROUP_VARIANT
 #undef HHG_GROUP_VARIANT_X
