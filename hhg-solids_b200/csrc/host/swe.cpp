@@ -672,8 +672,10 @@ size_t SWESim::footprint_estimate() const {
   b += nt_ * 2 * (2 * np_ + 1) * c16 * 3 / 2;                     // P, FP64 and FP32
   b += (4 * box + 4 * ns + 6 * hhg::kWindow) * w2 * c16 * 3 / 2;  // cell tables, both precisions
   b += (N1_ + N2_) * c16 * 3 / 2 + (size_t(1) << 20);
-  // Precomputed inner sums: 64 steps x N2 columns x (box rows of H0 and r_a, window rows) x nw2.
-  b += std::min<size_t>(64, nt_) * N2_ * ((size_t)4 * (np_ + 1) + 12) * w2 * c16;
+  // Precomputed inner sums: 64 steps (2 x 64 + 1 points for the k-space solver) x N2 columns x (box
+  // rows of H0 and r_a, window rows) x nw2.
+  const size_t pre_pts = solver == 1 ? 2 * std::min<size_t>(64, nt_) + 1 : std::min<size_t>(64, nt_);
+  b += pre_pts * N2_ * ((size_t)4 * (np_ + 1) + 12) * w2 * c16;
   return b;
 }
 
