@@ -205,8 +205,8 @@ struct GroupData {
   const double2* Pd;
   const double2* T1d;
   const double2* T2d;
-  const V* Gpre;          // precomputed inner sums [step in chunk][N2][nbrows][nw2] (or null)
-  const double2* GWpre;   // and of the window rows [step in chunk][N2][nwrows][nw2]
+  const V* Gpre;          // precomputed inner sums [point in chunk][N2][nbrows][nw2] (or null)
+  const double2* GWpre;   // window rows [point in chunk][N2][nwrows][nw2] (k-space solver: [N2][nwrows][nw2])
 };
 
 // 16-byte asynchronous copy global -> shared (completes at cp_async_wait_all).
