@@ -37,6 +37,25 @@ __device__ __forceinline__ double kc_warp_sum(double v) {
   for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
   return v;
 }
+// Sums 32 values over the 32 lanes of a warp with 31 shuffles: at each level every lane keeps half
+// of its values and sends the other half to its partner.  Lane l returns the sum of value l.
+__device__ __forceinline__ double kc_transpose_sum32(double (&v)[32], int lane) {
+#pragma unroll
+  for (int o = 16; o >= 1; o >>= 1) {
+    const bool hi = (lane & o) != 0;
+#pragma unroll
+    for (int i = 0; i < o; ++i) {
+      const double keep = hi ? v[i + o] : v[i];
+      const double send = hi ? v[i] : v[i + o];
+      v[i] = keep + __shfl_xor_sync(0xffffffffu, send, o);
+    }
+  }
+  return v[0];
+}
+
+// Steps per flush of the window-contracted current partials (see the kernel).
+constexpr int kRJ = 16;
+
 __device__ __forceinline__ int kc_wrap(long long x, int n) {
   int r = (int)(x % n);
   return r < 0 ? r + n : r;
@@ -47,7 +66,9 @@ constexpr int kKcolMaxThreads = 256;
 // Shared-memory layout (complex double units unless noted), shared by host planning and kernel.
 struct KcolLayout {
   size_t t1, G, GW, p2, total_cx, E_d, J_d;
+  bool rj;  // window-contracted current (nw = 2, real-space solver)
   __host__ __device__ KcolLayout(const SolveTables& t, int threads) {
+    rj = !t.kmode && t.nw == 2;
     const size_t nmat = 1 + t.nax, nw2 = t.nw2, pts = t.kmode ? 2 * kRing + 1 : kRing;
     size_t p = 0;
     t1 = p;
@@ -63,7 +84,8 @@ struct KcolLayout {
     J_d = kRing * 9;
   }
   __host__ __device__ size_t bytes(int threads) const {
-    return total_cx * sizeof(double2) + (J_d + (size_t)kRing * (threads / 32) * 2 * 3) * sizeof(double);
+    const size_t jd = rj ? (size_t)kRJ * (threads / 32) * 32 : (size_t)kRing * (threads / 32) * 2 * 3;
+    return total_cx * sizeof(double2) + (J_d + jd) * sizeof(double);
   }
 };
 
@@ -71,6 +93,12 @@ template <int NW, int NAXc, int NJc, bool KM>
 __global__ void __launch_bounds__(kKcolMaxThreads) propagate_kcol_kernel(SolveTables t, GroupTables gt, int R,
                                                                          int vctas, double2* rho, double2* Jpart) {
   constexpr int NW2 = NW * NW;
+  // Window-contracted current (nw = 2, real-space solver): J_a = sum_{w1,e} GW_a,e(w1) R(w1, e) with
+  // R(w1, e) = sum_k tw1(k, w1) conj(rho_e(k)), the same sum as sum_k Tr(W_a(k) rho(k)^*) in another
+  // order.  Each thread forms its 16 values of R per step (no per-k window sum), a warp reduces its
+  // 32 doubles with one transposed reduction, and every kRJ steps the CTA contracts them with the
+  // column's window sums.
+  constexpr bool RJ = NW == 2 && !KM;
   extern __shared__ __align__(16) unsigned char smraw[];
   const int nax = NAXc ? NAXc : t.nax, nj = NJc ? NJc : t.nj, nmat = 1 + nax;
   const int b1n = t.b1n, b2n = t.b2n, npw = 2 * t.np + 1;
@@ -160,6 +188,9 @@ __global__ void __launch_bounds__(kKcolMaxThreads) propagate_kcol_kernel(SolveTa
     for (int e = 0; e < NW2; ++e) r[e] = kval ? rho[k * NW2 + e] : make_double2(0.0, 0.0);
     for (int q = 0; q < b1n; ++q) sT1[q * nthr + tid] = t.T1[kc_wrap((long long)m1 * (t.b1lo + q), t.N1)];
     for (int q = 0; q < 4; ++q) sT1[(b1n + q) * nthr + tid] = t.T1[kc_wrap((long long)m1 * (q - 2), t.N1)];
+    double2 twr[4];  // this thread's window row twiddles (RJ)
+#pragma unroll
+    for (int q = 0; q < 4; ++q) twr[q] = t.T1[kc_wrap((long long)m1 * (q - 2), t.N1)];
 
     for (int ti0 = t.step0; ti0 < t.step1; ti0 += kRing) {
       const int nsteps = min(kRing, t.step1 - ti0);
@@ -211,7 +242,7 @@ __global__ void __launch_bounds__(kKcolMaxThreads) propagate_kcol_kernel(SolveTa
       for (int s = 0; s < nsteps; ++s) {
         if (!KM) {
           box_sums(s);
-          window_sums(s);
+          if (!RJ) window_sums(s);
         } else if (s == 0) {
           box_sums(0);  // point t of the chunk's first step; later steps carry it from stage 4
         }
@@ -281,6 +312,50 @@ __global__ void __launch_bounds__(kKcolMaxThreads) propagate_kcol_kernel(SolveTa
         }
 
         // Current partials.
+        if constexpr (RJ) {
+          double vals[32];
+#pragma unroll
+          for (int w1 = 0; w1 < 4; ++w1)
+#pragma unroll
+            for (int e = 0; e < 4; ++e) {
+              const double2 tw = twr[w1];
+              vals[(w1 * 4 + e) * 2] = kval ? fma(tw.x, r[e].x, tw.y * r[e].y) : 0.0;
+              vals[(w1 * 4 + e) * 2 + 1] = kval ? fma(tw.y, r[e].x, -tw.x * r[e].y) : 0.0;
+            }
+          const double val = kc_transpose_sum32(vals, lane);
+          sJ[((s % kRJ) * nwarps + warp) * 32 + lane] = val;
+          if (s % kRJ == kRJ - 1 || s == nsteps - 1) {
+            const int s0f = s - s % kRJ, ns = s - s0f + 1;
+            __syncthreads();
+            // Warps' partials, in warp order, into warp 0's slot.
+            for (int idx = tid; idx < ns * 32; idx += nthr) {
+              const int ss = idx >> 5, l = idx & 31;
+              double acc = 0.0;
+              for (int q = 0; q < nwarps; ++q) acc += sJ[(ss * nwarps + q) * 32 + l];
+              sJ[(ss * nwarps) * 32 + l] = acc;
+            }
+            __syncthreads();
+            for (int idx = tid; idx < ns * nj; idx += nthr) {
+              const int ss = idx / nj, a = idx % nj;
+              const double* Rv = sJ + (ss * nwarps) * 32;
+              double re = 0.0, im = 0.0;
+#pragma unroll
+              for (int w1 = 0; w1 < 4; ++w1) {
+                const double2* g = sGW + ((size_t)((s0f + ss) * 4 + w1) * nj + a) * NW2;
+#pragma unroll
+                for (int e = 0; e < 4; ++e) {
+                  const double rx = Rv[(w1 * 4 + e) * 2], ry = Rv[(w1 * 4 + e) * 2 + 1];
+                  re = fma(g[e].x, rx, fma(-g[e].y, ry, re));
+                  im = fma(g[e].x, ry, fma(g[e].y, rx, im));
+                }
+              }
+              double2* dst = Jpart + ((size_t)v * t.nt + ti0 + s0f + ss) * 3 + t.j_id[a];
+              const double2 old = *dst;
+              *dst = make_double2(old.x + re, old.y + im);
+            }
+            __syncthreads();  // the slots are rewritten by the next steps
+          }
+        } else {
 #pragma unroll
         for (int a = 0; a < 3; ++a)
           if (a < nj) {
@@ -299,7 +374,9 @@ __global__ void __launch_bounds__(kKcolMaxThreads) propagate_kcol_kernel(SolveTa
               sJ[(s * nwarps + warp) * 2 * nj + 2 * a + 1] = im;
             }
           }
+        }
       }
+      if constexpr (RJ) continue;  // flushed inside the step loop
       __syncthreads();
       // Add the chunk's per-warp partials into this virtual CTA's row.
       for (int idx = tid; idx < nsteps * nj; idx += nthr) {
