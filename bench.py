@@ -1,11 +1,17 @@
 #!/usr/bin/env python
 """Benchmark of the SBE propagation: k-point x RK4-step throughput of one B200 (or N, one process each).
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload c1|c0|c2] [--impl ours|reference]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload c2|c0|c1|c3|c4] [--precision mixed|fp64]
+                    [--batch B] [--impl ours|reference]
 
 A *step* is one full solve of the workload: nt RK4 steps of every k-point plus the current J(t).
-The default workload is "c1": the 2-orbital Haldane-like model on a 200 x 200 k-grid under the
-full pulse (nt = 4096), plain FP64 -- the drop-in configuration for the reference's propagation.
+The default workload is "c2" in the mixed form: the 11-orbital TMD-like model (seed 7, 49 R cells)
+on a 150 x 150 k-grid under the full pulse (nt = 4096), with complex-FP32 Wannier sums and
+commutators and an FP64 state, RK4 accumulation, window velocity and k-sum.  Beside it the same
+line carries the plain-FP64 solve of the same configuration (time, J error of the mixed form
+against it, per-odd-harmonic intensity errors up to the cutoff) and B = 4 mixed solves run as one
+SWEBatch (per-solve time and throughput against the FP64 solo solve).  --workload c1 --precision
+fp64 is the 2-orbital 200 x 200 drop-in configuration.
 
 Printed JSON line (rank 0):
   value         k-pt*RK4-steps/s of the whole job, from CUDA events around the propagation kernels
@@ -13,10 +19,15 @@ Printed JSON line (rank 0):
   e2e           the same metric through the reference-facing C ABI: SWESim_restart (TB parse,
                 placement, host->device tables, rho0 on the GPU) + SWESim_run_simulation +
                 SWESim_get_current into host arrays, wall-clocked.
-  roofline      the propagation kernel's algorithmic FP64 rate against the FP64 FMA peak measured
-                live on the same GPU (the driver's peaks file has HBM and bf16 only).
-  cpu_baseline  the reference's own CPU build (oracle/_ref/libwannier.so) on the host cores, one
-                single-threaded process per core (the reference's pol_scan model), bounded sample.
+  roofline      the propagation kernel's algorithmic rate against the FP64 (plain form) or blended
+                FP64+FP32 (mixed form) FMA peak measured live on the same GPU (the driver's peaks
+                file has HBM and bf16 only).
+  mixed_vs_fp64 (mixed form) the plain-FP64 solve's time, the speed-up, J rel-L2 and the largest
+                per-odd-harmonic intensity error of the mixed form against it, and the batched figure.
+  cpu_baseline  the reference's own CPU build (oracle/_ref/libwannier.so: its unmodified sources,
+                with an FFT shim standing in for the absent FFTW3) on the host cores, one
+                single-threaded process per core (the reference's pol_scan model); a few RK4 steps
+                are timed and the rate per k-point step is extrapolated to the full pulse.
 
 With --impl reference the line instead times that reference CPU build alone on all host cores.
 For N > 1 (torchrun), every rank runs its own solve at its own polarisation angle (replicas, no
@@ -41,11 +52,11 @@ sys.path.insert(0, PKG)
 PULSE = dict(tmax=90.0, dt=21.97e-3, intensity=1e12, tmax_field=80.0, phi_vec=[0.0, 0.0, 0.0], **{"lambda": 3000.0})
 WORKLOADS = {
     "c0": dict(model="haldane", n=60, window=5,
-               desc="2-orbital Haldane-like TB (a=2.5 A, 25 R cells), 60x60 k-grid, full pulse, plain FP64"),
+               desc="2-orbital Haldane-like TB (a=2.5 A, 25 R cells), 60x60 k-grid, full pulse"),
     "c1": dict(model="haldane", n=200, window=5,
-               desc="2-orbital Haldane-like TB (a=2.5 A, 25 R cells), 200x200 k-grid, full pulse, plain FP64"),
+               desc="2-orbital Haldane-like TB (a=2.5 A, 25 R cells), 200x200 k-grid, full pulse"),
     "c2": dict(model="tmd11_s7", n=150, window=7,
-               desc="11-orbital TMD-like TB (seed 7, 49 R cells), 150x150 k-grid, full pulse, plain FP64"),
+               desc="11-orbital TMD-like TB (seed 7, 49 R cells), 150x150 k-grid, full pulse"),
     "c3": dict(model=None, n=None, window=None,
                desc="batched scan: 64 solves, nw in {2,6,11} (seeds 1-3), grids {60,100,150,200}^2, 16 angles "
                     "0-180 deg, I in {0.5,1,1.5,2}e12, lambda in {2000,3000} nm (draws: seed 0)"),
@@ -191,6 +202,16 @@ def run_serve(args, local: int):
     }
 
 
+def batch_engine_desc() -> str:
+    """What SWEBatch runs, as selected by HHG_BATCH (the library reads the same variable)."""
+    if os.environ.get("HHG_BATCH") == "persistent":
+        return ("SWEBatch, HHG_BATCH=persistent: one persistent work-stealing launch per kernel shape over packed "
+                "(solve, virtual CTA) items, longest first (precomputed-sum shapes on their own streams), "
+                "captured in one CUDA graph")
+    return ("SWEBatch (default engine): every solve's launches on a stream of its own, all captured in one CUDA "
+            "graph and replayed")
+
+
 def run_scan(args, local: int):
     """Batched scan: the mixed form as one SWEBatch against the plain form as sequential solves."""
     import numpy as np
@@ -234,8 +255,7 @@ def run_scan(args, local: int):
         "scaling": "weak", "vs_baseline": None, "dtype": "c64 commutators/Wannier sums, f64 state/RK/k-sum",
         "data": "synthetic (seeded TB models, generated by hhg-solids_b200/tbgen.py)", "impl": "hhg-b200",
         "config": {"workload": f"c3: {WORKLOADS['c3']['desc']}", "solves": len(draws), "k_points_total": kpts,
-                   "nt": nt, "precision": "mixed", "batch": "SWEBatch: one persistent work-stealing launch per kernel "
-                   "shape over packed (solve, virtual CTA) items, longest first, captured CUDA graph"},
+                   "nt": nt, "precision": "mixed", "batch": batch_engine_desc()},
         "solves_per_hour": 3600.0 * len(draws) / (batch_ms * 1e-3),
         "fp64_sequential": {"ms": seq_ms, "value": kpts * nt / (seq_ms * 1e-3),
                             "solves_per_hour": 3600.0 * len(draws) / (seq_ms * 1e-3)},
@@ -480,6 +500,17 @@ def reference_sample_steps(workload: str) -> int:
     return {"c0": 400, "c1": 24, "c2": 2}[workload]
 
 
+REFERENCE_FFT = ("the reference's unmodified sources (oracle/_ref/libwannier.so) linked against this repository's "
+                 "FP64 Stockham FFT (oracle/shim/fft_shim.c) in place of FFTW3, which is absent from this image")
+
+
+def reference_sample_desc(cores: int, nt_sample: int, param: dict) -> str:
+    nt = int(param["tmax"] / param["dt"])
+    return (f"{cores} concurrent single-threaded processes x {nt_sample} RK4 steps of the same grid and model "
+            f"(the reference's pol_scan model, one solve per core); rate per k-point step extrapolated from the "
+            f"{nt_sample}-step sample to the {nt}-step pulse")
+
+
 def run_reference_arm(args, rank: int, world: int):
     if rank != 0:
         return
@@ -493,8 +524,13 @@ def run_reference_arm(args, rank: int, world: int):
     line = {"metric": "k-pt*RK4-steps/s", "impl": "reference", "unit": "k-pt*RK4-steps/s", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded TB model)",
-            "config": {"workload": f"{args.workload}: {WORKLOADS[args.workload]['desc']}", "solver": args.solver,
-                       "sample": f"{cores} concurrent single-threaded processes x {nt_sample} RK4 steps",
+            "config": {"workload": f"{args.workload}: {WORKLOADS[args.workload]['desc']}"
+                       + (", mixed form (complex-FP32 Wannier sums and commutators; FP64 state, RK4 accumulation, "
+                          "window velocity and k-sum)" if args.precision == "mixed" else ", plain FP64"),
+                       "k_grid": [param["nr1"], param["nr2"]], "nt": int(param["tmax"] / param["dt"]),
+                       "solver": args.solver,
+                       "reference_arithmetic": "FP64 throughout (the reference has one form)",
+                       "sample": reference_sample_desc(cores, nt_sample, param),
                        "l2": "n/a (CPU)"}}
     try:
         pool = ReferencePool(param, nt_sample, cores, args.solver)
@@ -511,7 +547,7 @@ def run_reference_arm(args, rank: int, world: int):
     value = pool.kpoint_steps() * len(times) / total
     line.update(value=value, ms_per_step=1e3 * total / len(times),
                 cpu_baseline={"value": value, "unit": "k-pt*RK4-steps/s", "cores": cores, "kind": "reference",
-                              "sample": line["config"]["sample"]},
+                              "sample": line["config"]["sample"], "fft": REFERENCE_FFT},
                 e2e={"value": value, "unit": "k-pt*RK4-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0})
     print(json.dumps(line), flush=True)
 
@@ -532,8 +568,7 @@ def cpu_baseline(workload: str, solver: str = "rspace") -> dict:
     finally:
         pool.close()
     return {"value": pool.kpoint_steps() / t, "unit": "k-pt*RK4-steps/s", "cores": cores, "kind": "reference",
-            "sample": f"{cores} concurrent single-threaded processes x {nt_sample} RK4 steps of the same grid and model "
-                      f"({t:.1f} s wall)"}
+            "sample": reference_sample_desc(cores, nt_sample, param) + f" ({t:.1f} s wall)", "fft": REFERENCE_FFT}
 
 
 # ---------------------------------------------------------------- our arm
@@ -596,15 +631,17 @@ def main():
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
-    ap.add_argument("--workload", default="c1", choices=sorted(WORKLOADS))
+    ap.add_argument("--workload", default="c2", choices=sorted(WORKLOADS))
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
-    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"],
+    ap.add_argument("--precision", default="mixed", choices=["fp64", "mixed"],
                     help="mixed: FP32 Wannier sums and commutators, FP64 state / RK accumulation / k-sum")
     ap.add_argument("--solver", default="rspace", choices=["rspace", "kspace"],
                     help="kspace: the reference's k-space solver (src/solver_kspace.cpp) instead of its real-space one")
-    ap.add_argument("--batch", type=int, default=1, help="mixed: also time this many solves of the workload as one SWEBatch")
+    ap.add_argument("--batch", type=int, default=4, help="mixed: also time this many solves of the workload as one SWEBatch")
+    ap.add_argument("--fp64-steps", type=int, default=3, help="mixed: timed plain-FP64 solves beside the mixed ones")
+    ap.add_argument("--batch-steps", type=int, default=3, help="mixed: timed runs of the --batch SWEBatch")
     ap.add_argument("--autotune", action="store_true", help="time candidate tile shapes at setup (SWESim_set_autotune)")
     ap.add_argument("--requests", type=int, default=200, help="c4: requests in the arrival stream")
     ap.add_argument("--max-active", type=int, default=32, help="c4: most solves running at once")
@@ -718,16 +755,27 @@ def main():
     shape = swe.launch_shape()
     mixed = None
     if args.precision == "mixed" and rank == 0:
-        # Error and speed against the plain FP64 form of the same solve.
+        # Error and speed against the plain FP64 form of the same solve: one warm-up solve (its
+        # current is the comparison), then args.fp64_steps timed solves with L2 flushed before each.
         swe.reset()
         swe.run_simulation()
         J_mixed = swe.get_current()[1:]
         ref = pyswe.SWE(pyswe.Settings(dict(param)), device=local, solver=args.solver, autotune=args.autotune)
         ref.run_simulation()
         J_fp64 = ref.get_current()[1:]
-        fp64_ms = ref.last_kernel_ms()
+        fms = []
+        for i in range(args.fp64_steps):
+            flush.fill_(float(i))
+            torch.cuda.synchronize()
+            ref.reset()
+            ref.run_simulation()
+            fms.append(ref.last_kernel_ms())
+        fp64_ms = statistics.mean(fms)
+        fp64_shape = ref.launch_shape()
         ref.delete()
         mixed = mixed_report(J_mixed, J_fp64, param, fp64_ms, total_ms / args.steps)
+        mixed["fp64_timed_solves"] = len(fms)
+        mixed["fp64_kernel"] = fp64_shape.get("kernel_name")
         if args.batch > 1:
             # The batched mixed form: args.batch solves of this configuration (polarisation angles
             # spread over the half circle) in one SWEBatch, against the plain FP64 solve's throughput.
@@ -741,16 +789,32 @@ def main():
             batch = pyswe.SWEBatch(solves)
             batch.run()
             bms = []
-            for _ in range(2):
+            for i in range(args.batch_steps):
+                flush.fill_(float(i))
+                torch.cuda.synchronize()
                 batch.run()
                 bms.append(batch.last_ms())
+            # The batch's error against FP64 solo solves of the same angles: the first and the middle one.
+            berr = []
+            for i in sorted({0, args.batch // 2}):
+                Jb = solves[i].get_current()[1:]
+                if i == 0:
+                    Jf = J_fp64
+                else:
+                    f = pyswe.SWE(pyswe.Settings(dict(solves[i].settings.param)), device=local, solver=args.solver)
+                    f.run_simulation()
+                    Jf = f.get_current()[1:]
+                    f.delete()
+                berr.append(float(np.linalg.norm(Jb - Jf) / np.linalg.norm(Jf)))
             batch.delete()
             for s in solves:
                 s.delete()
             per_solve = statistics.mean(bms) / args.batch
-            mixed["batched"] = {"solves": args.batch, "ms_per_batch": statistics.mean(bms), "ms_per_solve": per_solve,
-                                "k_pt_rk4_steps_per_s": nk * nt / (per_solve * 1e-3),
-                                "throughput_vs_fp64_solo": fp64_ms / per_solve}
+            mixed["batched"] = {"solves": args.batch, "timed_batches": len(bms), "ms_per_batch": statistics.mean(bms),
+                                "ms_per_solve": per_solve, "k_pt_rk4_steps_per_s": nk * nt / (per_solve * 1e-3),
+                                "throughput_vs_fp64_solo": fp64_ms / per_solve,
+                                "J_rel_l2_vs_fp64": berr,
+                                "engine": batch_engine_desc()}
     swe.delete()
     if dist is not None:
         dist.destroy_process_group()
@@ -787,7 +851,9 @@ def main():
         "data": "synthetic (seeded TB model, generated by hhg-solids_b200/tbgen.py)",
         "impl": "hhg-b200",
         "config": {"workload": f"{args.workload}: {WORKLOADS[args.workload]['desc']}"
-                   + (f" (grid overridden to {args.grid}x{args.grid})" if args.grid else ""),
+                   + (f" (grid overridden to {args.grid}x{args.grid})" if args.grid else "")
+                   + (", mixed form (complex-FP32 Wannier sums and commutators; FP64 state, RK4 accumulation, "
+                      "window velocity and k-sum)" if args.precision == "mixed" else ", plain FP64"),
                    "k_grid": [param["nr1"], param["nr2"]],
                    "nt": nt, "num_orb": nw, "precision": args.precision, "solver": args.solver,
                    "autotune": args.autotune, "parallelism": f"replicas x{world}" if world > 1 else "single",

@@ -7,10 +7,14 @@
 // used and keeps until the process exits.  A call therefore allocates nothing.
 //
 // Host code cannot use the array's name as a device address (on the host it names a stand-in
-// object), so the first call on each device looks the address up with cudaGetSymbolAddress while
-// that device is current and caches it per device.  All calls on a device share the one array:
-// it is cleared at the start of every call, and two calls whose work overlaps on the GPU (for
-// example on two streams) corrupt each other's current.
+// object), so every call looks the address up with cudaGetSymbolAddress while the device is
+// current.  The address is also kept per device for calls made while the stream is being captured
+// into a graph, where the lookup (which may load the module) is not made: such a call needs an
+// earlier call on the same device.  Looking it up again on every other call keeps the address
+// right when the context was torn down and created again (cudaDeviceReset, or a framework that
+// resets the primary context).  All calls on a device share the one array: it is cleared at the
+// start of every call, and two calls whose work overlaps on the GPU (for example on two streams)
+// corrupt each other's current.
 #include <cuda_runtime.h>
 
 #include <cstdio>
@@ -48,10 +52,16 @@ int propagate_static_scratch(const SolveTables& t, const GroupTables& gt, const 
              need, s.vctas, t.nt, kStaticScratchBytes);
     return -1;
   }
+  cudaStreamCaptureStatus capture = cudaStreamCaptureStatusNone;
+  e = cudaStreamIsCapturing(stream, &capture);
+  if (e != cudaSuccess) {
+    snprintf(why, why_len, "cudaStreamIsCapturing failed: %s", cudaGetErrorString(e));
+    return -1;
+  }
   void* scratch = nullptr;
   {
     std::lock_guard<std::mutex> lock(g_scratch_mutex);
-    if (!g_scratch_address[dev]) {
+    if (capture == cudaStreamCaptureStatusNone) {
       void* addr = nullptr;
       e = cudaGetSymbolAddress(&addr, g_current_scratch);
       if (e != cudaSuccess || addr == nullptr) {
@@ -60,6 +70,11 @@ int propagate_static_scratch(const SolveTables& t, const GroupTables& gt, const 
         return -1;
       }
       g_scratch_address[dev] = addr;
+    } else if (!g_scratch_address[dev]) {
+      snprintf(why, why_len,
+               "the first allocation-free call on device %d is being captured into a graph: make one call on "
+               "this device outside capture first, so that the scratch address is known", dev);
+      return -1;
     }
     scratch = g_scratch_address[dev];
   }

@@ -146,10 +146,16 @@ void SWESim_get_fields(SWESim* swe, double* t, double* E, double* A);
  * memory that the library holds on each device it is used on until the process exits.  Solves
  * that need more (virtual CTAs x nt x 48 bytes > 32 MiB: an element-group solve on 148 CTAs up to nt of about
  * 4700; a 200x200 2-orbital solve on 400 column tiles up to about 1740) are
- * rejected with -1 and a message.  The first call on a device looks up that array's address, so
- * make it before capturing the stream into a graph.  All calls on a device share the array and
- * clear it at their start: calls whose work overlaps on the GPU (different streams, or different
- * host threads) corrupt each other's result.  Returns 0, or -1 (message in SWESim_last_error). */
+ * rejected with -1 and a message.  Each call looks up that array's device address (a call made
+ * while the stream is being captured into a graph reuses the address of an earlier call on the same
+ * device, so make one call before capturing).  All calls on a device share the array and clear it
+ * at their start: calls whose work overlaps on the GPU (different streams, or different host
+ * threads) corrupt each other's result.
+ * The queued work also reads the SWESim's own device tables and, for solves whose kernel takes
+ * precomputed inner Wannier sums (models of 6, 11 or 12 orbitals), writes the SWESim's own buffer
+ * of those sums.  So synchronise `stream` before another SWESim_run_simulation or
+ * SWESim_run_simulation_noalloc, SWESim_restart, SWESim_init or SWESim_delete on the same SWESim.
+ * Returns 0, or -1 (message in SWESim_last_error). */
 int SWESim_run_simulation_noalloc(SWESim* swe, hhg_cdouble* rho_k, hhg_cdouble* current, void* stream);
 
 /* Batches: several initialised solves (each after SWESim_init, all on one device) propagated

@@ -12,7 +12,8 @@ for p in (PKG, os.path.join(REPO, "oracle")):
     if p not in sys.path:
         sys.path.insert(0, p)
 
-REFERENCE_CHECKOUT = "/root/reference"
+# The reference checkout (read-only; absent on machines that only run the GPU tests).
+REFERENCE_CHECKOUT = os.environ.get("HHG_REFERENCE", "/root/reference")
 
 
 def pytest_configure(config):

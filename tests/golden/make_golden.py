@@ -50,6 +50,10 @@ CASES = {
     "c0": case("haldane", 60),
     "c2_prefix": case("tmd11_s7", 150, tmax=2.2),
     "c1": case("haldane", 200),
+    # Full pulses of the 11- and 12-orbital models on a small grid: where the mixed form's per-harmonic
+    # error is measured on models whose mixed kernels differ from the FP64 ones.
+    "tmd11_12_full": case("tmd11_s7", 12),
+    "tmd12_12_full": case("tmd12_s2", 12, pol_vec=[0.6, 0.8, 0.0], intensity=2e12),
     "w90_tmd6_deg_8": case("tmd6_deg_equiv", 8, tmax=1.0, pol_vec=[0.6, 0.8, 0.0], intensity=2e12),
     "ks_haldane_12_pol": case("haldane", 12, tmax=4.0, pol_vec=[0.6, 0.8, 0.0], phi_vec=[0.3, 0.0, 0.0],
                               solver="kspace"),
@@ -106,7 +110,7 @@ def run_case(pyswe, lib: str, name: str, spec: dict) -> dict:
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--ref", default=os.environ.get("HHG_REFERENCE", "/root/reference"))
     ap.add_argument("--only", nargs="*")
     args = ap.parse_args()
     lib = os.path.join(REPO, "oracle", "_ref", "libwannier.so")

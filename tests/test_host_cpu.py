@@ -173,3 +173,40 @@ def test_spectrum_without_gpu_fails_loudly():
 
     with pytest.raises(pyswe.SWEError, match="no CUDA device"):
         pyswe.spectrum(np.zeros((3, 16), dtype=complex), 0.1)
+
+
+def test_wrapper_trace_is_the_reference_wrappers_traffic():
+    """The committed wrapper traces are what the reference's pySWE/pyswe.py declares and calls today."""
+    if not os.path.exists(os.path.join(REFERENCE_CHECKOUT, "pySWE", "pyswe.py")):
+        pytest.skip("reference checkout not present")
+    import json
+    import sys
+
+    sys.path.insert(0, os.path.join(REPO, "tests", "golden"))
+    import make_wrapper_trace
+
+    for name in make_wrapper_trace.CASES:
+        with open(os.path.join(REPO, "tests", "golden", "wrapper_trace", f"{name}.json")) as f:
+            committed = json.load(f)
+        assert make_wrapper_trace.record(REFERENCE_CHECKOUT, name) == committed, name
+
+
+def test_wrapper_trace_replay_reproduces_golden_on_reference_build(oracle_mod):
+    """Replaying a recorded wrapper trace against the reference's own build gives its golden current:
+    the replay is faithful, so the same replay against this library on a GPU is a drop-in check."""
+    if not oracle_mod.have_ref():
+        pytest.skip("reference build not present")
+    import json
+
+    from test_zy_reference_wrapper_gpu import TRACES, replay
+
+    from conftest import rel_l2
+
+    for name in ("tmd6_8", "haldane_12_pol"):
+        with open(os.path.join(TRACES, f"{name}.json")) as f:
+            trace = json.load(f)
+        meta, param, t_ref, J_ref = load_golden(name)
+        t, jx, jy, jz = replay(trace, oracle_mod.ref_paths()[0], param["path_tb"])
+        assert np.array_equal(t, t_ref)
+        for a, j in enumerate((jx, jy)):
+            assert rel_l2(j, J_ref[a]) < 1e-12, (name, a)

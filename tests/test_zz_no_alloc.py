@@ -4,8 +4,8 @@ synchronisation would stall their other streams).  It keeps its scratch in a fix
 array owned by the library, so the caller passes only the state and the result buffers.
 
 Checked here through the C ABI: two calls in a row give the current of the allocating entry point
-(SWESim_run_simulation), for both propagation kernels, and a solve that needs more scratch than the
-array holds is refused with a message.  This file is collected last on purpose."""
+(SWESim_run_simulation), for each of the three propagation kernels, and a solve that needs more
+scratch than the array holds is refused with a message.  This file is collected last on purpose."""
 import ctypes as ct
 
 import numpy as np
@@ -29,13 +29,29 @@ def _lib():
     return L
 
 
-@pytest.mark.parametrize("name", ["haldane_12_pol", "tmd11_10"])  # thread-per-k and element-group kernels
-def test_two_calls_match_the_allocating_entry_point(name):
+# (golden case, tmax override, HHG_KERNEL, expected kernel): the thread-per-k-point kernel, the
+# element-group kernel (precomputed-sum shape), the column-tile kernel on the 200 x 200 2-orbital grid
+# it is chosen for (a short pulse, within the scratch limit), and the column-tile kernel forced on a
+# small grid.
+CASES = [("haldane_12_pol", None, None, "propagate_kpt_kernel"),
+         ("tmd11_10", None, None, "propagate_"),
+         ("c1", 2.2, None, "propagate_kcol_kernel"),
+         ("haldane_12_pol", None, "kcol", "propagate_kcol_kernel")]
+
+
+@pytest.mark.parametrize("name,tmax,kernel,expect", CASES)
+def test_two_calls_match_the_allocating_entry_point(name, tmax, kernel, expect, monkeypatch):
     import torch
     from pySWE import pyswe
 
     meta, param, _, _ = load_golden(name)
+    if tmax:
+        param = dict(param, tmax=tmax)
+    if kernel:
+        monkeypatch.setenv("HHG_KERNEL", kernel)  # read at SWESim_init
     swe = pyswe.SWE(pyswe.Settings(param), device=0)
+    monkeypatch.delenv("HHG_KERNEL", raising=False)
+    assert swe.launch_shape()["kernel_name"].startswith(expect), swe.launch_shape()
     rho0 = swe.get_rho_k()  # equilibrium, before any propagation
     swe.run_simulation()
     J_alloc = swe.get_current()[1:]
