@@ -139,6 +139,8 @@ void SWESim::tune_tiles(int sms) {
     std::vector<int> hints;
     if (shape.kernel == 3) {
       hints = {1, 2, 3};
+    } else if (shape.kernel == 4) {
+      hints = {16, 8};  // fragment kernel: 16 or 8 k-points per CTA
     } else if (shape.kernel == 1 || shape.kernel == 2) {
       const int B = shape.k_per_cta;
       for (int b : {B, (3 * B + 3) / 4, (2 * B + 2) / 3, (B + 1) / 2}) hints.push_back(b);

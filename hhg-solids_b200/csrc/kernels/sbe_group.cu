@@ -816,6 +816,8 @@ __device__ __forceinline__ GroupData<Real> group_data(const GroupTables& gt) {
   return d;
 }
 
+#include "sbe_frag.cuh"
+
 // One solve: physical CTA b runs virtual CTAs b, b + gridDim.x, ...
 template <typename Real, int EPT, int NWc, int NAXc, int NJc, bool KM = false, int WBc = 0, bool KP = false,
           bool PG = false>
@@ -976,6 +978,94 @@ int launch_group_batch_t(const BatchDesc* descs, const int2* items, int nitems, 
   return grid;
 }
 
+// Tensor-core fragment kernel (mixed form): precomputed inner sums, compiled 7x7 box, KPC k-points per CTA.
+template <int NW, int NAX, int NJ, int KPC>
+bool plan_frag_t(const SolveTables& t, int sm_count, LaunchShape* out, char* why, int why_len) {
+  using FG = frag::Geom<NW, NAX, NJ, KPC>;
+  auto kern = frag::propagate_frag_kernel<NW, NAX, NJ, KPC>;
+  if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)FG::BYTES) != cudaSuccess) {
+    cudaGetLastError();
+    snprintf(why, why_len, "fragment kernel: %zu bytes of shared memory not available", FG::BYTES);
+    return false;
+  }
+  int occ = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, KPC * 32, FG::BYTES);
+  if (occ < 1) occ = 1;
+  const long slots = (long)occ * sm_count;
+  const int rows = t.row1 - t.row0;
+  const long ntiles = (long)t.N2 * ((rows + KPC - 1) / KPC);
+  out->kernel = 4;
+  out->kmode = 0;
+  out->ept = 8;
+  out->k_per_cta = KPC;
+  out->group = 32;
+  out->threads = KPC * 32;
+  out->ntiles = (int)ntiles;
+  out->ctas = (int)(ntiles < slots ? ntiles : slots);
+  out->vctas = out->ctas;
+  out->box_sm = out->win_sm = 0;
+  out->smem = FG::BYTES;
+  out->pre_chunk = std::min(kPreChunk, t.nt);
+  out->pre_bytes = (size_t)out->pre_chunk * t.N2 *
+                   ((size_t)FG::NBROWS * FG::NW2 * sizeof(float2) + (size_t)FG::NWROWS * FG::NW2 * sizeof(double2));
+  return true;
+}
+
+template <int NW, int NAX, int NJ, int KPC>
+int launch_frag_t(const SolveTables& t, const GroupTables& gt, const LaunchShape& s, double2* rho, double2* Jpart,
+                  cudaStream_t stream) {
+  using FG = frag::Geom<NW, NAX, NJ, KPC>;
+  if (!gt.pre || s.pre_chunk <= 0)
+    throw std::runtime_error("fragment kernel launch: needs its precomputed-sum scratch (GroupTables::pre)");
+  GroupData<float> d = {gt.Xbox32, gt.P32, gt.T1_32, gt.T2_32, gt.Xwin64, gt.P64, gt.T1_64, gt.T2_64, nullptr, nullptr};
+  const size_t gbuf = (size_t)FG::NBROWS * FG::NW2;
+  float2* Gpre = static_cast<float2*>(gt.pre);
+  double2* GWpre = reinterpret_cast<double2*>(Gpre + (size_t)s.pre_chunk * t.N2 * gbuf);
+  d.Gpre = Gpre;
+  d.GWpre = GWpre;
+  auto kern = frag::propagate_frag_kernel<NW, NAX, NJ, KPC>;
+  cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s.smem);
+  int launches = 0;
+  for (int c0 = t.step0; c0 < t.step1; c0 += s.pre_chunk) {
+    SolveTables tc = t;
+    tc.step0 = c0;
+    tc.step1 = std::min(c0 + s.pre_chunk, t.step1);
+    group_sums_kernel<float><<<(tc.step1 - c0) * t.N2, 256, 0, stream>>>(tc, d, 3, 4, FG::NBROWS, FG::NWROWS, Gpre,
+                                                                          GWpre);
+    kern<<<s.ctas, s.threads, s.smem, stream>>>(tc, d, s.vctas, rho, Jpart);
+    launches += 2;
+  }
+  return launches;
+}
+
+struct FragVariant {
+  int nw, nax, nj, kpc;
+  bool (*plan)(const SolveTables&, int, LaunchShape*, char*, int);
+  int (*launch)(const SolveTables&, const GroupTables&, const LaunchShape&, double2*, double2*, cudaStream_t);
+};
+#define HHG_FRAG_VARIANT(NW, NAX, NJ, KPC) {NW, NAX, NJ, KPC, plan_frag_t<NW, NAX, NJ, KPC>, launch_frag_t<NW, NAX, NJ, KPC>}
+const FragVariant kFragVariants[] = {
+    HHG_FRAG_VARIANT(11, 1, 2, 16), HHG_FRAG_VARIANT(11, 2, 2, 16), HHG_FRAG_VARIANT(12, 1, 2, 16),
+    HHG_FRAG_VARIANT(12, 2, 2, 16), HHG_FRAG_VARIANT(11, 1, 2, 8),  HHG_FRAG_VARIANT(11, 2, 2, 8),
+    HHG_FRAG_VARIANT(12, 1, 2, 8),  HHG_FRAG_VARIANT(12, 2, 2, 8),
+};
+#undef HHG_FRAG_VARIANT
+
+// The fragment variant for a mixed-form solve (Hermitian halved 7x7 box, real-space solver), or null.
+// tile_hint in 1..8 picks the 8-k-point CTAs.  Tuning overrides: HHG_FRAG=0 turns the kernel off,
+// HHG_FRAG_KPC=8|16 fixes the k-points per CTA.
+const FragVariant* find_frag(const SolveTables& t, int tile_hint) {
+  if (const char* env = std::getenv("HHG_FRAG"))
+    if (env[0] == '0') return nullptr;
+  const GroupGeom gg = group_geom(t);
+  if (t.kmode || !t.hermitian || !gg.half || t.b1n != 7 || t.b2n != 7) return nullptr;
+  int kpc = (tile_hint > 0 && tile_hint <= 8) ? 8 : 16;
+  if (const char* env = std::getenv("HHG_FRAG_KPC")) kpc = std::atoi(env) == 8 ? 8 : 16;
+  for (const FragVariant& v : kFragVariants)
+    if (v.nw == t.nw && v.nax == t.nax && v.nj == t.nj && v.kpc == kpc) return &v;
+  return nullptr;
+}
+
 // Compiled shapes: (orbitals, field axes, current axes) of the configurations this library is built
 // for, each in plain FP64 (one element per thread) and mixed precision (two elements per thread);
 // any other shape runs the runtime-shaped instance.
@@ -1067,6 +1157,11 @@ const GroupVariant* find_variant(const SolveTables& t, int precision) {
 
 bool plan_group(const SolveTables& t, int precision, int sm_count, LaunchShape* out, char* why, int why_len,
                 int tile_hint) {
+  if (precision == 1)
+    if (const FragVariant* f = find_frag(t, tile_hint)) {
+      out->variant = (int)(f - kFragVariants);
+      if (f->plan(t, sm_count, out, why, why_len)) return true;
+    }
   if (const GroupVariant* v = find_variant(t, precision)) {
     out->variant = (int)(v - kGroupVariants);
     return v->plan(t, sm_count, out, why, why_len, tile_hint);
@@ -1118,6 +1213,7 @@ int launch_group_batch(const LaunchShape& s, const BatchDesc* descs, const int2*
 
 int launch_group(const SolveTables& t, const GroupTables& gt, const LaunchShape& s, double2* rho, double2* Jpart,
                  cudaStream_t stream) {
+  if (s.kernel == 4) return kFragVariants[s.variant].launch(t, gt, s, rho, Jpart, stream);
   if (s.variant >= 0) return kGroupVariants[s.variant].launch(t, gt, s, rho, Jpart, stream);
   if (s.kmode) return launch_group_generic<true>(t, gt, s, rho, Jpart, stream);
   return launch_group_generic<false>(t, gt, s, rho, Jpart, stream);
