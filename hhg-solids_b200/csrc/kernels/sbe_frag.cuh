@@ -105,7 +105,7 @@ struct Geom {
 
 template <int NW, int NAX, int NJ, int KPC>
 __global__ void __launch_bounds__(KPC * 32, 16 / KPC)
-    propagate_frag_kernel(SolveTables t, GroupData<float> d, int vctas, double2* rho, double2* Jpart) {
+    propagate_frag_kernel(SolveTables t, GroupData<float> d, int vctas, double2* rho, double2* Jpart, int d_flags) {
   using FG = Geom<NW, NAX, NJ, KPC>;
   constexpr int NW2 = FG::NW2, NMAT = FG::NMAT, NTILE = FG::NTILE, HKS = FG::HKS;
   extern __shared__ __align__(16) unsigned char smraw[];
@@ -199,6 +199,25 @@ __global__ void __launch_bounds__(KPC * 32, 16 / KPC)
             nai[r] = negated(ai[r]);
           }
           const float2* G = GS + buf * gbuf;
+          if (d_flags & 1) {  // experiment: outer sums on the FP32 pipe (round to nearest)
+            for (int idx = tid; idx < KPC * NMAT * NW2; idx += NTHR) {
+              const int m = idx / (NMAT * NW2), mat = (idx / NW2) % NMAT, e = idx % NW2;
+              const float2* Gm = G + (size_t)mat * 4 * NW2;
+              float2 acc = fzero;
+              for (int q = 0; q < 7; ++q) {
+                const float2 ph = mul(TW1[m * 8 + q], P1[t.b1lo + q]);
+                float2 gv;
+                if (q < 3) {
+                  gv = Gm[(3 - q) * NW2 + (e % NW) * NW + e / NW];
+                  gv.y = -gv.y;
+                } else {
+                  gv = Gm[(q - 3) * NW2 + e];
+                }
+                acc = fmac(ph, gv, acc);
+              }
+              HK[((size_t)m * NMAT + mat) * HKS + e] = acc;
+            }
+          } else
 #pragma unroll 1
           for (int nt_ = w; nt_ < NMAT * NTILE; nt_ += KPC) {
             const int mat = nt_ / NTILE, j = nt_ % NTILE, e = 8 * j + g;

@@ -978,6 +978,11 @@ int launch_group_batch_t(const BatchDesc* descs, const int2* items, int nitems, 
   return grid;
 }
 
+int frag_flags() {
+  const char* e = std::getenv("HHG_FRAG_FLAGS");
+  return e ? std::atoi(e) : 0;
+}
+
 // Tensor-core fragment kernel (mixed form): precomputed inner sums, compiled 7x7 box, KPC k-points per CTA.
 template <int NW, int NAX, int NJ, int KPC>
 bool plan_frag_t(const SolveTables& t, int sm_count, LaunchShape* out, char* why, int why_len) {
@@ -1032,7 +1037,7 @@ int launch_frag_t(const SolveTables& t, const GroupTables& gt, const LaunchShape
     tc.step1 = std::min(c0 + s.pre_chunk, t.step1);
     group_sums_kernel<float><<<(tc.step1 - c0) * t.N2, 256, 0, stream>>>(tc, d, 3, 4, FG::NBROWS, FG::NWROWS, Gpre,
                                                                           GWpre);
-    kern<<<s.ctas, s.threads, s.smem, stream>>>(tc, d, s.vctas, rho, Jpart);
+    kern<<<s.ctas, s.threads, s.smem, stream>>>(tc, d, s.vctas, rho, Jpart, frag_flags());
     launches += 2;
   }
   return launches;
