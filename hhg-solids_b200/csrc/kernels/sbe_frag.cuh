@@ -97,7 +97,8 @@ struct Geom {
   static constexpr size_t TW1 = GWS + 2 * (size_t)NWROWS * NW2 * 16;  // [KPC][8] float2
   static constexpr size_t WTW1 = TW1 + (size_t)KPC * 8 * 8;           // [KPC][4] double2
   static constexpr size_t SJ = WTW1 + (size_t)KPC * 4 * 16;           // [2][kJRing][KPC][2 NJ] double
-  static constexpr size_t BYTES = SJ + 2 * (size_t)kJRing * KPC * 2 * NJ * 8;
+  static constexpr size_t SCR = SJ + 2 * (size_t)kJRing * KPC * 2 * NJ * 8;  // [KPC][2][256] float2 (experiments)
+  static constexpr size_t BYTES = SCR + (size_t)KPC * 2 * 256 * 8;
   static_assert(NW > 8 && NW <= 16, "fragment layout: 9..16 orbitals");
   static_assert((NBROWS * NW2 * 8) % 16 == 0, "16-byte copies of the inner sums");
   static_assert(KPC == 8 || KPC == 16, "k-points per CTA");
@@ -262,6 +263,7 @@ __global__ void __launch_bounds__(KPC * 32, 16 / KPC)
           const float2* Hm = HK + (size_t)w * NMAT * HKS;
           double2* Rm = RHO + (size_t)w * NW2;
           float2 r32[8], S[8], X[8];
+          double2 S64[8];
 #pragma unroll
           for (int s = 0; s < 8; ++s) {
             const int r = slot_row(s, g), cc = slot_col(s, c4);
@@ -271,6 +273,7 @@ __global__ void __launch_bounds__(KPC * 32, 16 / KPC)
               r32[s] = make_float2((float)x.x, (float)x.y);
             }
             S[s] = fzero;
+            S64[s] = make_double2(0.0, 0.0);
             X[s] = r32[s];
           }
           const double* esb = t.es + (size_t)ti * 9;
@@ -297,6 +300,26 @@ __global__ void __launch_bounds__(KPC * 32, 16 / KPC)
                 }
               }
             }
+            float Pr[8], Pi[8], Dr[8], Di[8];
+            if (d_flags & 2) {  // experiment: the product on the FP32 pipe through shared memory
+              float2* SH = reinterpret_cast<float2*>(smraw + FG::SCR) + (size_t)w * 512;
+              float2* SX = SH + 256;
+#pragma unroll
+              for (int s = 0; s < 8; ++s) {
+                SH[slot_row(s, g) * 16 + slot_col(s, c4)] = H[s];
+                SX[slot_row(s, g) * 16 + slot_col(s, c4)] = X[s];
+              }
+              __syncwarp();
+#pragma unroll
+              for (int s = 0; s < 8; ++s) {
+                const int r = slot_row(s, g), cc = slot_col(s, c4);
+                float2 acc = fzero;
+                for (int k = 0; k < 16; ++k) acc = fmac(SH[r * 16 + k], SX[k * 16 + cc], acc);
+                Pr[s] = acc.x;
+                Pi[s] = acc.y;
+              }
+              __syncwarp();
+            } else {
             // P = H X: Re P = Hr Xr + Hi Xi, Im P = Hr (-Xi) + Hi Xr over B = conj(X slots).
             float pr[2][4] = {}, pim[2][4] = {};
 #pragma unroll
@@ -321,7 +344,6 @@ __global__ void __launch_bounds__(KPC * 32, 16 / KPC)
               }
             }
             // Slots of P, and of D = P^+ by 8 x 8 transposes (block (rb, cb) of P lands in block (cb, rb)).
-            float Pr[8], Pi[8], Dr[8], Di[8];
 #pragma unroll
             for (int j = 0; j < 2; ++j) {
               Pr[2 * j] = pr[j][0];
@@ -332,6 +354,7 @@ __global__ void __launch_bounds__(KPC * 32, 16 / KPC)
               Pi[2 * j + 1] = pim[j][1];
               Pi[4 + 2 * j] = pim[j][2];
               Pi[5 + 2 * j] = pim[j][3];
+            }
             }
 #pragma unroll
             for (int rb = 0; rb < 2; ++rb)
@@ -349,6 +372,20 @@ __global__ void __launch_bounds__(KPC * 32, 16 / KPC)
             // k = -i (P - D); stage sum and the next stage's X = rho + c k.
             const float wgt = (st == 0 || st == 3) ? 1.f : 2.f;
             const float cn = (float)((st == 2 ? 1.0 : 0.5) * dt);
+            if (d_flags & 4) {  // experiment: X and the stage sum formed in FP64, as in the element-group kernel
+              const double cnd = (st == 2 ? 1.0 : 0.5) * dt;
+#pragma unroll
+              for (int s = 0; s < 8; ++s) {
+                const float kx = Pi[s] - Di[s], ky = -(Pr[s] - Dr[s]);
+                S64[s].x += (double)wgt * (double)kx;
+                S64[s].y += (double)wgt * (double)ky;
+                const int r = slot_row(s, g), cc = slot_col(s, c4);
+                if (r < NW && cc < NW) {
+                  const double2 x = Rm[r * NW + cc];
+                  X[s] = make_float2((float)(x.x + cnd * (double)kx), (float)(x.y + cnd * (double)ky));
+                }
+              }
+            } else {
 #pragma unroll
             for (int s = 0; s < 8; ++s) {
               const float kx = Pi[s] - Di[s], ky = -(Pr[s] - Dr[s]);
@@ -357,6 +394,7 @@ __global__ void __launch_bounds__(KPC * 32, 16 / KPC)
               X[s].x = fmaf(cn, kx, r32[s].x);
               X[s].y = fmaf(cn, ky, r32[s].y);
             }
+            }
           }
           // rho += dt/6 (k1 + 2 k2 + 2 k3 + k4) in FP64.
 #pragma unroll
@@ -364,8 +402,13 @@ __global__ void __launch_bounds__(KPC * 32, 16 / KPC)
             const int r = slot_row(s, g), cc = slot_col(s, c4);
             if (r < NW && cc < NW) {
               double2 x = Rm[r * NW + cc];
-              x.x = x.x + prefac * (double)S[s].x;
-              x.y = x.y + prefac * (double)S[s].y;
+              if (d_flags & 4) {
+                x.x = x.x + prefac * S64[s].x;
+                x.y = x.y + prefac * S64[s].y;
+              } else {
+                x.x = x.x + prefac * (double)S[s].x;
+                x.y = x.y + prefac * (double)S[s].y;
+              }
               Rm[r * NW + cc] = x;
             }
           }
