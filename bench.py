@@ -60,6 +60,7 @@ WORKLOADS = {
     "c3": dict(model=None, n=None, window=None,
                desc="batched scan: 64 solves, nw in {2,6,11} (seeds 1-3), grids {60,100,150,200}^2, 16 angles "
                     "0-180 deg, I in {0.5,1,1.5,2}e12, lambda in {2000,3000} nm (draws: seed 0)"),
+    "spectrum": dict(model=None, n=None, window=None, desc="HHG spectra of 1024 solves x 3 axes (HHG_spectrum)"),
     "c4": dict(model=None, n=None, window=None,
                desc="serving: Poisson arrivals at 20 req/s (seed 0), nw in {2,6,11,12} (seeds 1-3), k-grid side "
                     "even in 60-200, polarisation uniform on the circle, I log-uniform in [3e11,3e12] W/cm^2, "
@@ -112,15 +113,61 @@ def serve_requests(n: int, rate: float = 20.0, seed: int = 0):
     return out
 
 
+def serve_stream(srv, reqs, autotune: bool, local: int):
+    """Submits `reqs` to the server at their arrival times and waits for all; returns the solves, their
+    (submit, admit, start, done) times, the span and the sampled clocks."""
+    from pySWE import pyswe
+
+    solves = [None] * len(reqs)
+    tickets = [None] * len(reqs)
+    clocks = ClockSampler(local)
+    clocks.start()
+    t0 = time.perf_counter()
+    for i, (t_arr, model, nw, p) in enumerate(reqs):
+        delay = t0 + t_arr - time.perf_counter()
+        if delay > 0:
+            time.sleep(delay)
+        solves[i] = pyswe.SWE(pyswe.Settings(p), precision="mixed", defer_init=True, autotune=autotune)
+        tickets[i] = srv.submit(solves[i])
+    for tk in tickets:
+        srv.wait(tk)
+    wall = time.perf_counter() - t0
+    clk = clocks.stop()
+    times = [srv.times(tk) for tk in tickets]
+    first, last = min(tm["submit"] for tm in times), max(tm["done"] for tm in times)
+    return solves, times, last - first, wall, clk
+
+
+def latency_report(times, reqs, span):
+    """Latency (done - submit), split into queue wait (admit - submit) and service (done - admit)."""
+    import numpy as np
+
+    lat = np.array([tm["done"] - tm["submit"] for tm in times])
+    wait = np.array([tm["admit"] - tm["submit"] for tm in times])
+    service = np.array([tm["done"] - tm["admit"] for tm in times])
+
+    def pct(a):
+        return {"p50": float(np.percentile(a, 50)), "p95": float(np.percentile(a, 95)),
+                "p99": float(np.percentile(a, 99)), "max": float(a.max()), "mean": float(a.mean())}
+
+    n = len(times)
+    return {"requests": n, "offered_load_req_per_s": n / reqs[-1][0], "solves_per_hour": 3600.0 * n / span,
+            "span_s": span, "latency_s": pct(lat), "queue_wait_s": pct(wait), "service_s": pct(service)}
+
+
 def run_serve(args, local: int):
     """Serving: requests submitted at their Poisson arrival times to one SWEServer (mixed form,
-    continuous batching); latency = completion - submission.  Beside it the plain FP64 form run
-    sequentially (setup + propagation, one solve after another) on a sample of the same requests."""
+    continuous batching); latency = completion - submission, split into queue wait (admission -
+    submission) and service (completion - admission).  Two load points: the configuration's arrival
+    rate (args.rate, 20 req/s, several times what one GPU serves, so latency there is queueing) and a
+    sub-capacity rate of args.low_load x the throughput measured at the first point.  Beside them the
+    plain FP64 form run sequentially (setup + propagation, one solve after another) on a sample of the
+    same requests."""
     import numpy as np
     import tbgen
     from pySWE import pyswe
 
-    reqs = serve_requests(args.requests)  # generates the model files before the clock starts
+    reqs = serve_requests(args.requests, rate=args.rate)  # generates the model files before the clock starts
     srv = pyswe.SWEServer(device=local, max_active=args.max_active, chunk_steps=args.chunk)
     # Warm-up: small requests of every orbital count.
     warm = []
@@ -133,26 +180,8 @@ def run_serve(args, local: int):
         srv.wait(tk)
         s.delete()
     base = srv.stats()
-    solves = [None] * len(reqs)
-    tickets = [None] * len(reqs)
-    clocks = ClockSampler(local)
-    clocks.start()
-    t0 = time.perf_counter()
-    for i, (t_arr, model, nw, p) in enumerate(reqs):
-        delay = t0 + t_arr - time.perf_counter()
-        if delay > 0:
-            time.sleep(delay)
-        solves[i] = pyswe.SWE(pyswe.Settings(p), precision="mixed", defer_init=True, autotune=args.autotune)
-        tickets[i] = srv.submit(solves[i])
-    for tk in tickets:
-        srv.wait(tk)
-    wall = time.perf_counter() - t0
-    clk = clocks.stop()
-    times = [srv.times(tk) for tk in tickets]
-    lat = np.array([tm["done"] - tm["submit"] for tm in times])
-    queue_wait = np.array([tm["admit"] - tm["submit"] for tm in times])
-    first, last = min(tm["submit"] for tm in times), max(tm["done"] for tm in times)
-    span = last - first
+    solves, times, span, wall, clk = serve_stream(srv, reqs, args.autotune, local)
+    high = latency_report(times, reqs, span)
     st = srv.stats()
     nt = int(PULSE["tmax"] / PULSE["dt"])
     ksteps = sum(p["nr1"] * p["nr2"] * nt for _, _, _, p in reqs)
@@ -162,6 +191,17 @@ def run_serve(args, local: int):
     J_mixed = [solves[i].get_current()[1:] for i in sample]
     for s in solves:
         s.delete()
+    # Sub-capacity load point: the same request mix (its own seeded draw) at low_load x the measured rate.
+    low = None
+    if args.low_requests > 0:
+        low_rate = args.low_load * high["solves_per_hour"] / 3600.0
+        reqs_low = serve_requests(args.low_requests, rate=low_rate, seed=1)
+        solves_low, times_low, span_low, _, clk_low = serve_stream(srv, reqs_low, args.autotune, local)
+        low = latency_report(times_low, reqs_low, span_low)
+        low.update(rate_req_per_s=low_rate, seed=1, clocks=clk_low,
+                   largest_solve_service_s=float(max(tm["done"] - tm["admit"] for tm in times_low)))
+        for s in solves_low:
+            s.delete()
     srv.close()
     # Plain FP64, sequential, on the sample.
     seq_s, seq_k, errs = 0.0, 0, []
@@ -175,24 +215,19 @@ def run_serve(args, local: int):
         s.delete()
         errs.append(float(np.linalg.norm(Jm - J) / np.linalg.norm(J)))
     n = len(reqs)
-
-    def pct(a, q):
-        return float(np.percentile(a, q))
-
     return {
         "metric": "solves/h", "value": 3600.0 * n / span, "unit": "solves/h", "n_gpus": 1, "steps": n,
         "warmup": len(warm), "ms_per_step": 1e3 * span / n, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "c64 commutators/Wannier sums, f64 state/RK/k-sum",
         "data": "synthetic (seeded TB models and request stream, hhg-solids_b200/tbgen.py)", "impl": "hhg-b200",
-        "config": {"workload": f"c4: {WORKLOADS['c4']['desc']}", "requests": n, "nt": nt,
+        "config": {"workload": f"c4: {WORKLOADS['c4']['desc']}", "requests": n, "rate_req_per_s": args.rate, "nt": nt,
                    "max_active": args.max_active, "chunk_steps": args.chunk,
                    "server": "SWEServer: admission by device-memory footprint, chunked continuous batching, "
                              "each running solve's launches on a stream of a pool per chunk"},
-        "latency_s": {"p50": pct(lat, 50), "p95": pct(lat, 95), "p99": pct(lat, 99), "max": float(lat.max()),
-                      "mean": float(lat.mean())},
-        "queue_wait_s": {"p50": pct(queue_wait, 50), "p99": pct(queue_wait, 99)},
+        "latency_s": high["latency_s"], "queue_wait_s": high["queue_wait_s"], "service_s": high["service_s"],
         "k_pt_rk4_steps_per_s": ksteps / span, "span_s": span, "wall_s": wall,
-        "offered_load_req_per_s": n / reqs[-1][0],
+        "offered_load_req_per_s": high["offered_load_req_per_s"],
+        "sub_capacity": low,
         "server": {k: (st[k] - base.get(k, 0) if k in ("completed", "chunks", "gpu_ms", "gap_ms", "setup_ms", "finish_ms")
                        else st[k]) for k in st},
         "fp64_sequential_sample": {"requests": len(errs), "solves_per_hour": 3600.0 * len(errs) / seq_s,
@@ -200,6 +235,35 @@ def run_serve(args, local: int):
         "J_rel_l2_mixed_vs_fp64": {"max": max(errs), "median": statistics.median(errs)},
         "clocks": clk,
     }
+
+
+def run_spectrum(args, local: int):
+    """HHG spectra of many currents through the reference-facing post-processing call (HHG_spectrum:
+    fftshift(fft(ifftshift(gradient(J, dt)))) of scripts/pol_scan.py:34-40): 1024 solves x 3 axes of
+    4096 samples, host buffers in and out (wall-clocked)."""
+    import numpy as np
+    from pySWE import pyswe
+
+    rng = np.random.default_rng(0)
+    count, n = 3 * 1024, int(PULSE["tmax"] / PULSE["dt"])
+    J = (rng.standard_normal((count, n)) + 1j * rng.standard_normal((count, n))).astype(np.complex128)
+    for _ in range(args.warmup):
+        pyswe.spectrum(J, PULSE["dt"])
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        S = pyswe.spectrum(J, PULSE["dt"])
+    dt = (time.perf_counter() - t0) / args.steps
+    ref = np.abs(np.fft.fftshift(np.fft.fft(np.fft.ifftshift(np.gradient(J[:4], PULSE["dt"], axis=1), axes=1), axis=1),
+                                 axes=1)) ** 2
+    err = float(np.abs(np.abs(S[:4]) ** 2 - ref).max() / ref.max())
+    return {"metric": "spectra/s", "value": count / dt, "unit": "spectra/s", "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * dt, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded random currents)", "impl": "hhg-b200",
+            "config": {"workload": f"spectrum: {count} currents of {n} samples (1024 solves x 3 axes), HHG_spectrum "
+                                   "with host buffers"},
+            "e2e": {"value": count / dt, "unit": "spectra/s", "h2d_bytes_per_step": count * n * 16,
+                    "d2h_bytes_per_step": count * n * 16},
+            "max_rel_err_vs_numpy_first4": err}
 
 
 def batch_engine_desc() -> str:
@@ -514,13 +578,13 @@ def reference_sample_desc(cores: int, nt_sample: int, param: dict) -> str:
 def run_reference_arm(args, rank: int, world: int):
     if rank != 0:
         return
+    if args.workload in ("c3", "c4", "spectrum"):
+        print(json.dumps({"impl": "reference", "unavailable": "the batched-scan, serving and spectrum workloads have "
+                          "no reference C/C++ implementation; their CPU comparison is the c0-c2 arms"}))
+        return
     param = workload_param(args.workload)
     cores = os.cpu_count() or 1
     nt_sample = reference_sample_steps(args.workload)
-    if args.workload in ("c3", "c4"):
-        print(json.dumps({"impl": "reference", "unavailable": "the batched-scan and serving workloads have no "
-                          "reference implementation; their CPU comparison is the c0-c2 arms"}))
-        return
     line = {"metric": "k-pt*RK4-steps/s", "impl": "reference", "unit": "k-pt*RK4-steps/s", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded TB model)",
@@ -646,6 +710,10 @@ def main():
     ap.add_argument("--requests", type=int, default=200, help="c4: requests in the arrival stream")
     ap.add_argument("--max-active", type=int, default=32, help="c4: most solves running at once")
     ap.add_argument("--chunk", type=int, default=256, help="c4: RK4 steps per scheduling chunk")
+    ap.add_argument("--rate", type=float, default=20.0, help="c4: arrival rate (req/s) of the configuration")
+    ap.add_argument("--low-load", type=float, default=0.8,
+                    help="c4: second load point, as a fraction of the throughput measured at --rate")
+    ap.add_argument("--low-requests", type=int, default=100, help="c4: requests at the second load point (0: skip)")
     ap.add_argument("--baseline-sample", type=int, default=24,
                     help="c4: requests (spread evenly over the stream) run sequentially in FP64")
     ap.add_argument("--grid", type=int, default=None,
@@ -693,9 +761,10 @@ def main():
     lib.HHG_measure_peaks.argtypes = [ct.POINTER(ct.c_double), ct.POINTER(ct.c_double)]
     fp64_peak, fp32_peak = ct.c_double(), ct.c_double()
 
-    if args.workload in ("c3", "c4"):
+    if args.workload in ("c3", "c4", "spectrum"):
         if rank == 0:
-            print(json.dumps(run_scan(args, local) if args.workload == "c3" else run_serve(args, local)), flush=True)
+            fn = {"c3": run_scan, "c4": run_serve, "spectrum": run_spectrum}[args.workload]
+            print(json.dumps(fn(args, local)), flush=True)
         if dist is not None:
             dist.destroy_process_group()
         return

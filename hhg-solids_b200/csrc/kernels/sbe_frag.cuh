@@ -28,9 +28,16 @@
 //    one k-point and a strided set of elements, so no lane idles on the padding; the state rho stays
 //    in shared memory (FP64) where both layouts read it.
 //
-// Precision: the outer sums, the field coupling and the commutators are split-TF32 products with
-// FP32 accumulation (the accuracy of complex FP32); the stage sum k1 + 2 k2 + 2 k3 + k4 is formed
-// in FP32 and added to the FP64 state rho; the window velocity sum and the current's k-sum are FP64.
+// Precision: the outer sums, the field coupling and the commutators are split-TF32 products; the
+// stage sum k1 + 2 k2 + 2 k3 + k4 is formed in FP32 and added to the FP64 state rho; the window
+// velocity sum and the current's k-sum are FP64.  The tensor cores round each mma's FP32 accumulation
+// toward zero (measured on B200: 1 + 0.75 ulp accumulates to 1), so the products carry a one-sided
+// error that the RK4 integration accumulates over the pulse: on the full pulse of the 11-orbital
+// model on a 12 x 12 grid J drifts to 9.0e-6 of the reference (the FP32-pipe element-group kernel:
+// 3.3e-7; the same kernel with FP32-pipe outer sums 6.4e-6, with an FP32-pipe product 2.8e-6).  With
+// 128 registers per thread and the split and transpose instructions it also runs slower than the
+// element-group kernel (C2: 499 vs 441 ms per solve).  It is therefore not chosen by default; set
+// HHG_FRAG=1 to run it.
 
 namespace frag {
 
@@ -97,8 +104,7 @@ struct Geom {
   static constexpr size_t TW1 = GWS + 2 * (size_t)NWROWS * NW2 * 16;  // [KPC][8] float2
   static constexpr size_t WTW1 = TW1 + (size_t)KPC * 8 * 8;           // [KPC][4] double2
   static constexpr size_t SJ = WTW1 + (size_t)KPC * 4 * 16;           // [2][kJRing][KPC][2 NJ] double
-  static constexpr size_t SCR = SJ + 2 * (size_t)kJRing * KPC * 2 * NJ * 8;  // [KPC][2][256] float2 (experiments)
-  static constexpr size_t BYTES = SCR + (size_t)KPC * 2 * 256 * 8;
+  static constexpr size_t BYTES = SJ + 2 * (size_t)kJRing * KPC * 2 * NJ * 8;
   static_assert(NW > 8 && NW <= 16, "fragment layout: 9..16 orbitals");
   static_assert((NBROWS * NW2 * 8) % 16 == 0, "16-byte copies of the inner sums");
   static_assert(KPC == 8 || KPC == 16, "k-points per CTA");
@@ -106,7 +112,7 @@ struct Geom {
 
 template <int NW, int NAX, int NJ, int KPC>
 __global__ void __launch_bounds__(KPC * 32, 16 / KPC)
-    propagate_frag_kernel(SolveTables t, GroupData<float> d, int vctas, double2* rho, double2* Jpart, int d_flags) {
+    propagate_frag_kernel(SolveTables t, GroupData<float> d, int vctas, double2* rho, double2* Jpart) {
   using FG = Geom<NW, NAX, NJ, KPC>;
   constexpr int NW2 = FG::NW2, NMAT = FG::NMAT, NTILE = FG::NTILE, HKS = FG::HKS;
   extern __shared__ __align__(16) unsigned char smraw[];
@@ -200,25 +206,6 @@ __global__ void __launch_bounds__(KPC * 32, 16 / KPC)
             nai[r] = negated(ai[r]);
           }
           const float2* G = GS + buf * gbuf;
-          if (d_flags & 1) {  // experiment: outer sums on the FP32 pipe (round to nearest)
-            for (int idx = tid; idx < KPC * NMAT * NW2; idx += NTHR) {
-              const int m = idx / (NMAT * NW2), mat = (idx / NW2) % NMAT, e = idx % NW2;
-              const float2* Gm = G + (size_t)mat * 4 * NW2;
-              float2 acc = fzero;
-              for (int q = 0; q < 7; ++q) {
-                const float2 ph = mul(TW1[m * 8 + q], P1[t.b1lo + q]);
-                float2 gv;
-                if (q < 3) {
-                  gv = Gm[(3 - q) * NW2 + (e % NW) * NW + e / NW];
-                  gv.y = -gv.y;
-                } else {
-                  gv = Gm[(q - 3) * NW2 + e];
-                }
-                acc = fmac(ph, gv, acc);
-              }
-              HK[((size_t)m * NMAT + mat) * HKS + e] = acc;
-            }
-          } else
 #pragma unroll 1
           for (int nt_ = w; nt_ < NMAT * NTILE; nt_ += KPC) {
             const int mat = nt_ / NTILE, j = nt_ % NTILE, e = 8 * j + g;
@@ -263,7 +250,6 @@ __global__ void __launch_bounds__(KPC * 32, 16 / KPC)
           const float2* Hm = HK + (size_t)w * NMAT * HKS;
           double2* Rm = RHO + (size_t)w * NW2;
           float2 r32[8], S[8], X[8];
-          double2 S64[8];
 #pragma unroll
           for (int s = 0; s < 8; ++s) {
             const int r = slot_row(s, g), cc = slot_col(s, c4);
@@ -273,7 +259,6 @@ __global__ void __launch_bounds__(KPC * 32, 16 / KPC)
               r32[s] = make_float2((float)x.x, (float)x.y);
             }
             S[s] = fzero;
-            S64[s] = make_double2(0.0, 0.0);
             X[s] = r32[s];
           }
           const double* esb = t.es + (size_t)ti * 9;
@@ -300,26 +285,6 @@ __global__ void __launch_bounds__(KPC * 32, 16 / KPC)
                 }
               }
             }
-            float Pr[8], Pi[8], Dr[8], Di[8];
-            if (d_flags & 2) {  // experiment: the product on the FP32 pipe through shared memory
-              float2* SH = reinterpret_cast<float2*>(smraw + FG::SCR) + (size_t)w * 512;
-              float2* SX = SH + 256;
-#pragma unroll
-              for (int s = 0; s < 8; ++s) {
-                SH[slot_row(s, g) * 16 + slot_col(s, c4)] = H[s];
-                SX[slot_row(s, g) * 16 + slot_col(s, c4)] = X[s];
-              }
-              __syncwarp();
-#pragma unroll
-              for (int s = 0; s < 8; ++s) {
-                const int r = slot_row(s, g), cc = slot_col(s, c4);
-                float2 acc = fzero;
-                for (int k = 0; k < 16; ++k) acc = fmac(SH[r * 16 + k], SX[k * 16 + cc], acc);
-                Pr[s] = acc.x;
-                Pi[s] = acc.y;
-              }
-              __syncwarp();
-            } else {
             // P = H X: Re P = Hr Xr + Hi Xi, Im P = Hr (-Xi) + Hi Xr over B = conj(X slots).
             float pr[2][4] = {}, pim[2][4] = {};
 #pragma unroll
@@ -344,6 +309,7 @@ __global__ void __launch_bounds__(KPC * 32, 16 / KPC)
               }
             }
             // Slots of P, and of D = P^+ by 8 x 8 transposes (block (rb, cb) of P lands in block (cb, rb)).
+            float Pr[8], Pi[8], Dr[8], Di[8];
 #pragma unroll
             for (int j = 0; j < 2; ++j) {
               Pr[2 * j] = pr[j][0];
@@ -354,7 +320,6 @@ __global__ void __launch_bounds__(KPC * 32, 16 / KPC)
               Pi[2 * j + 1] = pim[j][1];
               Pi[4 + 2 * j] = pim[j][2];
               Pi[5 + 2 * j] = pim[j][3];
-            }
             }
 #pragma unroll
             for (int rb = 0; rb < 2; ++rb)
@@ -372,20 +337,6 @@ __global__ void __launch_bounds__(KPC * 32, 16 / KPC)
             // k = -i (P - D); stage sum and the next stage's X = rho + c k.
             const float wgt = (st == 0 || st == 3) ? 1.f : 2.f;
             const float cn = (float)((st == 2 ? 1.0 : 0.5) * dt);
-            if (d_flags & 4) {  // experiment: X and the stage sum formed in FP64, as in the element-group kernel
-              const double cnd = (st == 2 ? 1.0 : 0.5) * dt;
-#pragma unroll
-              for (int s = 0; s < 8; ++s) {
-                const float kx = Pi[s] - Di[s], ky = -(Pr[s] - Dr[s]);
-                S64[s].x += (double)wgt * (double)kx;
-                S64[s].y += (double)wgt * (double)ky;
-                const int r = slot_row(s, g), cc = slot_col(s, c4);
-                if (r < NW && cc < NW) {
-                  const double2 x = Rm[r * NW + cc];
-                  X[s] = make_float2((float)(x.x + cnd * (double)kx), (float)(x.y + cnd * (double)ky));
-                }
-              }
-            } else {
 #pragma unroll
             for (int s = 0; s < 8; ++s) {
               const float kx = Pi[s] - Di[s], ky = -(Pr[s] - Dr[s]);
@@ -394,7 +345,6 @@ __global__ void __launch_bounds__(KPC * 32, 16 / KPC)
               X[s].x = fmaf(cn, kx, r32[s].x);
               X[s].y = fmaf(cn, ky, r32[s].y);
             }
-            }
           }
           // rho += dt/6 (k1 + 2 k2 + 2 k3 + k4) in FP64.
 #pragma unroll
@@ -402,13 +352,8 @@ __global__ void __launch_bounds__(KPC * 32, 16 / KPC)
             const int r = slot_row(s, g), cc = slot_col(s, c4);
             if (r < NW && cc < NW) {
               double2 x = Rm[r * NW + cc];
-              if (d_flags & 4) {
-                x.x = x.x + prefac * S64[s].x;
-                x.y = x.y + prefac * S64[s].y;
-              } else {
-                x.x = x.x + prefac * (double)S[s].x;
-                x.y = x.y + prefac * (double)S[s].y;
-              }
+              x.x = x.x + prefac * (double)S[s].x;
+              x.y = x.y + prefac * (double)S[s].y;
               Rm[r * NW + cc] = x;
             }
           }

@@ -978,11 +978,6 @@ int launch_group_batch_t(const BatchDesc* descs, const int2* items, int nitems, 
   return grid;
 }
 
-int frag_flags() {
-  const char* e = std::getenv("HHG_FRAG_FLAGS");
-  return e ? std::atoi(e) : 0;
-}
-
 // Tensor-core fragment kernel (mixed form): precomputed inner sums, compiled 7x7 box, KPC k-points per CTA.
 template <int NW, int NAX, int NJ, int KPC>
 bool plan_frag_t(const SolveTables& t, int sm_count, LaunchShape* out, char* why, int why_len) {
@@ -1037,7 +1032,7 @@ int launch_frag_t(const SolveTables& t, const GroupTables& gt, const LaunchShape
     tc.step1 = std::min(c0 + s.pre_chunk, t.step1);
     group_sums_kernel<float><<<(tc.step1 - c0) * t.N2, 256, 0, stream>>>(tc, d, 3, 4, FG::NBROWS, FG::NWROWS, Gpre,
                                                                           GWpre);
-    kern<<<s.ctas, s.threads, s.smem, stream>>>(tc, d, s.vctas, rho, Jpart, frag_flags());
+    kern<<<s.ctas, s.threads, s.smem, stream>>>(tc, d, s.vctas, rho, Jpart);
     launches += 2;
   }
   return launches;
@@ -1057,11 +1052,12 @@ const FragVariant kFragVariants[] = {
 #undef HHG_FRAG_VARIANT
 
 // The fragment variant for a mixed-form solve (Hermitian halved 7x7 box, real-space solver), or null.
-// tile_hint in 1..8 picks the 8-k-point CTAs.  Tuning overrides: HHG_FRAG=0 turns the kernel off,
-// HHG_FRAG_KPC=8|16 fixes the k-points per CTA.
+// tile_hint in 1..8 picks the 8-k-point CTAs.  The kernel is opt-in (HHG_FRAG=1): its tensor-core
+// products accumulate with round-toward-zero and it is slower than the element-group kernel (see
+// sbe_frag.cuh).  HHG_FRAG_KPC=8|16 fixes the k-points per CTA.
 const FragVariant* find_frag(const SolveTables& t, int tile_hint) {
-  if (const char* env = std::getenv("HHG_FRAG"))
-    if (env[0] == '0') return nullptr;
+  const char* on = std::getenv("HHG_FRAG");
+  if (!on || on[0] != '1') return nullptr;
   const GroupGeom gg = group_geom(t);
   if (t.kmode || !t.hermitian || !gg.half || t.b1n != 7 || t.b2n != 7) return nullptr;
   int kpc = (tile_hint > 0 && tile_hint <= 8) ? 8 : 16;
