@@ -711,22 +711,65 @@ void SWESim::reset_state() {
   for (auto& j : Jhist) j.clear();
 }
 
+namespace {
+bool run_graphs_enabled() {
+  const char* e = std::getenv("HHG_GRAPH");  // HHG_GRAPH=0: launch the sequence directly (measurements)
+  return !(e && e[0] == '0');
+}
+}  // namespace
+
 void SWESim::run() {
   if (!ready) throw std::runtime_error("SWESim_run_simulation: SWESim_init has not succeeded");
   check_cuda(cudaSetDevice(device), "cudaSetDevice");
-  check_cuda(cudaMemsetAsync(d_Jpart.p, 0, sizeof(double2) * d_Jpart.n, stream), "memset");
-  check_cuda(cudaEventRecord(ev0, stream), "event");
-  last_launches = hhg::launch_propagate(tab, gtab, shape, d_rho.p, d_Jpart.p, d_J.p, stream, evm);
-  check_cuda(cudaGetLastError(), "propagate launch");
-  check_cuda(cudaEventRecord(ev1, stream), "event");
-  check_cuda(cudaMemcpyAsync(host_J(), d_J.p, sizeof(double2) * 3 * (size_t)nt, cudaMemcpyDeviceToHost, stream), "D2H");
+  double2* hJ = host_J();
+  // The time loop (src/swe.cpp:183-223) as one launch sequence: clear the current partials, the
+  // propagation launches (a pair per chunk of steps for precomputed-sum shapes), the reduction and the
+  // copy of J to pinned host memory.  It is captured into a CUDA graph at the first run of a setup and
+  // replayed afterwards, so a run costs one graph launch.
+  auto enqueue = [&] {
+    // (external event records: inside a captured graph they record when the graph runs)
+    check_cuda(cudaMemsetAsync(d_Jpart.p, 0, sizeof(double2) * d_Jpart.n, stream), "memset");
+    check_cuda(cudaEventRecordWithFlags(ev0, stream, cudaEventRecordExternal), "event");
+    const int n = hhg::launch_propagate(tab, gtab, shape, d_rho.p, d_Jpart.p, d_J.p, stream, evm);
+    check_cuda(cudaGetLastError(), "propagate launch");
+    check_cuda(cudaEventRecordWithFlags(ev1, stream, cudaEventRecordExternal), "event");
+    check_cuda(cudaMemcpyAsync(hJ, d_J.p, sizeof(double2) * 3 * (size_t)nt, cudaMemcpyDeviceToHost, stream), "D2H");
+    return n;
+  };
+  if (!run_graphs_enabled()) {
+    drop_run_graph();
+    last_launches = enqueue();
+  } else {
+    if (run_graph && (run_graph_gen != generation || run_graph_hJ != hJ)) drop_run_graph();
+    if (!run_graph) {
+      cudaGraph_t g = nullptr;
+      check_cuda(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal), "begin capture");
+      int n = 0;
+      try {
+        n = enqueue();
+      } catch (...) {
+        cudaStreamEndCapture(stream, &g);
+        if (g) cudaGraphDestroy(g);
+        throw;
+      }
+      check_cuda(cudaStreamEndCapture(stream, &g), "end capture");
+      const cudaError_t e = cudaGraphInstantiate(&run_graph, g, 0);
+      cudaGraphDestroy(g);
+      check_cuda(e, "graph instantiate");
+      run_graph_gen = generation;
+      run_graph_hJ = hJ;
+      graph_launches = n;
+    }
+    check_cuda(cudaGraphLaunch(run_graph, stream), "graph launch");
+    last_launches = graph_launches;
+  }
   check_cuda(cudaStreamSynchronize(stream), "run_simulation");
   check_cuda(cudaEventElapsedTime(&last_ms, ev0, ev1), "event time");
   check_cuda(cudaEventElapsedTime(&last_prop_ms, ev0, evm), "event time");
   // The reference appends one sample per step to each Observable (src/observable.cpp:29);
   // SWESim_get_current returns the first nt of them.
   for (int a = 0; a < 3; ++a)
-    for (int ti = 0; ti < nt; ++ti) Jhist[a].push_back(cd(h_J[(size_t)a * nt + ti].x, h_J[(size_t)a * nt + ti].y));
+    for (int ti = 0; ti < nt; ++ti) Jhist[a].push_back(cd(hJ[(size_t)a * nt + ti].x, hJ[(size_t)a * nt + ti].y));
 }
 
 namespace {

@@ -128,6 +128,16 @@ struct SWESim {
   size_t h_J_cap = 0;
   std::vector<hhg::cd> Jhist[3];
   float last_ms = 0.f, last_prop_ms = 0.f;
+  // run()'s launch sequence (clear, propagate, reduce, copy the current out) captured once per setup
+  // and replayed; rebuilt when a new setup or a new pinned buffer changes what it points at.
+  cudaGraphExec_t run_graph = nullptr;
+  unsigned run_graph_gen = 0;
+  const double2* run_graph_hJ = nullptr;
+  int graph_launches = 0;  // kernel launches inside run_graph
+  void drop_run_graph() {
+    if (run_graph) cudaGraphExecDestroy(run_graph);
+    run_graph = nullptr;
+  }
   size_t h2d_bytes = 0;
   int last_launches = 0;
 
@@ -136,6 +146,7 @@ struct SWESim {
   // Forget the previous setup but keep device buffers, stream, events and the pinned host
   // buffer for reuse: a restart then costs no cudaFree / cudaFreeHost (both synchronise).
   void invalidate() {
+    drop_run_graph();
     ready = false;
     for (auto& j : Jhist) j.clear();
   }
@@ -149,6 +160,7 @@ struct SWESim {
     for (auto* b : {&d_es, &d_A, &d_Rc, &d_x0}) b->astream = s;
   }
   void release() {
+    drop_run_graph();
     d_cell.release();
     d_cellp.release();
     d_win.release();

@@ -542,7 +542,7 @@ int launch_propagate_steps(const SolveTables& t, const GroupTables& gt, const La
 int launch_propagate(const SolveTables& t, const GroupTables& gt, const LaunchShape& s, double2* rho, double2* Jpart,
                      double2* J, cudaStream_t stream, cudaEvent_t after_propagate) {
   const int launches = launch_propagate_steps(t, gt, s, rho, Jpart, stream);
-  if (after_propagate) cudaEventRecord(after_propagate, stream);
+  if (after_propagate) cudaEventRecordWithFlags(after_propagate, stream, cudaEventRecordExternal);
   const int n = 3 * t.nt;
   reduce_current_kernel<<<(n + 255) / 256, 256, 0, stream>>>(Jpart, s.vctas, t.nt, 1.0 / (double)t.Nk, J);
   return launches + 1;

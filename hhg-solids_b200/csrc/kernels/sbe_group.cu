@@ -817,6 +817,7 @@ __device__ __forceinline__ GroupData<Real> group_data(const GroupTables& gt) {
 }
 
 #include "sbe_frag.cuh"
+#include "sbe_dfrag.cuh"
 
 // One solve: physical CTA b runs virtual CTAs b, b + gridDim.x, ...
 template <typename Real, int EPT, int NWc, int NAXc, int NJc, bool KM = false, int WBc = 0, bool KP = false,
@@ -1038,6 +1039,88 @@ int launch_frag_t(const SolveTables& t, const GroupTables& gt, const LaunchShape
   return launches;
 }
 
+// FP64 tensor-core fragment kernel (plain form): precomputed inner sums, compiled 7x7 box, 8 k-points per CTA.
+template <int NW, int NAX, int NJ>
+bool plan_dfrag_t(const SolveTables& t, int sm_count, LaunchShape* out, char* why, int why_len) {
+  using FG = dfrag::Geom<NW, NAX, NJ>;
+  auto kern = dfrag::propagate_dfrag_kernel<NW, NAX, NJ>;
+  if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)FG::BYTES) != cudaSuccess) {
+    cudaGetLastError();
+    snprintf(why, why_len, "FP64 fragment kernel: %zu bytes of shared memory not available", FG::BYTES);
+    return false;
+  }
+  int occ = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, FG::KPC * 32, FG::BYTES);
+  if (occ < 1) occ = 1;
+  const long slots = (long)occ * sm_count;
+  const int rows = t.row1 - t.row0;
+  const long ntiles = (long)t.N2 * ((rows + FG::KPC - 1) / FG::KPC);
+  out->kernel = 5;
+  out->kmode = 0;
+  out->ept = 8;
+  out->k_per_cta = FG::KPC;
+  out->group = 32;
+  out->threads = FG::KPC * 32;
+  out->ntiles = (int)ntiles;
+  out->ctas = (int)(ntiles < slots ? ntiles : slots);
+  out->vctas = out->ctas;
+  out->box_sm = out->win_sm = 0;
+  out->smem = FG::BYTES;
+  out->pre_chunk = std::min(kPreChunk, t.nt);
+  out->pre_bytes = (size_t)out->pre_chunk * t.N2 * ((size_t)(FG::NBROWS + FG::NWROWS) * FG::NW2 * sizeof(double2));
+  return true;
+}
+
+template <int NW, int NAX, int NJ>
+int launch_dfrag_t(const SolveTables& t, const GroupTables& gt, const LaunchShape& s, double2* rho, double2* Jpart,
+                   cudaStream_t stream) {
+  using FG = dfrag::Geom<NW, NAX, NJ>;
+  if (!gt.pre || s.pre_chunk <= 0)
+    throw std::runtime_error("FP64 fragment kernel launch: needs its precomputed-sum scratch (GroupTables::pre)");
+  GroupData<double> d = {gt.Xbox64, gt.P64, gt.T1_64, gt.T2_64, gt.Xwin64, gt.P64, gt.T1_64, gt.T2_64, nullptr, nullptr};
+  const size_t gbuf = (size_t)FG::NBROWS * FG::NW2;
+  double2* Gpre = static_cast<double2*>(gt.pre);
+  double2* GWpre = Gpre + (size_t)s.pre_chunk * t.N2 * gbuf;
+  d.Gpre = Gpre;
+  d.GWpre = GWpre;
+  auto kern = dfrag::propagate_dfrag_kernel<NW, NAX, NJ>;
+  cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s.smem);
+  int launches = 0;
+  for (int c0 = t.step0; c0 < t.step1; c0 += s.pre_chunk) {
+    SolveTables tc = t;
+    tc.step0 = c0;
+    tc.step1 = std::min(c0 + s.pre_chunk, t.step1);
+    group_sums_kernel<double><<<(tc.step1 - c0) * t.N2, 256, 0, stream>>>(tc, d, 3, 4, FG::NBROWS, FG::NWROWS, Gpre,
+                                                                           GWpre);
+    kern<<<s.ctas, s.threads, s.smem, stream>>>(tc, d, s.vctas, rho, Jpart);
+    launches += 2;
+  }
+  return launches;
+}
+
+struct DfragVariant {
+  int nw, nax, nj;
+  bool (*plan)(const SolveTables&, int, LaunchShape*, char*, int);
+  int (*launch)(const SolveTables&, const GroupTables&, const LaunchShape&, double2*, double2*, cudaStream_t);
+};
+#define HHG_DFRAG_VARIANT(NW, NAX, NJ) {NW, NAX, NJ, plan_dfrag_t<NW, NAX, NJ>, launch_dfrag_t<NW, NAX, NJ>}
+const DfragVariant kDfragVariants[] = {
+    HHG_DFRAG_VARIANT(11, 1, 2), HHG_DFRAG_VARIANT(11, 2, 2), HHG_DFRAG_VARIANT(12, 1, 2), HHG_DFRAG_VARIANT(12, 2, 2),
+};
+#undef HHG_DFRAG_VARIANT
+
+// The FP64 fragment variant for a plain-form solve (Hermitian halved 7x7 box, real-space solver), or
+// null.  HHG_DFRAG=0 turns it off (measurements).
+const DfragVariant* find_dfrag(const SolveTables& t) {
+  if (const char* env = std::getenv("HHG_DFRAG"))
+    if (env[0] == '0') return nullptr;
+  const GroupGeom gg = group_geom(t);
+  if (t.kmode || !t.hermitian || !gg.half || t.b1n != 7 || t.b2n != 7) return nullptr;
+  for (const DfragVariant& v : kDfragVariants)
+    if (v.nw == t.nw && v.nax == t.nax && v.nj == t.nj) return &v;
+  return nullptr;
+}
+
 struct FragVariant {
   int nw, nax, nj, kpc;
   bool (*plan)(const SolveTables&, int, LaunchShape*, char*, int);
@@ -1158,6 +1241,11 @@ const GroupVariant* find_variant(const SolveTables& t, int precision) {
 
 bool plan_group(const SolveTables& t, int precision, int sm_count, LaunchShape* out, char* why, int why_len,
                 int tile_hint) {
+  if (precision == 0)
+    if (const DfragVariant* f = find_dfrag(t)) {
+      out->variant = (int)(f - kDfragVariants);
+      if (f->plan(t, sm_count, out, why, why_len)) return true;
+    }
   if (precision == 1)
     if (const FragVariant* f = find_frag(t, tile_hint)) {
       out->variant = (int)(f - kFragVariants);
@@ -1215,6 +1303,7 @@ int launch_group_batch(const LaunchShape& s, const BatchDesc* descs, const int2*
 int launch_group(const SolveTables& t, const GroupTables& gt, const LaunchShape& s, double2* rho, double2* Jpart,
                  cudaStream_t stream) {
   if (s.kernel == 4) return kFragVariants[s.variant].launch(t, gt, s, rho, Jpart, stream);
+  if (s.kernel == 5) return kDfragVariants[s.variant].launch(t, gt, s, rho, Jpart, stream);
   if (s.variant >= 0) return kGroupVariants[s.variant].launch(t, gt, s, rho, Jpart, stream);
   if (s.kmode) return launch_group_generic<true>(t, gt, s, rho, Jpart, stream);
   return launch_group_generic<false>(t, gt, s, rho, Jpart, stream);

@@ -350,7 +350,8 @@ __global__ void __launch_bounds__(kKcolMaxThreads) propagate_kcol_kernel(SolveTa
                 }
               }
               double2* dst = Jpart + ((size_t)v * t.nt + ti0 + s0f + ss) * 3 + t.j_id[a];
-              const double2 old = *dst;
+              // the virtual CTA's first tile writes its row (cleared before the launch) without reading it
+              const double2 old = tile == v ? make_double2(0.0, 0.0) : *dst;
               *dst = make_double2(old.x + re, old.y + im);
             }
             __syncthreads();  // the slots are rewritten by the next steps
@@ -387,7 +388,7 @@ __global__ void __launch_bounds__(kKcolMaxThreads) propagate_kcol_kernel(SolveTa
           im += sJ[(s * nwarps + q) * 2 * nj + 2 * a + 1];
         }
         double2* dst = Jpart + ((size_t)v * t.nt + ti0 + s) * 3 + t.j_id[a];
-        const double2 old = *dst;
+        const double2 old = tile == v ? make_double2(0.0, 0.0) : *dst;
         *dst = make_double2(old.x + re, old.y + im);
       }
     }

@@ -4,8 +4,10 @@ and against the golden J(t) made by the reference build: precomputed sums give t
 in-kernel sums, and every variant stays within the parity bar (FP64 1e-10 per axis, mixed 1e-6).
 
 The HHG_GROUP_* variables only remove variants from the planner's list; they are read when a solve is
-set up.  The tensor-core fragment kernel (sbe_frag.cuh) is opt-in (HHG_FRAG=1) and checked
-separately, against its own measured accuracy."""
+set up.  The plain form of 11- and 12-orbital models on a 7x7 box runs the FP64 tensor-core fragment
+kernel (sbe_dfrag.cuh) before any of them; HHG_DFRAG=0 removes it, so the element-group variants are
+compared with it off.  The mixed-form tensor-core fragment kernel (sbe_frag.cuh) is opt-in
+(HHG_FRAG=1) and checked against its own measured accuracy."""
 import os
 
 import numpy as np
@@ -15,7 +17,7 @@ from conftest import load_golden, rel_l2
 
 pytestmark = pytest.mark.gpu
 
-FLAGS = ("HHG_GROUP_NOPRE", "HHG_GROUP_NOPAIR", "HHG_GROUP_ANYBOX", "HHG_FRAG", "HHG_FRAG_KPC")
+FLAGS = ("HHG_GROUP_NOPRE", "HHG_GROUP_NOPAIR", "HHG_GROUP_ANYBOX", "HHG_FRAG", "HHG_FRAG_KPC", "HHG_DFRAG")
 NAMES = ["tmd6_8", "tmd11_10", "tmd12_6", "c2_prefix", "ks_tmd11_10"]
 
 
@@ -44,8 +46,8 @@ def run(param, precision, env):
 @pytest.mark.parametrize("name", ["tmd6_8", "tmd11_10", "c2_prefix", "ks_tmd11_10"])  # grids of at least 7x7: a 7x7 box
 def test_precomputed_sums_are_bit_identical(name, precision):
     _, param, _, _ = load_golden(name)
-    J_pre, n_pre, shape_pre = run(param, precision, [])
-    J_in, n_in, shape_in = run(param, precision, ["HHG_GROUP_NOPRE"])
+    J_pre, n_pre, shape_pre = run(param, precision, ["HHG_DFRAG=0"])
+    J_in, n_in, shape_in = run(param, precision, ["HHG_GROUP_NOPRE", "HHG_DFRAG=0"])
     nt = J_pre.shape[1]
     # Precomputed: one (sums, propagation) launch pair per 64 steps; in-kernel: one propagation.
     # (Only the k-space solver's 11- and 12-orbital shapes have them among its compiled shapes.)
@@ -61,8 +63,8 @@ def test_precomputed_sums_are_bit_identical(name, precision):
         assert precision == "fp64" and rel_l2(J_pre, J_in) < 1e-13, (shape_pre, shape_in, rel_l2(J_pre, J_in))
 
 
-@pytest.mark.parametrize("env", [[], ["HHG_GROUP_NOPRE"], ["HHG_GROUP_NOPAIR"], ["HHG_GROUP_NOPRE", "HHG_GROUP_NOPAIR"],
-                                 ["HHG_GROUP_ANYBOX"]])
+@pytest.mark.parametrize("env", [[], ["HHG_DFRAG=0"], ["HHG_GROUP_NOPRE", "HHG_DFRAG=0"], ["HHG_GROUP_NOPAIR"],
+                                 ["HHG_GROUP_NOPRE", "HHG_GROUP_NOPAIR", "HHG_DFRAG=0"], ["HHG_GROUP_ANYBOX"]])
 @pytest.mark.parametrize("name", NAMES)
 def test_every_variant_within_the_parity_bar(name, env):
     _, param, _, J_ref = load_golden(name)
@@ -125,3 +127,64 @@ def test_fragment_kernel_tile_shapes_and_ragged_columns(kpc):
         os.environ.pop("HHG_FRAG", None)
         os.environ.pop("HHG_FRAG_KPC", None)
     assert rel_l2(out[0], out[1]) < 1e-6, rel_l2(out[0], out[1])
+
+
+@pytest.mark.parametrize("name", ["tmd11_10", "c2_prefix", "tmd11_12_full", "tmd12_12_full", "tmd12_6"])
+def test_fp64_fragment_kernel_against_element_groups(name):
+    """The FP64 tensor-core fragment kernel (mma.m8n8k4.f64 for the outer Wannier sums and the
+    commutator) is the plain form's kernel for 11 and 12 orbitals on a Hermitian 7x7 box: within the
+    parity bar of the reference's current (1e-10 per axis) and within FP64 rounding of the
+    element-group kernel.  (On the 6 x 6 and 12-orbital 12 x 12 grids the placement folds the model's
+    cells into another box or a non-Hermitian table, and the element-group kernel runs.)"""
+    _, param, _, J_ref = load_golden(name)
+    J_d, n_d, shape = run(param, "fp64", [])
+    J_g, _, shape_g = run(param, "fp64", ["HHG_DFRAG=0"])
+    assert shape_g[3] != "propagate_dfrag_kernel"
+    if name in ("tmd11_10", "c2_prefix", "tmd11_12_full"):
+        assert shape[3] == "propagate_dfrag_kernel", shape
+        nt = J_d.shape[1]
+        assert n_d == 2 * ((nt + 63) // 64) + 1
+    for a in range(3):
+        if np.abs(J_ref[a]).max() == 0:
+            assert np.abs(J_d[a]).max() == 0
+        else:
+            assert rel_l2(J_d[a], J_ref[a]) < 1e-10, (a, rel_l2(J_d[a], J_ref[a]))
+            assert rel_l2(J_d[a], J_g[a]) < 1e-11, (a, rel_l2(J_d[a], J_g[a]))
+
+
+def test_fp64_fragment_kernel_ragged_columns_and_slabs():
+    """Columns that do not divide into whole tiles of 8 k-points (10 and 14 rows), non-square grids, both
+    polarisation layouts (one and two field axes), 11 and 12 orbitals, and a row slab, against the
+    element-group kernel."""
+    import tbgen
+    from pySWE import pyswe
+
+    ran12 = False
+    for model, (n1, n2), pol in (("tmd11_s7", (10, 10), [0.0, 1.0, 0.0]), ("tmd11_s7", (14, 8), [0.6, 0.8, 0.0]),
+                                 ("tmd12_s1", (20, 20), [0.8, 0.6, 0.0]), ("tmd12_s1", (30, 30), [0.0, 1.0, 0.0]),
+                                 ("tmd12_s3", (18, 24), [0.0, 1.0, 0.0])):
+        p = {"path_tb": tbgen.model_path(model), "nr1": n1, "nr2": n2, "nr3": 1, "tmax": 2.0, "dt": 0.02197,
+             "intensity": 2e12, "lambda": 3000.0, "tmax_field": 80.0, "pol_vec": np.array(pol),
+             "phi_vec": np.zeros(3)}
+        Jd, _, shape = run(p, "fp64", [])
+        Jg, _, _ = run(p, "fp64", ["HHG_DFRAG=0"])
+        if model.startswith("tmd11"):
+            assert shape[3] == "propagate_dfrag_kernel", (model, n1, n2, shape)
+        ran12 = ran12 or (model.startswith("tmd12") and shape[3] == "propagate_dfrag_kernel")
+        assert rel_l2(Jd, Jg) < 1e-11, (model, n1, n2, rel_l2(Jd, Jg))
+    assert ran12
+    p = dict(p, path_tb=tbgen.model_path("tmd11_s7"), nr1=14, nr2=8)
+    out = []
+    for env in ([], ["HHG_DFRAG=0"]):
+        saved = os.environ.pop("HHG_DFRAG", None)
+        os.environ.update(dict(k.split("=") for k in env))
+        try:
+            s = pyswe.SWE(pyswe.Settings(dict(p)), k_rows=(3, 9))
+            s.run_simulation()
+            out.append(np.stack(s.get_current()[1:]))
+            s.delete()
+        finally:
+            os.environ.pop("HHG_DFRAG", None)
+            if saved is not None:
+                os.environ["HHG_DFRAG"] = saved
+    assert rel_l2(out[0], out[1]) < 1e-11, rel_l2(out[0], out[1])
