@@ -729,10 +729,10 @@ void SWESim::run() {
   auto enqueue = [&] {
     // (external event records: inside a captured graph they record when the graph runs)
     check_cuda(cudaMemsetAsync(d_Jpart.p, 0, sizeof(double2) * d_Jpart.n, stream), "memset");
-    check_cuda(cudaEventRecordWithFlags(ev0, stream, cudaEventRecordExternal), "event");
+    check_cuda(hhg::record_event(ev0, stream), "event");
     const int n = hhg::launch_propagate(tab, gtab, shape, d_rho.p, d_Jpart.p, d_J.p, stream, evm);
     check_cuda(cudaGetLastError(), "propagate launch");
-    check_cuda(cudaEventRecordWithFlags(ev1, stream, cudaEventRecordExternal), "event");
+    check_cuda(hhg::record_event(ev1, stream), "event");
     check_cuda(cudaMemcpyAsync(hJ, d_J.p, sizeof(double2) * 3 * (size_t)nt, cudaMemcpyDeviceToHost, stream), "D2H");
     return n;
   };

@@ -111,6 +111,9 @@ int launch_group_batch(const LaunchShape& s, const BatchDesc* descs, const int2*
 // If `after_propagate` is non-null it is recorded between the propagation and the reduction.
 int launch_propagate(const SolveTables& t, const GroupTables& gt, const LaunchShape& s, double2* rho, double2* Jpart,
                      double2* J, cudaStream_t stream, cudaEvent_t after_propagate = nullptr);
+// Records `ev` on `stream`, as a graph node that records it when the graph runs if the stream is being
+// captured.
+cudaError_t record_event(cudaEvent_t ev, cudaStream_t stream);
 // The propagation launches alone (steps [t.step0, t.step1)), without the reduction; returns their number.
 int launch_propagate_steps(const SolveTables& t, const GroupTables& gt, const LaunchShape& s, double2* rho,
                            double2* Jpart, cudaStream_t stream);

@@ -32,8 +32,9 @@
 
 namespace dfrag {
 
+// (not volatile: the compiler may interleave independent accumulations to hide the mma latency)
 __device__ __forceinline__ void dmma(double (&d)[2], double a, double b) {
-  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};"
+  asm("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};"
                : "+d"(d[0]), "+d"(d[1])
                : "d"(a), "d"(b));
 }
@@ -177,35 +178,50 @@ __global__ void __launch_bounds__(256, 1)
             pa[ks] = q < 7 ? mul(TW1[g * 8 + q], P1[t.b1lo + q]) : dzero;
           }
           const double2* G = GS + buf * gbuf;
-#pragma unroll 1
-          for (int nt_ = w; nt_ < NMAT * NTILE; nt_ += KPC) {
-            const int mat = nt_ / NTILE, j = nt_ % NTILE, e = 8 * j + g;
+          // The warp's n-tiles nt = w, w + KPC, ... together, so that their accumulations interleave.
+          constexpr int NTW = (NMAT * NTILE + KPC - 1) / KPC;
+          double2 b0[NTW], b1[NTW];
+#pragma unroll
+          for (int u = 0; u < NTW; ++u) {
+            const int nt_ = w + u * KPC, mat = nt_ / NTILE, j = nt_ % NTILE, e = 8 * j + g;
             // B[c][g] of k-step 0: G(n1 = c - 3)_e (row 3 - c, transposed and conjugated for n1 < 0);
             // of k-step 1: G(n1 = c + 1)_e (c + 4 = 7 is the zero row).
-            double2 b0 = dzero, b1 = dzero;
-            if (e < NW2) {
+            b0[u] = dzero;
+            b1[u] = dzero;
+            if (nt_ < NMAT * NTILE && e < NW2) {
               const double2* Gm = G + (size_t)mat * 4 * NW2;
               if (c4 == 3) {
-                b0 = Gm[e];
+                b0[u] = Gm[e];
               } else {
                 const double2 vv = Gm[(3 - c4) * NW2 + (e % NW) * NW + e / NW];
-                b0 = make_double2(vv.x, -vv.y);
-                b1 = Gm[(c4 + 1) * NW2 + e];
+                b0[u] = make_double2(vv.x, -vv.y);
+                b1[u] = Gm[(c4 + 1) * NW2 + e];
               }
             }
-            double cr[2] = {0.0, 0.0}, ci[2] = {0.0, 0.0};
-            dmma(cr, pa[0].x, b0.x);
-            dmma(cr, -pa[0].y, b0.y);
-            dmma(ci, pa[0].x, b0.y);
-            dmma(ci, pa[0].y, b0.x);
-            dmma(cr, pa[1].x, b1.x);
-            dmma(cr, -pa[1].y, b1.y);
-            dmma(ci, pa[1].x, b1.y);
-            dmma(ci, pa[1].y, b1.x);
+          }
+          double cr[NTW][2], ci[NTW][2];
+#pragma unroll
+          for (int u = 0; u < NTW; ++u) cr[u][0] = cr[u][1] = ci[u][0] = ci[u][1] = 0.0;
+#pragma unroll
+          for (int ks = 0; ks < 2; ++ks) {
+#pragma unroll
+            for (int u = 0; u < NTW; ++u) dmma(cr[u], pa[ks].x, ks ? b1[u].x : b0[u].x);
+#pragma unroll
+            for (int u = 0; u < NTW; ++u) dmma(ci[u], pa[ks].x, ks ? b1[u].y : b0[u].y);
+#pragma unroll
+            for (int u = 0; u < NTW; ++u) dmma(cr[u], -pa[ks].y, ks ? b1[u].y : b0[u].y);
+#pragma unroll
+            for (int u = 0; u < NTW; ++u) dmma(ci[u], pa[ks].y, ks ? b1[u].x : b0[u].x);
+          }
+#pragma unroll
+          for (int u = 0; u < NTW; ++u) {
+            const int nt_ = w + u * KPC, mat = nt_ / NTILE, j = nt_ % NTILE;
             const int e0 = 8 * j + 2 * c4;  // results (k-point g, e0) and (g, e0 + 1)
-            double2* dst = HK + ((size_t)g * NMAT + mat) * NW2;
-            if (e0 < NW2) dst[e0] = make_double2(cr[0], ci[0]);
-            if (e0 + 1 < NW2) dst[e0 + 1] = make_double2(cr[1], ci[1]);
+            if (nt_ < NMAT * NTILE) {
+              double2* dst = HK + ((size_t)g * NMAT + mat) * NW2;
+              if (e0 < NW2) dst[e0] = make_double2(cr[u][0], ci[u][0]);
+              if (e0 + 1 < NW2) dst[e0 + 1] = make_double2(cr[u][1], ci[u][1]);
+            }
           }
         }
         __syncthreads();
@@ -215,7 +231,7 @@ __global__ void __launch_bounds__(256, 1)
         // (2) RK4 stages of this warp's k-point (src/solver.cpp:157-180), fields at t, t+dt/2, t+dt/2, t+dt.
         if (w < nown) {
           const double2* Hm = HK + (size_t)w * NMAT * NW2;
-          double2 S[8], X[8];
+          double2 S[8], X[8], H[8];
 #pragma unroll
           for (int s = 0; s < 8; ++s) {
             S[s] = dzero;
@@ -228,9 +244,10 @@ __global__ void __launch_bounds__(256, 1)
             double ea[NAX];
 #pragma unroll
             for (int a = 0; a < NAX; ++a) ea[a] = esb[f * 3 + t.ax_id[a]];
-            double2 H[8];
+X
 #pragma unroll
             for (int s = 0; s < 8; ++s) {
+              if (st == 2) continue;
               H[s] = dzero;
               if (el[s] >= 0) {
                 H[s] = Hm[el[s]];
@@ -248,19 +265,21 @@ __global__ void __launch_bounds__(256, 1)
 #pragma unroll
             for (int rb = 0; rb < 2; ++rb)
 #pragma unroll
-              for (int nb = 0; nb < 2; ++nb) {
-                pr[rb][nb][0] = pr[rb][nb][1] = 0.0;
-                pim[rb][nb][0] = pim[rb][nb][1] = 0.0;
+              for (int nb = 0; nb < 2; ++nb) pr[rb][nb][0] = pr[rb][nb][1] = pim[rb][nb][0] = pim[rb][nb][1] = 0.0;
+            // eight independent accumulations per k-step, interleaved
 #pragma unroll
-                for (int ks = 0; ks < 3; ++ks) {
-                  const int cb = ks >> 1, e = ks & 1;
-                  const double2 a = H[4 * rb + 2 * cb + e], b = X[4 * nb + 2 * cb + e];
-                  dmma(pr[rb][nb], a.x, b.x);
-                  dmma(pr[rb][nb], a.y, b.y);
-                  dmma(pim[rb][nb], a.x, -b.y);
-                  dmma(pim[rb][nb], a.y, b.x);
-                }
-              }
+            for (int ks = 0; ks < 3; ++ks) {
+              const int cb = ks >> 1, e = ks & 1;
+              const double2 a[2] = {H[2 * cb + e], H[4 + 2 * cb + e]}, b[2] = {X[2 * cb + e], X[4 + 2 * cb + e]};
+#pragma unroll
+              for (int q = 0; q < 4; ++q) dmma(pr[q >> 1][q & 1], a[q >> 1].x, b[q & 1].x);
+#pragma unroll
+              for (int q = 0; q < 4; ++q) dmma(pim[q >> 1][q & 1], a[q >> 1].x, -b[q & 1].y);
+#pragma unroll
+              for (int q = 0; q < 4; ++q) dmma(pr[q >> 1][q & 1], a[q >> 1].y, b[q & 1].y);
+#pragma unroll
+              for (int q = 0; q < 4; ++q) dmma(pim[q >> 1][q & 1], a[q >> 1].y, b[q & 1].x);
+            }
             // k = -i (P - P^+): block (rb, nb) of P^+ is block (nb, rb) of P transposed, conjugated.
             const double wgt = (st == 0 || st == 3) ? 1.0 : 2.0;
             const double cn = (st == 2 ? 1.0 : 0.5) * dt;

@@ -539,10 +539,20 @@ int launch_propagate_steps(const SolveTables& t, const GroupTables& gt, const La
   return launch_group(t, gt, s, rho, Jpart, stream);
 }
 
+cudaError_t record_event(cudaEvent_t ev, cudaStream_t stream) {
+  cudaStreamCaptureStatus st = cudaStreamCaptureStatusNone;
+  const cudaError_t e = cudaStreamIsCapturing(stream, &st);
+  if (e != cudaSuccess) return e;
+  // Inside a capture an external record becomes a graph node that records the event when the graph
+  // runs; outside one the flag is not accepted.
+  return st == cudaStreamCaptureStatusActive ? cudaEventRecordWithFlags(ev, stream, cudaEventRecordExternal)
+                                             : cudaEventRecord(ev, stream);
+}
+
 int launch_propagate(const SolveTables& t, const GroupTables& gt, const LaunchShape& s, double2* rho, double2* Jpart,
                      double2* J, cudaStream_t stream, cudaEvent_t after_propagate) {
   const int launches = launch_propagate_steps(t, gt, s, rho, Jpart, stream);
-  if (after_propagate) cudaEventRecordWithFlags(after_propagate, stream, cudaEventRecordExternal);
+  if (after_propagate) record_event(after_propagate, stream);
   const int n = 3 * t.nt;
   reduce_current_kernel<<<(n + 255) / 256, 256, 0, stream>>>(Jpart, s.vctas, t.nt, 1.0 / (double)t.Nk, J);
   return launches + 1;
