@@ -244,7 +244,7 @@ __global__ void __launch_bounds__(256, 1)
             double ea[NAX];
 #pragma unroll
             for (int a = 0; a < NAX; ++a) ea[a] = esb[f * 3 + t.ax_id[a]];
-X
+            // (the second and third stages share the field at t + dt/2: the third keeps the second's H)
 #pragma unroll
             for (int s = 0; s < 8; ++s) {
               if (st == 2) continue;
