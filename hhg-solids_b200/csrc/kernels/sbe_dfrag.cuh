@@ -18,8 +18,8 @@
 //  * Commutator.  k-step (cb, e) contracts frame columns 8 cb + 2c + e (c = 0..3 of the lanes): its A
 //    operand (A[g][c] = H[8 rb + g][8 cb + 2c + e]) is the lane's slot (rb, cb, e) of H, and because X
 //    is Hermitian its B operand (B[c][g] = X[8 cb + 2c + e][8 nb + g] = conj(X[8 nb + g][8 cb + 2c + e]))
-//    is the conjugate of the lane's slot (nb, cb, e) of X.  So P = H X (four 8 x 8 blocks, 48 mma per
-//    stage for the complex product) is formed from registers, P^+ comes from the same registers by
+//    is the conjugate of the lane's slot (nb, cb, e) of X.  So P = H X (four 8 x 8 blocks, 36 mma per
+//    stage: three real products per complex one) is formed from registers, P^+ comes from the same registers by
 //    movmatrix transposes of the 16-bit pieces of each double, and k = -i (P - P^+) and the next
 //    stage's X = rho + c k stay in the lane's slots.
 //  * Outer Wannier sums.  H0(k) and r_a(k) of the CTA's 8 k-points are one complex GEMM per step,
@@ -199,20 +199,29 @@ __global__ void __launch_bounds__(256, 1)
               }
             }
           }
-          double cr[NTW][2], ci[NTW][2];
+          // Complex products with three real ones (Gauss): T1 = pr gr, T2 = pi gi, T3 = (pr + pi)(gr + gi),
+          // re = T1 - T2, im = T3 - T1 - T2.
+          double t1[NTW][2], t2[NTW][2], t3[NTW][2];
 #pragma unroll
-          for (int u = 0; u < NTW; ++u) cr[u][0] = cr[u][1] = ci[u][0] = ci[u][1] = 0.0;
+          for (int u = 0; u < NTW; ++u) t1[u][0] = t1[u][1] = t2[u][0] = t2[u][1] = t3[u][0] = t3[u][1] = 0.0;
 #pragma unroll
           for (int ks = 0; ks < 2; ++ks) {
+            const double ps = pa[ks].x + pa[ks].y;
 #pragma unroll
-            for (int u = 0; u < NTW; ++u) dmma(cr[u], pa[ks].x, ks ? b1[u].x : b0[u].x);
+            for (int u = 0; u < NTW; ++u) dmma(t1[u], pa[ks].x, ks ? b1[u].x : b0[u].x);
 #pragma unroll
-            for (int u = 0; u < NTW; ++u) dmma(ci[u], pa[ks].x, ks ? b1[u].y : b0[u].y);
+            for (int u = 0; u < NTW; ++u) dmma(t2[u], pa[ks].y, ks ? b1[u].y : b0[u].y);
 #pragma unroll
-            for (int u = 0; u < NTW; ++u) dmma(cr[u], -pa[ks].y, ks ? b1[u].y : b0[u].y);
-#pragma unroll
-            for (int u = 0; u < NTW; ++u) dmma(ci[u], pa[ks].y, ks ? b1[u].x : b0[u].x);
+            for (int u = 0; u < NTW; ++u) dmma(t3[u], ps, ks ? b1[u].x + b1[u].y : b0[u].x + b0[u].y);
           }
+          double cr[NTW][2], ci[NTW][2];
+#pragma unroll
+          for (int u = 0; u < NTW; ++u)
+#pragma unroll
+            for (int i = 0; i < 2; ++i) {
+              cr[u][i] = t1[u][i] - t2[u][i];
+              ci[u][i] = t3[u][i] - t1[u][i] - t2[u][i];
+            }
 #pragma unroll
           for (int u = 0; u < NTW; ++u) {
             const int nt_ = w + u * KPC, mat = nt_ / NTILE, j = nt_ % NTILE;
@@ -259,27 +268,35 @@ __global__ void __launch_bounds__(256, 1)
                 }
               }
             }
-            // P = H X, block (rb, nb): Re += Hr Xr + Hi Xi, Im += Hr (-Xi) + Hi Xr over k-steps
-            // (cb, e) = (0, 0), (0, 1), (1, 0) (frame columns 9, 11, 13, 15 are empty).
-            double pr[2][2][2], pim[2][2][2];
+            // P = H X over k-steps (cb, e) = (0, 0), (0, 1), (1, 0) (frame columns 9, 11, 13, 15 are
+            // empty), with B = conj(X slots) and three real products per complex one (Gauss):
+            // T1 = Hr Xr, T2 = Hi (-Xi), T3 = (Hr + Hi)(Xr - Xi); Re P = T1 - T2, Im P = T3 - T1 - T2.
+            // Twelve independent accumulations per k-step, interleaved.
+            double t1[2][2][2], t2[2][2][2], t3[2][2][2];
 #pragma unroll
-            for (int rb = 0; rb < 2; ++rb)
+            for (int q = 0; q < 4; ++q)
 #pragma unroll
-              for (int nb = 0; nb < 2; ++nb) pr[rb][nb][0] = pr[rb][nb][1] = pim[rb][nb][0] = pim[rb][nb][1] = 0.0;
-            // eight independent accumulations per k-step, interleaved
+              for (int i = 0; i < 2; ++i) t1[q >> 1][q & 1][i] = t2[q >> 1][q & 1][i] = t3[q >> 1][q & 1][i] = 0.0;
 #pragma unroll
             for (int ks = 0; ks < 3; ++ks) {
               const int cb = ks >> 1, e = ks & 1;
               const double2 a[2] = {H[2 * cb + e], H[4 + 2 * cb + e]}, b[2] = {X[2 * cb + e], X[4 + 2 * cb + e]};
+              const double as[2] = {a[0].x + a[0].y, a[1].x + a[1].y}, bs[2] = {b[0].x - b[0].y, b[1].x - b[1].y};
 #pragma unroll
-              for (int q = 0; q < 4; ++q) dmma(pr[q >> 1][q & 1], a[q >> 1].x, b[q & 1].x);
+              for (int q = 0; q < 4; ++q) dmma(t1[q >> 1][q & 1], a[q >> 1].x, b[q & 1].x);
 #pragma unroll
-              for (int q = 0; q < 4; ++q) dmma(pim[q >> 1][q & 1], a[q >> 1].x, -b[q & 1].y);
+              for (int q = 0; q < 4; ++q) dmma(t2[q >> 1][q & 1], a[q >> 1].y, -b[q & 1].y);
 #pragma unroll
-              for (int q = 0; q < 4; ++q) dmma(pr[q >> 1][q & 1], a[q >> 1].y, b[q & 1].y);
-#pragma unroll
-              for (int q = 0; q < 4; ++q) dmma(pim[q >> 1][q & 1], a[q >> 1].y, b[q & 1].x);
+              for (int q = 0; q < 4; ++q) dmma(t3[q >> 1][q & 1], as[q >> 1], bs[q & 1]);
             }
+            double pr[2][2][2], pim[2][2][2];
+#pragma unroll
+            for (int q = 0; q < 4; ++q)
+#pragma unroll
+              for (int i = 0; i < 2; ++i) {
+                pr[q >> 1][q & 1][i] = t1[q >> 1][q & 1][i] - t2[q >> 1][q & 1][i];
+                pim[q >> 1][q & 1][i] = t3[q >> 1][q & 1][i] - t1[q >> 1][q & 1][i] - t2[q >> 1][q & 1][i];
+              }
             // k = -i (P - P^+): block (rb, nb) of P^+ is block (nb, rb) of P transposed, conjugated.
             const double wgt = (st == 0 || st == 3) ? 1.0 : 2.0;
             const double cn = (st == 2 ? 1.0 : 0.5) * dt;
