@@ -676,6 +676,34 @@ def mixed_report(J_mixed, J_fp64, param, fp64_ms, mixed_ms):
             "fp64_ms_per_solve": fp64_ms, "mixed_ms_per_solve": mixed_ms, "speedup_vs_fp64": fp64_ms / mixed_ms}
 
 
+def executed_form(nw: int, kernel: str, fpk: float, ms: float, nk: int, nt: int, peak: float):
+    """The flop count of the form the kernel actually executes, where it differs from the minimal one:
+    the closed-form commutator of two Hermitian 2x2 matrices (sbe_herm2.cuh: 15 flops per stage instead of
+    8 nw^3 = 64), or the 16 x 16 frame of the FP64 tensor-core kernel (3 k-steps x 4 blocks x 3 real
+    m8n8k4 products = 18 432 flops per stage instead of 8 nw^3)."""
+    if nw == 2 and kernel in ("propagate_kcol_kernel", "propagate_kpt_kernel"):
+        f = fpk - 32.0 * nw ** 3 + 4 * 15.0
+        form = "closed-form Hermitian 2x2 commutator (15 flops per stage)"
+    elif kernel == "propagate_dfrag_kernel":
+        f = fpk - 32.0 * nw ** 3 + 4 * 36 * 512.0
+        form = "commutator on the FP64 tensor cores: 16x16 frame, 3 k-steps x 4 blocks x 3 real m8n8k4 products per stage"
+    else:
+        return None
+    achieved = f * nk * nt / (ms * 1e-3) / 1e12
+    return {"form": form, "flops_per_kstep": f, "achieved": achieved, "frac": achieved / peak if peak > 0 else None}
+
+
+def load_profile_counters(workload: str, kernel: str):
+    """Pipe-activity counters of this kernel on this workload from the committed ncu summary, if any."""
+    name = (kernel or "").split("<")[0].replace("_kernel", "")
+    path = os.path.join(REPO, "profiles", f"{name}_{workload}_traffic.json")
+    if not os.path.exists(path):
+        return None
+    with open(path) as f:
+        d = json.load(f)
+    return d.get("counters")
+
+
 def load_traffic(workload: str, kernel: str):
     """DRAM bytes per launch of this kernel on this workload, from a committed ncu capture summary."""
     name = kernel or ""
@@ -933,7 +961,9 @@ def main():
                      "kernel": shape.get("kernel_name"), "flops_per_kstep": fpk, "flops_split": split,
                      "peak_source": "live FP64 / FP32 FMA-chain probes on this GPU (HHG_measure_peaks); "
                                     "MEASURED_PEAKS.json has no FP64 or FP32 figure",
-                     "fp32_peak": fp32_peak.value, "kernel_ms": prop_mean, "traffic_source": traffic_src},
+                     "fp32_peak": fp32_peak.value, "kernel_ms": prop_mean, "traffic_source": traffic_src,
+                     "executed_form": executed_form(nw, shape.get("kernel_name"), fpk, prop_mean, nk, nt, peak),
+                     "ncu_counters": load_profile_counters(args.workload, shape.get("kernel_name"))},
         "gpu_launches": launches,
         "clocks": clk,
         "wall_s_timed_region": t_wall,
