@@ -271,23 +271,22 @@ __global__ void __launch_bounds__(256, 1)
             // P = H X over k-steps (cb, e) = (0, 0), (0, 1), (1, 0) (frame columns 9, 11, 13, 15 are
             // empty), with B = conj(X slots) and three real products per complex one (Gauss):
             // T1 = Hr Xr, T2 = Hi (-Xi), T3 = (Hr + Hi)(Xr - Xi); Re P = T1 - T2, Im P = T3 - T1 - T2.
-            // Twelve independent accumulations per k-step, interleaved.
+            // Block by block, diagonal blocks first, each block's three accumulations interleaved, so
+            // that the transposes of finished blocks can overlap the products of the later ones.
             double t1[2][2][2], t2[2][2][2], t3[2][2][2];
 #pragma unroll
-            for (int q = 0; q < 4; ++q)
+            for (int q = 0; q < 4; ++q) {
+              const int rb = q < 2 ? q : 0, nb = q < 2 ? q : 1;  // (0,0), (1,1), (0,1), (1,0)
+              const int rr = q == 3 ? 1 : rb, nn = q == 3 ? 0 : nb;
+              t1[rr][nn][0] = t1[rr][nn][1] = t2[rr][nn][0] = t2[rr][nn][1] = t3[rr][nn][0] = t3[rr][nn][1] = 0.0;
 #pragma unroll
-              for (int i = 0; i < 2; ++i) t1[q >> 1][q & 1][i] = t2[q >> 1][q & 1][i] = t3[q >> 1][q & 1][i] = 0.0;
-#pragma unroll
-            for (int ks = 0; ks < 3; ++ks) {
-              const int cb = ks >> 1, e = ks & 1;
-              const double2 a[2] = {H[2 * cb + e], H[4 + 2 * cb + e]}, b[2] = {X[2 * cb + e], X[4 + 2 * cb + e]};
-              const double as[2] = {a[0].x + a[0].y, a[1].x + a[1].y}, bs[2] = {b[0].x - b[0].y, b[1].x - b[1].y};
-#pragma unroll
-              for (int q = 0; q < 4; ++q) dmma(t1[q >> 1][q & 1], a[q >> 1].x, b[q & 1].x);
-#pragma unroll
-              for (int q = 0; q < 4; ++q) dmma(t2[q >> 1][q & 1], a[q >> 1].y, -b[q & 1].y);
-#pragma unroll
-              for (int q = 0; q < 4; ++q) dmma(t3[q >> 1][q & 1], as[q >> 1], bs[q & 1]);
+              for (int ks = 0; ks < 3; ++ks) {
+                const int cb = ks >> 1, e = ks & 1;
+                const double2 a = H[4 * rr + 2 * cb + e], b = X[4 * nn + 2 * cb + e];
+                dmma(t1[rr][nn], a.x, b.x);
+                dmma(t2[rr][nn], a.y, -b.y);
+                dmma(t3[rr][nn], a.x + a.y, b.x - b.y);
+              }
             }
             double pr[2][2][2], pim[2][2][2];
 #pragma unroll
