@@ -873,6 +873,27 @@ def main():
         mixed = mixed_report(J_mixed, J_fp64, param, fp64_ms, total_ms / args.steps)
         mixed["fp64_timed_solves"] = len(fms)
         mixed["fp64_kernel"] = fp64_shape.get("kernel_name")
+        if fp64_shape.get("kernel_name") == "propagate_dfrag_kernel":
+            # The plain form on the FP64 pipe as well (the element-group kernel the FP64 tensor-core
+            # kernel replaced for these shapes), for the mixed form's speed-up over FP64 arithmetic
+            # on the same pipes.
+            os.environ["HHG_DFRAG"] = "0"
+            try:
+                ref2 = pyswe.SWE(pyswe.Settings(dict(param)), device=local, solver=args.solver)
+            finally:
+                os.environ.pop("HHG_DFRAG", None)
+            ref2.run_simulation()
+            fms2 = []
+            for i in range(args.fp64_steps):
+                flush.fill_(float(i))
+                torch.cuda.synchronize()
+                ref2.reset()
+                ref2.run_simulation()
+                fms2.append(ref2.last_kernel_ms())
+            mixed["fp64_pipe_kernel"] = {"kernel": ref2.launch_shape().get("kernel_name"),
+                                         "ms_per_solve": statistics.mean(fms2),
+                                         "mixed_speedup": statistics.mean(fms2) / (total_ms / args.steps)}
+            ref2.delete()
         if args.batch > 1:
             # The batched mixed form: args.batch solves of this configuration (polarisation angles
             # spread over the half circle) in one SWEBatch, against the plain FP64 solve's throughput.
@@ -910,6 +931,8 @@ def main():
             mixed["batched"] = {"solves": args.batch, "timed_batches": len(bms), "ms_per_batch": statistics.mean(bms),
                                 "ms_per_solve": per_solve, "k_pt_rk4_steps_per_s": nk * nt / (per_solve * 1e-3),
                                 "throughput_vs_fp64_solo": fp64_ms / per_solve,
+                                "throughput_vs_fp64_pipe_solo": (mixed["fp64_pipe_kernel"]["ms_per_solve"] / per_solve
+                                                                 if "fp64_pipe_kernel" in mixed else None),
                                 "J_rel_l2_vs_fp64": berr,
                                 "engine": batch_engine_desc()}
     swe.delete()
