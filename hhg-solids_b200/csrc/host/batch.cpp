@@ -446,6 +446,7 @@ struct SWEServer {
   }
 
   void launch_chunk() {
+    hhg::TraceRange range("hhg SWEServer chunk");
     const bool persistent = persistent_batch_mode();
     int sms = 0;
     check_cuda(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device), "cudaDeviceGetAttribute");
@@ -538,6 +539,7 @@ struct SWEServer {
   }
 
   void finish_chunk() {
+    hhg::TraceRange range("hhg SWEServer finish");
     check_cuda(cudaEventSynchronize(chunk_end), "chunk");
     float ms = 0.f;
     if (cudaEventElapsedTime(&ms, chunk_begin, chunk_end) == cudaSuccess) gpu_ms += ms;
@@ -694,6 +696,7 @@ int SWEBatch_add(SWEBatch* b, SWESim* swe) {
 }
 
 int SWEBatch_run(SWEBatch* b) {
+  hhg::TraceRange range("hhg SWEBatch_run");
   if (!b) return -1;
   try {
     b->has_err = false;

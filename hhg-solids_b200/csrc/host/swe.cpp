@@ -56,6 +56,7 @@ struct PhaseTrace {
     t0 = last = std::chrono::steady_clock::now();
   }
   void mark(const char* name) {
+    nvtxMarkA(name);
     if (!on) return;
     const auto now = std::chrono::steady_clock::now();
     char buf[96];
@@ -198,6 +199,7 @@ void SWESim::tune_tiles(int sms) {
 }
 
 void SWESim::init() {
+  hhg::TraceRange range("hhg SWESim_init");
   PhaseTrace trace;
   invalidate();
   served = false;
@@ -719,6 +721,7 @@ bool run_graphs_enabled() {
 }  // namespace
 
 void SWESim::run() {
+  hhg::TraceRange range("hhg SWESim_run_simulation");
   if (!ready) throw std::runtime_error("SWESim_run_simulation: SWESim_init has not succeeded");
   check_cuda(cudaSetDevice(device), "cudaSetDevice");
   double2* hJ = host_J();

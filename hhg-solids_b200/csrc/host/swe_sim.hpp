@@ -7,6 +7,8 @@
 #include <string>
 #include <vector>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include "../kernels/sbe_device.h"
 #include "hhg_swe.h"
 #include "tb_model.hpp"
@@ -25,6 +27,14 @@ struct Settings {
 };
 
 namespace hhg {
+
+// A named range on the profiler timeline (NVTX; costs nothing without a profiler attached).
+struct TraceRange {
+  explicit TraceRange(const char* name) { nvtxRangePushA(name); }
+  ~TraceRange() { nvtxRangePop(); }
+  TraceRange(const TraceRange&) = delete;
+  TraceRange& operator=(const TraceRange&) = delete;
+};
 
 inline void check_cuda(cudaError_t e, const char* what) {
   if (e != cudaSuccess) throw std::runtime_error(std::string(what) + ": " + cudaGetErrorString(e));
