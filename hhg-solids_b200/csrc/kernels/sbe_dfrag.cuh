@@ -244,15 +244,14 @@ __global__ void __launch_bounds__(256 * WPK, 1)
               pim[nb][i] = t3[nb][i] - t1[nb][i] - t2[nb][i];
             }
           // The off-diagonal block P(h, 1-h) to the partner, P(1-h, h) from it.
-          // (component-major [h][2][32]: consecutive lanes, consecutive 16-byte words)
           {
-            double2* mine = xp + (size_t)h * 2 * 32 + lane;
+            double2* mine = xp + ((size_t)h * 32 + lane) * 2;
             mine[0] = h ? make_double2(pr[0][0], pr[0][1]) : make_double2(pr[1][0], pr[1][1]);
-            mine[32] = h ? make_double2(pim[0][0], pim[0][1]) : make_double2(pim[1][0], pim[1][1]);
+            mine[1] = h ? make_double2(pim[0][0], pim[0][1]) : make_double2(pim[1][0], pim[1][1]);
           }
           pair_sync(1 + m);
-          const double2* theirs = xp + (size_t)(1 - h) * 2 * 32 + lane;
-          const double2 opr = theirs[0], opi = theirs[32];
+          const double2* theirs = xp + ((size_t)(1 - h) * 32 + lane) * 2;
+          const double2 opr = theirs[0], opi = theirs[1];
           // D(h, h) = P(h, h)^+ and D(h, 1-h) = P(1-h, h)^+ by transposes.
           double dr[2][2], di[2][2];  // [nb][e]
           {
@@ -290,23 +289,23 @@ __global__ void __launch_bounds__(256 * WPK, 1)
             }
           if (st == 3) break;  // the last stage's X is not needed
           {
-            double2* mine = xx + (size_t)h * 4 * 32 + lane;  // [h][j][32]
+            double2* mine = xx + ((size_t)h * 32 + lane) * 4;
 #pragma unroll
-            for (int j = 0; j < 4; ++j) mine[j * 32] = xo[j];
+            for (int j = 0; j < 4; ++j) mine[j] = xo[j];
           }
           pair_sync(1 + m);
-          const double2* theirs_x = xx + (size_t)(1 - h) * 4 * 32 + lane;
+          const double2* theirs_x = xx + ((size_t)(1 - h) * 32 + lane) * 4;
           if (h == 0) {
 #pragma unroll
             for (int j = 0; j < 4; ++j) {
               X[j] = xo[j];
-              X[4 + j] = theirs_x[j * 32];
+              X[4 + j] = theirs_x[j];
             }
           } else {
 #pragma unroll
             for (int j = 0; j < 4; ++j) {
               X[4 + j] = xo[j];
-              X[j] = theirs_x[j * 32];
+              X[j] = theirs_x[j];
             }
           }
         }
