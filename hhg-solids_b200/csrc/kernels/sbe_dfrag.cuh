@@ -60,10 +60,9 @@ __device__ __forceinline__ int frame_orbital(int p, int nw) {
   return o < nw ? o : -1;
 }
 
-template <int NW, int NAX, int NJ, int WPK>
+template <int NW, int NAX, int NJ>
 struct Geom {
   static constexpr int KPC = 8;
-  static constexpr int NWARPS = KPC * WPK;      // WPK warps per k-point
   static constexpr int NW2 = NW * NW;
   static constexpr int NMAT = 1 + NAX;
   static constexpr int NBROWS = NMAT * 4;      // halved 7 x 7 box: inner-sum rows n1 = 0..3 per matrix
@@ -75,26 +74,16 @@ struct Geom {
   static constexpr size_t GWS = GS + 2 * (size_t)NBROWS * NW2 * 16;    // [2][NWROWS][NW2] double2
   static constexpr size_t TW1 = GWS + 2 * (size_t)NWROWS * NW2 * 16;   // [KPC][8] double2
   static constexpr size_t WTW1 = TW1 + (size_t)KPC * 8 * 16;           // [KPC][4] double2
-  static constexpr size_t SJ = WTW1 + (size_t)KPC * 4 * 16;            // [2][kJRing][NWARPS][2 NJ] double
-  static constexpr size_t XP = SJ + 2 * (size_t)kJRing * NWARPS * 2 * NJ * 8;  // WPK = 2: [KPC][2][32][2] double2
-  static constexpr size_t XX = XP + (WPK == 2 ? (size_t)KPC * 2 * 32 * 2 * 16 : 0);  // WPK = 2: [KPC][2][32][4] double2
-  static constexpr size_t BYTES = XX + (WPK == 2 ? (size_t)KPC * 2 * 32 * 4 * 16 : 0);
-  static_assert(WPK == 1 || WPK == 2, "one or two warps per k-point");
+  static constexpr size_t SJ = WTW1 + (size_t)KPC * 4 * 16;            // [2][kJRing][KPC][2 NJ] double
+  static constexpr size_t BYTES = SJ + 2 * (size_t)kJRing * KPC * 2 * NJ * 8;
   static_assert(NW > 8 && NW <= 12, "frame: 9..12 orbitals (positions 0..7, 8, 10, 12, 14)");
 };
 
-__device__ __forceinline__ void pair_sync(int id) { asm volatile("bar.sync %0, 64;" ::"r"(id) : "memory"); }
-
-// WPK = 1: one warp per k-point (all four 8 x 8 blocks of each product).  WPK = 2: a pair of warps per
-// k-point, warp h computing block row h of each product (18 instead of 36 tensor-core products per
-// stage and warp, half the registers, twice the warps per SM); the pair exchanges the off-diagonal
-// product block (for (HX)^+) and its halves of the next X through shared memory, synchronised by
-// a named barrier per k-point.
-template <int NW, int NAX, int NJ, int WPK>
-__global__ void __launch_bounds__(256 * WPK, 1)
+template <int NW, int NAX, int NJ>
+__global__ void __launch_bounds__(256, 1)
     propagate_dfrag_kernel(SolveTables t, GroupData<double> d, int vctas, double2* rho, double2* Jpart) {
-  using FG = Geom<NW, NAX, NJ, WPK>;
-  constexpr int KPC = FG::KPC, NW2 = FG::NW2, NMAT = FG::NMAT, NTILE = FG::NTILE, NWARPS = FG::NWARPS;
+  using FG = Geom<NW, NAX, NJ>;
+  constexpr int KPC = FG::KPC, NW2 = FG::NW2, NMAT = FG::NMAT, NTILE = FG::NTILE;
   extern __shared__ __align__(16) unsigned char smraw[];
   double2* RHO = reinterpret_cast<double2*>(smraw + FG::RHO);
   double2* HK = reinterpret_cast<double2*>(smraw + FG::HK);
@@ -103,11 +92,9 @@ __global__ void __launch_bounds__(256 * WPK, 1)
   double2* TW1 = reinterpret_cast<double2*>(smraw + FG::TW1);
   double2* WTW1 = reinterpret_cast<double2*>(smraw + FG::WTW1);
   double* SJ = reinterpret_cast<double*>(smraw + FG::SJ);
-  double2* XP = reinterpret_cast<double2*>(smraw + FG::XP);
-  double2* XX = reinterpret_cast<double2*>(smraw + FG::XX);
 
   const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5, g = lane >> 2, c4 = lane & 3;
-  constexpr int NTHR = NWARPS * 32;
+  constexpr int NTHR = KPC * 32;
   const int rows = t.row1 - t.row0, bpc = (rows + KPC - 1) / KPC, ntiles = t.N2 * bpc;
   const int step0 = t.step0, step1 = t.step1, npw = 2 * t.np + 1;
   const double dt = t.dt, prefac = 0.1666666666666 * dt;
@@ -144,13 +131,13 @@ __global__ void __launch_bounds__(256 * WPK, 1)
       auto flush = [&](int ti_end) {
         const int slot = (ti_end / kJRing) & 1, s = ti_end % kJRing;
         const int ti0 = max(ti_end - s, step0), nsteps = ti_end - ti0 + 1;
-        const double* half = SJ + ((size_t)slot * kJRing + (ti0 % kJRing)) * NWARPS * 2 * NJ;
+        const double* half = SJ + ((size_t)slot * kJRing + (ti0 % kJRing)) * KPC * 2 * NJ;
         for (int idx = tid; idx < nsteps * NJ; idx += NTHR) {
           const int ss = idx / NJ, a = idx % NJ;
           double re = 0.0, im = 0.0;
-          for (int ww = 0; ww < NWARPS; ++ww) {
-            re += half[(ss * NWARPS + ww) * 2 * NJ + 2 * a];
-            im += half[(ss * NWARPS + ww) * 2 * NJ + 2 * a + 1];
+          for (int ww = 0; ww < KPC; ++ww) {
+            re += half[(ss * KPC + ww) * 2 * NJ + 2 * a];
+            im += half[(ss * KPC + ww) * 2 * NJ + 2 * a + 1];
           }
           const int ja = a == 0 ? t.j_id[0] : (a == 1 ? t.j_id[1] : t.j_id[2]);
           double2* dst = Jpart + ((size_t)v * t.nt + ti0 + ss) * 3 + ja;
@@ -175,152 +162,9 @@ __global__ void __launch_bounds__(256 * WPK, 1)
       cp_async_wait_all();
       __syncthreads();
       // This warp's state in its slots (registers for the whole tile; RHO mirrors it for the current).
-      double2 r64[WPK == 1 ? 8 : 1];
-      if constexpr (WPK == 1) {
+      double2 r64[8];
 #pragma unroll
-        for (int s = 0; s < 8; ++s) r64[s] = (w < nown && el[s] >= 0) ? RHO[w * NW2 + el[s]] : dzero;
-      }
-
-      // The RK4 stages of step ti with a warp pair per k-point: warp h (0, 1) of pair m holds all slots
-      // of X (the B operand of both block columns) and computes block row h of P = H X, i.e. its own
-      // slots s = 4h + j (j = 2 cb + e).  rho stays in shared memory (RHO, read for every stage's X).
-      auto stages_pair = [&](int ti) {
-        const int m = w >> 1, h = w & 1;
-        if (m >= nown) return;
-        const double2* Hm = HK + (size_t)m * NMAT * NW2;
-        double2* Rm = RHO + (size_t)m * NW2;
-        double2* xp = XP + (size_t)m * 2 * 32 * 2;
-        double2* xx = XX + (size_t)m * 2 * 32 * 4;
-        int elo[4];  // elements of the own slots (block row h)
-#pragma unroll
-        for (int j = 0; j < 4; ++j) elo[j] = h ? el[4 + j] : el[j];
-        double2 X[8], S[4], H[4];
-#pragma unroll
-        for (int s = 0; s < 8; ++s) X[s] = el[s] >= 0 ? Rm[el[s]] : dzero;
-#pragma unroll
-        for (int j = 0; j < 4; ++j) S[j] = dzero;
-        const double* esb = t.es + (size_t)ti * 9;
-#pragma unroll 1
-        for (int st = 0; st < 4; ++st) {
-          const int f = st == 0 ? 0 : (st == 3 ? 2 : 1);
-          double ea[NAX];
-#pragma unroll
-          for (int a = 0; a < NAX; ++a) ea[a] = esb[f * 3 + t.ax_id[a]];
-          // (the second and third stages share the field at t + dt/2: the third keeps the second's H)
-#pragma unroll
-          for (int j = 0; j < 4; ++j) {
-            if (st == 2) continue;
-            H[j] = dzero;
-            if (elo[j] >= 0) {
-              H[j] = Hm[elo[j]];
-#pragma unroll
-              for (int a = 0; a < NAX; ++a) {
-                const double2 rv = Hm[(1 + a) * NW2 + elo[j]];
-                H[j].x = fma(ea[a], rv.x, H[j].x);
-                H[j].y = fma(ea[a], rv.y, H[j].y);
-              }
-            }
-          }
-          // Blocks (h, 0) and (h, 1) of P with three real products per complex one.
-          double t1[2][2], t2[2][2], t3[2][2];
-#pragma unroll
-          for (int nb = 0; nb < 2; ++nb) {
-            t1[nb][0] = t1[nb][1] = t2[nb][0] = t2[nb][1] = t3[nb][0] = t3[nb][1] = 0.0;
-#pragma unroll
-            for (int ks = 0; ks < 3; ++ks) {
-              const int cb = ks >> 1, e = ks & 1;
-              const double2 a = H[2 * cb + e], b = X[4 * nb + 2 * cb + e];
-              dmma(t1[nb], a.x, b.x);
-              dmma(t2[nb], a.y, -b.y);
-              dmma(t3[nb], a.x + a.y, b.x - b.y);
-            }
-          }
-          double pr[2][2], pim[2][2];
-#pragma unroll
-          for (int nb = 0; nb < 2; ++nb)
-#pragma unroll
-            for (int i = 0; i < 2; ++i) {
-              pr[nb][i] = t1[nb][i] - t2[nb][i];
-              pim[nb][i] = t3[nb][i] - t1[nb][i] - t2[nb][i];
-            }
-          // The off-diagonal block P(h, 1-h) to the partner, P(1-h, h) from it.
-          {
-            double2* mine = xp + ((size_t)h * 32 + lane) * 2;
-            mine[0] = h ? make_double2(pr[0][0], pr[0][1]) : make_double2(pr[1][0], pr[1][1]);
-            mine[1] = h ? make_double2(pim[0][0], pim[0][1]) : make_double2(pim[1][0], pim[1][1]);
-          }
-          pair_sync(1 + m);
-          const double2* theirs = xp + ((size_t)(1 - h) * 32 + lane) * 2;
-          const double2 opr = theirs[0], opi = theirs[1];
-          // D(h, h) = P(h, h)^+ and D(h, 1-h) = P(1-h, h)^+ by transposes.
-          double dr[2][2], di[2][2];  // [nb][e]
-          {
-            double a0 = h ? pr[1][0] : pr[0][0], a1 = h ? pr[1][1] : pr[0][1];
-            double b0 = h ? pim[1][0] : pim[0][0], b1 = h ? pim[1][1] : pim[0][1];
-            transpose8(a0, a1);
-            transpose8(b0, b1);
-            double c0 = opr.x, c1 = opr.y, e0 = opi.x, e1 = opi.y;
-            transpose8(c0, c1);
-            transpose8(e0, e1);
-            // nb = h: diagonal; nb = 1 - h: the partner's block
-            dr[0][0] = h ? c0 : a0;
-            dr[0][1] = h ? c1 : a1;
-            di[0][0] = h ? -e0 : -b0;
-            di[0][1] = h ? -e1 : -b1;
-            dr[1][0] = h ? a0 : c0;
-            dr[1][1] = h ? a1 : c1;
-            di[1][0] = h ? -b0 : -e0;
-            di[1][1] = h ? -b1 : -e1;
-          }
-          // k = -i (P - P^+) on the own slots; stage sum; the own slots of the next X.
-          const double wgt = (st == 0 || st == 3) ? 1.0 : 2.0;
-          const double cn = (st == 2 ? 1.0 : 0.5) * dt;
-          double2 xo[4];
-#pragma unroll
-          for (int nb = 0; nb < 2; ++nb)
-#pragma unroll
-            for (int e = 0; e < 2; ++e) {
-              const int j = 2 * nb + e;
-              const double kx = pim[nb][e] - di[nb][e], ky = -(pr[nb][e] - dr[nb][e]);
-              S[j].x = fma(wgt, kx, S[j].x);
-              S[j].y = fma(wgt, ky, S[j].y);
-              const double2 r = elo[j] >= 0 ? Rm[elo[j]] : dzero;
-              xo[j] = make_double2(fma(cn, kx, r.x), fma(cn, ky, r.y));
-            }
-          if (st == 3) break;  // the last stage's X is not needed
-          {
-            double2* mine = xx + ((size_t)h * 32 + lane) * 4;
-#pragma unroll
-            for (int j = 0; j < 4; ++j) mine[j] = xo[j];
-          }
-          pair_sync(1 + m);
-          const double2* theirs_x = xx + ((size_t)(1 - h) * 32 + lane) * 4;
-          if (h == 0) {
-#pragma unroll
-            for (int j = 0; j < 4; ++j) {
-              X[j] = xo[j];
-              X[4 + j] = theirs_x[j];
-            }
-          } else {
-#pragma unroll
-            for (int j = 0; j < 4; ++j) {
-              X[4 + j] = xo[j];
-              X[j] = theirs_x[j];
-            }
-          }
-        }
-        // Both warps read all of rho for their X above: update it only after the partner is done.
-        pair_sync(1 + m);
-        // rho += dt/6 (k1 + 2 k2 + 2 k3 + k4) (src/solver.cpp:170-180) on the own slots
-#pragma unroll
-        for (int j = 0; j < 4; ++j)
-          if (elo[j] >= 0) {
-            double2 r = Rm[elo[j]];
-            r.x = r.x + prefac * S[j].x;
-            r.y = r.y + prefac * S[j].y;
-            Rm[elo[j]] = r;
-          }
-      };
+      for (int s = 0; s < 8; ++s) r64[s] = (w < nown && el[s] >= 0) ? RHO[w * NW2 + el[s]] : dzero;
 
       for (int ti = step0; ti < step1; ++ti) {
         const int buf = ti & 1;
@@ -334,12 +178,12 @@ __global__ void __launch_bounds__(256 * WPK, 1)
             pa[ks] = q < 7 ? mul(TW1[g * 8 + q], P1[t.b1lo + q]) : dzero;
           }
           const double2* G = GS + buf * gbuf;
-          // The warp's n-tiles nt = w, w + NWARPS, ... together, so that their accumulations interleave.
-          constexpr int NTW = (NMAT * NTILE + NWARPS - 1) / NWARPS;
+          // The warp's n-tiles nt = w, w + KPC, ... together, so that their accumulations interleave.
+          constexpr int NTW = (NMAT * NTILE + KPC - 1) / KPC;
           double2 b0[NTW], b1[NTW];
 #pragma unroll
           for (int u = 0; u < NTW; ++u) {
-            const int nt_ = w + u * NWARPS, mat = nt_ / NTILE, j = nt_ % NTILE, e = 8 * j + g;
+            const int nt_ = w + u * KPC, mat = nt_ / NTILE, j = nt_ % NTILE, e = 8 * j + g;
             // B[c][g] of k-step 0: G(n1 = c - 3)_e (row 3 - c, transposed and conjugated for n1 < 0);
             // of k-step 1: G(n1 = c + 1)_e (c + 4 = 7 is the zero row).
             b0[u] = dzero;
@@ -380,7 +224,7 @@ __global__ void __launch_bounds__(256 * WPK, 1)
             }
 #pragma unroll
           for (int u = 0; u < NTW; ++u) {
-            const int nt_ = w + u * NWARPS, mat = nt_ / NTILE, j = nt_ % NTILE;
+            const int nt_ = w + u * KPC, mat = nt_ / NTILE, j = nt_ % NTILE;
             const int e0 = 8 * j + 2 * c4;  // results (k-point g, e0) and (g, e0 + 1)
             if (nt_ < NMAT * NTILE) {
               double2* dst = HK + ((size_t)g * NMAT + mat) * NW2;
@@ -394,9 +238,7 @@ __global__ void __launch_bounds__(256 * WPK, 1)
         if (ti + 1 < step1) fetch(ti + 1);
 
         // (2) RK4 stages of this warp's k-point (src/solver.cpp:157-180), fields at t, t+dt/2, t+dt/2, t+dt.
-        if constexpr (WPK == 2) {
-          stages_pair(ti);
-        } else if (w < nown) {
+        if (w < nown) {
           const double2* Hm = HK + (size_t)w * NMAT * NW2;
           double2 S[8], X[8], H[8];
 #pragma unroll
@@ -487,7 +329,7 @@ __global__ void __launch_bounds__(256 * WPK, 1)
         if (ti + 1 < step1) cp_async_wait_all();
         __syncthreads();
 
-        // (3) Current partials of step ti (FP64): thread = k-point m, elements e = w 4 + sub + 4 NWARPS p.
+        // (3) Current partials of step ti (FP64): thread = k-point m, elements e = w 4 + sub + 32 p.
         {
           const int m = lane % KPC, sub = lane / KPC;
           const double2* P1d = d.Pd + (size_t)ti * 2 * npw + t.np;
@@ -498,7 +340,7 @@ __global__ void __launch_bounds__(256 * WPK, 1)
           const double2* GW = GWS + buf * wbuf;
           if (m < nown) {
 #pragma unroll 1
-            for (int e = w * 4 + sub; e < NW2; e += 4 * NWARPS) {
+            for (int e = w * 4 + sub; e < NW2; e += 32) {
               const double2 r = RHO[m * NW2 + e];
 #pragma unroll
               for (int a = 0; a < NJ; ++a) {
@@ -511,7 +353,7 @@ __global__ void __launch_bounds__(256 * WPK, 1)
             }
           }
           const int slot = (ti / kJRing) & 1, s = ti % kJRing;
-          warp_store_current(re, im, NJ, lane, SJ + (((size_t)slot * kJRing + s) * NWARPS + w) * 2 * NJ);
+          warp_store_current(re, im, NJ, lane, SJ + (((size_t)slot * kJRing + s) * KPC + w) * 2 * NJ);
         }
       }
       __syncthreads();

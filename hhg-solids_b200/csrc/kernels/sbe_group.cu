@@ -1040,17 +1040,17 @@ int launch_frag_t(const SolveTables& t, const GroupTables& gt, const LaunchShape
 }
 
 // FP64 tensor-core fragment kernel (plain form): precomputed inner sums, compiled 7x7 box, 8 k-points per CTA.
-template <int NW, int NAX, int NJ, int WPK>
+template <int NW, int NAX, int NJ>
 bool plan_dfrag_t(const SolveTables& t, int sm_count, LaunchShape* out, char* why, int why_len) {
-  using FG = dfrag::Geom<NW, NAX, NJ, WPK>;
-  auto kern = dfrag::propagate_dfrag_kernel<NW, NAX, NJ, WPK>;
+  using FG = dfrag::Geom<NW, NAX, NJ>;
+  auto kern = dfrag::propagate_dfrag_kernel<NW, NAX, NJ>;
   if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)FG::BYTES) != cudaSuccess) {
     cudaGetLastError();
     snprintf(why, why_len, "FP64 fragment kernel: %zu bytes of shared memory not available", FG::BYTES);
     return false;
   }
   int occ = 0;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, FG::NWARPS * 32, FG::BYTES);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, FG::KPC * 32, FG::BYTES);
   if (occ < 1) occ = 1;
   const long slots = (long)occ * sm_count;
   const int rows = t.row1 - t.row0;
@@ -1059,8 +1059,8 @@ bool plan_dfrag_t(const SolveTables& t, int sm_count, LaunchShape* out, char* wh
   out->kmode = 0;
   out->ept = 8;
   out->k_per_cta = FG::KPC;
-  out->group = 32 * WPK;
-  out->threads = FG::NWARPS * 32;
+  out->group = 32;
+  out->threads = FG::KPC * 32;
   out->ntiles = (int)ntiles;
   out->ctas = (int)(ntiles < slots ? ntiles : slots);
   out->vctas = out->ctas;
@@ -1071,10 +1071,10 @@ bool plan_dfrag_t(const SolveTables& t, int sm_count, LaunchShape* out, char* wh
   return true;
 }
 
-template <int NW, int NAX, int NJ, int WPK>
+template <int NW, int NAX, int NJ>
 int launch_dfrag_t(const SolveTables& t, const GroupTables& gt, const LaunchShape& s, double2* rho, double2* Jpart,
                    cudaStream_t stream) {
-  using FG = dfrag::Geom<NW, NAX, NJ, WPK>;
+  using FG = dfrag::Geom<NW, NAX, NJ>;
   if (!gt.pre || s.pre_chunk <= 0)
     throw std::runtime_error("FP64 fragment kernel launch: needs its precomputed-sum scratch (GroupTables::pre)");
   GroupData<double> d = {gt.Xbox64, gt.P64, gt.T1_64, gt.T2_64, gt.Xwin64, gt.P64, gt.T1_64, gt.T2_64, nullptr, nullptr};
@@ -1083,7 +1083,7 @@ int launch_dfrag_t(const SolveTables& t, const GroupTables& gt, const LaunchShap
   double2* GWpre = Gpre + (size_t)s.pre_chunk * t.N2 * gbuf;
   d.Gpre = Gpre;
   d.GWpre = GWpre;
-  auto kern = dfrag::propagate_dfrag_kernel<NW, NAX, NJ, WPK>;
+  auto kern = dfrag::propagate_dfrag_kernel<NW, NAX, NJ>;
   cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s.smem);
   int launches = 0;
   for (int c0 = t.step0; c0 < t.step1; c0 += s.pre_chunk) {
@@ -1099,32 +1099,25 @@ int launch_dfrag_t(const SolveTables& t, const GroupTables& gt, const LaunchShap
 }
 
 struct DfragVariant {
-  int nw, nax, nj, wpk;
+  int nw, nax, nj;
   bool (*plan)(const SolveTables&, int, LaunchShape*, char*, int);
   int (*launch)(const SolveTables&, const GroupTables&, const LaunchShape&, double2*, double2*, cudaStream_t);
 };
-#define HHG_DFRAG_VARIANT(NW, NAX, NJ, WPK) \
-  {NW, NAX, NJ, WPK, plan_dfrag_t<NW, NAX, NJ, WPK>, launch_dfrag_t<NW, NAX, NJ, WPK>}
+#define HHG_DFRAG_VARIANT(NW, NAX, NJ) {NW, NAX, NJ, plan_dfrag_t<NW, NAX, NJ>, launch_dfrag_t<NW, NAX, NJ>}
 const DfragVariant kDfragVariants[] = {
-    HHG_DFRAG_VARIANT(11, 1, 2, 2), HHG_DFRAG_VARIANT(11, 2, 2, 2), HHG_DFRAG_VARIANT(12, 1, 2, 2),
-    HHG_DFRAG_VARIANT(12, 2, 2, 2), HHG_DFRAG_VARIANT(11, 1, 2, 1), HHG_DFRAG_VARIANT(11, 2, 2, 1),
-    HHG_DFRAG_VARIANT(12, 1, 2, 1), HHG_DFRAG_VARIANT(12, 2, 2, 1),
+    HHG_DFRAG_VARIANT(11, 1, 2), HHG_DFRAG_VARIANT(11, 2, 2), HHG_DFRAG_VARIANT(12, 1, 2), HHG_DFRAG_VARIANT(12, 2, 2),
 };
 #undef HHG_DFRAG_VARIANT
 
 // The FP64 fragment variant for a plain-form solve (Hermitian halved 7x7 box, real-space solver), or
-// null.  wpk: warps per k-point (the pair form first; it needs more shared memory, so 12 orbitals
-// with two field axes fall back to one warp).  Tuning overrides: HHG_DFRAG=0 turns it off,
-// HHG_DFRAG_WPK=1 skips the pair form.
-const DfragVariant* find_dfrag(const SolveTables& t, int wpk) {
+// null.  HHG_DFRAG=0 turns it off (measurements).
+const DfragVariant* find_dfrag(const SolveTables& t) {
   if (const char* env = std::getenv("HHG_DFRAG"))
     if (env[0] == '0') return nullptr;
   const GroupGeom gg = group_geom(t);
   if (t.kmode || !t.hermitian || !gg.half || t.b1n != 7 || t.b2n != 7) return nullptr;
-  if (const char* env = std::getenv("HHG_DFRAG_WPK"))
-    if (std::atoi(env) == 1 && wpk == 2) return nullptr;
   for (const DfragVariant& v : kDfragVariants)
-    if (v.nw == t.nw && v.nax == t.nax && v.nj == t.nj && v.wpk == wpk) return &v;
+    if (v.nw == t.nw && v.nax == t.nax && v.nj == t.nj) return &v;
   return nullptr;
 }
 
@@ -1249,11 +1242,10 @@ const GroupVariant* find_variant(const SolveTables& t, int precision) {
 bool plan_group(const SolveTables& t, int precision, int sm_count, LaunchShape* out, char* why, int why_len,
                 int tile_hint) {
   if (precision == 0)
-    for (int wpk : {2, 1})
-      if (const DfragVariant* f = find_dfrag(t, wpk)) {
-        out->variant = (int)(f - kDfragVariants);
-        if (f->plan(t, sm_count, out, why, why_len)) return true;
-      }
+    if (const DfragVariant* f = find_dfrag(t)) {
+      out->variant = (int)(f - kDfragVariants);
+      if (f->plan(t, sm_count, out, why, why_len)) return true;
+    }
   if (precision == 1)
     if (const FragVariant* f = find_frag(t, tile_hint)) {
       out->variant = (int)(f - kFragVariants);
