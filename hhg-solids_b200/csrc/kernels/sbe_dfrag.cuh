@@ -60,7 +60,7 @@ __device__ __forceinline__ int frame_orbital(int p, int nw) {
   return o < nw ? o : -1;
 }
 
-template <int NW, int NAX, int NJ>
+template <int NW, int NAX, int NJ, bool KM>
 struct Geom {
   static constexpr int KPC = 8;
   static constexpr int NW2 = NW * NW;
@@ -68,21 +68,31 @@ struct Geom {
   static constexpr int NBROWS = NMAT * 4;      // halved 7 x 7 box: inner-sum rows n1 = 0..3 per matrix
   static constexpr int NWROWS = NJ * 4;        // window rows
   static constexpr int NTILE = (NW2 + 7) / 8;  // n-tiles of one matrix in the outer sums
-  static constexpr size_t RHO = 0;                                     // [KPC][NW2] double2
-  static constexpr size_t HK = RHO + (size_t)KPC * NW2 * 16;           // [KPC][NMAT][NW2] double2
-  static constexpr size_t GS = HK + (size_t)KPC * NMAT * NW2 * 16;     // [2][NBROWS][NW2] double2
-  static constexpr size_t GWS = GS + 2 * (size_t)NBROWS * NW2 * 16;    // [2][NWROWS][NW2] double2
-  static constexpr size_t TW1 = GWS + 2 * (size_t)NWROWS * NW2 * 16;   // [KPC][8] double2
-  static constexpr size_t WTW1 = TW1 + (size_t)KPC * 8 * 16;           // [KPC][4] double2
-  static constexpr size_t SJ = WTW1 + (size_t)KPC * 4 * 16;            // [2][kJRing][KPC][2 NJ] double
+  // Outer-sum buffers: one point per step (real-space solver), or the k-space solver's points t (carried
+  // from the previous step, two buffers by step parity), t + dt/2 and t + dt.
+  static constexpr int NHK = KM ? 3 : 1;
+  // Inner-sum buffers: real-space solver, this step's point and the next one's (prefetched); k-space
+  // solver, the step's two new points (refilled for the next step once the outer sums have read them).
+  // Window rows: per point and double-buffered (real-space solver), constant (k-space solver).
+  static constexpr int NWB = KM ? 1 : 2;
+  static constexpr size_t RHO = 0;                                       // [KPC][NW2] double2
+  static constexpr size_t HK = RHO + (size_t)KPC * NW2 * 16;             // [NHK][KPC][NMAT][NW2] double2
+  static constexpr size_t GS = HK + (size_t)NHK * KPC * NMAT * NW2 * 16;  // [2][NBROWS][NW2] double2
+  static constexpr size_t GWS = GS + 2 * (size_t)NBROWS * NW2 * 16;      // [NWB][NWROWS][NW2] double2
+  static constexpr size_t TW1 = GWS + (size_t)NWB * NWROWS * NW2 * 16;   // [KPC][8] double2
+  static constexpr size_t WTW1 = TW1 + (size_t)KPC * 8 * 16;             // [KPC][4] double2
+  static constexpr size_t SJ = WTW1 + (size_t)KPC * 4 * 16;              // [2][kJRing][KPC][2 NJ] double
   static constexpr size_t BYTES = SJ + 2 * (size_t)kJRing * KPC * 2 * NJ * 8;
   static_assert(NW > 8 && NW <= 12, "frame: 9..12 orbitals (positions 0..7, 8, 10, 12, 14)");
 };
 
-template <int NW, int NAX, int NJ>
+// KM: the reference's k-space solver (src/solver_kspace.cpp:167-270): the stages see H at points
+// 2 ti (t), 2 ti + 1 (t + dt/2) and 2 ti + 2 (t + dt) of the interpolation tables, and the window of
+// the current has no phase (its sums are one block per column).
+template <int NW, int NAX, int NJ, bool KM>
 __global__ void __launch_bounds__(256, 1)
     propagate_dfrag_kernel(SolveTables t, GroupData<double> d, int vctas, double2* rho, double2* Jpart) {
-  using FG = Geom<NW, NAX, NJ>;
+  using FG = Geom<NW, NAX, NJ, KM>;
   constexpr int KPC = FG::KPC, NW2 = FG::NW2, NMAT = FG::NMAT, NTILE = FG::NTILE;
   extern __shared__ __align__(16) unsigned char smraw[];
   double2* RHO = reinterpret_cast<double2*>(smraw + FG::RHO);
@@ -98,7 +108,7 @@ __global__ void __launch_bounds__(256, 1)
   const int rows = t.row1 - t.row0, bpc = (rows + KPC - 1) / KPC, ntiles = t.N2 * bpc;
   const int step0 = t.step0, step1 = t.step1, npw = 2 * t.np + 1;
   const double dt = t.dt, prefac = 0.1666666666666 * dt;
-  constexpr size_t gbuf = (size_t)FG::NBROWS * NW2, wbuf = (size_t)FG::NWROWS * NW2;
+  constexpr size_t gbuf = (size_t)FG::NBROWS * NW2, wbuf = (size_t)FG::NWROWS * NW2, hbuf = (size_t)KPC * NMAT * NW2;
   const double2 dzero = make_double2(0.0, 0.0);
 
   // This lane's slots: element index (or -1 on the frame's padding).
@@ -108,25 +118,28 @@ __global__ void __launch_bounds__(256, 1)
     const int orow = frame_orbital(8 * (s >> 2) + g, NW), ocol = frame_orbital(8 * ((s >> 1) & 1) + 2 * c4 + (s & 1), NW);
     el[s] = (orow >= 0 && ocol >= 0) ? orow * NW + ocol : -1;
   }
+  // Outer-sum buffer of evaluation point p (k-space solver: even points by step parity, odd ones in one).
+  auto hk_of = [&](int p) { return KM ? HK + (size_t)((p & 1) ? 2 : (p >> 1) & 1) * hbuf : HK; };
 
   for (int v = blockIdx.x; v < vctas; v += gridDim.x)
     for (int tile = v; tile < ntiles; tile += vctas) {
       const int m2 = tile / bpc, m10 = t.row0 + (tile % bpc) * KPC;
       const int nown = min(KPC, t.row1 - m10);
 
-      auto fetch = [&](int s) {
-        const size_t blk = (size_t)(s - step0) * t.N2 + m2;
+      // Inner sums of point p into GS[slot] (and, real-space solver, its window rows into GWS[slot]).
+      auto fetch_point = [&](int p, int slot) {
+        const size_t blk = (size_t)(p - (KM ? 2 * step0 : step0)) * t.N2 + m2;
         const double2* src = d.Gpre + blk * gbuf;
-        double2* dst = GS + (s & 1) * gbuf;
+        double2* dst = GS + (size_t)slot * gbuf;
+        const int nw_rows = KM ? 0 : (int)wbuf;
         const double2* wsrc = d.GWpre + blk * wbuf;
-        double2* wdst = GWS + (s & 1) * wbuf;
-        for (int idx = tid; idx < (int)(gbuf + wbuf); idx += NTHR) {
+        double2* wdst = GWS + (size_t)slot * wbuf;
+        for (int idx = tid; idx < (int)gbuf + nw_rows; idx += NTHR) {
           if (idx < (int)gbuf)
             cp_async16(dst + idx, src + idx);
           else
             cp_async16(wdst + (idx - gbuf), wsrc + (idx - gbuf));
         }
-        cp_async_commit();
       };
       auto flush = [&](int ti_end) {
         const int slot = (ti_end / kJRing) & 1, s = ti_end % kJRing;
@@ -145,6 +158,64 @@ __global__ void __launch_bounds__(256, 1)
           *dst = make_double2(old.x + re, old.y + im);
         }
       };
+      // Outer sums of point p from GS[slot]: HK(p)[m][mat][e] = sum_q p1(m, q) G(mat, n1 = q - 3)_e.
+      auto outer_sums = [&](int p, int slot) {
+        const double2* P1 = d.P + (size_t)p * 2 * npw + t.np;
+        double2 pa[2];  // A[g][c] of k-steps 0 and 1: p1(k-point g, box row c and c + 4)
+#pragma unroll
+        for (int ks = 0; ks < 2; ++ks) {
+          const int q = c4 + 4 * ks;
+          pa[ks] = q < 7 ? mul(TW1[g * 8 + q], P1[t.b1lo + q]) : dzero;
+        }
+        const double2* G = GS + (size_t)slot * gbuf;
+        double2* HKp = hk_of(p);
+        // The warp's n-tiles nt = w, w + KPC, ... together, so that their accumulations interleave.
+        constexpr int NTW = (NMAT * NTILE + KPC - 1) / KPC;
+        double2 b0[NTW], b1[NTW];
+#pragma unroll
+        for (int u = 0; u < NTW; ++u) {
+          const int nt_ = w + u * KPC, mat = nt_ / NTILE, j = nt_ % NTILE, e = 8 * j + g;
+          // B[c][g] of k-step 0: G(n1 = c - 3)_e (row 3 - c, transposed and conjugated for n1 < 0);
+          // of k-step 1: G(n1 = c + 1)_e (c + 4 = 7 is the zero row).
+          b0[u] = dzero;
+          b1[u] = dzero;
+          if (nt_ < NMAT * NTILE && e < NW2) {
+            const double2* Gm = G + (size_t)mat * 4 * NW2;
+            if (c4 == 3) {
+              b0[u] = Gm[e];
+            } else {
+              const double2 vv = Gm[(3 - c4) * NW2 + (e % NW) * NW + e / NW];
+              b0[u] = make_double2(vv.x, -vv.y);
+              b1[u] = Gm[(c4 + 1) * NW2 + e];
+            }
+          }
+        }
+        // Complex products with three real ones (Gauss): T1 = pr gr, T2 = pi gi, T3 = (pr + pi)(gr + gi),
+        // re = T1 - T2, im = T3 - T1 - T2.
+        double t1[NTW][2], t2[NTW][2], t3[NTW][2];
+#pragma unroll
+        for (int u = 0; u < NTW; ++u) t1[u][0] = t1[u][1] = t2[u][0] = t2[u][1] = t3[u][0] = t3[u][1] = 0.0;
+#pragma unroll
+        for (int ks = 0; ks < 2; ++ks) {
+          const double ps = pa[ks].x + pa[ks].y;
+#pragma unroll
+          for (int u = 0; u < NTW; ++u) dmma(t1[u], pa[ks].x, ks ? b1[u].x : b0[u].x);
+#pragma unroll
+          for (int u = 0; u < NTW; ++u) dmma(t2[u], pa[ks].y, ks ? b1[u].y : b0[u].y);
+#pragma unroll
+          for (int u = 0; u < NTW; ++u) dmma(t3[u], ps, ks ? b1[u].x + b1[u].y : b0[u].x + b0[u].y);
+        }
+#pragma unroll
+        for (int u = 0; u < NTW; ++u) {
+          const int nt_ = w + u * KPC, mat = nt_ / NTILE, j = nt_ % NTILE;
+          const int e0 = 8 * j + 2 * c4;  // results (k-point g, e0) and (g, e0 + 1)
+          if (nt_ < NMAT * NTILE) {
+            double2* dst = HKp + ((size_t)g * NMAT + mat) * NW2;
+            if (e0 < NW2) dst[e0] = make_double2(t1[u][0] - t2[u][0], t3[u][0] - t1[u][0] - t2[u][0]);
+            if (e0 + 1 < NW2) dst[e0 + 1] = make_double2(t1[u][1] - t2[u][1], t3[u][1] - t1[u][1] - t2[u][1]);
+          }
+        }
+      };
 
       for (int idx = tid; idx < KPC * NW2; idx += NTHR) {
         const int m = idx / NW2, e = idx % NW2;
@@ -158,7 +229,21 @@ __global__ void __launch_bounds__(256, 1)
         const int m = idx / 4, q = idx % 4, m1 = min(m10 + m, t.row1 - 1);
         WTW1[idx] = d.T1d[wrap_mod((long long)m1 * (q - 2), t.N1)];
       }
-      fetch(step0);
+      if constexpr (KM) {
+        // The chunk's first point t (then carried from step to step) and the constant window rows.
+        fetch_point(2 * step0, 0);
+        for (int idx = tid; idx < (int)wbuf; idx += NTHR) cp_async16(GWS + idx, d.GWpre + (size_t)m2 * wbuf + idx);
+        cp_async_commit();
+        cp_async_wait_all();
+        __syncthreads();
+        outer_sums(2 * step0, 0);
+        __syncthreads();
+        fetch_point(2 * step0 + 1, 0);
+        fetch_point(2 * step0 + 2, 1);
+      } else {
+        fetch_point(step0, step0 & 1);
+      }
+      cp_async_commit();
       cp_async_wait_all();
       __syncthreads();
       // This warp's state in its slots (registers for the whole tile; RHO mirrors it for the current).
@@ -168,78 +253,28 @@ __global__ void __launch_bounds__(256, 1)
 
       for (int ti = step0; ti < step1; ++ti) {
         const int buf = ti & 1;
-        // (1) Outer sums of point ti: HK[m][mat][e] = sum_q p1(m, q) G(mat, n1 = q - 3)_e.
-        {
-          const double2* P1 = d.P + (size_t)ti * 2 * npw + t.np;
-          double2 pa[2];  // A[g][c] of k-steps 0 and 1: p1(k-point g, box row c and c + 4)
-#pragma unroll
-          for (int ks = 0; ks < 2; ++ks) {
-            const int q = c4 + 4 * ks;
-            pa[ks] = q < 7 ? mul(TW1[g * 8 + q], P1[t.b1lo + q]) : dzero;
-          }
-          const double2* G = GS + buf * gbuf;
-          // The warp's n-tiles nt = w, w + KPC, ... together, so that their accumulations interleave.
-          constexpr int NTW = (NMAT * NTILE + KPC - 1) / KPC;
-          double2 b0[NTW], b1[NTW];
-#pragma unroll
-          for (int u = 0; u < NTW; ++u) {
-            const int nt_ = w + u * KPC, mat = nt_ / NTILE, j = nt_ % NTILE, e = 8 * j + g;
-            // B[c][g] of k-step 0: G(n1 = c - 3)_e (row 3 - c, transposed and conjugated for n1 < 0);
-            // of k-step 1: G(n1 = c + 1)_e (c + 4 = 7 is the zero row).
-            b0[u] = dzero;
-            b1[u] = dzero;
-            if (nt_ < NMAT * NTILE && e < NW2) {
-              const double2* Gm = G + (size_t)mat * 4 * NW2;
-              if (c4 == 3) {
-                b0[u] = Gm[e];
-              } else {
-                const double2 vv = Gm[(3 - c4) * NW2 + (e % NW) * NW + e / NW];
-                b0[u] = make_double2(vv.x, -vv.y);
-                b1[u] = Gm[(c4 + 1) * NW2 + e];
-              }
-            }
-          }
-          // Complex products with three real ones (Gauss): T1 = pr gr, T2 = pi gi, T3 = (pr + pi)(gr + gi),
-          // re = T1 - T2, im = T3 - T1 - T2.
-          double t1[NTW][2], t2[NTW][2], t3[NTW][2];
-#pragma unroll
-          for (int u = 0; u < NTW; ++u) t1[u][0] = t1[u][1] = t2[u][0] = t2[u][1] = t3[u][0] = t3[u][1] = 0.0;
-#pragma unroll
-          for (int ks = 0; ks < 2; ++ks) {
-            const double ps = pa[ks].x + pa[ks].y;
-#pragma unroll
-            for (int u = 0; u < NTW; ++u) dmma(t1[u], pa[ks].x, ks ? b1[u].x : b0[u].x);
-#pragma unroll
-            for (int u = 0; u < NTW; ++u) dmma(t2[u], pa[ks].y, ks ? b1[u].y : b0[u].y);
-#pragma unroll
-            for (int u = 0; u < NTW; ++u) dmma(t3[u], ps, ks ? b1[u].x + b1[u].y : b0[u].x + b0[u].y);
-          }
-          double cr[NTW][2], ci[NTW][2];
-#pragma unroll
-          for (int u = 0; u < NTW; ++u)
-#pragma unroll
-            for (int i = 0; i < 2; ++i) {
-              cr[u][i] = t1[u][i] - t2[u][i];
-              ci[u][i] = t3[u][i] - t1[u][i] - t2[u][i];
-            }
-#pragma unroll
-          for (int u = 0; u < NTW; ++u) {
-            const int nt_ = w + u * KPC, mat = nt_ / NTILE, j = nt_ % NTILE;
-            const int e0 = 8 * j + 2 * c4;  // results (k-point g, e0) and (g, e0 + 1)
-            if (nt_ < NMAT * NTILE) {
-              double2* dst = HK + ((size_t)g * NMAT + mat) * NW2;
-              if (e0 < NW2) dst[e0] = make_double2(cr[u][0], ci[u][0]);
-              if (e0 + 1 < NW2) dst[e0 + 1] = make_double2(cr[u][1], ci[u][1]);
-            }
-          }
+        // (1) Outer sums: the step's point (real-space solver), or its points t + dt/2 and t + dt.
+        if constexpr (KM) {
+          outer_sums(2 * ti + 1, 0);
+          outer_sums(2 * ti + 2, 1);
+        } else {
+          outer_sums(ti, buf);
         }
         __syncthreads();
         if (ti > step0 && (ti - 1) % kJRing == kJRing - 1) flush(ti - 1);
-        if (ti + 1 < step1) fetch(ti + 1);
+        // The next step's inner sums (the buffers the outer sums just read, or the other one).
+        if (ti + 1 < step1) {
+          if constexpr (KM) {
+            fetch_point(2 * ti + 3, 0);
+            fetch_point(2 * ti + 4, 1);
+          } else {
+            fetch_point(ti + 1, (ti + 1) & 1);
+          }
+          cp_async_commit();
+        }
 
         // (2) RK4 stages of this warp's k-point (src/solver.cpp:157-180), fields at t, t+dt/2, t+dt/2, t+dt.
         if (w < nown) {
-          const double2* Hm = HK + (size_t)w * NMAT * NW2;
           double2 S[8], X[8], H[8];
 #pragma unroll
           for (int s = 0; s < 8; ++s) {
@@ -250,10 +285,13 @@ __global__ void __launch_bounds__(256, 1)
 #pragma unroll 1
           for (int st = 0; st < 4; ++st) {
             const int f = st == 0 ? 0 : (st == 3 ? 2 : 1);
+            // k-space solver: the stage's evaluation point 2 ti + f
+            const double2* Hm = (KM ? hk_of(2 * ti + f) : HK) + (size_t)w * NMAT * NW2;
             double ea[NAX];
 #pragma unroll
             for (int a = 0; a < NAX; ++a) ea[a] = esb[f * 3 + t.ax_id[a]];
-            // (the second and third stages share the field at t + dt/2: the third keeps the second's H)
+            // (the second and third stages share the field and point at t + dt/2: the third keeps the
+            // second's H)
 #pragma unroll
             for (int s = 0; s < 8; ++s) {
               if (st == 2) continue;
@@ -332,12 +370,13 @@ __global__ void __launch_bounds__(256, 1)
         // (3) Current partials of step ti (FP64): thread = k-point m, elements e = w 4 + sub + 32 p.
         {
           const int m = lane % KPC, sub = lane / KPC;
+          // (the k-space solver's window carries no phase)
           const double2* P1d = d.Pd + (size_t)ti * 2 * npw + t.np;
           double2 wp[4];
 #pragma unroll
-          for (int q = 0; q < 4; ++q) wp[q] = mul(WTW1[m * 4 + q], P1d[q - 2]);
+          for (int q = 0; q < 4; ++q) wp[q] = KM ? WTW1[m * 4 + q] : mul(WTW1[m * 4 + q], P1d[q - 2]);
           double re[3] = {0.0, 0.0, 0.0}, im[3] = {0.0, 0.0, 0.0};
-          const double2* GW = GWS + buf * wbuf;
+          const double2* GW = GWS + (KM ? 0 : buf * wbuf);
           if (m < nown) {
 #pragma unroll 1
             for (int e = w * 4 + sub; e < NW2; e += 32) {

@@ -1040,10 +1040,10 @@ int launch_frag_t(const SolveTables& t, const GroupTables& gt, const LaunchShape
 }
 
 // FP64 tensor-core fragment kernel (plain form): precomputed inner sums, compiled 7x7 box, 8 k-points per CTA.
-template <int NW, int NAX, int NJ>
+template <int NW, int NAX, int NJ, bool KM>
 bool plan_dfrag_t(const SolveTables& t, int sm_count, LaunchShape* out, char* why, int why_len) {
-  using FG = dfrag::Geom<NW, NAX, NJ>;
-  auto kern = dfrag::propagate_dfrag_kernel<NW, NAX, NJ>;
+  using FG = dfrag::Geom<NW, NAX, NJ, KM>;
+  auto kern = dfrag::propagate_dfrag_kernel<NW, NAX, NJ, KM>;
   if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)FG::BYTES) != cudaSuccess) {
     cudaGetLastError();
     snprintf(why, why_len, "FP64 fragment kernel: %zu bytes of shared memory not available", FG::BYTES);
@@ -1056,7 +1056,7 @@ bool plan_dfrag_t(const SolveTables& t, int sm_count, LaunchShape* out, char* wh
   const int rows = t.row1 - t.row0;
   const long ntiles = (long)t.N2 * ((rows + FG::KPC - 1) / FG::KPC);
   out->kernel = 5;
-  out->kmode = 0;
+  out->kmode = KM ? 1 : 0;
   out->ept = 8;
   out->k_per_cta = FG::KPC;
   out->group = 32;
@@ -1067,31 +1067,34 @@ bool plan_dfrag_t(const SolveTables& t, int sm_count, LaunchShape* out, char* wh
   out->box_sm = out->win_sm = 0;
   out->smem = FG::BYTES;
   out->pre_chunk = std::min(kPreChunk, t.nt);
-  out->pre_bytes = (size_t)out->pre_chunk * t.N2 * ((size_t)(FG::NBROWS + FG::NWROWS) * FG::NW2 * sizeof(double2));
+  const size_t gbytes = (size_t)FG::NBROWS * FG::NW2 * sizeof(double2), wbytes = (size_t)FG::NWROWS * FG::NW2 * sizeof(double2);
+  out->pre_bytes = KM ? (size_t)(2 * out->pre_chunk + 1) * t.N2 * gbytes + (size_t)t.N2 * wbytes
+                      : (size_t)out->pre_chunk * t.N2 * (gbytes + wbytes);
   return true;
 }
 
-template <int NW, int NAX, int NJ>
+template <int NW, int NAX, int NJ, bool KM>
 int launch_dfrag_t(const SolveTables& t, const GroupTables& gt, const LaunchShape& s, double2* rho, double2* Jpart,
                    cudaStream_t stream) {
-  using FG = dfrag::Geom<NW, NAX, NJ>;
+  using FG = dfrag::Geom<NW, NAX, NJ, KM>;
   if (!gt.pre || s.pre_chunk <= 0)
     throw std::runtime_error("FP64 fragment kernel launch: needs its precomputed-sum scratch (GroupTables::pre)");
   GroupData<double> d = {gt.Xbox64, gt.P64, gt.T1_64, gt.T2_64, gt.Xwin64, gt.P64, gt.T1_64, gt.T2_64, nullptr, nullptr};
   const size_t gbuf = (size_t)FG::NBROWS * FG::NW2;
   double2* Gpre = static_cast<double2*>(gt.pre);
-  double2* GWpre = Gpre + (size_t)s.pre_chunk * t.N2 * gbuf;
+  const size_t npts_max = KM ? 2 * (size_t)s.pre_chunk + 1 : (size_t)s.pre_chunk;
+  double2* GWpre = Gpre + npts_max * t.N2 * gbuf;
   d.Gpre = Gpre;
   d.GWpre = GWpre;
-  auto kern = dfrag::propagate_dfrag_kernel<NW, NAX, NJ>;
+  auto kern = dfrag::propagate_dfrag_kernel<NW, NAX, NJ, KM>;
   cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s.smem);
   int launches = 0;
   for (int c0 = t.step0; c0 < t.step1; c0 += s.pre_chunk) {
     SolveTables tc = t;
     tc.step0 = c0;
     tc.step1 = std::min(c0 + s.pre_chunk, t.step1);
-    group_sums_kernel<double><<<(tc.step1 - c0) * t.N2, 256, 0, stream>>>(tc, d, 3, 4, FG::NBROWS, FG::NWROWS, Gpre,
-                                                                           GWpre);
+    const int npts = KM ? 2 * (tc.step1 - c0) + 1 : tc.step1 - c0;
+    group_sums_kernel<double><<<npts * t.N2, 256, 0, stream>>>(tc, d, 3, 4, FG::NBROWS, FG::NWROWS, Gpre, GWpre);
     kern<<<s.ctas, s.threads, s.smem, stream>>>(tc, d, s.vctas, rho, Jpart);
     launches += 2;
   }
@@ -1100,24 +1103,30 @@ int launch_dfrag_t(const SolveTables& t, const GroupTables& gt, const LaunchShap
 
 struct DfragVariant {
   int nw, nax, nj;
+  bool km;
   bool (*plan)(const SolveTables&, int, LaunchShape*, char*, int);
   int (*launch)(const SolveTables&, const GroupTables&, const LaunchShape&, double2*, double2*, cudaStream_t);
 };
-#define HHG_DFRAG_VARIANT(NW, NAX, NJ) {NW, NAX, NJ, plan_dfrag_t<NW, NAX, NJ>, launch_dfrag_t<NW, NAX, NJ>}
+#define HHG_DFRAG_VARIANT(NW, NAX, NJ, KM) \
+  {NW, NAX, NJ, KM, plan_dfrag_t<NW, NAX, NJ, KM>, launch_dfrag_t<NW, NAX, NJ, KM>}
+// (The k-space solver's 12-orbital two-axis shape needs more shared memory than a CTA has: the
+// element-group kernel runs it.)
 const DfragVariant kDfragVariants[] = {
-    HHG_DFRAG_VARIANT(11, 1, 2), HHG_DFRAG_VARIANT(11, 2, 2), HHG_DFRAG_VARIANT(12, 1, 2), HHG_DFRAG_VARIANT(12, 2, 2),
+    HHG_DFRAG_VARIANT(11, 1, 2, false), HHG_DFRAG_VARIANT(11, 2, 2, false), HHG_DFRAG_VARIANT(12, 1, 2, false),
+    HHG_DFRAG_VARIANT(12, 2, 2, false), HHG_DFRAG_VARIANT(11, 1, 2, true),  HHG_DFRAG_VARIANT(11, 2, 2, true),
+    HHG_DFRAG_VARIANT(12, 1, 2, true),
 };
 #undef HHG_DFRAG_VARIANT
 
-// The FP64 fragment variant for a plain-form solve (Hermitian halved 7x7 box, real-space solver), or
+// The FP64 fragment variant for a plain-form solve (Hermitian halved 7x7 box; either solver), or
 // null.  HHG_DFRAG=0 turns it off (measurements).
 const DfragVariant* find_dfrag(const SolveTables& t) {
   if (const char* env = std::getenv("HHG_DFRAG"))
     if (env[0] == '0') return nullptr;
   const GroupGeom gg = group_geom(t);
-  if (t.kmode || !t.hermitian || !gg.half || t.b1n != 7 || t.b2n != 7) return nullptr;
+  if (!t.hermitian || !gg.half || t.b1n != 7 || t.b2n != 7) return nullptr;
   for (const DfragVariant& v : kDfragVariants)
-    if (v.nw == t.nw && v.nax == t.nax && v.nj == t.nj) return &v;
+    if (v.nw == t.nw && v.nax == t.nax && v.nj == t.nj && v.km == (t.kmode != 0)) return &v;
   return nullptr;
 }
 

@@ -37,7 +37,7 @@ def _solo(pyswe, specs=SPECS):
     return out
 
 
-@pytest.mark.parametrize("chunk", [20, 256])
+@pytest.mark.parametrize("chunk", [20, 33, 256])  # 33: chunks that start on odd steps
 def test_each_result_is_the_same_alone_and_in_the_mix(chunk):
     from pySWE import pyswe
 

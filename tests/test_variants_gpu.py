@@ -129,7 +129,7 @@ def test_fragment_kernel_tile_shapes_and_ragged_columns(kpc):
     assert rel_l2(out[0], out[1]) < 1e-6, rel_l2(out[0], out[1])
 
 
-@pytest.mark.parametrize("name", ["tmd11_10", "c2_prefix", "tmd11_12_full", "tmd12_12_full", "tmd12_6"])
+@pytest.mark.parametrize("name", ["tmd11_10", "c2_prefix", "tmd11_12_full", "tmd12_12_full", "tmd12_6", "ks_tmd11_10"])
 def test_fp64_fragment_kernel_against_element_groups(name):
     """The FP64 tensor-core fragment kernel (mma.m8n8k4.f64 for the outer Wannier sums and the
     commutator) is the plain form's kernel for 11 and 12 orbitals on a Hermitian 7x7 box: within the
@@ -140,7 +140,7 @@ def test_fp64_fragment_kernel_against_element_groups(name):
     J_d, n_d, shape = run(param, "fp64", [])
     J_g, _, shape_g = run(param, "fp64", ["HHG_DFRAG=0"])
     assert shape_g[3] != "propagate_dfrag_kernel"
-    if name in ("tmd11_10", "c2_prefix", "tmd11_12_full"):
+    if name in ("tmd11_10", "c2_prefix", "tmd11_12_full", "ks_tmd11_10"):
         assert shape[3] == "propagate_dfrag_kernel", shape
         nt = J_d.shape[1]
         assert n_d == 2 * ((nt + 63) // 64) + 1
@@ -188,3 +188,20 @@ def test_fp64_fragment_kernel_ragged_columns_and_slabs():
             if saved is not None:
                 os.environ["HHG_DFRAG"] = saved
     assert rel_l2(out[0], out[1]) < 1e-11, rel_l2(out[0], out[1])
+
+
+def test_fp64_fragment_kernel_kspace_solver():
+    """The k-space solver's form of the FP64 fragment kernel (evaluation points t, t + dt/2, t + dt of
+    the interpolation tables, the point t carried between steps, a constant window) against the
+    element-group kernel on square grids, one and two field axes, a whole 64-step chunk and a ragged
+    last chunk."""
+    import tbgen
+
+    for n, pol, tmax in ((10, [0.0, 1.0, 0.0], 3.0), (14, [0.6, 0.8, 0.0], 2.0)):
+        p = {"path_tb": tbgen.model_path("tmd11_s7"), "nr1": n, "nr2": n, "nr3": 1, "tmax": tmax, "dt": 0.02197,
+             "intensity": 2e12, "lambda": 3000.0, "tmax_field": 80.0, "pol_vec": np.array(pol),
+             "phi_vec": np.zeros(3), "solver": "kspace"}
+        Jd, _, shape = run(p, "fp64", [])
+        Jg, _, _ = run(p, "fp64", ["HHG_DFRAG=0"])
+        assert shape[3] == "propagate_dfrag_kernel", shape
+        assert rel_l2(Jd, Jg) < 1e-11, (n, rel_l2(Jd, Jg))
