@@ -68,7 +68,8 @@ struct LaunchShape {
   int ntiles;      // work tiles
   int box_sm, win_sm;  // element groups: cell tables staged in shared memory
   int ept;             // element groups: matrix elements per thread
-  int variant;         // element groups: compiled shape (-1: runtime-shaped instance)
+  int variant;         // element groups: compiled shape (-1: runtime-shaped instance); column tiles: 1 when
+                       // the box rows are Hermitian-halved
   int kmode;           // instance for the k-space solver (SolveTables::kmode)
   size_t smem;     // dynamic shared memory bytes
   int pre_chunk;     // element groups: > 0 when the inner Wannier sums of every column are precomputed

@@ -10,8 +10,9 @@
 // factors) and likewise for the current window.  A CTA owns R consecutive rows m1 of one column m2,
 // one thread per k-point with its state in registers.  Every kRing steps the CTA computes the
 // column's G for all points of the chunk into shared memory (one pair of barriers per chunk); per
-// step each thread then sums b1n box rows and 4 window rows with its own row twiddles, instead of
-// every cell of the support and window.
+// step each thread then sums the box rows (n1 >= 0 only when the placement is Hermitian and the box
+// symmetric) and 4 window rows with its own row twiddles, instead of every cell of the support and
+// window.
 #include <cstdio>
 #include <algorithm>
 #include <cstdlib>
@@ -37,24 +38,11 @@ __device__ __forceinline__ double kc_warp_sum(double v) {
   for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
   return v;
 }
-// Sums 32 values over the 32 lanes of a warp with 31 shuffles: at each level every lane keeps half
-// of its values and sends the other half to its partner.  Lane l returns the sum of value l.
-__device__ __forceinline__ double kc_transpose_sum32(double (&v)[32], int lane) {
-#pragma unroll
-  for (int o = 16; o >= 1; o >>= 1) {
-    const bool hi = (lane & o) != 0;
-#pragma unroll
-    for (int i = 0; i < o; ++i) {
-      const double keep = hi ? v[i + o] : v[i];
-      const double send = hi ? v[i] : v[i + o];
-      v[i] = keep + __shfl_xor_sync(0xffffffffu, send, o);
-    }
-  }
-  return v[0];
-}
-
 // Steps per flush of the window-contracted current partials (see the kernel).
 constexpr int kRJ = 16;
+// Row stride (doubles) of a warp's staged state in the current contraction: 32 lanes + 4, so the
+// eight addresses one load instruction touches (4 state values x 2 lane halves) fall in distinct banks.
+constexpr int kYS = 36;
 
 __device__ __forceinline__ int kc_wrap(long long x, int n) {
   int r = (int)(x % n);
@@ -63,18 +51,27 @@ __device__ __forceinline__ int kc_wrap(long long x, int n) {
 
 constexpr int kKcolMaxThreads = 256;
 
+// Hermitian halving of the box rows: with H(-n) = H(n)^+ on the grid and a box symmetric about
+// zero, G(-n1) = G(n1)^+, so only n1 = 0 .. (b1n - 1)/2 are summed per column.
+__host__ __device__ inline bool kcol_half(const SolveTables& t) {
+  return t.hermitian && t.b1lo == -(t.b1n - 1) / 2 && t.b1n % 2 == 1 && t.b2lo == -(t.b2n - 1) / 2 && t.b2n % 2 == 1;
+}
+
 // Shared-memory layout (complex double units unless noted), shared by host planning and kernel.
 struct KcolLayout {
-  size_t t1, G, GW, p2, total_cx, E_d, J_d;
+  size_t t1, G, GW, p2, total_cx, E_d, J_d, Y_d;
+  int nq1, tstride;
   bool rj;  // window-contracted current (nw = 2, real-space solver)
-  __host__ __device__ KcolLayout(const SolveTables& t, int threads) {
+  __host__ __device__ KcolLayout(const SolveTables& t, int threads, bool half) {
     rj = !t.kmode && t.nw == 2;
+    nq1 = half ? (t.b1n + 1) / 2 : t.b1n;
+    tstride = threads + 2;  // twiddle rows: +2 keeps the current contraction's loads conflict-free
     const size_t nmat = 1 + t.nax, nw2 = t.nw2, pts = t.kmode ? 2 * kRing + 1 : kRing;
     size_t p = 0;
     t1 = p;
-    p += (size_t)(t.b1n + 4) * threads;          // per-thread row twiddles: box rows, window rows
+    p += (size_t)(nq1 + 4) * tstride;            // per-thread row twiddles: box rows, window rows
     G = p;
-    p += pts * t.b1n * nmat * nw2;               // column sums of the chunk's points
+    p += pts * nq1 * nmat * nw2;                 // column sums of the chunk's points
     GW = p;
     p += (t.kmode ? 1 : kRing) * 4 * (size_t)t.nj * nw2;  // window column sums (constant: k-space solver)
     p2 = p;
@@ -82,28 +79,35 @@ struct KcolLayout {
     total_cx = p;
     E_d = 0;
     J_d = kRing * 9;
+    Y_d = J_d + (rj ? (size_t)kRJ * (threads / 32) * 32 : (size_t)kRing * (threads / 32) * 2 * 3);
   }
   __host__ __device__ size_t bytes(int threads) const {
-    const size_t jd = rj ? (size_t)kRJ * (threads / 32) * 32 : (size_t)kRing * (threads / 32) * 2 * 3;
-    return total_cx * sizeof(double2) + (J_d + jd) * sizeof(double);
+    const size_t yd = rj ? (size_t)(threads / 32) * 4 * kYS : 0;
+    return total_cx * sizeof(double2) + (Y_d + yd) * sizeof(double);
   }
 };
 
-template <int NW, int NAXc, int NJc, bool KM>
+// HALF: the box sums run over n1 >= 0 with G(-n1) = G(n1)^+.  Per point, box row q = n1 and matrix
+// the column sums are stored as: q = 0, G(0) in slots (G00, G11, G01, G10); q > 0, (2 G00, 2 G11,
+// G01 + conj(G10), G01 - conj(G10)), so that with t = e^{-2 pi i m1 n1 / N1} = a + ib the pair
+// t G(n1) + conj(t) G(n1)^+ adds 2 Re(t G_ii) on the diagonal and a S + i b D to the upper element.
+template <int NW, int NAXc, int NJc, bool KM, bool HALF>
 __global__ void __launch_bounds__(kKcolMaxThreads) propagate_kcol_kernel(SolveTables t, GroupTables gt, int R,
                                                                          int vctas, double2* rho, double2* Jpart) {
   constexpr int NW2 = NW * NW;
   // Window-contracted current (nw = 2, real-space solver): J_a = sum_{w1,e} GW_a,e(w1) R(w1, e) with
   // R(w1, e) = sum_k tw1(k, w1) conj(rho_e(k)), the same sum as sum_k Tr(W_a(k) rho(k)^*) in another
-  // order.  Each thread forms its 16 values of R per step (no per-k window sum), a warp reduces its
-  // 32 doubles with one transposed reduction, and every kRJ steps the CTA contracts them with the
-  // column's window sums.
+  // order.  Each step a warp stages its 32 k-points' state (rho00, rho11, rho01) in shared memory and
+  // lane (h, w1, c) sums tw1(k, w1) times state value c over the k-points of lane half h (both parts
+  // of tw1); every kRJ steps the CTA adds the warps' sums and contracts them with the column's window
+  // sums.
   constexpr bool RJ = NW == 2 && !KM;
   extern __shared__ __align__(16) unsigned char smraw[];
   const int nax = NAXc ? NAXc : t.nax, nj = NJc ? NJc : t.nj, nmat = 1 + nax;
   const int b1n = t.b1n, b2n = t.b2n, npw = 2 * t.np + 1;
   const int nthr = blockDim.x, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarps = nthr >> 5;
-  const KcolLayout L(t, nthr);
+  const KcolLayout L(t, nthr, HALF);
+  const int nq1 = L.nq1, q1s = b1n - nq1, ts = L.tstride;
   double2* sm = reinterpret_cast<double2*>(smraw);
   double2* sT1 = sm + L.t1;
   double2* sG = sm + L.G;
@@ -111,6 +115,7 @@ __global__ void __launch_bounds__(kKcolMaxThreads) propagate_kcol_kernel(SolveTa
   double2* sp2 = sm + L.p2;
   double* sE = reinterpret_cast<double*>(sm + L.total_cx) + L.E_d;
   double* sJ = reinterpret_cast<double*>(sm + L.total_cx) + L.J_d;
+  double* sY = reinterpret_cast<double*>(sm + L.total_cx) + L.Y_d + (size_t)warp * 4 * kYS;
   const double2* X = gt.Xbox64;  // [nmat][b1n][b2n][NW2]
   const double2* V = gt.Xwin64;  // [nj][4][4][NW2]
   const double2* P = gt.P64;     // [points][2][npw]
@@ -123,39 +128,78 @@ __global__ void __launch_bounds__(kKcolMaxThreads) propagate_kcol_kernel(SolveTa
   double2 hu[NW2], ru[3][NW2], w[3][NW2];
   // Box sums of chunk point pt (Hermitian parts: diagonal real, upper triangle complex).
   auto box_sums = [&](int pt) {
-#pragma unroll
-    for (int i = 0; i < NW; ++i) {
-      hd[i] = 0.0;
-#pragma unroll
-      for (int a = 0; a < 3; ++a) rd[a][i] = 0.0;
-    }
-#pragma unroll
-    for (int e = 0; e < NW2; ++e) {
-      hu[e] = make_double2(0.0, 0.0);
-#pragma unroll
-      for (int a = 0; a < 3; ++a) ru[a][e] = make_double2(0.0, 0.0);
-    }
-#pragma unroll 4
-    for (int q1 = 0; q1 < b1n; ++q1) {
-      const double2 tw = sT1[q1 * nthr + tid];
-      const double2* g = sG + ((size_t)pt * b1n + q1) * nmat * NW2;
+    if constexpr (HALF) {
+      const double2* g0 = sG + (size_t)pt * nq1 * nmat * NW2;  // n1 = 0
 #pragma unroll
       for (int i = 0; i < NW; ++i) {
-        hd[i] = fma(tw.x, g[i * NW + i].x, fma(-tw.y, g[i * NW + i].y, hd[i]));
+        hd[i] = g0[i].x;
 #pragma unroll
-        for (int j = i + 1; j < NW; ++j) hu[i * NW + j] = kc_fma(tw, g[i * NW + j], hu[i * NW + j]);
+        for (int a = 0; a < 3; ++a) rd[a][i] = a < nax ? g0[(1 + a) * NW2 + i].x : 0.0;
+      }
+      if constexpr (NW == 2) {
+        hu[1] = g0[2];
+#pragma unroll
+        for (int a = 0; a < 3; ++a) ru[a][1] = a < nax ? g0[(1 + a) * NW2 + 2] : make_double2(0.0, 0.0);
+      }
+#pragma unroll 2
+      for (int q = 1; q < nq1; ++q) {
+        const double2 tw = sT1[q * ts + tid];
+        const double2* g = g0 + (size_t)q * nmat * NW2;
+#pragma unroll
+        for (int i = 0; i < NW; ++i) hd[i] = fma(tw.x, g[i].x, fma(-tw.y, g[i].y, hd[i]));
+        if constexpr (NW == 2) {
+          const double2 S = g[2], D = g[3];
+          hu[1].x = fma(tw.x, S.x, fma(-tw.y, D.y, hu[1].x));
+          hu[1].y = fma(tw.x, S.y, fma(tw.y, D.x, hu[1].y));
+        }
+#pragma unroll
+        for (int a = 0; a < 3; ++a)
+          if (a < nax) {
+            const double2* ga = g + (1 + a) * NW2;
+#pragma unroll
+            for (int i = 0; i < NW; ++i) rd[a][i] = fma(tw.x, ga[i].x, fma(-tw.y, ga[i].y, rd[a][i]));
+            if constexpr (NW == 2) {
+              const double2 S = ga[2], D = ga[3];
+              ru[a][1].x = fma(tw.x, S.x, fma(-tw.y, D.y, ru[a][1].x));
+              ru[a][1].y = fma(tw.x, S.y, fma(tw.y, D.x, ru[a][1].y));
+            }
+          }
+      }
+    } else {
+#pragma unroll
+      for (int i = 0; i < NW; ++i) {
+        hd[i] = 0.0;
+#pragma unroll
+        for (int a = 0; a < 3; ++a) rd[a][i] = 0.0;
       }
 #pragma unroll
-      for (int a = 0; a < 3; ++a)
-        if (a < nax) {
-          const double2* ga = g + (1 + a) * NW2;
+      for (int e = 0; e < NW2; ++e) {
+        hu[e] = make_double2(0.0, 0.0);
 #pragma unroll
-          for (int i = 0; i < NW; ++i) {
-            rd[a][i] = fma(tw.x, ga[i * NW + i].x, fma(-tw.y, ga[i * NW + i].y, rd[a][i]));
+        for (int a = 0; a < 3; ++a) ru[a][e] = make_double2(0.0, 0.0);
+      }
+#pragma unroll 4
+      for (int q1 = 0; q1 < b1n; ++q1) {
+        const double2 tw = sT1[q1 * ts + tid];
+        const double2* g = sG + ((size_t)pt * b1n + q1) * nmat * NW2;
 #pragma unroll
-            for (int j = i + 1; j < NW; ++j) ru[a][i * NW + j] = kc_fma(tw, ga[i * NW + j], ru[a][i * NW + j]);
-          }
+        for (int i = 0; i < NW; ++i) {
+          hd[i] = fma(tw.x, g[i * NW + i].x, fma(-tw.y, g[i * NW + i].y, hd[i]));
+#pragma unroll
+          for (int j = i + 1; j < NW; ++j) hu[i * NW + j] = kc_fma(tw, g[i * NW + j], hu[i * NW + j]);
         }
+#pragma unroll
+        for (int a = 0; a < 3; ++a)
+          if (a < nax) {
+            const double2* ga = g + (1 + a) * NW2;
+#pragma unroll
+            for (int i = 0; i < NW; ++i) {
+              rd[a][i] = fma(tw.x, ga[i * NW + i].x, fma(-tw.y, ga[i * NW + i].y, rd[a][i]));
+#pragma unroll
+              for (int j = i + 1; j < NW; ++j) ru[a][i * NW + j] = kc_fma(tw, ga[i * NW + j], ru[a][i * NW + j]);
+            }
+          }
+      }
     }
   };
   // Window velocity W_a(k) from the column sums of slot s.
@@ -166,7 +210,7 @@ __global__ void __launch_bounds__(kKcolMaxThreads) propagate_kcol_kernel(SolveTa
       for (int a = 0; a < 3; ++a) w[a][e] = make_double2(0.0, 0.0);
 #pragma unroll
     for (int w1 = 0; w1 < 4; ++w1) {
-      const double2 tw = sT1[(b1n + w1) * nthr + tid];
+      const double2 tw = sT1[(nq1 + w1) * ts + tid];
       const double2* g = sGW + ((size_t)s * 4 + w1) * nj * NW2;
 #pragma unroll
       for (int a = 0; a < 3; ++a)
@@ -174,6 +218,14 @@ __global__ void __launch_bounds__(kKcolMaxThreads) propagate_kcol_kernel(SolveTa
 #pragma unroll
           for (int e = 0; e < NW2; ++e) w[a][e] = kc_fma(tw, g[a * NW2 + e], w[a][e]);
     }
+  };
+  // Column sum of point s, box row q1 (table index), matrix mat, element e, times the row factor.
+  auto column_sum = [&](int s, int q1, int mat, int e, int j0) {
+    const double2* x = X + ((size_t)(mat * b1n + q1) * b2n) * NW2 + e;
+    const double2* p2 = sp2 + s * cstride;
+    double2 acc = make_double2(0.0, 0.0);
+    for (int q2 = 0; q2 < b2n; ++q2) acc = kc_fma(p2[q2], x[(size_t)q2 * NW2], acc);
+    return kc_mul(P[(size_t)(j0 + s) * 2 * npw + t.np + t.b1lo + q1], acc);
   };
 
   // Virtual CTA v owns tiles v, v + vctas, ... and its own row of current partials.
@@ -186,11 +238,8 @@ __global__ void __launch_bounds__(kKcolMaxThreads) propagate_kcol_kernel(SolveTa
     double2 r[NW2];
 #pragma unroll
     for (int e = 0; e < NW2; ++e) r[e] = kval ? rho[k * NW2 + e] : make_double2(0.0, 0.0);
-    for (int q = 0; q < b1n; ++q) sT1[q * nthr + tid] = t.T1[kc_wrap((long long)m1 * (t.b1lo + q), t.N1)];
-    for (int q = 0; q < 4; ++q) sT1[(b1n + q) * nthr + tid] = t.T1[kc_wrap((long long)m1 * (q - 2), t.N1)];
-    double2 twr[4];  // this thread's window row twiddles (RJ)
-#pragma unroll
-    for (int q = 0; q < 4; ++q) twr[q] = t.T1[kc_wrap((long long)m1 * (q - 2), t.N1)];
+    for (int q = 0; q < nq1; ++q) sT1[q * ts + tid] = t.T1[kc_wrap((long long)m1 * (t.b1lo + q1s + q), t.N1)];
+    for (int q = 0; q < 4; ++q) sT1[(nq1 + q) * ts + tid] = t.T1[kc_wrap((long long)m1 * (q - 2), t.N1)];
 
     for (int ti0 = t.step0; ti0 < t.step1; ti0 += kRing) {
       const int nsteps = min(kRing, t.step1 - ti0);
@@ -206,18 +255,28 @@ __global__ void __launch_bounds__(kKcolMaxThreads) propagate_kcol_kernel(SolveTa
       for (int idx = tid; idx < nsteps * 9; idx += nthr) sE[idx] = t.es[(size_t)ti0 * 9 + idx];
       __syncthreads();
       // (b) the column's sums G(n1) of each point, times the row factor P1(n1)
-      const int nG = npts * b1n * nmat * NW2;
+      const int nG = npts * nq1 * nmat * NW2;
       for (int idx = tid; idx < nG; idx += nthr) {
         const int e = idx % NW2;
         int rest = idx / NW2;
         const int mat = rest % nmat;
         rest /= nmat;
-        const int q1 = rest % b1n, s = rest / b1n;
-        const double2* x = X + ((size_t)(mat * b1n + q1) * b2n) * NW2 + e;
-        const double2* p2 = sp2 + s * cstride;
-        double2 acc = make_double2(0.0, 0.0);
-        for (int q2 = 0; q2 < b2n; ++q2) acc = kc_fma(p2[q2], x[(size_t)q2 * NW2], acc);
-        sG[idx] = kc_mul(P[(size_t)(j0 + s) * 2 * npw + t.np + t.b1lo + q1], acc);
+        const int q = rest % nq1, s = rest / nq1;
+        double2 val;
+        if constexpr (HALF) {
+          // slot e of the stored form (see above); element index i * NW + j
+          if (q == 0 || e < NW) {
+            const int src = NW == 2 ? (e == 0 ? 0 : e == 1 ? 3 : e == 2 ? 1 : 2) : 0;
+            val = column_sum(s, q1s + q, mat, src, j0);
+            if (q > 0) val = make_double2(2.0 * val.x, 2.0 * val.y);
+          } else {
+            const double2 g01 = column_sum(s, q1s + q, mat, 1, j0), g10 = column_sum(s, q1s + q, mat, 2, j0);
+            val = e == 2 ? make_double2(g01.x + g10.x, g01.y - g10.y) : make_double2(g01.x - g10.x, g01.y + g10.y);
+          }
+        } else {
+          val = column_sum(s, q, mat, e, j0);
+        }
+        sG[idx] = val;
       }
       const bool win_now = !KM || ti0 == t.step0;  // the k-space solver's window sums are constant
       if (win_now) {
@@ -251,79 +310,47 @@ __global__ void __launch_bounds__(kKcolMaxThreads) propagate_kcol_kernel(SolveTa
             if (KM) box_sums(2 * s + f);  // the k-space solver's points t + dt/2, t + dt
           });
         } else {
-          // Four RK4 stages (src/solver.cpp:157-163), fields at t, t+dt/2, t+dt/2, t+dt.
-          double2 K[NW2], S[NW2];
+          // One orbital: k = -i (h x - conj(h x)) = 2 h Im(x) is real, so Im(x) = Im(rho) in every stage
+          // (src/solver.cpp:157-163: fields at t, t+dt/2, t+dt/2, t+dt).
+          double sk = 0.0;
 #pragma unroll
           for (int st = 0; st < 4; ++st) {
             const int f = st == 0 ? 0 : (st == 3 ? 2 : 1);
             const double* es = sE + s * 9 + f * 3;
-            if (KM && st > 0 && st != 2) box_sums(2 * s + f);  // points t + dt/2, t + dt
-            double2 H[NW2], Xm[NW2];
+            if (KM && (st == 1 || st == 3)) box_sums(2 * s + f);  // points t + dt/2, t + dt
+            double h = hd[0];
 #pragma unroll
-            for (int i = 0; i < NW; ++i) {
-              double d = hd[i];
-#pragma unroll
-              for (int a = 0; a < 3; ++a)
-                if (a < nax) d = fma(es[t.ax_id[a]], rd[a][i], d);
-              H[i * NW + i] = make_double2(d, 0.0);
-#pragma unroll
-              for (int j = i + 1; j < NW; ++j) {
-                double2 u = hu[i * NW + j];
-#pragma unroll
-                for (int a = 0; a < 3; ++a)
-                  if (a < nax) {
-                    const double ea = es[t.ax_id[a]];
-                    u.x = fma(ea, ru[a][i * NW + j].x, u.x);
-                    u.y = fma(ea, ru[a][i * NW + j].y, u.y);
-                  }
-                H[i * NW + j] = u;
-                H[j * NW + i] = make_double2(u.x, -u.y);
-              }
-            }
-            const double cs = (st == 3 ? 1.0 : 0.5) * dt;
-#pragma unroll
-            for (int e = 0; e < NW2; ++e)
-              Xm[e] = st == 0 ? r[e] : make_double2(r[e].x + cs * K[e].x, r[e].y + cs * K[e].y);
-            double2 HX[NW2];
-#pragma unroll
-            for (int i = 0; i < NW; ++i)
-#pragma unroll
-              for (int j = 0; j < NW; ++j) {
-                double2 acc = make_double2(0.0, 0.0);
-#pragma unroll
-                for (int l = 0; l < NW; ++l) acc = kc_fma(H[i * NW + l], Xm[l * NW + j], acc);
-                HX[i * NW + j] = acc;
-              }
-#pragma unroll
-            for (int i = 0; i < NW; ++i)
-#pragma unroll
-              for (int j = 0; j < NW; ++j) {
-                // k = -i (HX - (HX)^+)
-                const double cx = HX[i * NW + j].x - HX[j * NW + i].x, cy = HX[i * NW + j].y + HX[j * NW + i].y;
-                K[i * NW + j] = make_double2(cy, -cx);
-              }
-            const double wgt = st == 3 ? 1.0 : 2.0;
-#pragma unroll
-            for (int e = 0; e < NW2; ++e)
-              S[e] = st == 0 ? K[e] : make_double2(S[e].x + wgt * K[e].x, S[e].y + wgt * K[e].y);
+            for (int a = 0; a < 3; ++a)
+              if (a < nax) h = fma(es[t.ax_id[a]], rd[a][0], h);
+            const double kx = 2.0 * (h * r[0].y);
+            sk = st == 0 ? kx : fma(st == 3 ? 1.0 : 2.0, kx, sk);
           }
-#pragma unroll
-          for (int e = 0; e < NW2; ++e) r[e] = make_double2(r[e].x + prefac * S[e].x, r[e].y + prefac * S[e].y);
+          r[0].x = fma(prefac, sk, r[0].x);
         }
 
         // Current partials.
         if constexpr (RJ) {
-          double vals[32];
+          __syncwarp();  // the previous step's readers of this warp's staging rows are done
+          sY[lane] = kval ? r[0].x : 0.0;
+          sY[kYS + lane] = kval ? r[3].x : 0.0;
+          sY[2 * kYS + lane] = kval ? r[1].x : 0.0;
+          sY[3 * kYS + lane] = kval ? r[1].y : 0.0;
+          __syncwarp();
+          const int h = lane >> 4, w1 = (lane >> 2) & 3, c = lane & 3;
+          const double2* twp = sT1 + (nq1 + w1) * ts + warp * 32 + h;
+          const double* yp = sY + c * kYS + h;
+          double bx = 0.0, by = 0.0;
 #pragma unroll
-          for (int w1 = 0; w1 < 4; ++w1)
-#pragma unroll
-            for (int e = 0; e < 4; ++e) {
-              const double2 tw = twr[w1];
-              vals[(w1 * 4 + e) * 2] = kval ? fma(tw.x, r[e].x, tw.y * r[e].y) : 0.0;
-              vals[(w1 * 4 + e) * 2 + 1] = kval ? fma(tw.y, r[e].x, -tw.x * r[e].y) : 0.0;
-            }
-          const double val = kc_transpose_sum32(vals, lane);
-          sJ[((s % kRJ) * nwarps + warp) * 32 + lane] = val;
+          for (int j = 0; j < 16; ++j) {
+            const double2 tw = twp[2 * j];
+            const double y = yp[2 * j];
+            bx = fma(tw.x, y, bx);
+            by = fma(tw.y, y, by);
+          }
+          bx += __shfl_xor_sync(0xffffffffu, bx, 16);
+          by += __shfl_xor_sync(0xffffffffu, by, 16);
+          if (h == 0)
+            reinterpret_cast<double2*>(sJ)[((s % kRJ) * nwarps + warp) * 16 + w1 * 4 + c] = make_double2(bx, by);
           if (s % kRJ == kRJ - 1 || s == nsteps - 1) {
             const int s0f = s - s % kRJ, ns = s - s0f + 1;
             __syncthreads();
@@ -337,16 +364,19 @@ __global__ void __launch_bounds__(kKcolMaxThreads) propagate_kcol_kernel(SolveTa
             __syncthreads();
             for (int idx = tid; idx < ns * nj; idx += nthr) {
               const int ss = idx / nj, a = idx % nj;
-              const double* Rv = sJ + (ss * nwarps) * 32;
+              const double* B = sJ + (ss * nwarps) * 32;  // B[(w1 * 4 + c) * 2 + part]
               double re = 0.0, im = 0.0;
 #pragma unroll
               for (int w1 = 0; w1 < 4; ++w1) {
                 const double2* g = sGW + ((size_t)((s0f + ss) * 4 + w1) * nj + a) * NW2;
+                const double* b = B + w1 * 8;
+                // R(w1, e) = sum_k tw1 conj(rho_e): e = 00, 01, 10, 11 from the state values' sums
+                const double2 Rv[4] = {make_double2(b[0], b[1]), make_double2(b[4] + b[7], b[5] - b[6]),
+                                       make_double2(b[4] - b[7], b[5] + b[6]), make_double2(b[2], b[3])};
 #pragma unroll
                 for (int e = 0; e < 4; ++e) {
-                  const double rx = Rv[(w1 * 4 + e) * 2], ry = Rv[(w1 * 4 + e) * 2 + 1];
-                  re = fma(g[e].x, rx, fma(-g[e].y, ry, re));
-                  im = fma(g[e].x, ry, fma(g[e].y, rx, im));
+                  re = fma(g[e].x, Rv[e].x, fma(-g[e].y, Rv[e].y, re));
+                  im = fma(g[e].x, Rv[e].y, fma(g[e].y, Rv[e].x, im));
                 }
               }
               double2* dst = Jpart + ((size_t)v * t.nt + ti0 + s0f + ss) * 3 + t.j_id[a];
@@ -401,15 +431,24 @@ __global__ void __launch_bounds__(kKcolMaxThreads) propagate_kcol_kernel(SolveTa
 
 using KcolKernel = void (*)(SolveTables, GroupTables, int, int, double2*, double2*);
 
-template <bool KM>
+// Halving applies unless HHG_KCOL_FULLBOX=1 (both forms are tested against the goldens).
+bool kcol_use_half(const SolveTables& t) {
+  const char* e = std::getenv("HHG_KCOL_FULLBOX");
+  return kcol_half(t) && !(e && e[0] == '1');
+}
+
+template <bool KM, bool HALF>
 KcolKernel kcol_kernel_t(const SolveTables& t) {
   if (t.nw == 2 && t.nj == 2) {
-    if (t.nax == 1) return propagate_kcol_kernel<2, 1, 2, KM>;
-    if (t.nax == 2) return propagate_kcol_kernel<2, 2, 2, KM>;
+    if (t.nax == 1) return propagate_kcol_kernel<2, 1, 2, KM, HALF>;
+    if (t.nax == 2) return propagate_kcol_kernel<2, 2, 2, KM, HALF>;
   }
-  return t.nw == 1 ? propagate_kcol_kernel<1, 0, 0, KM> : propagate_kcol_kernel<2, 0, 0, KM>;
+  return t.nw == 1 ? propagate_kcol_kernel<1, 0, 0, KM, HALF> : propagate_kcol_kernel<2, 0, 0, KM, HALF>;
 }
-KcolKernel kcol_kernel_for(const SolveTables& t) { return t.kmode ? kcol_kernel_t<true>(t) : kcol_kernel_t<false>(t); }
+KcolKernel kcol_kernel_for(const SolveTables& t, bool half) {
+  if (t.kmode) return half ? kcol_kernel_t<true, true>(t) : kcol_kernel_t<true, false>(t);
+  return half ? kcol_kernel_t<false, true>(t) : kcol_kernel_t<false, false>(t);
+}
 
 }  // namespace
 
@@ -424,10 +463,11 @@ bool plan_kcol(const SolveTables& t, int sm_count, LaunchShape* out, size_t smem
   const int R = (rows + parts - 1) / parts;
   const int threads = (R + 31) / 32 * 32;
   const long ntiles = (long)t.N2 * ((rows + R - 1) / R);
-  const KcolLayout L(t, threads);
+  const bool half = kcol_use_half(t);
+  const KcolLayout L(t, threads, half);
   const size_t smem = L.bytes(threads);
   if (smem > smem_max || threads > kKcolMaxThreads) return false;
-  KcolKernel kern = kcol_kernel_for(t);
+  KcolKernel kern = kcol_kernel_for(t, half);
   cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   int occ = 0;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, threads, smem);
@@ -443,14 +483,14 @@ bool plan_kcol(const SolveTables& t, int sm_count, LaunchShape* out, size_t smem
   out->vctas = out->ctas;
   out->box_sm = out->win_sm = 0;
   out->ept = 1;
-  out->variant = -1;
+  out->variant = half ? 1 : 0;
   out->smem = smem;
   return true;
 }
 
 void launch_kcol(const SolveTables& t, const GroupTables& gt, const LaunchShape& s, double2* rho, double2* Jpart,
                  cudaStream_t stream) {
-  KcolKernel kern = kcol_kernel_for(t);
+  KcolKernel kern = kcol_kernel_for(t, s.variant == 1);
   cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s.smem);
   kern<<<s.ctas, s.threads, s.smem, stream>>>(t, gt, s.k_per_cta, s.vctas, rho, Jpart);
 }

@@ -40,6 +40,26 @@ def test_kcol_matches_golden(force_kcol, name):
             assert rel_l2(J[a], J_ref[a]) < 1e-10, (name, a, rel_l2(J[a], J_ref[a]))
 
 
+@pytest.mark.parametrize("name", ["haldane_12_pol", "ks_haldane_12_pol"])
+def test_kcol_full_box_form_matches_golden(force_kcol, name):
+    """HHG_KCOL_FULLBOX=1 sums every box row instead of the Hermitian-halved ones."""
+    from pySWE import pyswe
+
+    _, param, t_ref, J_ref = load_golden(name)
+    os.environ["HHG_KCOL_FULLBOX"] = "1"
+    try:
+        s = pyswe.SWE(pyswe.Settings(dict(param)), solver=param.get("solver", "rspace"))
+        assert s.launch_shape()["kernel_name"] == "propagate_kcol_kernel"
+        s.run_simulation()
+        J = s.get_current()[1:]
+        s.delete()
+    finally:
+        del os.environ["HHG_KCOL_FULLBOX"]
+    for a in range(3):
+        if np.abs(J_ref[a]).max() > 0:
+            assert rel_l2(J[a], J_ref[a]) < 1e-10, (name, a, rel_l2(J[a], J_ref[a]))
+
+
 def test_kcol_tile_split_does_not_change_the_result(force_kcol):
     from pySWE import pyswe
 
