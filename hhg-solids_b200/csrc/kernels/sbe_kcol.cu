@@ -41,7 +41,8 @@ __device__ __forceinline__ double kc_warp_sum(double v) {
 // Steps per flush of the window-contracted current partials (see the kernel).
 constexpr int kRJ = 16;
 // Row stride (doubles) of a warp's staged state in the current contraction: 32 lanes + 4, so the
-// eight addresses one load instruction touches (4 state values x 2 lane halves) fall in distinct banks.
+// eight 16-byte pairs one load instruction touches (4 state values x 2 lane halves, the halves
+// interleaved by pairs) fall in distinct banks.
 constexpr int kYS = 36;
 
 __device__ __forceinline__ int kc_wrap(long long x, int n) {
@@ -98,9 +99,9 @@ __global__ void __launch_bounds__(kKcolMaxThreads) propagate_kcol_kernel(SolveTa
   // Window-contracted current (nw = 2, real-space solver): J_a = sum_{w1,e} GW_a,e(w1) R(w1, e) with
   // R(w1, e) = sum_k tw1(k, w1) conj(rho_e(k)), the same sum as sum_k Tr(W_a(k) rho(k)^*) in another
   // order.  Each step a warp stages its 32 k-points' state (rho00, rho11, rho01) in shared memory and
-  // lane (h, w1, c) sums tw1(k, w1) times state value c over the k-points of lane half h (both parts
-  // of tw1); every kRJ steps the CTA adds the warps' sums and contracts them with the column's window
-  // sums.
+  // lane (h, w1, c) sums tw1(k, w1) (held in registers for the tile) times state value c over the
+  // k-points of lane half h (both parts of tw1); every kRJ steps the CTA adds the warps' sums and
+  // contracts them with the column's window sums.
   constexpr bool RJ = NW == 2 && !KM;
   extern __shared__ __align__(16) unsigned char smraw[];
   const int nax = NAXc ? NAXc : t.nax, nj = NJc ? NJc : t.nj, nmat = 1 + nax;
@@ -240,6 +241,15 @@ __global__ void __launch_bounds__(kKcolMaxThreads) propagate_kcol_kernel(SolveTa
     for (int e = 0; e < NW2; ++e) r[e] = kval ? rho[k * NW2 + e] : make_double2(0.0, 0.0);
     for (int q = 0; q < nq1; ++q) sT1[q * ts + tid] = t.T1[kc_wrap((long long)m1 * (t.b1lo + q1s + q), t.N1)];
     for (int q = 0; q < 4; ++q) sT1[(nq1 + q) * ts + tid] = t.T1[kc_wrap((long long)m1 * (q - 2), t.N1)];
+    // This lane's twiddles in the current contraction (RJ): tw1(k, w1) of the warp's k-points
+    // k = 4j + 2h + b (j < 8, b < 2) of lane half h, for the lane's window row w1.
+    double2 twc[RJ ? 16 : 1];
+    if constexpr (RJ) {
+      const int h = lane >> 4, w1 = (lane >> 2) & 3, m1w = t.row0 + (tile % tpc) * R + warp * 32;
+#pragma unroll
+      for (int j = 0; j < 16; ++j)
+        twc[j] = t.T1[kc_wrap((long long)(m1w + 4 * (j >> 1) + 2 * h + (j & 1)) * (w1 - 2), t.N1)];
+    }
 
     for (int ti0 = t.step0; ti0 < t.step1; ti0 += kRing) {
       const int nsteps = min(kRing, t.step1 - ti0);
@@ -337,16 +347,17 @@ __global__ void __launch_bounds__(kKcolMaxThreads) propagate_kcol_kernel(SolveTa
           sY[3 * kYS + lane] = kval ? r[1].y : 0.0;
           __syncwarp();
           const int h = lane >> 4, w1 = (lane >> 2) & 3, c = lane & 3;
-          const double2* twp = sT1 + (nq1 + w1) * ts + warp * 32 + h;
-          const double* yp = sY + c * kYS + h;
-          double bx = 0.0, by = 0.0;
+          const double* yp = sY + c * kYS + 2 * h;
+          double bx0 = 0.0, by0 = 0.0, bx1 = 0.0, by1 = 0.0;
 #pragma unroll
-          for (int j = 0; j < 16; ++j) {
-            const double2 tw = twp[2 * j];
-            const double y = yp[2 * j];
-            bx = fma(tw.x, y, bx);
-            by = fma(tw.y, y, by);
+          for (int j = 0; j < 8; ++j) {
+            const double2 y = *reinterpret_cast<const double2*>(yp + 4 * j);  // k = 4j + 2h, 4j + 2h + 1
+            bx0 = fma(twc[2 * j].x, y.x, bx0);
+            by0 = fma(twc[2 * j].y, y.x, by0);
+            bx1 = fma(twc[2 * j + 1].x, y.y, bx1);
+            by1 = fma(twc[2 * j + 1].y, y.y, by1);
           }
+          double bx = bx0 + bx1, by = by0 + by1;
           bx += __shfl_xor_sync(0xffffffffu, bx, 16);
           by += __shfl_xor_sync(0xffffffffu, by, 16);
           if (h == 0)
