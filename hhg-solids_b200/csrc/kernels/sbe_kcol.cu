@@ -62,9 +62,9 @@ __host__ __device__ inline bool kcol_half(const SolveTables& t) {
 struct KcolLayout {
   size_t t1, G, GW, p2, total_cx, E_d, J_d, Y_d;
   int nq1, tstride;
-  bool rj;  // window-contracted current (nw = 2, real-space solver)
+  bool rj;  // window-contracted current (nw = 2)
   __host__ __device__ KcolLayout(const SolveTables& t, int threads, bool half) {
-    rj = !t.kmode && t.nw == 2;
+    rj = t.nw == 2;
     nq1 = half ? (t.b1n + 1) / 2 : t.b1n;
     tstride = threads + 2;  // twiddle rows: +2 keeps the current contraction's loads conflict-free
     const size_t nmat = 1 + t.nax, nw2 = t.nw2, pts = t.kmode ? 2 * kRing + 1 : kRing;
@@ -93,16 +93,16 @@ struct KcolLayout {
 // G01 + conj(G10), G01 - conj(G10)), so that with t = e^{-2 pi i m1 n1 / N1} = a + ib the pair
 // t G(n1) + conj(t) G(n1)^+ adds 2 Re(t G_ii) on the diagonal and a S + i b D to the upper element.
 template <int NW, int NAXc, int NJc, bool KM, bool HALF>
-__global__ void __launch_bounds__(kKcolMaxThreads) propagate_kcol_kernel(SolveTables t, GroupTables gt, int R,
+__global__ void __maxnreg__(168) propagate_kcol_kernel(SolveTables t, GroupTables gt, int R,
                                                                          int vctas, double2* rho, double2* Jpart) {
   constexpr int NW2 = NW * NW;
-  // Window-contracted current (nw = 2, real-space solver): J_a = sum_{w1,e} GW_a,e(w1) R(w1, e) with
+  // Window-contracted current (nw = 2): J_a = sum_{w1,e} GW_a,e(w1) R(w1, e) with
   // R(w1, e) = sum_k tw1(k, w1) conj(rho_e(k)), the same sum as sum_k Tr(W_a(k) rho(k)^*) in another
   // order.  Each step a warp stages its 32 k-points' state (rho00, rho11, rho01) in shared memory and
   // lane (h, w1, c) sums tw1(k, w1) (held in registers for the tile) times state value c over the
   // k-points of lane half h (both parts of tw1); every kRJ steps the CTA adds the warps' sums and
   // contracts them with the column's window sums.
-  constexpr bool RJ = NW == 2 && !KM;
+  constexpr bool RJ = NW == 2;  // (the k-space solver's window sums GW are the same for every step)
   extern __shared__ __align__(16) unsigned char smraw[];
   const int nax = NAXc ? NAXc : t.nax, nj = NJc ? NJc : t.nj, nmat = 1 + nax;
   const int b1n = t.b1n, b2n = t.b2n, npw = 2 * t.np + 1;
@@ -306,7 +306,7 @@ __global__ void __launch_bounds__(kKcolMaxThreads) propagate_kcol_kernel(SolveTa
         }
       }
       __syncthreads();
-      if (KM && ti0 == t.step0) window_sums(0);
+      if (KM && !RJ && ti0 == t.step0) window_sums(0);
 
       for (int s = 0; s < nsteps; ++s) {
         if (!KM) {
@@ -379,7 +379,7 @@ __global__ void __launch_bounds__(kKcolMaxThreads) propagate_kcol_kernel(SolveTa
               double re = 0.0, im = 0.0;
 #pragma unroll
               for (int w1 = 0; w1 < 4; ++w1) {
-                const double2* g = sGW + ((size_t)((s0f + ss) * 4 + w1) * nj + a) * NW2;
+                const double2* g = sGW + ((size_t)((KM ? 0 : s0f + ss) * 4 + w1) * nj + a) * NW2;
                 const double* b = B + w1 * 8;
                 // R(w1, e) = sum_k tw1 conj(rho_e): e = 00, 01, 10, 11 from the state values' sums
                 const double2 Rv[4] = {make_double2(b[0], b[1]), make_double2(b[4] + b[7], b[5] - b[6]),
