@@ -676,12 +676,36 @@ def mixed_report(J_mixed, J_fp64, param, fp64_ms, mixed_ms):
             "fp64_ms_per_solve": fp64_ms, "mixed_ms_per_solve": mixed_ms, "speedup_vs_fp64": fp64_ms / mixed_ms}
 
 
-def executed_form(nw: int, kernel: str, fpk: float, ms: float, nk: int, nt: int, peak: float):
+def kcol_executed_flops(window: int, n_op: int, n_j: int, rows_per_tile: int, kspace: bool) -> float:
+    """Flops per k-point step that the column kernel (sbe_kcol.cu) executes for nw = 2 with a Hermitian
+    placement and a symmetric box: the closed-form commutator (15 flops per stage); the box rows n1 > 0
+    only, each pair t G(n1) + conj(t) G(n1)^+ as 2 Re(t G_ii) plus a S + i b D (16 flops per row and
+    operator); the column sums G(n1 >= 0) of the tile's points (4 + 6 per row pair of window-long
+    complex sums per operator), shared by the tile's rows; the current contracted after the k-sum (32
+    products of a twiddle and a state value per k-point, the column's window sums and the contraction
+    with them per tile and step); and the RK axpys.  The k-space solver evaluates the box at two new
+    points per step and keeps its window sums."""
+    h = (window - 1) // 2
+    pts = 2 if kspace else 1
+    box = pts * n_op * h * 16.0
+    col = pts * n_op * (4 + 6 * h) * window * 8.0 / rows_per_tile
+    win = 0.0 if kspace else 4 * n_j * 4 * (4 * 8.0 + 6.0) / rows_per_tile
+    cur = 64.0 + win + n_j * 4 * 4 * 8.0 / rows_per_tile
+    return 4 * 15.0 + box + col + cur + 12.0 * 4
+
+
+def executed_form(nw: int, kernel: str, fpk: float, ms: float, nk: int, nt: int, peak: float,
+                  window: int = 0, n_op: int = 0, n_j: int = 0, rows_per_tile: int = 0, kspace: bool = False):
     """The flop count of the form the kernel actually executes, where it differs from the minimal one:
-    the closed-form commutator of two Hermitian 2x2 matrices (sbe_herm2.cuh: 15 flops per stage instead of
-    8 nw^3 = 64), or the 16 x 16 frame of the FP64 tensor-core kernel (3 k-steps x 4 blocks x 3 real
+    for nw = 2 the column kernel's form (kcol_executed_flops) or, in the thread-per-k-point kernel, the
+    closed-form commutator of two Hermitian 2x2 matrices (sbe_herm2.cuh: 15 flops per stage instead of
+    8 nw^3 = 64); or the 16 x 16 frame of the FP64 tensor-core kernel (3 k-steps x 4 blocks x 3 real
     m8n8k4 products = 18 432 flops per stage instead of 8 nw^3)."""
-    if nw == 2 and kernel in ("propagate_kcol_kernel", "propagate_kpt_kernel"):
+    if nw == 2 and kernel == "propagate_kcol_kernel" and window % 2 == 1 and rows_per_tile > 0:
+        f = kcol_executed_flops(window, n_op, n_j, rows_per_tile, kspace)
+        form = ("column kernel: closed-form Hermitian 2x2 commutator, Hermitian-halved box rows, current "
+                "contracted after the k-sum")
+    elif nw == 2 and kernel in ("propagate_kcol_kernel", "propagate_kpt_kernel"):
         f = fpk - 32.0 * nw ** 3 + 4 * 15.0
         form = "closed-form Hermitian 2x2 commutator (15 flops per stage)"
     elif kernel == "propagate_dfrag_kernel":
@@ -985,7 +1009,9 @@ def main():
                      "peak_source": "live FP64 / FP32 FMA-chain probes on this GPU (HHG_measure_peaks); "
                                     "MEASURED_PEAKS.json has no FP64 or FP32 figure",
                      "fp32_peak": fp32_peak.value, "kernel_ms": prop_mean, "traffic_source": traffic_src,
-                     "executed_form": executed_form(nw, shape.get("kernel_name"), fpk, prop_mean, nk, nt, peak),
+                     "executed_form": executed_form(nw, shape.get("kernel_name"), fpk, prop_mean, nk, nt, peak,
+                                                    w["window"], n_op, n_j, shape.get("k_per_cta", 0),
+                                                    args.solver == "kspace"),
                      "ncu_counters": load_profile_counters(args.workload, shape.get("kernel_name"))},
         "gpu_launches": launches,
         "clocks": clk,
