@@ -59,7 +59,8 @@ struct LaunchShape {
   int kernel;      // 0: thread per k-point (FP64, nw <= 2, Hermitian); 1: element groups FP64; 2: element groups mixed;
                    // 3: column tiles, thread per k-point (FP64, nw <= 2, Hermitian); 4: tensor-core fragment
                    // kernel (mixed, 11 or 12 orbitals; variant indexes its shape table); 5: FP64 tensor-core
-                   // fragment kernel (plain form, 11 or 12 orbitals)
+                   // fragment kernel (plain form, 11 or 12 orbitals); 6: tile kernel (mixed, 11 or 12 orbitals,
+                   // half a warp per k-point)
   int k_per_cta;   // k-points per CTA
   int group;       // threads per k-point
   int threads;     // threads per CTA

@@ -818,6 +818,7 @@ __device__ __forceinline__ GroupData<Real> group_data(const GroupTables& gt) {
 
 #include "sbe_frag.cuh"
 #include "sbe_dfrag.cuh"
+#include "sbe_mtile.cuh"
 
 // One solve: physical CTA b runs virtual CTAs b, b + gridDim.x, ...
 template <typename Real, int EPT, int NWc, int NAXc, int NJc, bool KM = false, int WBc = 0, bool KP = false,
@@ -1039,6 +1040,91 @@ int launch_frag_t(const SolveTables& t, const GroupTables& gt, const LaunchShape
   return launches;
 }
 
+// Mixed-form tile kernel: precomputed inner sums, compiled 7x7 box, KPC k-points per CTA (half a warp each).
+template <int NW, int NAX, int NJ, int KPC>
+bool plan_mtile_t(const SolveTables& t, int sm_count, LaunchShape* out, char* why, int why_len) {
+  using FG = mtile::Geom<NW, NAX, NJ, KPC>;
+  auto kern = mtile::propagate_mtile_kernel<NW, NAX, NJ, KPC>;
+  if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)FG::BYTES) != cudaSuccess) {
+    cudaGetLastError();
+    snprintf(why, why_len, "tile kernel: %zu bytes of shared memory not available", FG::BYTES);
+    return false;
+  }
+  int occ = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, FG::NTHR, FG::BYTES);
+  if (occ < 1) occ = 1;
+  const long slots = (long)occ * sm_count;
+  const int rows = t.row1 - t.row0;
+  const long ntiles = (long)t.N2 * ((rows + KPC - 1) / KPC);
+  out->kernel = 6;
+  out->kmode = 0;
+  out->ept = 9;
+  out->k_per_cta = KPC;
+  out->group = 16;
+  out->threads = FG::NTHR;
+  out->ntiles = (int)ntiles;
+  out->ctas = (int)(ntiles < slots ? ntiles : slots);
+  out->vctas = out->ctas;
+  out->box_sm = out->win_sm = 0;
+  out->smem = FG::BYTES;
+  out->pre_chunk = std::min(kPreChunk, t.nt);
+  out->pre_bytes = (size_t)out->pre_chunk * t.N2 *
+                   ((size_t)FG::NBROWS * FG::NW2 * sizeof(float2) + (size_t)FG::NWROWS * FG::NW2 * sizeof(double2));
+  return true;
+}
+
+template <int NW, int NAX, int NJ, int KPC>
+int launch_mtile_t(const SolveTables& t, const GroupTables& gt, const LaunchShape& s, double2* rho, double2* Jpart,
+                   cudaStream_t stream) {
+  using FG = mtile::Geom<NW, NAX, NJ, KPC>;
+  if (!gt.pre || s.pre_chunk <= 0)
+    throw std::runtime_error("tile kernel launch: needs its precomputed-sum scratch (GroupTables::pre)");
+  GroupData<float> d = {gt.Xbox32, gt.P32, gt.T1_32, gt.T2_32, gt.Xwin64, gt.P64, gt.T1_64, gt.T2_64, nullptr, nullptr};
+  const size_t gbuf = (size_t)FG::NBROWS * FG::NW2;
+  float2* Gpre = static_cast<float2*>(gt.pre);
+  double2* GWpre = reinterpret_cast<double2*>(Gpre + (size_t)s.pre_chunk * t.N2 * gbuf);
+  d.Gpre = Gpre;
+  d.GWpre = GWpre;
+  auto kern = mtile::propagate_mtile_kernel<NW, NAX, NJ, KPC>;
+  cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s.smem);
+  int launches = 0;
+  for (int c0 = t.step0; c0 < t.step1; c0 += s.pre_chunk) {
+    SolveTables tc = t;
+    tc.step0 = c0;
+    tc.step1 = std::min(c0 + s.pre_chunk, t.step1);
+    group_sums_kernel<float><<<(tc.step1 - c0) * t.N2, 256, 0, stream>>>(tc, d, 3, 4, FG::NBROWS, FG::NWROWS, Gpre,
+                                                                          GWpre);
+    kern<<<s.ctas, s.threads, s.smem, stream>>>(tc, d, s.vctas, rho, Jpart);
+    launches += 2;
+  }
+  return launches;
+}
+
+struct MtileVariant {
+  int nw, nax, nj, kpc;
+  bool (*plan)(const SolveTables&, int, LaunchShape*, char*, int);
+  int (*launch)(const SolveTables&, const GroupTables&, const LaunchShape&, double2*, double2*, cudaStream_t);
+};
+#define HHG_MTILE_VARIANT(NW, NAX, NJ, KPC) \
+  {NW, NAX, NJ, KPC, plan_mtile_t<NW, NAX, NJ, KPC>, launch_mtile_t<NW, NAX, NJ, KPC>}
+const MtileVariant kMtileVariants[] = {
+    HHG_MTILE_VARIANT(11, 1, 2, 8), HHG_MTILE_VARIANT(11, 2, 2, 8),
+    HHG_MTILE_VARIANT(12, 1, 2, 8), HHG_MTILE_VARIANT(12, 2, 2, 8),
+};
+#undef HHG_MTILE_VARIANT
+
+// The tile kernel for a mixed-form solve (Hermitian halved 7x7 box, real-space solver), or null.
+// HHG_MTILE=0 turns it off (measurements): the element-group kernel then runs the solve.
+const MtileVariant* find_mtile(const SolveTables& t) {
+  if (const char* off = std::getenv("HHG_MTILE"))
+    if (off[0] == '0') return nullptr;
+  const GroupGeom gg = group_geom(t);
+  if (t.kmode || !t.hermitian || !gg.half || t.b1n != 7 || t.b2n != 7) return nullptr;
+  for (const MtileVariant& v : kMtileVariants)
+    if (v.nw == t.nw && v.nax == t.nax && v.nj == t.nj) return &v;
+  return nullptr;
+}
+
 // FP64 tensor-core fragment kernel (plain form): precomputed inner sums, compiled 7x7 box, 8 k-points per CTA.
 template <int NW, int NAX, int NJ, bool KM>
 bool plan_dfrag_t(const SolveTables& t, int sm_count, LaunchShape* out, char* why, int why_len) {
@@ -1255,10 +1341,15 @@ bool plan_group(const SolveTables& t, int precision, int sm_count, LaunchShape* 
       out->variant = (int)(f - kDfragVariants);
       if (f->plan(t, sm_count, out, why, why_len)) return true;
     }
-  if (precision == 1)
+  if (precision == 1)  // (the opt-in fragment kernel first: HHG_FRAG=1 asks for it)
     if (const FragVariant* f = find_frag(t, tile_hint)) {
       out->variant = (int)(f - kFragVariants);
       if (f->plan(t, sm_count, out, why, why_len)) return true;
+    }
+  if (precision == 1)
+    if (const MtileVariant* m = find_mtile(t)) {
+      out->variant = (int)(m - kMtileVariants);
+      if (m->plan(t, sm_count, out, why, why_len)) return true;
     }
   if (const GroupVariant* v = find_variant(t, precision)) {
     out->variant = (int)(v - kGroupVariants);
@@ -1313,6 +1404,7 @@ int launch_group(const SolveTables& t, const GroupTables& gt, const LaunchShape&
                  cudaStream_t stream) {
   if (s.kernel == 4) return kFragVariants[s.variant].launch(t, gt, s, rho, Jpart, stream);
   if (s.kernel == 5) return kDfragVariants[s.variant].launch(t, gt, s, rho, Jpart, stream);
+  if (s.kernel == 6) return kMtileVariants[s.variant].launch(t, gt, s, rho, Jpart, stream);
   if (s.variant >= 0) return kGroupVariants[s.variant].launch(t, gt, s, rho, Jpart, stream);
   if (s.kmode) return launch_group_generic<true>(t, gt, s, rho, Jpart, stream);
   return launch_group_generic<false>(t, gt, s, rho, Jpart, stream);

@@ -1,0 +1,301 @@
+// Mixed-form propagation for 9..12 orbitals with half a warp per k-point and 3 x 3 register tiles
+// (included by sbe_group.cu, inside its anonymous namespace: it uses GroupData, the precomputed inner
+// sums of group_sums_kernel and the helpers defined there).
+//
+// Same propagation as group_vctas in its mixed form (k-space-resident RK4 of the reference's
+// src/solver.cpp:86-181, 1428-1726, and the windowed current of src/observable.cpp:16-30), for solves
+// whose cell box is the Hermitian-halved 7x7 one and whose inner Wannier sums come precomputed per
+// column and step (real-space solver).
+//
+// Layout.  A CTA holds KPC consecutive k-points (rows m1) of one k-grid column; the 16 lanes of each
+// half warp own one k-point, lane s its 3 x 3 tile (rows 3 (s / 4) .. +2, columns 3 (s % 4) .. +2) of
+// the k-point's matrices padded to 12 x 12.  Each lane keeps its tile of the state rho and of the RK4
+// sum in FP64 registers, and of the outer Wannier sums H0(k), r_a(k) in FP32 registers for the step.
+// Per stage:
+//  * H = H0 + E.r of the tile goes to shared memory, transposed (H(i, j) at [j][i]), X = rho + c k
+//    (FP32) is already there;
+//  * the lane forms its tile of P = H X in FP32 from rows l of both arrays (three H and three X
+//    values per l: 36 FMA per 6 loads, every load a broadcast to the 4 lanes of its tile row or
+//    column);
+//  * P replaces X in shared memory, and k = -i (P - P^+) takes P^+ from the transposed tile;
+//  * the RK4 sum and the next stage's X are formed in FP64 (X stored as FP32).
+// Only the k-point's half warp exchanges data, so the stages need __syncwarp only; the CTA meets twice
+// per step (before the current, whose FP64 window rows are copied in during the step, and at its end:
+// the next step's inner sums, copied in with cp.async meanwhile, and the current partials).  The window
+// velocity and the current are FP64, per lane on its own tile.
+//
+// Precision: as the element-group kernel's mixed form (complex-FP32 Wannier sums and commutator
+// products, FP64 state, RK4 accumulation, window velocity and k-sum).
+
+namespace mtile {
+
+// Waits until at most one committed group of this thread's cp.async copies is still in flight.
+__device__ __forceinline__ void cp_async_wait_one() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
+
+template <int NW, int NAX, int NJ, int KPC>
+struct Geom {
+  static constexpr int NW2 = NW * NW;
+  static constexpr int NMAT = 1 + NAX;
+  static constexpr int NBROWS = NMAT * 4;   // halved 7 x 7 box: inner-sum rows n1 = 0..3 per matrix
+  static constexpr int NWROWS = NJ * 4;     // window rows
+  static constexpr int NWARP = KPC / 2;
+  static constexpr int NTHR = KPC * 16;
+  static constexpr int MS = 12;             // row stride (float2) of a padded matrix
+  static constexpr int KS = 12 * 12 + 1;    // float2 per k-point matrix: the odd 8-byte unit puts the
+                                            // warp's two k-points two banks apart
+  static constexpr size_t HS = 0;                                     // [KPC][KS] float2: H, transposed
+  static constexpr size_t XP = HS + (size_t)KPC * KS * 8;             // [KPC][KS] float2: X, then P
+  static constexpr size_t GS = (XP + (size_t)KPC * KS * 8 + 15) / 16 * 16;  // [2][NBROWS][NW2] float2
+  static constexpr size_t GWS = GS + 2 * (size_t)NBROWS * NW2 * 8;    // [NWROWS][NW2] double2 (one step's)
+  static constexpr size_t TW1 = GWS + (size_t)NWROWS * NW2 * 16;      // [KPC][8] float2: box rows q = 0..6
+  static constexpr size_t WTW1 = TW1 + (size_t)KPC * 8 * 8;           // [KPC][4] double2: window rows
+  static constexpr size_t SJ = WTW1 + (size_t)KPC * 4 * 16;           // [2][kJRing][NWARP][2 NJ] double
+  static constexpr size_t BYTES = SJ + 2 * (size_t)kJRing * NWARP * 2 * NJ * 8;
+  static_assert(NW > 8 && NW <= 12, "3 x 3 tiles of a 12 x 12 frame: 9..12 orbitals");
+  static_assert(KPC % 2 == 0 && KPC * 16 <= 1024, "k-points per CTA");
+  static_assert((NBROWS * NW2 * 8) % 16 == 0, "16-byte copies of the inner sums");
+};
+
+// 8 k-points per CTA run three CTAs per SM (at most 168 registers per thread): 12 warps per SM, against
+// 8 for 16 k-points per CTA at 218 registers (C2: 324 against 416 ms per solve).
+template <int NW, int NAX, int NJ, int KPC>
+__global__ void __launch_bounds__(KPC * 16, KPC <= 8 ? 3 : 1)
+    propagate_mtile_kernel(SolveTables t, GroupData<float> d, int vctas, double2* rho, double2* Jpart) {
+  using FG = Geom<NW, NAX, NJ, KPC>;
+  constexpr int NW2 = FG::NW2, NMAT = FG::NMAT, NWARP = FG::NWARP, NTHR = FG::NTHR, MS = FG::MS, KS = FG::KS;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  float2* HS = reinterpret_cast<float2*>(smraw + FG::HS);
+  float2* XPb = reinterpret_cast<float2*>(smraw + FG::XP);
+  float2* GS = reinterpret_cast<float2*>(smraw + FG::GS);
+  double2* GWS = reinterpret_cast<double2*>(smraw + FG::GWS);
+  float2* TW1 = reinterpret_cast<float2*>(smraw + FG::TW1);
+  double2* WTW1 = reinterpret_cast<double2*>(smraw + FG::WTW1);
+  double* SJ = reinterpret_cast<double*>(smraw + FG::SJ);
+
+  const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+  const int kp = 2 * w + (lane >> 4), sub = lane & 15, i0 = 3 * (sub >> 2), j0 = 3 * (sub & 3);
+  const int rows = t.row1 - t.row0, bpc = (rows + KPC - 1) / KPC, ntiles = t.N2 * bpc;
+  const int step0 = t.step0, step1 = t.step1, npw = 2 * t.np + 1;
+  const double dt = t.dt, prefac = 0.1666666666666 * dt;
+  constexpr size_t gbuf = (size_t)FG::NBROWS * NW2, wbuf = (size_t)FG::NWROWS * NW2;
+  float2* Hk = HS + kp * KS;
+  float2* Xk = XPb + kp * KS;
+  const float2 fzero = make_float2(0.f, 0.f);
+  const double2 dzero = make_double2(0.0, 0.0);
+  // Tile slot u = 3 a + b is element (i0 + a, j0 + b); on the padding (row or column >= NW) it stays 0.
+  auto valid = [&](int u) { return i0 + u / 3 < NW && j0 + u % 3 < NW; };
+  auto own = [&](int u) { return (i0 + u / 3) * MS + j0 + u % 3; };   // (i, j) in X, P
+  auto tra = [&](int u) { return (j0 + u % 3) * MS + i0 + u / 3; };   // (j, i): H, P^+
+
+  for (int v = blockIdx.x; v < vctas; v += gridDim.x)
+    for (int tile = v; tile < ntiles; tile += vctas) {
+      const int m2 = tile / bpc, m10 = t.row0 + (tile % bpc) * KPC;
+      const int nown = min(KPC, t.row1 - m10);
+      const bool kval = kp < nown;
+
+      // Inner sums of point p into slot `slot`, and window rows of point p (16-byte asynchronous copies).
+      auto fetch_sums = [&](int p, int slot) {
+        const size_t blk = (size_t)(p - step0) * t.N2 + m2;
+        const char* src = reinterpret_cast<const char*>(d.Gpre + blk * gbuf);
+        char* dst = reinterpret_cast<char*>(GS + (size_t)slot * gbuf);
+        constexpr int nA = (int)(gbuf * 8 / 16);
+        for (int idx = tid; idx < nA; idx += NTHR) cp_async16(dst + (size_t)idx * 16, src + (size_t)idx * 16);
+      };
+      auto fetch_window = [&](int p) {
+        const double2* wsrc = d.GWpre + ((size_t)(p - step0) * t.N2 + m2) * wbuf;
+        for (int idx = tid; idx < (int)wbuf; idx += NTHR) cp_async16(GWS + idx, wsrc + idx);
+      };
+      // The warps' current partials of the ring half ending at step ti_end, into this virtual CTA's row.
+      auto flush = [&](int ti_end) {
+        const int slot = (ti_end / kJRing) & 1, s = ti_end % kJRing;
+        const int ti0 = max(ti_end - s, step0), nsteps = ti_end - ti0 + 1;
+        const double* half = SJ + ((size_t)slot * kJRing + (ti0 % kJRing)) * NWARP * 2 * NJ;
+        for (int idx = tid; idx < nsteps * NJ; idx += NTHR) {
+          const int ss = idx / NJ, a = idx % NJ;
+          double re = 0.0, im = 0.0;
+          for (int ww = 0; ww < NWARP; ++ww) {
+            re += half[(ss * NWARP + ww) * 2 * NJ + 2 * a];
+            im += half[(ss * NWARP + ww) * 2 * NJ + 2 * a + 1];
+          }
+          const int ja = a == 0 ? t.j_id[0] : (a == 1 ? t.j_id[1] : t.j_id[2]);
+          double2* dst = Jpart + ((size_t)v * t.nt + ti0 + ss) * 3 + ja;
+          const double2 old = *dst;
+          *dst = make_double2(old.x + re, old.y + im);
+        }
+      };
+
+      for (int idx = tid; idx < KPC * 8; idx += NTHR) {
+        const int m = idx / 8, q = idx % 8, m1 = min(m10 + m, t.row1 - 1);
+        TW1[idx] = q < 7 ? d.T1[wrap_mod((long long)m1 * (t.b1lo + q), t.N1)] : fzero;
+      }
+      for (int idx = tid; idx < KPC * 4; idx += NTHR) {
+        const int m = idx / 4, q = idx % 4, m1 = min(m10 + m, t.row1 - 1);
+        WTW1[idx] = d.T1d[wrap_mod((long long)m1 * (q - 2), t.N1)];
+      }
+      fetch_sums(step0, step0 & 1);
+      cp_async_commit();
+      // This lane's tile of the state (FP64 registers for the whole tile), and X = rho for the first stage.
+      const size_t kg = ((size_t)(m10 + (kval ? kp : 0)) * t.N2 + m2) * NW2;
+      double2 r[9];
+#pragma unroll
+      for (int u = 0; u < 9; ++u) {
+        r[u] = (kval && valid(u)) ? rho[kg + (i0 + u / 3) * NW + j0 + u % 3] : dzero;
+        Xk[own(u)] = make_float2((float)r[u].x, (float)r[u].y);
+      }
+      cp_async_wait_all();
+      __syncthreads();
+
+      for (int ti = step0; ti < step1; ++ti) {
+        const int buf = ti & 1;
+        if (ti > step0 && (ti - 1) % kJRing == kJRing - 1) flush(ti - 1);
+        // This step's window rows (read by the current at its end), then the next step's inner sums into
+        // the other slot: both buffers' last readers finished before the barrier that ended the previous
+        // step.  Two groups, so that the current can wait for the first alone.
+        fetch_window(ti);
+        cp_async_commit();
+        if (ti + 1 < step1) fetch_sums(ti + 1, (ti + 1) & 1);
+        cp_async_commit();
+        // (1) Outer sums of the tile's elements at the step's point: for matrix mat (H0, then r_a),
+        //     sum_{q=0..6} p1(k, q) G'(q)_e with G'(q) = G(n1 = q - 3) for q >= 3 and G(3 - q)^+ below.
+        float2 hm[NMAT][9];
+        {
+          const float2* P1 = d.P + (size_t)ti * 2 * npw + t.np;
+          float2 p1[7];
+#pragma unroll
+          for (int q = 0; q < 7; ++q) p1[q] = mul(TW1[kp * 8 + q], P1[t.b1lo + q]);
+          const float2* G = GS + (size_t)buf * gbuf;
+#pragma unroll
+          for (int mat = 0; mat < NMAT; ++mat)
+#pragma unroll
+            for (int u = 0; u < 9; ++u) {
+              float2 acc = fzero;
+              if (valid(u)) {
+                const int i = i0 + u / 3, j = j0 + u % 3, e = i * NW + j, eT = j * NW + i;
+                const float2* Gm = G + (size_t)mat * 4 * NW2;
+                acc = mul(p1[3], Gm[e]);
+#pragma unroll
+                for (int n = 1; n < 4; ++n) {
+                  acc = fmac(p1[3 + n], Gm[n * NW2 + e], acc);
+                  acc = fmac(p1[3 - n], conjugate(Gm[n * NW2 + eT]), acc);
+                }
+              }
+              hm[mat][u] = acc;
+            }
+        }
+        // (2) RK4 stages (src/solver.cpp:157-180), fields at t, t+dt/2, t+dt/2, t+dt.
+        const double* esb = t.es + (size_t)ti * 9;
+        double2 S[9];
+#pragma unroll 1
+        for (int st = 0; st < 4; ++st) {
+          const int f = st == 0 ? 0 : (st == 3 ? 2 : 1);
+          if (st != 2) {  // (the third stage keeps the second's H: same field)
+            float ea[NAX];
+#pragma unroll
+            for (int a = 0; a < NAX; ++a) ea[a] = (float)esb[f * 3 + t.ax_id[a]];
+#pragma unroll
+            for (int u = 0; u < 9; ++u) {
+              float2 h = hm[0][u];
+#pragma unroll
+              for (int a = 0; a < NAX; ++a) {
+                h.x = fmaf(ea[a], hm[1 + a][u].x, h.x);
+                h.y = fmaf(ea[a], hm[1 + a][u].y, h.y);
+              }
+              Hk[tra(u)] = h;
+            }
+          }
+          __syncwarp();
+          // P = H X on the tile: P(i, j) = sum_l H(i, l) X(l, j), H(i, l) from row l of the transposed H.
+          float2 P[9];
+#pragma unroll
+          for (int u = 0; u < 9; ++u) P[u] = fzero;
+#pragma unroll
+          for (int l = 0; l < NW; ++l) {
+            const float2* hr = Hk + l * MS + i0;
+            const float2* xr = Xk + l * MS + j0;
+            const float2 h0 = hr[0], h1 = hr[1], h2 = hr[2], x0 = xr[0], x1 = xr[1], x2 = xr[2];
+            P[0] = fmac(h0, x0, P[0]);
+            P[1] = fmac(h0, x1, P[1]);
+            P[2] = fmac(h0, x2, P[2]);
+            P[3] = fmac(h1, x0, P[3]);
+            P[4] = fmac(h1, x1, P[4]);
+            P[5] = fmac(h1, x2, P[5]);
+            P[6] = fmac(h2, x0, P[6]);
+            P[7] = fmac(h2, x1, P[7]);
+            P[8] = fmac(h2, x2, P[8]);
+          }
+          __syncwarp();  // every lane of the k-point has read X
+#pragma unroll
+          for (int u = 0; u < 9; ++u) Xk[own(u)] = P[u];
+          __syncwarp();
+          const double wgt = (st == 0 || st == 3) ? 1.0 : 2.0;
+          const double cn = (st == 2 ? 1.0 : 0.5) * dt;
+          float2 xn[9];
+#pragma unroll
+          for (int u = 0; u < 9; ++u) {
+            const float2 pt = Xk[tra(u)];
+            const float kx = P[u].y + pt.y, ky = -(P[u].x - pt.x);  // k = -i (P - P^+)
+            if (st == 0) {
+              S[u] = make_double2((double)kx, (double)ky);
+            } else {
+              S[u].x += wgt * (double)kx;
+              S[u].y += wgt * (double)ky;
+            }
+            xn[u] = make_float2((float)(r[u].x + cn * (double)kx), (float)(r[u].y + cn * (double)ky));
+          }
+          __syncwarp();  // every lane of the k-point has read P
+          if (st < 3) {
+#pragma unroll
+            for (int u = 0; u < 9; ++u) Xk[own(u)] = xn[u];
+          }
+        }
+        // rho += dt/6 (k1 + 2 k2 + 2 k3 + k4) (src/solver.cpp:170-180); X = rho for the next step.
+#pragma unroll
+        for (int u = 0; u < 9; ++u) {
+          r[u].x = r[u].x + prefac * S[u].x;
+          r[u].y = r[u].y + prefac * S[u].y;
+          Xk[own(u)] = make_float2((float)r[u].x, (float)r[u].y);
+        }
+
+        // (3) Current partials of step ti (FP64) on the lane's tile: W_a(k)_e = sum_q wp(k, q) GW(a, q)_e,
+        //     J_a += W_a,e conj(rho_e).
+        cp_async_wait_one();  // this step's window rows
+        __syncthreads();
+        {
+          const double2* P1d = d.Pd + (size_t)ti * 2 * npw + t.np;
+          double2 wp[4];
+#pragma unroll
+          for (int q = 0; q < 4; ++q) wp[q] = mul(WTW1[kp * 4 + q], P1d[q - 2]);
+          double re[3] = {0.0, 0.0, 0.0}, im[3] = {0.0, 0.0, 0.0};
+          const double2* GW = GWS;
+          if (kval) {
+#pragma unroll
+            for (int u = 0; u < 9; ++u)
+              if (valid(u)) {
+                const int e = (i0 + u / 3) * NW + j0 + u % 3;
+#pragma unroll
+                for (int a = 0; a < NJ; ++a) {
+                  double2 W = dzero;
+#pragma unroll
+                  for (int q = 0; q < 4; ++q) W = fmac(wp[q], GW[(a * 4 + q) * NW2 + e], W);
+                  re[a] = fma(W.x, r[u].x, fma(W.y, r[u].y, re[a]));
+                  im[a] = fma(W.y, r[u].x, fma(-W.x, r[u].y, im[a]));
+                }
+              }
+          }
+          const int slot = (ti / kJRing) & 1, s = ti % kJRing;
+          warp_store_current(re, im, NJ, lane, SJ + (((size_t)slot * kJRing + s) * NWARP + w) * 2 * NJ);
+        }
+        cp_async_wait_all();
+        __syncthreads();
+      }
+      flush(step1 - 1);
+      if (kval) {
+#pragma unroll
+        for (int u = 0; u < 9; ++u)
+          if (valid(u)) rho[kg + (i0 + u / 3) * NW + j0 + u % 3] = r[u];
+      }
+      __syncthreads();
+    }
+}
+
+}  // namespace mtile

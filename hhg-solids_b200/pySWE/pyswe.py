@@ -248,7 +248,8 @@ class SWE:
         s = ct.c_longlong()
         kind = int(self.swe_cpp.SWESim_launch_shape(self.ptr, ct.byref(c), ct.byref(t), ct.byref(k), ct.byref(s)))
         names = {0: "propagate_kpt_kernel", 1: "propagate_group_kernel<double>", 2: "propagate_group_kernel<float>",
-                 3: "propagate_kcol_kernel", 4: "propagate_frag_kernel", 5: "propagate_dfrag_kernel"}
+                 3: "propagate_kcol_kernel", 4: "propagate_frag_kernel", 5: "propagate_dfrag_kernel",
+                 6: "propagate_mtile_kernel"}
         return {"ctas": c.value, "threads": t.value, "k_per_cta": k.value, "smem_bytes": s.value,
                 "kernel_name": names.get(kind, "none")}
 

@@ -5,9 +5,10 @@ in-kernel sums, and every variant stays within the parity bar (FP64 1e-10 per ax
 
 The HHG_GROUP_* variables only remove variants from the planner's list; they are read when a solve is
 set up.  The plain form of 11- and 12-orbital models on a 7x7 box runs the FP64 tensor-core fragment
-kernel (sbe_dfrag.cuh) before any of them; HHG_DFRAG=0 removes it, so the element-group variants are
-compared with it off.  The mixed-form tensor-core fragment kernel (sbe_frag.cuh) is opt-in
-(HHG_FRAG=1) and checked against its own measured accuracy."""
+kernel (sbe_dfrag.cuh) before any of them, and their mixed form the tile kernel (sbe_mtile.cuh);
+HHG_DFRAG=0 and HHG_MTILE=0 remove them, so the element-group variants are compared with them off.
+The mixed-form tensor-core fragment kernel (sbe_frag.cuh) is opt-in (HHG_FRAG=1) and checked against
+its own measured accuracy."""
 import os
 
 import numpy as np
@@ -17,7 +18,7 @@ from conftest import load_golden, rel_l2
 
 pytestmark = pytest.mark.gpu
 
-FLAGS = ("HHG_GROUP_NOPRE", "HHG_GROUP_NOPAIR", "HHG_GROUP_ANYBOX", "HHG_FRAG", "HHG_FRAG_KPC", "HHG_DFRAG")
+FLAGS = ("HHG_GROUP_NOPRE", "HHG_GROUP_NOPAIR", "HHG_GROUP_ANYBOX", "HHG_FRAG", "HHG_FRAG_KPC", "HHG_DFRAG", "HHG_MTILE")
 NAMES = ["tmd6_8", "tmd11_10", "tmd12_6", "c2_prefix", "ks_tmd11_10"]
 
 
@@ -46,8 +47,8 @@ def run(param, precision, env):
 @pytest.mark.parametrize("name", ["tmd6_8", "tmd11_10", "c2_prefix", "ks_tmd11_10"])  # grids of at least 7x7: a 7x7 box
 def test_precomputed_sums_are_bit_identical(name, precision):
     _, param, _, _ = load_golden(name)
-    J_pre, n_pre, shape_pre = run(param, precision, ["HHG_DFRAG=0"])
-    J_in, n_in, shape_in = run(param, precision, ["HHG_GROUP_NOPRE", "HHG_DFRAG=0"])
+    J_pre, n_pre, shape_pre = run(param, precision, ["HHG_DFRAG=0", "HHG_MTILE=0"])
+    J_in, n_in, shape_in = run(param, precision, ["HHG_GROUP_NOPRE", "HHG_DFRAG=0", "HHG_MTILE=0"])
     nt = J_pre.shape[1]
     # Precomputed: one (sums, propagation) launch pair per 64 steps; in-kernel: one propagation.
     # (Only the k-space solver's 11- and 12-orbital shapes have them among its compiled shapes.)
@@ -63,8 +64,10 @@ def test_precomputed_sums_are_bit_identical(name, precision):
         assert precision == "fp64" and rel_l2(J_pre, J_in) < 1e-13, (shape_pre, shape_in, rel_l2(J_pre, J_in))
 
 
-@pytest.mark.parametrize("env", [[], ["HHG_DFRAG=0"], ["HHG_GROUP_NOPRE", "HHG_DFRAG=0"], ["HHG_GROUP_NOPAIR"],
-                                 ["HHG_GROUP_NOPRE", "HHG_GROUP_NOPAIR", "HHG_DFRAG=0"], ["HHG_GROUP_ANYBOX"]])
+@pytest.mark.parametrize("env", [[], ["HHG_DFRAG=0", "HHG_MTILE=0"], ["HHG_GROUP_NOPRE", "HHG_DFRAG=0", "HHG_MTILE=0"],
+                                 ["HHG_GROUP_NOPAIR", "HHG_MTILE=0"],
+                                 ["HHG_GROUP_NOPRE", "HHG_GROUP_NOPAIR", "HHG_DFRAG=0", "HHG_MTILE=0"],
+                                 ["HHG_GROUP_ANYBOX", "HHG_MTILE=0"]])
 @pytest.mark.parametrize("name", NAMES)
 def test_every_variant_within_the_parity_bar(name, env):
     _, param, _, J_ref = load_golden(name)
@@ -90,8 +93,8 @@ def test_fragment_kernel_against_element_groups(name):
     _, param, _, J_ref = load_golden(name)
     J_frag, n_frag, shape = run(param, "mixed", ["HHG_FRAG=1"])
     assert shape[3] == "propagate_frag_kernel", shape
-    J_grp, _, shape_grp = run(param, "mixed", [])
-    assert shape_grp[3] != "propagate_frag_kernel"
+    J_grp, _, shape_grp = run(param, "mixed", ["HHG_MTILE=0"])
+    assert shape_grp[3].startswith("propagate_group_kernel"), shape_grp
     nt = J_frag.shape[1]
     assert n_frag == 2 * ((nt + 63) // 64) + 1
     assert rel_l2(J_frag, J_ref) < FRAG_TOL[name], rel_l2(J_frag, J_ref)
@@ -205,3 +208,46 @@ def test_fp64_fragment_kernel_kspace_solver():
         Jg, _, _ = run(p, "fp64", ["HHG_DFRAG=0"])
         assert shape[3] == "propagate_dfrag_kernel", shape
         assert rel_l2(Jd, Jg) < 1e-11, (n, rel_l2(Jd, Jg))
+
+
+@pytest.mark.parametrize("name", ["tmd11_10", "c2_prefix", "tmd11_12_full", "tmd12_12_full"])
+def test_tile_kernel_against_element_groups_and_golden(name):
+    """The mixed form's default kernel for 11- and 12-orbital models on a 7x7 box (half a warp per
+    k-point, 3x3 register tiles) against the reference's current and the element-group kernel's, within
+    the mixed form's 1e-6 (full pulses of 4096 steps included)."""
+    _, param, _, J_ref = load_golden(name)
+    Jt, n_t, shape = run(param, "mixed", [])
+    assert shape[3] == "propagate_mtile_kernel", shape
+    Jg, _, shape_g = run(param, "mixed", ["HHG_MTILE=0"])
+    assert shape_g[3].startswith("propagate_group_kernel"), shape_g
+    nt = Jt.shape[1]
+    assert n_t == 2 * ((nt + 63) // 64) + 1
+    assert rel_l2(Jt, J_ref) < 1e-6, rel_l2(Jt, J_ref)
+    assert rel_l2(Jt, Jg) < 1e-6, rel_l2(Jt, Jg)
+
+
+def test_tile_kernel_ragged_columns_two_axes_and_slabs():
+    """Columns that do not divide into 8-k-point tiles (10 and 22 rows), a non-square grid, two field
+    axes (polarisation in the plane), and a row slab, against the FP64 solve of the same case."""
+    import tbgen
+    from pySWE import pyswe
+
+    for n1, n2 in ((10, 10), (14, 8), (22, 10)):
+        p = {"path_tb": tbgen.model_path("tmd11_s7"), "nr1": n1, "nr2": n2, "nr3": 1, "tmax": 3.0, "dt": 0.02197,
+             "intensity": 2e12, "lambda": 3000.0, "tmax_field": 80.0, "pol_vec": np.array([0.6, 0.8, 0.0]),
+             "phi_vec": np.zeros(3)}
+        Jt, _, shape = run(p, "mixed", [])
+        J64, _, _ = run(p, "fp64", [])
+        assert shape[1] == 8 and shape[3] == "propagate_mtile_kernel", shape
+        assert rel_l2(Jt, J64) < 1e-6, (n1, n2, rel_l2(Jt, J64))
+    # rows [3, 12) of a 14 x 8 grid: the slab's partial current against the FP64 slab's
+    p = dict(p, nr1=14, nr2=8)
+    out = []
+    for precision in ("mixed", "fp64"):
+        s = pyswe.SWE(pyswe.Settings(dict(p)), precision=precision, k_rows=(3, 12))
+        if precision == "mixed":
+            assert s.launch_shape()["kernel_name"] == "propagate_mtile_kernel"
+        s.run_simulation()
+        out.append(np.stack(s.get_current()[1:]))
+        s.delete()
+    assert rel_l2(out[0], out[1]) < 1e-6, rel_l2(out[0], out[1])
