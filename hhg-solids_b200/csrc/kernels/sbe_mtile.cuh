@@ -20,9 +20,10 @@
 //  * P replaces X in shared memory, and k = -i (P - P^+) takes P^+ from the transposed tile;
 //  * the RK4 sum and the next stage's X are formed in FP64 (X stored as FP32).
 // Only the k-point's half warp exchanges data, so the stages need __syncwarp only; the CTA meets twice
-// per step (before the current, whose FP64 window rows are copied in during the step, and at its end:
-// the next step's inner sums, copied in with cp.async meanwhile, and the current partials).  The window
-// velocity and the current are FP64, per lane on its own tile.
+// per step for the current (its FP64 window rows copied in during the step, then the FP64 state staged
+// for it) and once at its end (the next step's inner sums, copied in with cp.async meanwhile, and the
+// current partials).  The current is FP64: summed over the CTA's k-points on the FP64 tensor cores, then
+// contracted with the window rows.
 //
 // Precision: as the element-group kernel's mixed form (complex-FP32 Wannier sums and commutator
 // products, FP64 state, RK4 accumulation, window velocity and k-sum).
@@ -54,6 +55,8 @@ struct Geom {
   static_assert(NW > 8 && NW <= 12, "3 x 3 tiles of a 12 x 12 frame: 9..12 orbitals");
   static_assert(KPC % 2 == 0 && KPC * 16 <= 1024, "k-points per CTA");
   static_assert((NBROWS * NW2 * 8) % 16 == 0, "16-byte copies of the inner sums");
+  static_assert((size_t)KPC * NW2 * 16 <= 2 * (size_t)KPC * KS * 8, "the FP64 state fits over the H and X area");
+  static_assert(KPC == 8, "the current's product takes the CTA's k-points as its K dimension (two k-steps)");
 };
 
 // 8 k-points per CTA run three CTAs per SM (at most 168 registers per thread): 12 warps per SM, against
@@ -134,14 +137,11 @@ __global__ void __launch_bounds__(KPC * 16, KPC <= 8 ? 3 : 1)
       }
       fetch_sums(step0, step0 & 1);
       cp_async_commit();
-      // This lane's tile of the state (FP64 registers for the whole tile), and X = rho for the first stage.
+      // This lane's tile of the state (FP64 registers for the whole tile).
       const size_t kg = ((size_t)(m10 + (kval ? kp : 0)) * t.N2 + m2) * NW2;
       double2 r[9];
 #pragma unroll
-      for (int u = 0; u < 9; ++u) {
-        r[u] = (kval && valid(u)) ? rho[kg + (i0 + u / 3) * NW + j0 + u % 3] : dzero;
-        Xk[own(u)] = make_float2((float)r[u].x, (float)r[u].y);
-      }
+      for (int u = 0; u < 9; ++u) r[u] = (kval && valid(u)) ? rho[kg + (i0 + u / 3) * NW + j0 + u % 3] : dzero;
       cp_async_wait_all();
       __syncthreads();
 
@@ -182,7 +182,10 @@ __global__ void __launch_bounds__(KPC * 16, KPC <= 8 ? 3 : 1)
               hm[mat][u] = acc;
             }
         }
-        // (2) RK4 stages (src/solver.cpp:157-180), fields at t, t+dt/2, t+dt/2, t+dt.
+        // (2) RK4 stages (src/solver.cpp:157-180), fields at t, t+dt/2, t+dt/2, t+dt; X = rho for the first
+        //     (the area held the previous step's FP64 state for the current).
+#pragma unroll
+        for (int u = 0; u < 9; ++u) Xk[own(u)] = make_float2((float)r[u].x, (float)r[u].y);
         const double* esb = t.es + (size_t)ti * 9;
         double2 S[9];
 #pragma unroll 1
@@ -248,39 +251,68 @@ __global__ void __launch_bounds__(KPC * 16, KPC <= 8 ? 3 : 1)
             for (int u = 0; u < 9; ++u) Xk[own(u)] = xn[u];
           }
         }
-        // rho += dt/6 (k1 + 2 k2 + 2 k3 + k4) (src/solver.cpp:170-180); X = rho for the next step.
+        // rho += dt/6 (k1 + 2 k2 + 2 k3 + k4) (src/solver.cpp:170-180).
 #pragma unroll
         for (int u = 0; u < 9; ++u) {
           r[u].x = r[u].x + prefac * S[u].x;
           r[u].y = r[u].y + prefac * S[u].y;
-          Xk[own(u)] = make_float2((float)r[u].x, (float)r[u].y);
         }
 
-        // (3) Current partials of step ti (FP64) on the lane's tile: W_a(k)_e = sum_q wp(k, q) GW(a, q)_e,
-        //     J_a += W_a,e conj(rho_e).
+        // (3) Current partials of step ti (FP64), summed over the CTA's k-points before the window:
+        //     J_a = sum_{q,e} GW(a, q)_e R(q, e) with R(q, e) = sum_k wp(k, q) conj(rho_e(k)), the same sum
+        //     as sum_k sum_e W_a(k)_e conj(rho_e(k)), W_a(k)_e = sum_q wp(k, q) GW(a, q)_e, in another order.
+        //     R is a [4 window rows (of 8)] x [8 k-points] x [nw^2 elements] product on the FP64 tensor
+        //     cores (three real m8n8k4 products per complex one) from the state staged in FP64 over the H
+        //     and X area, which every k-point's stages have finished with at the barrier.
         cp_async_wait_one();  // this step's window rows
         __syncthreads();
+        double2* RS = reinterpret_cast<double2*>(HS);  // [KPC][NW2] double2
+        if (kval) {
+#pragma unroll
+          for (int u = 0; u < 9; ++u)
+            if (valid(u)) RS[kp * NW2 + (i0 + u / 3) * NW + j0 + u % 3] = r[u];
+        } else {
+#pragma unroll
+          for (int u = 0; u < 9; ++u)
+            if (valid(u)) RS[kp * NW2 + (i0 + u / 3) * NW + j0 + u % 3] = dzero;
+        }
+        __syncthreads();
         {
+          const int g = lane >> 2, c4 = lane & 3;
           const double2* P1d = d.Pd + (size_t)ti * 2 * npw + t.np;
-          double2 wp[4];
+          // A[g][c] of k-step ks: wp(k-point 4 ks + c, window row g), rows 4..7 zero.
+          double2 wa[2];
 #pragma unroll
-          for (int q = 0; q < 4; ++q) wp[q] = mul(WTW1[kp * 4 + q], P1d[q - 2]);
+          for (int ks = 0; ks < 2; ++ks)
+            wa[ks] = g < 4 ? mul(WTW1[(4 * ks + c4) * 4 + g], P1d[g - 2]) : dzero;
           double re[3] = {0.0, 0.0, 0.0}, im[3] = {0.0, 0.0, 0.0};
-          const double2* GW = GWS;
-          if (kval) {
+          constexpr int NTR = (NW2 + 7) / 8;
+#pragma unroll 1
+          for (int nt = w; nt < NTR; nt += NWARP) {
+            double t1[2] = {0.0, 0.0}, t2[2] = {0.0, 0.0}, t3[2] = {0.0, 0.0};
+            const int eb = 8 * nt + g;  // B[c][g]: conj(rho_eb(k-point 4 ks + c))
 #pragma unroll
-            for (int u = 0; u < 9; ++u)
-              if (valid(u)) {
-                const int e = (i0 + u / 3) * NW + j0 + u % 3;
+            for (int ks = 0; ks < 2; ++ks) {
+              const double2 b = eb < NW2 ? RS[(4 * ks + c4) * NW2 + eb] : dzero;
+              dfrag::dmma(t1, wa[ks].x, b.x);
+              dfrag::dmma(t2, wa[ks].y, -b.y);
+              dfrag::dmma(t3, wa[ks].x + wa[ks].y, b.x - b.y);
+            }
+            if (g < 4) {
 #pragma unroll
-                for (int a = 0; a < NJ; ++a) {
-                  double2 W = dzero;
+              for (int jj = 0; jj < 2; ++jj) {
+                const int e = 8 * nt + 2 * c4 + jj;  // R(g, e)
+                if (e < NW2) {
+                  const double rr = t1[jj] - t2[jj], ri = t3[jj] - t1[jj] - t2[jj];
 #pragma unroll
-                  for (int q = 0; q < 4; ++q) W = fmac(wp[q], GW[(a * 4 + q) * NW2 + e], W);
-                  re[a] = fma(W.x, r[u].x, fma(W.y, r[u].y, re[a]));
-                  im[a] = fma(W.y, r[u].x, fma(-W.x, r[u].y, im[a]));
+                  for (int a = 0; a < NJ; ++a) {
+                    const double2 gw = GWS[(a * 4 + g) * NW2 + e];
+                    re[a] = fma(gw.x, rr, fma(-gw.y, ri, re[a]));
+                    im[a] = fma(gw.x, ri, fma(gw.y, rr, im[a]));
+                  }
                 }
               }
+            }
           }
           const int slot = (ti / kJRing) & 1, s = ti % kJRing;
           warp_store_current(re, im, NJ, lane, SJ + (((size_t)slot * kJRing + s) * NWARP + w) * 2 * NJ);
