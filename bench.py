@@ -9,8 +9,9 @@ The default workload is "c2" in the mixed form: the 11-orbital TMD-like model (s
 on a 150 x 150 k-grid under the full pulse (nt = 4096), with complex-FP32 Wannier sums and
 commutators and an FP64 state, RK4 accumulation, window velocity and k-sum.  Beside it the same
 line carries the plain-FP64 solve of the same configuration (time, J error of the mixed form
-against it, per-odd-harmonic intensity errors up to the cutoff) and B = 4 mixed solves run as one
-SWEBatch (per-solve time and throughput against the FP64 solo solve).  --workload c1 --precision
+against it, per-odd-harmonic intensity errors up to the cutoff) and B = 4 mixed solves (polarisation
+0, 45, 90 and 135 degrees) run as one SWEBatch: per-solve time, throughput against the FP64 solo
+solve, and time against FP64 solo solves of the same four angles.  --workload c1 --precision
 fp64 is the 2-orbital 200 x 200 drop-in configuration.
 
 Printed JSON line (rank 0):
@@ -925,7 +926,8 @@ def main():
             for i in range(args.batch):
                 pi = dict(param)
                 ang = math.pi * i / args.batch
-                pi["pol_vec"] = np.array([math.sin(ang), math.cos(ang), 0.0])
+                # (components below 1e-12 are zero: 90 degrees is the x axis alone, not x plus 6e-17 y)
+                pi["pol_vec"] = np.array([v if abs(v) > 1e-12 else 0.0 for v in (math.sin(ang), math.cos(ang))] + [0.0])
                 solves.append(pyswe.SWE(pyswe.Settings(pi), device=local, precision="mixed", solver=args.solver,
                                         autotune=args.autotune))
             batch = pyswe.SWEBatch(solves)
@@ -936,17 +938,20 @@ def main():
                 torch.cuda.synchronize()
                 batch.run()
                 bms.append(batch.last_ms())
-            # The batch's error against FP64 solo solves of the same angles: the first and the middle one.
-            berr = []
-            for i in sorted({0, args.batch // 2}):
+            # The batch against FP64 solo solves of the same angles (one or two field axes): their device
+            # time (a second run, L2 flushed before it) and the batch's error against their currents.
+            berr, fms_same = [], []
+            for i in range(args.batch):
                 Jb = solves[i].get_current()[1:]
-                if i == 0:
-                    Jf = J_fp64
-                else:
-                    f = pyswe.SWE(pyswe.Settings(dict(solves[i].settings.param)), device=local, solver=args.solver)
-                    f.run_simulation()
-                    Jf = f.get_current()[1:]
-                    f.delete()
+                f = pyswe.SWE(pyswe.Settings(dict(solves[i].settings.param)), device=local, solver=args.solver)
+                f.run_simulation()
+                f.reset()
+                flush.fill_(float(i))
+                torch.cuda.synchronize()
+                f.run_simulation()
+                fms_same.append(f.last_kernel_ms())
+                Jf = f.get_current()[1:]
+                f.delete()
                 berr.append(float(np.linalg.norm(Jb - Jf) / np.linalg.norm(Jf)))
             batch.delete()
             for s in solves:
@@ -955,6 +960,9 @@ def main():
             mixed["batched"] = {"solves": args.batch, "timed_batches": len(bms), "ms_per_batch": statistics.mean(bms),
                                 "ms_per_solve": per_solve, "k_pt_rk4_steps_per_s": nk * nt / (per_solve * 1e-3),
                                 "throughput_vs_fp64_solo": fp64_ms / per_solve,
+                                "pol_angles_deg": [180.0 * i / args.batch for i in range(args.batch)],
+                                "fp64_same_solves_ms": sum(fms_same),
+                                "speedup_vs_fp64_same_solves": sum(fms_same) / statistics.mean(bms),
                                 "throughput_vs_fp64_pipe_solo": (mixed["fp64_pipe_kernel"]["ms_per_solve"] / per_solve
                                                                  if "fp64_pipe_kernel" in mixed else None),
                                 "J_rel_l2_vs_fp64": berr,

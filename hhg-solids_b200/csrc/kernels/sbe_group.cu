@@ -1041,10 +1041,10 @@ int launch_frag_t(const SolveTables& t, const GroupTables& gt, const LaunchShape
 }
 
 // Mixed-form tile kernel: precomputed inner sums, compiled 7x7 box, KPC k-points per CTA (half a warp each).
-template <int NW, int NAX, int NJ, int KPC>
+template <int NW, int NAX, int NJ, int KPC, bool KM>
 bool plan_mtile_t(const SolveTables& t, int sm_count, LaunchShape* out, char* why, int why_len) {
-  using FG = mtile::Geom<NW, NAX, NJ, KPC>;
-  auto kern = mtile::propagate_mtile_kernel<NW, NAX, NJ, KPC>;
+  using FG = mtile::Geom<NW, NAX, NJ, KPC, KM>;
+  auto kern = mtile::propagate_mtile_kernel<NW, NAX, NJ, KPC, KM>;
   if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)FG::BYTES) != cudaSuccess) {
     cudaGetLastError();
     snprintf(why, why_len, "tile kernel: %zu bytes of shared memory not available", FG::BYTES);
@@ -1057,7 +1057,7 @@ bool plan_mtile_t(const SolveTables& t, int sm_count, LaunchShape* out, char* wh
   const int rows = t.row1 - t.row0;
   const long ntiles = (long)t.N2 * ((rows + KPC - 1) / KPC);
   out->kernel = 6;
-  out->kmode = 0;
+  out->kmode = KM ? 1 : 0;
   out->ept = 9;
   out->k_per_cta = KPC;
   out->group = 16;
@@ -1068,32 +1068,34 @@ bool plan_mtile_t(const SolveTables& t, int sm_count, LaunchShape* out, char* wh
   out->box_sm = out->win_sm = 0;
   out->smem = FG::BYTES;
   out->pre_chunk = std::min(kPreChunk, t.nt);
-  out->pre_bytes = (size_t)out->pre_chunk * t.N2 *
-                   ((size_t)FG::NBROWS * FG::NW2 * sizeof(float2) + (size_t)FG::NWROWS * FG::NW2 * sizeof(double2));
+  const size_t gbytes = (size_t)FG::NBROWS * FG::NW2 * sizeof(float2), wbytes = (size_t)FG::NWROWS * FG::NW2 * sizeof(double2);
+  out->pre_bytes = KM ? (size_t)(2 * out->pre_chunk + 1) * t.N2 * gbytes + (size_t)t.N2 * wbytes
+                      : (size_t)out->pre_chunk * t.N2 * (gbytes + wbytes);
   return true;
 }
 
-template <int NW, int NAX, int NJ, int KPC>
+template <int NW, int NAX, int NJ, int KPC, bool KM>
 int launch_mtile_t(const SolveTables& t, const GroupTables& gt, const LaunchShape& s, double2* rho, double2* Jpart,
                    cudaStream_t stream) {
-  using FG = mtile::Geom<NW, NAX, NJ, KPC>;
+  using FG = mtile::Geom<NW, NAX, NJ, KPC, KM>;
   if (!gt.pre || s.pre_chunk <= 0)
     throw std::runtime_error("tile kernel launch: needs its precomputed-sum scratch (GroupTables::pre)");
   GroupData<float> d = {gt.Xbox32, gt.P32, gt.T1_32, gt.T2_32, gt.Xwin64, gt.P64, gt.T1_64, gt.T2_64, nullptr, nullptr};
   const size_t gbuf = (size_t)FG::NBROWS * FG::NW2;
   float2* Gpre = static_cast<float2*>(gt.pre);
-  double2* GWpre = reinterpret_cast<double2*>(Gpre + (size_t)s.pre_chunk * t.N2 * gbuf);
+  const size_t npts_max = KM ? 2 * (size_t)s.pre_chunk + 1 : (size_t)s.pre_chunk;
+  double2* GWpre = reinterpret_cast<double2*>(Gpre + npts_max * t.N2 * gbuf);
   d.Gpre = Gpre;
   d.GWpre = GWpre;
-  auto kern = mtile::propagate_mtile_kernel<NW, NAX, NJ, KPC>;
+  auto kern = mtile::propagate_mtile_kernel<NW, NAX, NJ, KPC, KM>;
   cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s.smem);
   int launches = 0;
   for (int c0 = t.step0; c0 < t.step1; c0 += s.pre_chunk) {
     SolveTables tc = t;
     tc.step0 = c0;
     tc.step1 = std::min(c0 + s.pre_chunk, t.step1);
-    group_sums_kernel<float><<<(tc.step1 - c0) * t.N2, 256, 0, stream>>>(tc, d, 3, 4, FG::NBROWS, FG::NWROWS, Gpre,
-                                                                          GWpre);
+    const int npts = KM ? 2 * (tc.step1 - c0) + 1 : tc.step1 - c0;
+    group_sums_kernel<float><<<npts * t.N2, 256, 0, stream>>>(tc, d, 3, 4, FG::NBROWS, FG::NWROWS, Gpre, GWpre);
     kern<<<s.ctas, s.threads, s.smem, stream>>>(tc, d, s.vctas, rho, Jpart);
     launches += 2;
   }
@@ -1102,26 +1104,30 @@ int launch_mtile_t(const SolveTables& t, const GroupTables& gt, const LaunchShap
 
 struct MtileVariant {
   int nw, nax, nj, kpc;
+  bool km;
   bool (*plan)(const SolveTables&, int, LaunchShape*, char*, int);
   int (*launch)(const SolveTables&, const GroupTables&, const LaunchShape&, double2*, double2*, cudaStream_t);
 };
-#define HHG_MTILE_VARIANT(NW, NAX, NJ, KPC) \
-  {NW, NAX, NJ, KPC, plan_mtile_t<NW, NAX, NJ, KPC>, launch_mtile_t<NW, NAX, NJ, KPC>}
+#define HHG_MTILE_VARIANT(NW, NAX, NJ, KPC, KM) \
+  {NW, NAX, NJ, KPC, KM, plan_mtile_t<NW, NAX, NJ, KPC, KM>, launch_mtile_t<NW, NAX, NJ, KPC, KM>}
+// (The k-space solver's ring of four inner-sum slots leaves three CTAs per SM only for 11 orbitals
+// and one field axis; its other shapes run the element-group kernel.)
 const MtileVariant kMtileVariants[] = {
-    HHG_MTILE_VARIANT(11, 1, 2, 8), HHG_MTILE_VARIANT(11, 2, 2, 8),
-    HHG_MTILE_VARIANT(12, 1, 2, 8), HHG_MTILE_VARIANT(12, 2, 2, 8),
+    HHG_MTILE_VARIANT(11, 1, 2, 8, false), HHG_MTILE_VARIANT(11, 2, 2, 8, false),
+    HHG_MTILE_VARIANT(12, 1, 2, 8, false), HHG_MTILE_VARIANT(12, 2, 2, 8, false),
+    HHG_MTILE_VARIANT(11, 1, 2, 8, true),
 };
 #undef HHG_MTILE_VARIANT
 
-// The tile kernel for a mixed-form solve (Hermitian halved 7x7 box, real-space solver), or null.
+// The tile kernel for a mixed-form solve (Hermitian halved 7x7 box; either solver), or null.
 // HHG_MTILE=0 turns it off (measurements): the element-group kernel then runs the solve.
 const MtileVariant* find_mtile(const SolveTables& t) {
   if (const char* off = std::getenv("HHG_MTILE"))
     if (off[0] == '0') return nullptr;
   const GroupGeom gg = group_geom(t);
-  if (t.kmode || !t.hermitian || !gg.half || t.b1n != 7 || t.b2n != 7) return nullptr;
+  if (!t.hermitian || !gg.half || t.b1n != 7 || t.b2n != 7) return nullptr;
   for (const MtileVariant& v : kMtileVariants)
-    if (v.nw == t.nw && v.nax == t.nax && v.nj == t.nj) return &v;
+    if (v.nw == t.nw && v.nax == t.nax && v.nj == t.nj && v.km == (t.kmode != 0)) return &v;
   return nullptr;
 }
 

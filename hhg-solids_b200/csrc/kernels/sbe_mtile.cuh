@@ -33,21 +33,25 @@ namespace mtile {
 // Waits until at most one committed group of this thread's cp.async copies is still in flight.
 __device__ __forceinline__ void cp_async_wait_one() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
 
-template <int NW, int NAX, int NJ, int KPC>
+template <int NW, int NAX, int NJ, int KPC, bool KM = false>
 struct Geom {
   static constexpr int NW2 = NW * NW;
   static constexpr int NMAT = 1 + NAX;
   static constexpr int NBROWS = NMAT * 4;   // halved 7 x 7 box: inner-sum rows n1 = 0..3 per matrix
   static constexpr int NWROWS = NJ * 4;     // window rows
   static constexpr int NWARP = KPC / 2;
+  // Inner-sum slots: this step's point and the next one's (real-space solver); the k-space solver's
+  // points t + dt/2 and t + dt of this step and of the next, in a ring of four (point p in (p + 3) % 4).
+  static constexpr int NGS = KM ? 4 : 2;
   static constexpr int NTHR = KPC * 16;
   static constexpr int MS = 12;             // row stride (float2) of a padded matrix
   static constexpr int KS = 12 * 12 + 1;    // float2 per k-point matrix: the odd 8-byte unit puts the
                                             // warp's two k-points two banks apart
   static constexpr size_t HS = 0;                                     // [KPC][KS] float2: H, transposed
   static constexpr size_t XP = HS + (size_t)KPC * KS * 8;             // [KPC][KS] float2: X, then P
-  static constexpr size_t GS = (XP + (size_t)KPC * KS * 8 + 15) / 16 * 16;  // [2][NBROWS][NW2] float2
-  static constexpr size_t GWS = GS + 2 * (size_t)NBROWS * NW2 * 8;    // [NWROWS][NW2] double2 (one step's)
+  static constexpr size_t GS = (XP + (size_t)KPC * KS * 8 + 15) / 16 * 16;  // [NGS][NBROWS][NW2] float2
+  static constexpr size_t GWS = GS + NGS * (size_t)NBROWS * NW2 * 8;  // [NWROWS][NW2] double2: one step's
+                                                                      // (k-space solver: the column's)
   static constexpr size_t TW1 = GWS + (size_t)NWROWS * NW2 * 16;      // [KPC][8] float2: box rows q = 0..6
   static constexpr size_t WTW1 = TW1 + (size_t)KPC * 8 * 8;           // [KPC][4] double2: window rows
   static constexpr size_t SJ = WTW1 + (size_t)KPC * 4 * 16;           // [2][kJRing][NWARP][2 NJ] double
@@ -61,10 +65,13 @@ struct Geom {
 
 // 8 k-points per CTA run three CTAs per SM (at most 168 registers per thread): 12 warps per SM, against
 // 8 for 16 k-points per CTA at 218 registers (C2: 324 against 416 ms per solve).
-template <int NW, int NAX, int NJ, int KPC>
+// KM: the reference's k-space solver (src/solver_kspace.cpp:167-270): the stages see H at points
+// 2 ti (t), 2 ti + 1 (t + dt/2) and 2 ti + 2 (t + dt) of the interpolation tables; the outer sums of
+// 2 ti + 2 stay in registers for the next step's first stage, and the window has no phase.
+template <int NW, int NAX, int NJ, int KPC, bool KM = false>
 __global__ void __launch_bounds__(KPC * 16, KPC <= 8 ? 3 : 1)
     propagate_mtile_kernel(SolveTables t, GroupData<float> d, int vctas, double2* rho, double2* Jpart) {
-  using FG = Geom<NW, NAX, NJ, KPC>;
+  using FG = Geom<NW, NAX, NJ, KPC, KM>;
   constexpr int NW2 = FG::NW2, NMAT = FG::NMAT, NWARP = FG::NWARP, NTHR = FG::NTHR, MS = FG::MS, KS = FG::KS;
   extern __shared__ __align__(16) unsigned char smraw[];
   float2* HS = reinterpret_cast<float2*>(smraw + FG::HS);
@@ -98,14 +105,14 @@ __global__ void __launch_bounds__(KPC * 16, KPC <= 8 ? 3 : 1)
 
       // Inner sums of point p into slot `slot`, and window rows of point p (16-byte asynchronous copies).
       auto fetch_sums = [&](int p, int slot) {
-        const size_t blk = (size_t)(p - step0) * t.N2 + m2;
+        const size_t blk = (size_t)(p - (KM ? 2 * step0 : step0)) * t.N2 + m2;
         const char* src = reinterpret_cast<const char*>(d.Gpre + blk * gbuf);
         char* dst = reinterpret_cast<char*>(GS + (size_t)slot * gbuf);
         constexpr int nA = (int)(gbuf * 8 / 16);
         for (int idx = tid; idx < nA; idx += NTHR) cp_async16(dst + (size_t)idx * 16, src + (size_t)idx * 16);
       };
       auto fetch_window = [&](int p) {
-        const double2* wsrc = d.GWpre + ((size_t)(p - step0) * t.N2 + m2) * wbuf;
+        const double2* wsrc = d.GWpre + ((KM ? 0 : (size_t)(p - step0) * t.N2) + m2) * wbuf;
         for (int idx = tid; idx < (int)wbuf; idx += NTHR) cp_async16(GWS + idx, wsrc + idx);
       };
       // The warps' current partials of the ring half ending at step ti_end, into this virtual CTA's row.
@@ -135,7 +142,41 @@ __global__ void __launch_bounds__(KPC * 16, KPC <= 8 ? 3 : 1)
         const int m = idx / 4, q = idx % 4, m1 = min(m10 + m, t.row1 - 1);
         WTW1[idx] = d.T1d[wrap_mod((long long)m1 * (q - 2), t.N1)];
       }
-      fetch_sums(step0, step0 & 1);
+      // Outer sums of the tile's elements at point p from GS slot `slot`: for matrix mat (H0, then r_a),
+      // sum_{q=0..6} p1(k, q) G'(q)_e with G'(q) = G(n1 = q - 3) for q >= 3 and G(3 - q)^+ below.
+      float2 hm[NMAT][9];
+      auto outer = [&](int p, int slot) {
+        const float2* P1 = d.P + (size_t)p * 2 * npw + t.np;
+        float2 p1[7];
+#pragma unroll
+        for (int q = 0; q < 7; ++q) p1[q] = mul(TW1[kp * 8 + q], P1[t.b1lo + q]);
+        const float2* G = GS + (size_t)slot * gbuf;
+#pragma unroll
+        for (int mat = 0; mat < NMAT; ++mat)
+#pragma unroll
+          for (int u = 0; u < 9; ++u) {
+            float2 acc = fzero;
+            if (valid(u)) {
+              const int i = i0 + u / 3, j = j0 + u % 3, e = i * NW + j, eT = j * NW + i;
+              const float2* Gm = G + (size_t)mat * 4 * NW2;
+              acc = mul(p1[3], Gm[e]);
+#pragma unroll
+              for (int n = 1; n < 4; ++n) {
+                acc = fmac(p1[3 + n], Gm[n * NW2 + e], acc);
+                acc = fmac(p1[3 - n], conjugate(Gm[n * NW2 + eT]), acc);
+              }
+            }
+            hm[mat][u] = acc;
+          }
+      };
+      auto gslot = [&](int p) { return KM ? (p + 3) & 3 : p & 1; };
+
+      if constexpr (KM) {
+        fetch_sums(2 * step0, gslot(2 * step0));
+        fetch_window(0);  // the column's window rows, the same for every step
+      } else {
+        fetch_sums(step0, gslot(step0));
+      }
       cp_async_commit();
       // This lane's tile of the state (FP64 registers for the whole tile).
       const size_t kg = ((size_t)(m10 + (kval ? kp : 0)) * t.N2 + m2) * NW2;
@@ -144,43 +185,37 @@ __global__ void __launch_bounds__(KPC * 16, KPC <= 8 ? 3 : 1)
       for (int u = 0; u < 9; ++u) r[u] = (kval && valid(u)) ? rho[kg + (i0 + u / 3) * NW + j0 + u % 3] : dzero;
       cp_async_wait_all();
       __syncthreads();
+      if constexpr (KM) {
+        // The chunk's first point t (then carried from step to step), and the first step's other two.
+        outer(2 * step0, gslot(2 * step0));
+        fetch_sums(2 * step0 + 1, gslot(2 * step0 + 1));
+        fetch_sums(2 * step0 + 2, gslot(2 * step0 + 2));
+        cp_async_commit();
+        cp_async_wait_all();
+        __syncthreads();
+      }
 
       for (int ti = step0; ti < step1; ++ti) {
         const int buf = ti & 1;
         if (ti > step0 && (ti - 1) % kJRing == kJRing - 1) flush(ti - 1);
-        // This step's window rows (read by the current at its end), then the next step's inner sums into
-        // the other slot: both buffers' last readers finished before the barrier that ended the previous
-        // step.  Two groups, so that the current can wait for the first alone.
-        fetch_window(ti);
-        cp_async_commit();
-        if (ti + 1 < step1) fetch_sums(ti + 1, (ti + 1) & 1);
-        cp_async_commit();
-        // (1) Outer sums of the tile's elements at the step's point: for matrix mat (H0, then r_a),
-        //     sum_{q=0..6} p1(k, q) G'(q)_e with G'(q) = G(n1 = q - 3) for q >= 3 and G(3 - q)^+ below.
-        float2 hm[NMAT][9];
-        {
-          const float2* P1 = d.P + (size_t)ti * 2 * npw + t.np;
-          float2 p1[7];
-#pragma unroll
-          for (int q = 0; q < 7; ++q) p1[q] = mul(TW1[kp * 8 + q], P1[t.b1lo + q]);
-          const float2* G = GS + (size_t)buf * gbuf;
-#pragma unroll
-          for (int mat = 0; mat < NMAT; ++mat)
-#pragma unroll
-            for (int u = 0; u < 9; ++u) {
-              float2 acc = fzero;
-              if (valid(u)) {
-                const int i = i0 + u / 3, j = j0 + u % 3, e = i * NW + j, eT = j * NW + i;
-                const float2* Gm = G + (size_t)mat * 4 * NW2;
-                acc = mul(p1[3], Gm[e]);
-#pragma unroll
-                for (int n = 1; n < 4; ++n) {
-                  acc = fmac(p1[3 + n], Gm[n * NW2 + e], acc);
-                  acc = fmac(p1[3 - n], conjugate(Gm[n * NW2 + eT]), acc);
-                }
-              }
-              hm[mat][u] = acc;
-            }
+        if constexpr (KM) {
+          // The next step's points t + dt/2 and t + dt, into the slots of this step's t and of the
+          // previous step's t + dt/2, whose last readers finished before the barrier that ended it.
+          if (ti + 1 < step1) {
+            fetch_sums(2 * ti + 3, gslot(2 * ti + 3));
+            fetch_sums(2 * ti + 4, gslot(2 * ti + 4));
+          }
+          cp_async_commit();
+        } else {
+          // This step's window rows (read by the current at its end), then the next step's inner sums
+          // into the other slot: both buffers' last readers finished before the barrier that ended the
+          // previous step.  Two groups, so that the current can wait for the first alone.
+          fetch_window(ti);
+          cp_async_commit();
+          if (ti + 1 < step1) fetch_sums(ti + 1, gslot(ti + 1));
+          cp_async_commit();
+          // (1) Outer sums at the step's point.
+          outer(ti, buf);
         }
         // (2) RK4 stages (src/solver.cpp:157-180), fields at t, t+dt/2, t+dt/2, t+dt; X = rho for the first
         //     (the area held the previous step's FP64 state for the current).
@@ -191,7 +226,10 @@ __global__ void __launch_bounds__(KPC * 16, KPC <= 8 ? 3 : 1)
 #pragma unroll 1
         for (int st = 0; st < 4; ++st) {
           const int f = st == 0 ? 0 : (st == 3 ? 2 : 1);
-          if (st != 2) {  // (the third stage keeps the second's H: same field)
+          if (st != 2) {  // (the third stage keeps the second's H: same field and point)
+            // k-space solver: the outer sums at t + dt/2 (second stage) and t + dt (fourth, carried on)
+            if (KM && st == 1) outer(2 * ti + 1, gslot(2 * ti + 1));
+            if (KM && st == 3) outer(2 * ti + 2, gslot(2 * ti + 2));
             float ea[NAX];
 #pragma unroll
             for (int a = 0; a < NAX; ++a) ea[a] = (float)esb[f * 3 + t.ax_id[a]];
@@ -264,7 +302,7 @@ __global__ void __launch_bounds__(KPC * 16, KPC <= 8 ? 3 : 1)
         //     R is a [4 window rows (of 8)] x [8 k-points] x [nw^2 elements] product on the FP64 tensor
         //     cores (three real m8n8k4 products per complex one) from the state staged in FP64 over the H
         //     and X area, which every k-point's stages have finished with at the barrier.
-        cp_async_wait_one();  // this step's window rows
+        if constexpr (!KM) cp_async_wait_one();  // this step's window rows
         __syncthreads();
         double2* RS = reinterpret_cast<double2*>(HS);  // [KPC][NW2] double2
         if (kval) {
@@ -284,7 +322,7 @@ __global__ void __launch_bounds__(KPC * 16, KPC <= 8 ? 3 : 1)
           double2 wa[2];
 #pragma unroll
           for (int ks = 0; ks < 2; ++ks)
-            wa[ks] = g < 4 ? mul(WTW1[(4 * ks + c4) * 4 + g], P1d[g - 2]) : dzero;
+            wa[ks] = g < 4 ? (KM ? WTW1[(4 * ks + c4) * 4 + g] : mul(WTW1[(4 * ks + c4) * 4 + g], P1d[g - 2])) : dzero;
           double re[3] = {0.0, 0.0, 0.0}, im[3] = {0.0, 0.0, 0.0};
           constexpr int NTR = (NW2 + 7) / 8;
 #pragma unroll 1

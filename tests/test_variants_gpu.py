@@ -251,3 +251,36 @@ def test_tile_kernel_ragged_columns_two_axes_and_slabs():
         out.append(np.stack(s.get_current()[1:]))
         s.delete()
     assert rel_l2(out[0], out[1]) < 1e-6, rel_l2(out[0], out[1])
+
+
+def test_tile_kernel_kspace_solver():
+    """The k-space solver's form of the tile kernel (outer sums at t + dt/2 and t + dt per step, those
+    at t carried from the previous step, a constant window) against the reference's current and the
+    element-group kernel's; a pulse served in chunks that start on odd steps gives the same bits; the
+    two-axis shape, whose slot ring would not leave three CTAs per SM, stays on the element-group kernel."""
+    import tbgen
+    from pySWE import pyswe
+
+    _, param, _, J_ref = load_golden("ks_tmd11_10")
+    Jt, _, shape = run(param, "mixed", [])
+    assert shape[3] == "propagate_mtile_kernel", shape
+    Jg, _, shape_g = run(param, "mixed", ["HHG_MTILE=0"])
+    assert shape_g[3].startswith("propagate_group_kernel"), shape_g
+    assert rel_l2(Jt, J_ref) < 1e-6, rel_l2(Jt, J_ref)
+    assert rel_l2(Jt, Jg) < 1e-6, rel_l2(Jt, Jg)
+    p = {"path_tb": tbgen.model_path("tmd11_s7"), "nr1": 10, "nr2": 10, "nr3": 1, "tmax": 3.0, "dt": 0.02197,
+         "intensity": 2e12, "lambda": 3000.0, "tmax_field": 80.0, "pol_vec": np.array([0.0, 1.0, 0.0]),
+         "phi_vec": np.zeros(3), "solver": "kspace"}
+    Jt, n_t, shape = run(p, "mixed", [])
+    J64, _, _ = run(p, "fp64", [])
+    assert shape[3] == "propagate_mtile_kernel", shape
+    assert n_t == 2 * ((Jt.shape[1] + 63) // 64) + 1
+    assert rel_l2(Jt, J64) < 1e-6, rel_l2(Jt, J64)
+    srv = pyswe.SWEServer(device=0, chunk_steps=33)
+    r = pyswe.SWE(pyswe.Settings(dict(p)), precision="mixed", solver="kspace", defer_init=True)
+    tk = srv.submit(r)
+    assert srv.wait(tk, timeout=120.0)
+    assert np.array_equal(np.stack(r.get_current()[1:]), Jt)
+    srv.close()
+    _, _, shape2 = run(dict(p, pol_vec=np.array([0.6, 0.8, 0.0])), "mixed", [])
+    assert shape2[3].startswith("propagate_group_kernel"), shape2
