@@ -10,7 +10,8 @@
 // Layout.  A CTA holds KPC consecutive k-points (rows m1) of one k-grid column; the 16 lanes of each
 // half warp own one k-point, lane s its 3 x 3 tile (rows 3 (s / 4) .. +2, columns 3 (s % 4) .. +2) of
 // the k-point's matrices padded to 12 x 12.  Each lane keeps its tile of the state rho and of the RK4
-// sum in FP64 registers, and of the outer Wannier sums H0(k), r_a(k) in FP32 registers for the step.
+// sum in FP64 registers; the outer Wannier sums H0(k), r_a(k) of its tile give H = H0 + E.r at the
+// step's field samples, the later ones kept in FP32 registers for their stages.
 // Per stage:
 //  * H = H0 + E.r of the tile goes to shared memory, transposed (H(i, j) at [j][i]), X = rho + c k
 //    (FP32) is already there;
@@ -143,18 +144,19 @@ __global__ void __launch_bounds__(KPC * 16, KPC <= 8 ? 3 : 1)
         WTW1[idx] = d.T1d[wrap_mod((long long)m1 * (q - 2), t.N1)];
       }
       // Outer sums of the tile's elements at point p from GS slot `slot`: for matrix mat (H0, then r_a),
-      // sum_{q=0..6} p1(k, q) G'(q)_e with G'(q) = G(n1 = q - 3) for q >= 3 and G(3 - q)^+ below.
-      float2 hm[NMAT][9];
-      auto outer = [&](int p, int slot) {
+      // sum_{q=0..6} p1(k, q) G'(q)_e with G'(q) = G(n1 = q - 3) for q >= 3 and G(3 - q)^+ below;
+      // take(u, m) receives element u's NMAT sums.
+      auto outer = [&](int p, int slot, auto&& take) {
         const float2* P1 = d.P + (size_t)p * 2 * npw + t.np;
         float2 p1[7];
 #pragma unroll
         for (int q = 0; q < 7; ++q) p1[q] = mul(TW1[kp * 8 + q], P1[t.b1lo + q]);
         const float2* G = GS + (size_t)slot * gbuf;
 #pragma unroll
-        for (int mat = 0; mat < NMAT; ++mat)
+        for (int u = 0; u < 9; ++u) {
+          float2 m[NMAT];
 #pragma unroll
-          for (int u = 0; u < 9; ++u) {
+          for (int mat = 0; mat < NMAT; ++mat) {
             float2 acc = fzero;
             if (valid(u)) {
               const int i = i0 + u / 3, j = j0 + u % 3, e = i * NW + j, eT = j * NW + i;
@@ -166,9 +168,31 @@ __global__ void __launch_bounds__(KPC * 16, KPC <= 8 ? 3 : 1)
                 acc = fmac(p1[3 - n], conjugate(Gm[n * NW2 + eT]), acc);
               }
             }
-            hm[mat][u] = acc;
+            m[mat] = acc;
           }
+          take(u, m);
+        }
       };
+      // The field samples of step ts (t, t + dt/2, t + dt) on the active axes, and H = H0 + E.r.
+      auto fields = [&](int ts, float (&ea)[3][NAX]) {
+        const double* es = t.es + (size_t)ts * 9;
+#pragma unroll
+        for (int f = 0; f < 3; ++f)
+#pragma unroll
+          for (int a = 0; a < NAX; ++a) ea[f][a] = (float)es[f * 3 + t.ax_id[a]];
+      };
+      auto field_h = [&](const float2 (&m)[NMAT], const float (&e)[NAX]) {
+        float2 h = m[0];
+#pragma unroll
+        for (int a = 0; a < NAX; ++a) {
+          h.x = fmaf(e[a], m[1 + a].x, h.x);
+          h.y = fmaf(e[a], m[1 + a].y, h.y);
+        }
+        return h;
+      };
+      // H of the tile at the step's later stages (registers): real-space solver, at t + dt/2 and t + dt
+      // (H at t goes to shared memory as the sums are formed); k-space solver, the next step's H at t.
+      float2 Hn[KM ? 1 : 2][9];
       auto gslot = [&](int p) { return KM ? (p + 3) & 3 : p & 1; };
 
       if constexpr (KM) {
@@ -187,7 +211,11 @@ __global__ void __launch_bounds__(KPC * 16, KPC <= 8 ? 3 : 1)
       __syncthreads();
       if constexpr (KM) {
         // The chunk's first point t (then carried from step to step), and the first step's other two.
-        outer(2 * step0, gslot(2 * step0));
+        {
+          float ea[3][NAX];
+          fields(step0, ea);
+          outer(2 * step0, gslot(2 * step0), [&](int u, const float2 (&m)[NMAT]) { Hn[0][u] = field_h(m, ea[0]); });
+        }
         fetch_sums(2 * step0 + 1, gslot(2 * step0 + 1));
         fetch_sums(2 * step0 + 2, gslot(2 * step0 + 2));
         cp_async_commit();
@@ -214,34 +242,48 @@ __global__ void __launch_bounds__(KPC * 16, KPC <= 8 ? 3 : 1)
           cp_async_commit();
           if (ti + 1 < step1) fetch_sums(ti + 1, gslot(ti + 1));
           cp_async_commit();
-          // (1) Outer sums at the step's point.
-          outer(ti, buf);
+          // (1) Outer sums at the step's point: H at t into shared memory (the area's last readers, the
+          //     previous step's current, finished before the barrier), at t + dt/2 and t + dt kept.
+          float ea[3][NAX];
+          fields(ti, ea);
+          outer(ti, buf, [&](int u, const float2 (&m)[NMAT]) {
+            Hk[tra(u)] = field_h(m, ea[0]);
+            Hn[0][u] = field_h(m, ea[1]);
+            Hn[1][u] = field_h(m, ea[2]);
+          });
         }
         // (2) RK4 stages (src/solver.cpp:157-180), fields at t, t+dt/2, t+dt/2, t+dt; X = rho for the first
         //     (the area held the previous step's FP64 state for the current).
 #pragma unroll
         for (int u = 0; u < 9; ++u) Xk[own(u)] = make_float2((float)r[u].x, (float)r[u].y);
-        const double* esb = t.es + (size_t)ti * 9;
         double2 S[9];
 #pragma unroll 1
         for (int st = 0; st < 4; ++st) {
-          const int f = st == 0 ? 0 : (st == 3 ? 2 : 1);
-          if (st != 2) {  // (the third stage keeps the second's H: same field and point)
-            // k-space solver: the outer sums at t + dt/2 (second stage) and t + dt (fourth, carried on)
-            if (KM && st == 1) outer(2 * ti + 1, gslot(2 * ti + 1));
-            if (KM && st == 3) outer(2 * ti + 2, gslot(2 * ti + 2));
-            float ea[NAX];
+          // H of the stage (the third keeps the second's: same field and point).
+          if constexpr (KM) {
+            float ea[3][NAX];
+            fields(ti, ea);
+            if (st == 0) {
 #pragma unroll
-            for (int a = 0; a < NAX; ++a) ea[a] = (float)esb[f * 3 + t.ax_id[a]];
+              for (int u = 0; u < 9; ++u) Hk[tra(u)] = Hn[0][u];
+            } else if (st == 1) {
+              outer(2 * ti + 1, gslot(2 * ti + 1), [&](int u, const float2 (&m)[NMAT]) { Hk[tra(u)] = field_h(m, ea[1]); });
+            } else if (st == 3) {
+              // the point t + dt: this stage's H, and the next step's H at t (its first field sample)
+              float en[3][NAX];
+              fields(ti + 1 < step1 ? ti + 1 : ti, en);
+              outer(2 * ti + 2, gslot(2 * ti + 2), [&](int u, const float2 (&m)[NMAT]) {
+                Hk[tra(u)] = field_h(m, ea[2]);
+                Hn[0][u] = field_h(m, en[0]);
+              });
+            }
+          } else {
+            if (st == 1) {
 #pragma unroll
-            for (int u = 0; u < 9; ++u) {
-              float2 h = hm[0][u];
+              for (int u = 0; u < 9; ++u) Hk[tra(u)] = Hn[0][u];
+            } else if (st == 3) {
 #pragma unroll
-              for (int a = 0; a < NAX; ++a) {
-                h.x = fmaf(ea[a], hm[1 + a][u].x, h.x);
-                h.y = fmaf(ea[a], hm[1 + a][u].y, h.y);
-              }
-              Hk[tra(u)] = h;
+              for (int u = 0; u < 9; ++u) Hk[tra(u)] = Hn[1][u];
             }
           }
           __syncwarp();
