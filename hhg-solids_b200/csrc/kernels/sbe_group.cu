@@ -760,49 +760,75 @@ __device__ __forceinline__ void group_vctas(const SolveTables& t, const GroupDat
 constexpr int kMaxPreBox = 64;  // widest cell box of the precomputed-sum shapes
 constexpr int kPreChunk = 64;   // steps per precompute + propagate launch pair
 
-// Inner Wannier sums of every column for the steps [t.step0, t.step1): block (s, m2) forms the box
-// rows G_e = sum_q p2(q) X(mat, q1s + qq, q)_e and the window rows with the operations (and their
-// order) of group_vctas's inner_sums, into [s - t.step0][m2][row][nw2].  For the k-space solver the
-// points are 2 step0 ... 2 step1 and the window rows, the same for every point, are written once per
-// column ([m2][row][nw2], by the blocks of the first point).
+// Inner Wannier sums of every column for the steps [t.step0, t.step1): block (point group, m2) forms,
+// for kSumPts consecutive points s of the chunk, the box rows G_e = sum_q p2(q) X(mat, q1s + qq, q)_e
+// and the window rows, with the operations (and their order) of group_vctas's inner_sums, into
+// [s - t.step0][m2][row][nw2]; each thread loads a row's X values once for all of the block's points.
+// For the k-space solver the points are 2 step0 ... 2 step1 and the window rows, the same for every
+// point, are written once per column ([m2][row][nw2], by the block of the first point).
+constexpr int kSumPts = 8;
 template <typename Real>
 __global__ void __launch_bounds__(256) group_sums_kernel(SolveTables t, GroupData<Real> d, int q1s, int nq1,
                                                          int nbrows, int nwrows, typename Cx<Real>::T* Gpre,
-                                                         double2* GWpre) {
+                                                         double2* GWpre, int npts) {
   using V = typename Cx<Real>::T;
-  __shared__ V q2[kMaxPreBox];
-  __shared__ double2 w2[4];
-  const int sl = blockIdx.x / t.N2, m2 = blockIdx.x % t.N2, s = (t.kmode ? 2 * t.step0 : t.step0) + sl;
+  __shared__ V q2[kSumPts][kMaxPreBox];
+  __shared__ double2 w2[kSumPts][4];
+  const int sg = blockIdx.x / t.N2, m2 = blockIdx.x % t.N2, sl0 = sg * kSumPts;
+  const int ns = min(kSumPts, npts - sl0);
   const int npw = 2 * t.np + 1, W1n = t.b1n, W2n = t.b2n, nw2 = t.nw2;
-  const V* P2 = d.P + (size_t)s * 2 * npw + t.np + npw;
-  const double2* P2d = d.Pd + (size_t)s * 2 * npw + t.np + npw;
-  for (int idx = threadIdx.x; idx < W2n + 4; idx += blockDim.x) {
-    if (idx < W2n) {
-      q2[idx] = mul(d.T2[wrap_mod((long long)m2 * (t.b2lo + idx), t.N2)], P2[t.b2lo + idx]);
+  for (int idx = threadIdx.x; idx < ns * (W2n + 4); idx += blockDim.x) {
+    const int j = idx / (W2n + 4), q = idx % (W2n + 4);
+    const int s = (t.kmode ? 2 * t.step0 : t.step0) + sl0 + j;
+    if (q < W2n) {
+      const V* P2 = d.P + (size_t)s * 2 * npw + t.np + npw;
+      q2[j][q] = mul(d.T2[wrap_mod((long long)m2 * (t.b2lo + q), t.N2)], P2[t.b2lo + q]);
     } else {
-      const int q = idx - W2n;
-      const double2 tw = d.T2d[wrap_mod((long long)m2 * (q - 2), t.N2)];
-      w2[q] = t.kmode ? tw : mul(tw, P2d[q - 2]);
+      const int qw = q - W2n;
+      const double2* P2d = d.Pd + (size_t)s * 2 * npw + t.np + npw;
+      const double2 tw = d.T2d[wrap_mod((long long)m2 * (qw - 2), t.N2)];
+      w2[j][qw] = t.kmode ? tw : mul(tw, P2d[qw - 2]);
     }
   }
   __syncthreads();
-  V* G = Gpre + (size_t)blockIdx.x * nbrows * nw2;
   for (int idx = threadIdx.x; idx < nbrows * nw2; idx += blockDim.x) {
     const int row = idx / nw2, e = idx % nw2, mat = row / nq1, qq = row % nq1;
     const V* X = d.Xbox + ((size_t)(mat * W1n + q1s + qq) * W2n) * nw2;
-    V acc = Cx<Real>::make(0, 0);
-    for (int q = 0; q < W2n; ++q) acc = fmac(q2[q], X[(size_t)q * nw2 + e], acc);
-    G[idx] = acc;
+    V acc[kSumPts];
+#pragma unroll
+    for (int j = 0; j < kSumPts; ++j) acc[j] = Cx<Real>::make(0, 0);
+    for (int q = 0; q < W2n; ++q) {
+      const V x = X[(size_t)q * nw2 + e];
+#pragma unroll
+      for (int j = 0; j < kSumPts; ++j)
+        if (j < ns) acc[j] = fmac(q2[j][q], x, acc[j]);
+    }
+#pragma unroll
+    for (int j = 0; j < kSumPts; ++j)
+      if (j < ns) Gpre[((size_t)(sl0 + j) * t.N2 + m2) * nbrows * nw2 + idx] = acc[j];
   }
-  if (t.kmode && sl > 0) return;
-  double2* GW = GWpre + (size_t)(t.kmode ? m2 : blockIdx.x) * nwrows * nw2;
+  const int nwp = t.kmode ? (sl0 == 0 ? 1 : 0) : ns;  // points whose window rows this block writes
   for (int idx = threadIdx.x; idx < nwrows * nw2; idx += blockDim.x) {
     const int wr = idx / nw2, e = idx % nw2;
     const double2* X = d.Xwin + (size_t)wr * 4 * nw2;
-    double2 acc = make_double2(0.0, 0.0);
-    for (int q = 0; q < 4; ++q) acc = fmac(w2[q], X[(size_t)q * nw2 + e], acc);
-    GW[idx] = acc;
+    double2 xv[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) xv[q] = X[(size_t)q * nw2 + e];
+    for (int j = 0; j < nwp; ++j) {
+      double2 acc = make_double2(0.0, 0.0);
+#pragma unroll
+      for (int q = 0; q < 4; ++q) acc = fmac(w2[j][q], xv[q], acc);
+      GWpre[((size_t)(t.kmode ? m2 : (sl0 + j) * t.N2 + m2)) * nwrows * nw2 + idx] = acc;
+    }
   }
+}
+
+// Launches group_sums_kernel over the npts points of the chunk that starts at t.step0.
+template <typename Real>
+void launch_group_sums(const SolveTables& t, const GroupData<Real>& d, int q1s, int nq1, int nbrows, int nwrows,
+                       typename Cx<Real>::T* Gpre, double2* GWpre, int npts, cudaStream_t stream) {
+  const int groups = (npts + kSumPts - 1) / kSumPts;
+  group_sums_kernel<Real><<<groups * t.N2, 256, 0, stream>>>(t, d, q1s, nq1, nbrows, nwrows, Gpre, GWpre, npts);
 }
 
 template <typename Real>
@@ -952,8 +978,7 @@ int launch_group_t(const SolveTables& t, const GroupTables& gt, const LaunchShap
       tc.step0 = c0;
       tc.step1 = std::min(c0 + s.pre_chunk, t.step1);
       const int npts = KM ? 2 * (tc.step1 - c0) + 1 : tc.step1 - c0;
-      group_sums_kernel<Real><<<npts * t.N2, 256, 0, stream>>>(tc, d, gg.q1s, gg.nq1, gg.nbrows, gg.nwrows, Gpre,
-                                                               GWpre);
+      launch_group_sums<Real>(tc, d, gg.q1s, gg.nq1, gg.nbrows, gg.nwrows, Gpre, GWpre, npts, stream);
       kern<<<s.ctas, s.threads, s.smem, stream>>>(tc, d, s.k_per_cta, s.group, s.box_sm, s.win_sm, s.vctas, rho, Jpart);
       launches += 2;
     }
@@ -1032,8 +1057,7 @@ int launch_frag_t(const SolveTables& t, const GroupTables& gt, const LaunchShape
     SolveTables tc = t;
     tc.step0 = c0;
     tc.step1 = std::min(c0 + s.pre_chunk, t.step1);
-    group_sums_kernel<float><<<(tc.step1 - c0) * t.N2, 256, 0, stream>>>(tc, d, 3, 4, FG::NBROWS, FG::NWROWS, Gpre,
-                                                                          GWpre);
+    launch_group_sums<float>(tc, d, 3, 4, FG::NBROWS, FG::NWROWS, Gpre, GWpre, tc.step1 - c0, stream);
     kern<<<s.ctas, s.threads, s.smem, stream>>>(tc, d, s.vctas, rho, Jpart);
     launches += 2;
   }
@@ -1095,7 +1119,7 @@ int launch_mtile_t(const SolveTables& t, const GroupTables& gt, const LaunchShap
     tc.step0 = c0;
     tc.step1 = std::min(c0 + s.pre_chunk, t.step1);
     const int npts = KM ? 2 * (tc.step1 - c0) + 1 : tc.step1 - c0;
-    group_sums_kernel<float><<<npts * t.N2, 256, 0, stream>>>(tc, d, 3, 4, FG::NBROWS, FG::NWROWS, Gpre, GWpre);
+    launch_group_sums<float>(tc, d, 3, 4, FG::NBROWS, FG::NWROWS, Gpre, GWpre, npts, stream);
     kern<<<s.ctas, s.threads, s.smem, stream>>>(tc, d, s.vctas, rho, Jpart);
     launches += 2;
   }
@@ -1186,7 +1210,7 @@ int launch_dfrag_t(const SolveTables& t, const GroupTables& gt, const LaunchShap
     tc.step0 = c0;
     tc.step1 = std::min(c0 + s.pre_chunk, t.step1);
     const int npts = KM ? 2 * (tc.step1 - c0) + 1 : tc.step1 - c0;
-    group_sums_kernel<double><<<npts * t.N2, 256, 0, stream>>>(tc, d, 3, 4, FG::NBROWS, FG::NWROWS, Gpre, GWpre);
+    launch_group_sums<double>(tc, d, 3, 4, FG::NBROWS, FG::NWROWS, Gpre, GWpre, npts, stream);
     kern<<<s.ctas, s.threads, s.smem, stream>>>(tc, d, s.vctas, rho, Jpart);
     launches += 2;
   }
