@@ -9,6 +9,8 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
+#include <thread>
 #include <chrono>
 #include <cstdlib>
 #include <cmath>
@@ -340,10 +342,15 @@ void SWESim::init() {
   for (int c = 0; c < Nk; ++c)
     if (site_of_cell[c] >= 0) placed.push_back(c);
   std::vector<cd> vw((size_t)3 * hhg::kWindow * nw2, cd(0, 0));
+  bool r_nonzero_of[3];  // an axis without position elements has no convolution term
   for (int a = 0; a < 3; ++a) {
-    bool r_nonzero = false;  // an axis without position elements has no convolution term
-    for (const cd& z : model.bc[a]) r_nonzero = r_nonzero || z != cd(0, 0);
-    for (int w = 0; w < hhg::kWindow; ++w) {
+    r_nonzero_of[a] = false;
+    for (const cd& z : model.bc[a]) r_nonzero_of[a] = r_nonzero_of[a] || z != cd(0, 0);
+  }
+  // One task per (axis, window cell), each with its own sum in a fixed order: the tasks run on host
+  // threads and give the same bits on any number of them.
+  auto window_cell = [&](int a, int w) {
+      const bool r_nonzero = r_nonzero_of[a];
       const int n1 = w / 4 - 2, n2 = w % 4 - 2;
       const int c = cell_of(n1, n2);
       std::vector<cd> acc(nw2, cd(0, 0));
@@ -374,7 +381,18 @@ void SWESim::init() {
         const cd h = sc >= 0 ? model.hop[(size_t)sc * nw2 + o] : cd(0, 0);
         vw[((size_t)a * hhg::kWindow + w) * nw2 + o] = cd(0, 1) * (Ra * h - acc[o]);
       }
-    }
+  };
+  {
+    const int ntask = 3 * hhg::kWindow;
+    const int nthr = std::max(1, std::min<int>(ntask, (int)std::thread::hardware_concurrency()));
+    std::atomic<int> next{0};
+    auto worker = [&] {
+      for (int k = next++; k < ntask; k = next++) window_cell(k / hhg::kWindow, k % hhg::kWindow);
+    };
+    std::vector<std::thread> pool;
+    for (int i = 1; i < nthr; ++i) pool.emplace_back(worker);
+    worker();
+    for (auto& th : pool) th.join();
   }
   nj = 0;
   for (int a = 0; a < 3; ++a) {
