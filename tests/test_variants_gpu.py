@@ -227,19 +227,20 @@ def test_tile_kernel_against_element_groups_and_golden(name):
 
 
 def test_tile_kernel_ragged_columns_two_axes_and_slabs():
-    """Columns that do not divide into 8-k-point tiles (10 and 22 rows), a non-square grid, two field
-    axes (polarisation in the plane), and a row slab, against the FP64 solve of the same case."""
+    """Columns that do not divide into 8-k-point tiles (10 and 22 rows), non-square grids, two field
+    axes (polarisation in the plane) with 11 and 12 orbitals, and a row slab, against the FP64 solve of
+    the same case."""
     import tbgen
     from pySWE import pyswe
 
-    for n1, n2 in ((10, 10), (14, 8), (22, 10)):
-        p = {"path_tb": tbgen.model_path("tmd11_s7"), "nr1": n1, "nr2": n2, "nr3": 1, "tmax": 3.0, "dt": 0.02197,
+    for model, n1, n2 in (("tmd11_s7", 10, 10), ("tmd11_s7", 14, 8), ("tmd11_s7", 22, 10), ("tmd12_s3", 10, 12)):
+        p = {"path_tb": tbgen.model_path(model), "nr1": n1, "nr2": n2, "nr3": 1, "tmax": 3.0, "dt": 0.02197,
              "intensity": 2e12, "lambda": 3000.0, "tmax_field": 80.0, "pol_vec": np.array([0.6, 0.8, 0.0]),
              "phi_vec": np.zeros(3)}
         Jt, _, shape = run(p, "mixed", [])
         J64, _, _ = run(p, "fp64", [])
         assert shape[1] == 8 and shape[3] == "propagate_mtile_kernel", shape
-        assert rel_l2(Jt, J64) < 1e-6, (n1, n2, rel_l2(Jt, J64))
+        assert rel_l2(Jt, J64) < 1e-6, (model, n1, n2, rel_l2(Jt, J64))
     # rows [3, 12) of a 14 x 8 grid: the slab's partial current against the FP64 slab's
     p = dict(p, nr1=14, nr2=8)
     out = []
