@@ -384,7 +384,9 @@ void SWESim::init() {
   };
   {
     const int ntask = 3 * hhg::kWindow;
-    const int nthr = std::max(1, std::min<int>(ntask, (int)std::thread::hardware_concurrency()));
+    // (threads only where the sums are large: for small models starting them costs more than the sums)
+    const double work = (double)ntask * (double)placed.size() * nw * nw * nw;
+    const int nthr = work < 2e5 ? 1 : std::max(1, std::min<int>(ntask, (int)std::thread::hardware_concurrency()));
     std::atomic<int> next{0};
     auto worker = [&] {
       for (int k = next++; k < ntask; k = next++) window_cell(k / hhg::kWindow, k % hhg::kWindow);
