@@ -1084,7 +1084,7 @@ bool plan_mtile_t(const SolveTables& t, int sm_count, LaunchShape* out, char* wh
   out->kmode = KM ? 1 : 0;
   out->ept = 9;
   out->k_per_cta = KPC;
-  out->group = 16;
+  out->group = FG::LPK;
   out->threads = FG::NTHR;
   out->ntiles = (int)ntiles;
   out->ctas = (int)(ntiles < slots ? ntiles : slots);
@@ -1134,12 +1134,15 @@ struct MtileVariant {
 };
 #define HHG_MTILE_VARIANT(NW, NAX, NJ, KPC, KM) \
   {NW, NAX, NJ, KPC, KM, plan_mtile_t<NW, NAX, NJ, KPC, KM>, launch_mtile_t<NW, NAX, NJ, KPC, KM>}
-// (The k-space solver's ring of four inner-sum slots leaves three CTAs per SM only for 11 orbitals
-// and one field axis; its other shapes run the element-group kernel.)
+// (12 x 12 frame: 8 k-points per CTA; 6 x 6 frame: 32.  The k-space solver's ring of four inner-sum
+// slots leaves three CTAs per SM for 11 orbitals only with one field axis; its other shapes of that
+// frame run the element-group kernel.)
 const MtileVariant kMtileVariants[] = {
     HHG_MTILE_VARIANT(11, 1, 2, 8, false), HHG_MTILE_VARIANT(11, 2, 2, 8, false),
     HHG_MTILE_VARIANT(12, 1, 2, 8, false), HHG_MTILE_VARIANT(12, 2, 2, 8, false),
     HHG_MTILE_VARIANT(11, 1, 2, 8, true),
+    HHG_MTILE_VARIANT(6, 1, 2, 32, false),  HHG_MTILE_VARIANT(6, 2, 2, 32, false),
+    HHG_MTILE_VARIANT(6, 1, 2, 32, true),   HHG_MTILE_VARIANT(6, 2, 2, 32, true),
 };
 #undef HHG_MTILE_VARIANT
 

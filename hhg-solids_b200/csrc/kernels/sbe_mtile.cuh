@@ -7,20 +7,21 @@
 // whose cell box is the Hermitian-halved 7x7 one and whose inner Wannier sums come precomputed per
 // column and step (real-space solver).
 //
-// Layout.  A CTA holds KPC consecutive k-points (rows m1) of one k-grid column; the 16 lanes of each
-// half warp own one k-point, lane s its 3 x 3 tile (rows 3 (s / 4) .. +2, columns 3 (s % 4) .. +2) of
-// the k-point's matrices padded to 12 x 12.  Each lane keeps its tile of the state rho and of the RK4
+// Layout.  A CTA holds KPC consecutive k-points (rows m1) of one k-grid column; the k-point's matrices
+// are padded to a 12 x 12 frame (9..12 orbitals: 16 lanes, half a warp, per k-point, 8 per CTA) or a
+// 6 x 6 one (4..6 orbitals: 4 lanes per k-point, 32 per CTA), lane s owning its 3 x 3 tile (rows
+// 3 (s / T) .. +2, columns 3 (s % T) .. +2, T tiles per frame row).  Each lane keeps its tile of the state rho and of the RK4
 // sum in FP64 registers; the outer Wannier sums H0(k), r_a(k) of its tile give H = H0 + E.r at the
 // step's field samples, the later ones kept in FP32 registers for their stages.
 // Per stage:
 //  * H = H0 + E.r of the tile goes to shared memory, transposed (H(i, j) at [j][i]), X = rho + c k
 //    (FP32) is already there;
 //  * the lane forms its tile of P = H X in FP32 from rows l of both arrays (three H and three X
-//    values per l: 36 FMA per 6 loads, every load a broadcast to the 4 lanes of its tile row or
+//    values per l: 36 FMA per 6 loads, every load a broadcast to the lanes of its tile row or
 //    column);
 //  * P replaces X in shared memory, and k = -i (P - P^+) takes P^+ from the transposed tile;
 //  * the RK4 sum and the next stage's X are formed in FP64 (X stored as FP32).
-// Only the k-point's half warp exchanges data, so the stages need __syncwarp only; the CTA meets twice
+// Only the k-point's lanes (within one warp) exchange data, so the stages need __syncwarp only; the CTA meets twice
 // per step for the current (its FP64 window rows copied in during the step, then the FP64 state staged
 // for it) and once at its end (the next step's inner sums, copied in with cp.async meanwhile, and the
 // current partials).  The current is FP64: summed over the CTA's k-points on the FP64 tensor cores, then
@@ -40,14 +41,19 @@ struct Geom {
   static constexpr int NMAT = 1 + NAX;
   static constexpr int NBROWS = NMAT * 4;   // halved 7 x 7 box: inner-sum rows n1 = 0..3 per matrix
   static constexpr int NWROWS = NJ * 4;     // window rows
-  static constexpr int NWARP = KPC / 2;
+  // The frame: 12 x 12 (9..12 orbitals) or 6 x 6 (4..6), in 3 x 3 tiles, one lane per tile; a CTA of
+  // 128 threads holds KPC = 128 / (lanes per k-point) k-points (8 or 32).
+  static constexpr int NWP = NW > 6 ? 12 : 6;
+  static constexpr int TD = NWP / 3;        // tiles per frame row
+  static constexpr int LPK = TD * TD;       // lanes per k-point
+  static constexpr int NWARP = KPC * LPK / 32;
   // Inner-sum slots: this step's point and the next one's (real-space solver); the k-space solver's
   // points t + dt/2 and t + dt of this step and of the next, in a ring of four (point p in (p + 3) % 4).
   static constexpr int NGS = KM ? 4 : 2;
-  static constexpr int NTHR = KPC * 16;
-  static constexpr int MS = 12;             // row stride (float2) of a padded matrix
-  static constexpr int KS = 12 * 12 + 1;    // float2 per k-point matrix: the odd 8-byte unit puts the
-                                            // warp's two k-points two banks apart
+  static constexpr int NTHR = KPC * LPK;
+  static constexpr int MS = NWP;            // row stride (float2) of a padded matrix
+  static constexpr int KS = NWP * NWP + 1;  // float2 per k-point matrix: the odd 8-byte unit puts a
+                                            // warp's k-points in different banks
   static constexpr size_t HS = 0;                                     // [KPC][KS] float2: H, transposed
   static constexpr size_t XP = HS + (size_t)KPC * KS * 8;             // [KPC][KS] float2: X, then P
   static constexpr size_t GS = (XP + (size_t)KPC * KS * 8 + 15) / 16 * 16;  // [NGS][NBROWS][NW2] float2
@@ -57,20 +63,20 @@ struct Geom {
   static constexpr size_t WTW1 = TW1 + (size_t)KPC * 8 * 8;           // [KPC][4] double2: window rows
   static constexpr size_t SJ = WTW1 + (size_t)KPC * 4 * 16;           // [2][kJRing][NWARP][2 NJ] double
   static constexpr size_t BYTES = SJ + 2 * (size_t)kJRing * NWARP * 2 * NJ * 8;
-  static_assert(NW > 8 && NW <= 12, "3 x 3 tiles of a 12 x 12 frame: 9..12 orbitals");
-  static_assert(KPC % 2 == 0 && KPC * 16 <= 1024, "k-points per CTA");
+  static_assert((NW > 8 && NW <= 12) || (NW >= 4 && NW <= 6), "3 x 3 tiles of a 12 x 12 or 6 x 6 frame");
+  static_assert(KPC * LPK == 128, "128 threads per CTA");
   static_assert((NBROWS * NW2 * 8) % 16 == 0, "16-byte copies of the inner sums");
   static_assert((size_t)KPC * NW2 * 16 <= 2 * (size_t)KPC * KS * 8, "the FP64 state fits over the H and X area");
-  static_assert(KPC == 8, "the current's product takes the CTA's k-points as its K dimension (two k-steps)");
+  static_assert(KPC % 4 == 0, "the current's product takes the CTA's k-points as its K dimension (k-steps of 4)");
 };
 
-// 8 k-points per CTA run three CTAs per SM (at most 168 registers per thread): 12 warps per SM, against
-// 8 for 16 k-points per CTA at 218 registers (C2: 324 against 416 ms per solve).
+// 128 threads per CTA run three CTAs per SM (at most 168 registers per thread): 12 warps per SM, against
+// 8 for 16 k-points of 11 orbitals per CTA at 218 registers (C2: 324 against 416 ms per solve).
 // KM: the reference's k-space solver (src/solver_kspace.cpp:167-270): the stages see H at points
 // 2 ti (t), 2 ti + 1 (t + dt/2) and 2 ti + 2 (t + dt) of the interpolation tables; the outer sums of
 // 2 ti + 2 stay in registers for the next step's first stage, and the window has no phase.
 template <int NW, int NAX, int NJ, int KPC, bool KM = false>
-__global__ void __launch_bounds__(KPC * 16, KPC <= 8 ? 3 : 1)
+__global__ void __launch_bounds__(128, 3)
     propagate_mtile_kernel(SolveTables t, GroupData<float> d, int vctas, double2* rho, double2* Jpart) {
   using FG = Geom<NW, NAX, NJ, KPC, KM>;
   constexpr int NW2 = FG::NW2, NMAT = FG::NMAT, NWARP = FG::NWARP, NTHR = FG::NTHR, MS = FG::MS, KS = FG::KS;
@@ -84,7 +90,7 @@ __global__ void __launch_bounds__(KPC * 16, KPC <= 8 ? 3 : 1)
   double* SJ = reinterpret_cast<double*>(smraw + FG::SJ);
 
   const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
-  const int kp = 2 * w + (lane >> 4), sub = lane & 15, i0 = 3 * (sub >> 2), j0 = 3 * (sub & 3);
+  const int kp = tid / FG::LPK, sub = tid % FG::LPK, i0 = 3 * (sub / FG::TD), j0 = 3 * (sub % FG::TD);
   const int rows = t.row1 - t.row0, bpc = (rows + KPC - 1) / KPC, ntiles = t.N2 * bpc;
   const int step0 = t.step0, step1 = t.step1, npw = 2 * t.np + 1;
   const double dt = t.dt, prefac = 0.1666666666666 * dt;
@@ -361,9 +367,10 @@ __global__ void __launch_bounds__(KPC * 16, KPC <= 8 ? 3 : 1)
           const int g = lane >> 2, c4 = lane & 3;
           const double2* P1d = d.Pd + (size_t)ti * 2 * npw + t.np;
           // A[g][c] of k-step ks: wp(k-point 4 ks + c, window row g), rows 4..7 zero.
-          double2 wa[2];
+          constexpr int NKS = KPC / 4;
+          double2 wa[NKS];
 #pragma unroll
-          for (int ks = 0; ks < 2; ++ks)
+          for (int ks = 0; ks < NKS; ++ks)
             wa[ks] = g < 4 ? (KM ? WTW1[(4 * ks + c4) * 4 + g] : mul(WTW1[(4 * ks + c4) * 4 + g], P1d[g - 2])) : dzero;
           double re[3] = {0.0, 0.0, 0.0}, im[3] = {0.0, 0.0, 0.0};
           constexpr int NTR = (NW2 + 7) / 8;
@@ -372,7 +379,7 @@ __global__ void __launch_bounds__(KPC * 16, KPC <= 8 ? 3 : 1)
             double t1[2] = {0.0, 0.0}, t2[2] = {0.0, 0.0}, t3[2] = {0.0, 0.0};
             const int eb = 8 * nt + g;  // B[c][g]: conj(rho_eb(k-point 4 ks + c))
 #pragma unroll
-            for (int ks = 0; ks < 2; ++ks) {
+            for (int ks = 0; ks < NKS; ++ks) {
               const double2 b = eb < NW2 ? RS[(4 * ks + c4) * NW2 + eb] : dzero;
               dfrag::dmma(t1, wa[ks].x, b.x);
               dfrag::dmma(t2, wa[ks].y, -b.y);

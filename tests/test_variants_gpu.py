@@ -285,3 +285,39 @@ def test_tile_kernel_kspace_solver():
     srv.close()
     _, _, shape2 = run(dict(p, pol_vec=np.array([0.6, 0.8, 0.0])), "mixed", [])
     assert shape2[3].startswith("propagate_group_kernel"), shape2
+
+
+@pytest.mark.parametrize("name", ["tmd6_8", "ks_tmd6_8"])
+def test_tile_kernel_six_orbitals_against_golden(name):
+    """The 6 x 6 frame of the tile kernel (4 lanes per k-point, 32 k-points per CTA) against the
+    reference's current and the element-group kernel's (two field axes; the k-space solver's form)."""
+    _, param, _, J_ref = load_golden(name)
+    Jt, _, shape = run(param, "mixed", [])
+    assert shape[3] == "propagate_mtile_kernel" and shape[1] == 32, shape
+    Jg, _, shape_g = run(param, "mixed", ["HHG_MTILE=0"])
+    assert shape_g[3].startswith("propagate_group_kernel"), shape_g
+    assert rel_l2(Jt, J_ref) < 1e-6, rel_l2(Jt, J_ref)
+    assert rel_l2(Jt, Jg) < 1e-6, rel_l2(Jt, Jg)
+
+
+def test_tile_kernel_six_orbitals_ragged_columns_and_chunks():
+    """Columns of 40 and 10 rows (tiles of 32 k-points: 32 + 8 and 10), one and two field axes, against
+    the FP64 solve; a pulse served in chunks that start on odd steps gives the same bits."""
+    import tbgen
+    from pySWE import pyswe
+
+    for n1, n2, pol in ((40, 8, [0.0, 1.0, 0.0]), (10, 12, [0.6, 0.8, 0.0])):
+        p = {"path_tb": tbgen.model_path("tmd6_s1"), "nr1": n1, "nr2": n2, "nr3": 1, "tmax": 3.0, "dt": 0.02197,
+             "intensity": 2e12, "lambda": 3000.0, "tmax_field": 80.0, "pol_vec": np.array(pol),
+             "phi_vec": np.zeros(3)}
+        Jt, n_t, shape = run(p, "mixed", [])
+        J64, _, _ = run(p, "fp64", [])
+        assert shape[3] == "propagate_mtile_kernel", shape
+        assert n_t == 2 * ((Jt.shape[1] + 63) // 64) + 1
+        assert rel_l2(Jt, J64) < 1e-6, (n1, n2, rel_l2(Jt, J64))
+    srv = pyswe.SWEServer(device=0, chunk_steps=33)
+    r = pyswe.SWE(pyswe.Settings(dict(p)), precision="mixed", defer_init=True)
+    tk = srv.submit(r)
+    assert srv.wait(tk, timeout=120.0)
+    assert np.array_equal(np.stack(r.get_current()[1:]), Jt)
+    srv.close()
