@@ -257,8 +257,8 @@ def test_tile_kernel_ragged_columns_two_axes_and_slabs():
 def test_tile_kernel_kspace_solver():
     """The k-space solver's form of the tile kernel (outer sums at t + dt/2 and t + dt per step, those
     at t carried from the previous step, a constant window) against the reference's current and the
-    element-group kernel's; a pulse served in chunks that start on odd steps gives the same bits; the
-    two-axis shape, whose slot ring would not leave three CTAs per SM, stays on the element-group kernel."""
+    element-group kernel's; a pulse served in chunks that start on odd steps gives the same bits; two
+    field axes and 12 orbitals (two CTAs per SM) against the FP64 solve."""
     import tbgen
     from pySWE import pyswe
 
@@ -283,8 +283,12 @@ def test_tile_kernel_kspace_solver():
     assert srv.wait(tk, timeout=120.0)
     assert np.array_equal(np.stack(r.get_current()[1:]), Jt)
     srv.close()
-    _, _, shape2 = run(dict(p, pol_vec=np.array([0.6, 0.8, 0.0])), "mixed", [])
-    assert shape2[3].startswith("propagate_group_kernel"), shape2
+    for model, pol in (("tmd11_s7", [0.6, 0.8, 0.0]), ("tmd12_s3", [0.0, 1.0, 0.0]), ("tmd12_s3", [0.6, 0.8, 0.0])):
+        p2 = dict(p, path_tb=tbgen.model_path(model), pol_vec=np.array(pol))
+        J2, _, shape2 = run(p2, "mixed", [])
+        J64, _, _ = run(p2, "fp64", [])
+        assert shape2[3] == "propagate_mtile_kernel", (model, pol, shape2)
+        assert rel_l2(J2, J64) < 1e-6, (model, pol, rel_l2(J2, J64))
 
 
 @pytest.mark.parametrize("name", ["tmd6_8", "ks_tmd6_8"])
